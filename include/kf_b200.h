@@ -1,0 +1,334 @@
+/*
+ * kf_b200.h - C ABI of the B200 (sm_100a) KinectFusion per-frame pipeline.
+ *
+ * Every entry point is extern "C", takes plain pointers, sizes and POD
+ * structs, and returns a kf_status (0 = KF_OK).  kf_last_error() returns a
+ * thread-local description of the last failure.  Device buffers are owned by
+ * the library objects (pipelines, pyramids, trackers); caller buffers are
+ * borrowed for the duration of a call only.
+ *
+ * Reference interfaces replaced (paths within maximsolodukhin/KinectFusion):
+ *   Pipeline::device_available / create_device   include/kinectfusion/pipeline.hpp:154-158
+ *                                                 (CPU stubs src/kinectfusion/pipeline.cpp:120-127)
+ *   Pipeline::{integrate,raycast,track,observed_voxel_count,host_view,extract_mesh}
+ *                                                 include/kinectfusion/pipeline.hpp:72-97
+ *   PyramidSource::create_device / build / level  include/kinectfusion/depth_processing.hpp:422-463
+ *   DepthUploader::create                          include/kinectfusion/tsdf_integration.hpp:108-109
+ *   BasicDeviceCorrespondenceSweep::{run,run_loop} include/kinectfusion/icp_correspondence.hpp:363-369
+ *   ProjectiveIcpTracker::estimate_pose(DeviceTrackingRequest)
+ *                                                 include/kinectfusion/icp_optimizer.hpp:115-116
+ */
+#ifndef KF_B200_H
+#define KF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KF_B200_ABI_VERSION 1
+
+typedef int kf_status;
+enum {
+  KF_OK = 0,
+  KF_ERR_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference (validation.hpp:9-13) */
+  KF_ERR_CUDA = 2,             /* std::runtime_error from cuda::check (cuda/check.cuh:11-16) */
+  KF_ERR_NO_DEVICE = 3,        /* create_device without a CUDA device */
+  KF_ERR_OUT_OF_MEMORY = 4,
+  KF_ERR_DEVICE_TIMEOUT = 5,   /* a bounded device-side wait gave up */
+  KF_ERR_UNSUPPORTED = 6       /* storage combination not offered (pipeline.cpp:104-118) */
+};
+
+/* Memory space of a caller buffer passed through the ABI. */
+enum { KF_MEMORY_HOST = 0, KF_MEMORY_DEVICE = 1 };
+
+/* Enumerations mirror include/kinectfusion/pipeline.hpp:24-26, raycasting.hpp:22,
+ * tsdf_integration.hpp:28, trilinear.hpp:18-21, icp_correspondence.hpp:56. */
+enum { KF_VOXEL_FLOAT = 0, KF_VOXEL_QUANTIZED = 1, KF_VOXEL_BF16 = 2 };
+enum { KF_COLOR_FLOAT = 0, KF_COLOR_NONE = 1 };
+enum { KF_STORAGE_DENSE = 0, KF_STORAGE_SPARSE = 1 };
+enum { KF_RULE_CLASSIC = 0, KF_RULE_ANGLE_WEIGHTED = 1 };
+enum { KF_INTEGRATION_FULL = 0, KF_INTEGRATION_BAND = 1 };
+enum { KF_RAYCAST_MARCH = 0, KF_RAYCAST_BITMAP_MARCH = 1, KF_RAYCAST_BAND_MARCH = 2 };
+enum { KF_CORNERS_SKIP_MISSING = 0, KF_CORNERS_REQUIRE_ALL = 1 };
+enum { KF_DAMPING_NONE = 0, KF_DAMPING_IDENTITY = 1, KF_DAMPING_DIAGONAL = 2 };
+
+/* IcpFailure (icp_optimizer.hpp:22-28) plus the two success kinds. */
+enum {
+  KF_ICP_MAX_ITERATIONS = 0,
+  KF_ICP_CONVERGED = 1,
+  KF_ICP_TOO_FEW_CORRESPONDENCES = 2,
+  KF_ICP_SOLVE_FAILED = 3,
+  KF_ICP_UPDATE_TOO_LARGE = 4,
+  KF_ICP_UNCONSTRAINED_SYSTEM = 5,
+  KF_ICP_INVALID_INPUT = 6,
+  KF_ICP_NOT_RUN = 7
+};
+
+/* CameraIntrinsics (rgbd.hpp:26-74). */
+typedef struct {
+  float fx, fy, cx, cy;
+} kf_intrinsics;
+
+/* RigidTransform (vector.hpp:209-236): row-major rotation, then translation. */
+typedef struct {
+  float r[9];
+  float t[3];
+} kf_rigid;
+
+/* DepthProcessingOptions (depth_processing.hpp:31-47). */
+typedef struct {
+  uint32_t levels;
+  float depth_scale;
+  float min_depth;
+  float max_depth;
+  float max_normal_depth_jump;
+  float max_downsample_depth_jump;
+  int32_t bilateral_filter;
+  int32_t bilateral_radius;
+  float bilateral_spatial_sigma;
+  float bilateral_depth_sigma;
+} kf_depth_options;
+
+/* TsdfIntegrationOptions (tsdf_integration.hpp:31-50). */
+typedef struct {
+  float depth_scale;
+  float observation_weight;
+  float max_weight;
+  float min_depth;
+  float max_depth;
+  int32_t projective_distance;
+  int32_t distance_scaled_truncation;
+  float truncation_distance_scale;
+  int32_t mode; /* KF_INTEGRATION_* */
+} kf_integration_options;
+
+/* RaycastOptions (raycasting.hpp:66-78). */
+typedef struct {
+  float min_depth;
+  float max_depth;
+  float step_scale;
+  int32_t corner_policy; /* KF_CORNERS_* */
+  int32_t cell_gradient_normals;
+  int32_t seed_from_previous;
+} kf_raycast_options;
+
+/* VolumeGeometry (volume.hpp:265-287). */
+typedef struct {
+  uint32_t res_x, res_y, res_z;
+  float voxel_size;
+  float origin[3];
+  float truncation_distance;
+} kf_volume_geometry;
+
+/* PipelineConfig (pipeline.hpp:29-46) without the name and memory space. */
+typedef struct {
+  kf_volume_geometry volume;
+  int32_t voxel;           /* KF_VOXEL_* */
+  int32_t color;           /* KF_COLOR_* */
+  int32_t storage;         /* KF_STORAGE_* */
+  uint64_t sparse_block_capacity; /* 0 = block_count / 4 */
+  int32_t tsdf_rule;       /* KF_RULE_* */
+  kf_integration_options integration;
+  kf_raycast_options raycast;
+  int32_t raycast_backend; /* KF_RAYCAST_* */
+} kf_pipeline_config;
+
+/* One depth-camera observation (DepthFrameView, tsdf_integration.hpp:54-61).
+ * depth: width*height uint16; color: RGBA8 packed uint32 or NULL; normals:
+ * width*height*3 float (camera frame) or NULL.  `memory` says where all three
+ * live. */
+typedef struct {
+  const uint16_t* depth;
+  const uint32_t* color;
+  const float* normals;
+  uint32_t width, height;
+  kf_intrinsics intrinsics;
+  kf_rigid world_to_camera;
+  int32_t memory; /* KF_MEMORY_* */
+} kf_frame_view;
+
+/* RaycastCamera (raycasting.hpp:80-90). */
+typedef struct {
+  kf_intrinsics intrinsics;
+  uint32_t width, height;
+  kf_rigid camera_to_world;
+} kf_raycast_camera;
+
+/* SurfaceMaps (volume.hpp:172-185): points/normals width*height*3 float
+ * (world frame, NaN = no surface), colors width*height RGBA8. */
+typedef struct {
+  float* points;
+  float* normals;
+  uint32_t* colors;
+  uint32_t width, height;
+  int32_t memory; /* KF_MEMORY_* */
+} kf_surface_maps;
+
+/* One pyramid level as device views (PyramidLevel, depth_processing.hpp:412-416). */
+typedef struct {
+  const uint16_t* depth;  /* filtered (level 0) or downsampled depth */
+  const float* vertices;  /* width*height*3, camera frame */
+  const float* normals;   /* width*height*3 */
+  uint32_t width, height;
+  kf_intrinsics intrinsics;
+} kf_level_view;
+
+/* ProjectiveIcpOptions (icp_optimizer.hpp:80-101) + damping (icp_correspondence.hpp:56-98). */
+typedef struct {
+  uint64_t min_correspondences;
+  float max_point_distance;
+  float min_normal_dot;
+  float min_update_translation;
+  float min_update_rotation;
+  float max_update_translation;
+  float max_update_rotation;
+  float min_system_eigenvalue;
+  float max_condition_number;
+  int32_t damping_mode; /* KF_DAMPING_* */
+  float damping_lambda;
+  int32_t adaptive_damping;
+  float lambda_increase, lambda_decrease, min_lambda, max_lambda;
+} kf_icp_options;
+
+/* IcpOutcome + IcpDiagnostics (icp_optimizer.hpp:41-62).  pose is the
+ * camera_to_world after the call (on failure: the last pose reached). */
+typedef struct {
+  kf_rigid pose;
+  double pose_f64[12];
+  int32_t status; /* KF_ICP_* */
+  int32_t iterations;
+  uint64_t correspondences;
+  float mean_point_distance;
+  float mean_squared_residual;
+  float min_system_eigenvalue;
+  float condition_number;
+  float update_translation;
+  float update_rotation;
+  float damping_lambda;
+  uint64_t rejected_steps;
+} kf_icp_outcome;
+
+/* Per-frame result of kf_frame_process. */
+typedef struct {
+  kf_rigid camera_to_world;
+  int32_t tracked;      /* 1 when every level succeeded and the frame was fused */
+  int32_t status[4];    /* per pyramid level, KF_ICP_* (index = level) */
+  int32_t iterations[4];
+  uint64_t correspondences[4];
+} kf_frame_result;
+
+/* Welded triangle mesh (MarchingCubes::Mesh, marching_cubes.hpp:20-25). */
+typedef struct {
+  float* positions;   /* vertex_count*3 */
+  float* normals;     /* vertex_count*3 */
+  float* colors;      /* vertex_count*3, 0..255 */
+  uint32_t* triangles;/* triangle_count*3 */
+  uint64_t vertex_count;
+  uint64_t triangle_count;
+} kf_mesh;
+
+typedef struct kf_pipeline kf_pipeline;
+typedef struct kf_pyramid kf_pyramid;
+typedef struct kf_tracker kf_tracker;
+
+/* ---- library ---------------------------------------------------------- */
+const char* kf_last_error(void);
+int kf_abi_version(void);
+/* Pipeline::device_available (pipeline.hpp:154). */
+kf_status kf_device_available(int32_t* available);
+/* Reference defaults of each options struct (the C++ default member values). */
+void kf_default_depth_options(kf_depth_options* out);
+void kf_default_integration_options(kf_integration_options* out);
+void kf_default_raycast_options(kf_raycast_options* out);
+void kf_default_icp_options(kf_icp_options* out);
+void kf_default_pipeline_config(kf_pipeline_config* out);
+
+/* ---- pyramid: PyramidSource::create_device (depth_processing.hpp:460-462) */
+kf_status kf_pyramid_create(const kf_depth_options* options, kf_pyramid** out);
+kf_status kf_pyramid_destroy(kf_pyramid* pyramid);
+/* PyramidSource::build (depth_processing.hpp:434-435); returns the level count. */
+kf_status kf_pyramid_build(kf_pyramid* pyramid, const uint16_t* depth, uint32_t width,
+                           uint32_t height, kf_intrinsics intrinsics, int32_t memory,
+                           uint32_t* level_count);
+/* PyramidSource::level (depth_processing.hpp:437): device views, valid until the next build. */
+kf_status kf_pyramid_level(const kf_pyramid* pyramid, uint32_t index, kf_level_view* out);
+/* Host copies of one level (any pointer may be NULL). */
+kf_status kf_pyramid_download_level(const kf_pyramid* pyramid, uint32_t index, uint16_t* depth,
+                                    float* vertices, float* normals);
+
+/* ---- pipeline: Pipeline::create_device (pipeline.hpp:99-109, device_pipeline.cu:176-182) */
+kf_status kf_pipeline_create(const kf_pipeline_config* config, kf_pipeline** out);
+kf_status kf_pipeline_destroy(kf_pipeline* pipeline);
+/* Refill the volume with unobserved voxels (BasicVolume construction fill). */
+kf_status kf_pipeline_reset(kf_pipeline* pipeline);
+/* Pipeline::integrate (pipeline.hpp:75-79). */
+kf_status kf_pipeline_integrate(kf_pipeline* pipeline, const kf_frame_view* frame);
+/* Pipeline::raycast (pipeline.hpp:81): renders into `out` (host or device buffers). */
+kf_status kf_pipeline_raycast(kf_pipeline* pipeline, const kf_raycast_camera* camera,
+                              const kf_surface_maps* out);
+/* Pipeline::observed_voxel_count (pipeline.hpp:87). */
+kf_status kf_pipeline_observed_voxel_count(kf_pipeline* pipeline, uint64_t* count);
+/* Pipeline::host_view (pipeline.hpp:90): dense float staging copy.  tsdf and
+ * weight are voxel_count floats; color (voxel_count*4 floats) may be NULL. */
+kf_status kf_pipeline_download_volume(kf_pipeline* pipeline, float* tsdf, float* weight,
+                                      float* color);
+/* Raw storage bytes of the volume (dense: voxel_count*voxel_bytes). */
+kf_status kf_pipeline_download_raw(kf_pipeline* pipeline, void* voxels, size_t voxel_bytes,
+                                   void* colors, size_t color_bytes);
+/* Pipeline::extract_mesh (pipeline.hpp:95) on the device; free with kf_mesh_free. */
+kf_status kf_pipeline_extract_mesh(kf_pipeline* pipeline, float min_weight, kf_mesh* out);
+void kf_mesh_free(kf_mesh* mesh);
+/* Waits for the pipeline's stream. */
+kf_status kf_pipeline_synchronize(kf_pipeline* pipeline);
+
+/* ---- tracker: ProjectiveIcpTracker::estimate_pose(DeviceTrackingRequest)
+ * (icp_optimizer.hpp:115-116, icp_optimizer.cpp:58-76) with the device solve. */
+kf_status kf_tracker_create(const kf_icp_options* options, kf_tracker** out);
+kf_status kf_tracker_destroy(kf_tracker* tracker);
+/* Renders the model at `camera` and tracks `live` against it for `iterations`
+ * Gauss-Newton steps starting from camera->camera_to_world
+ * (Pipeline::track, pipeline.hpp:84-85 + IcpConsumer, reconstruction.cpp:63-67). */
+kf_status kf_pipeline_track(kf_pipeline* pipeline, kf_tracker* tracker,
+                            const kf_raycast_camera* camera, const kf_level_view* live,
+                            uint32_t iterations, kf_icp_outcome* outcome);
+/* One correspondence sweep (BasicDeviceCorrespondenceSweep::run,
+ * icp_correspondence.cu:572-597): fills sums[29] (21 JtJ + 6 Jtr + distance
+ * sum + squared residual sum) and the match count.  Device views. */
+kf_status kf_icp_normal_equations(kf_tracker* tracker, const kf_level_view* live,
+                                  const float* model_points, const float* model_normals,
+                                  uint32_t model_width, uint32_t model_height,
+                                  kf_intrinsics model_intrinsics, const kf_rigid* camera,
+                                  const kf_rigid* model_world_to_camera, float* sums,
+                                  uint64_t* count);
+
+/* ---- whole frame (Reconstruction::process_frame, reconstruction.cpp:184-216)
+ * pyramid -> per level (raycast at the current estimate, ICP) -> integrate at
+ * the tracked pose, as one CUDA graph with one host sync.  depth is
+ * width*height uint16 in `memory`; color may be NULL.  `pose` is the
+ * camera_to_world the frame starts from and receives the result.  When
+ * `first_frame` is set the frame is fused at `pose` without tracking
+ * (Reconstruction::initialize, reconstruction.cpp:143-182). */
+kf_status kf_frame_process(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker,
+                           const uint16_t* depth, const uint32_t* color, uint32_t width,
+                           uint32_t height, kf_intrinsics intrinsics, int32_t memory,
+                           const uint32_t* iterations_per_level, int32_t first_frame,
+                           kf_rigid* pose, kf_frame_result* result);
+/* Same, without the host sync: the pose stays on the device, result may be
+ * read later with kf_frame_result_fetch. */
+kf_status kf_frame_enqueue(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker,
+                           const uint16_t* depth, const uint32_t* color, uint32_t width,
+                           uint32_t height, kf_intrinsics intrinsics, int32_t memory,
+                           const uint32_t* iterations_per_level, int32_t first_frame);
+kf_status kf_frame_result_fetch(kf_pipeline* pipeline, kf_frame_result* result);
+/* Sets the device-resident camera_to_world that the next enqueued frame
+ * starts from (ordered on the pipeline's stream). */
+kf_status kf_frame_set_pose(kf_pipeline* pipeline, kf_tracker* tracker, const kf_rigid* pose);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KF_B200_H */

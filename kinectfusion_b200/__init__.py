@@ -1,0 +1,15 @@
+"""kinectfusion_b200: KinectFusion's per-frame pipeline on NVIDIA B200 (sm_100a).
+
+The compute lives in libkf_b200.so (hand-written CUDA behind the C ABI of
+include/kf_b200.h); this package is the Python host mirror of the reference's
+Pipeline / PyramidSource / ProjectiveIcpTracker interfaces over that ABI.
+"""
+
+from . import abi, synthetic  # noqa: F401
+from .pipeline import (ICP_ITERATIONS, Pipeline, ProjectiveIcpTracker, PyramidSource,  # noqa: F401
+                       Reconstruction, SurfaceMaps, default_depth_options, default_icp_options,
+                       device_available, pipeline_config)
+
+__all__ = ["abi", "synthetic", "Pipeline", "PyramidSource", "ProjectiveIcpTracker", "Reconstruction",
+           "SurfaceMaps", "pipeline_config", "default_depth_options", "default_icp_options",
+           "device_available", "ICP_ITERATIONS"]

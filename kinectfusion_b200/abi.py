@@ -1,0 +1,238 @@
+"""ctypes binding of the C ABI in include/kf_b200.h.
+
+The structures below mirror the header field by field.  Loading fails loudly
+when the in-tree library (kinectfusion_b200/libkf_b200.so) is missing: there
+is no CPU fallback behind this package.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "libkf_b200.so"
+HEADER = HERE.parent / "include" / "kf_b200.h"
+
+KF_OK = 0
+KF_ERR_INVALID_ARGUMENT = 1
+KF_ERR_CUDA = 2
+KF_ERR_NO_DEVICE = 3
+KF_ERR_OUT_OF_MEMORY = 4
+KF_ERR_DEVICE_TIMEOUT = 5
+KF_ERR_UNSUPPORTED = 6
+
+KF_MEMORY_HOST = 0
+KF_MEMORY_DEVICE = 1
+
+KF_VOXEL_FLOAT, KF_VOXEL_QUANTIZED, KF_VOXEL_BF16 = 0, 1, 2
+KF_COLOR_FLOAT, KF_COLOR_NONE = 0, 1
+KF_STORAGE_DENSE, KF_STORAGE_SPARSE = 0, 1
+KF_RULE_CLASSIC, KF_RULE_ANGLE_WEIGHTED = 0, 1
+KF_INTEGRATION_FULL, KF_INTEGRATION_BAND = 0, 1
+KF_RAYCAST_MARCH, KF_RAYCAST_BITMAP_MARCH, KF_RAYCAST_BAND_MARCH = 0, 1, 2
+KF_CORNERS_SKIP_MISSING, KF_CORNERS_REQUIRE_ALL = 0, 1
+KF_DAMPING_NONE, KF_DAMPING_IDENTITY, KF_DAMPING_DIAGONAL = 0, 1, 2
+
+KF_ICP_MAX_ITERATIONS = 0
+KF_ICP_CONVERGED = 1
+KF_ICP_TOO_FEW_CORRESPONDENCES = 2
+KF_ICP_SOLVE_FAILED = 3
+KF_ICP_UPDATE_TOO_LARGE = 4
+KF_ICP_UNCONSTRAINED_SYSTEM = 5
+KF_ICP_INVALID_INPUT = 6
+KF_ICP_NOT_RUN = 7
+
+ICP_STATUS_NAMES = {
+    0: "max_iterations", 1: "converged", 2: "too_few_correspondences", 3: "solve_failed",
+    4: "update_too_large", 5: "unconstrained_system", 6: "invalid_input", 7: "not_run",
+}
+
+
+class Intrinsics(C.Structure):
+    _fields_ = [("fx", C.c_float), ("fy", C.c_float), ("cx", C.c_float), ("cy", C.c_float)]
+
+
+class Rigid(C.Structure):
+    _fields_ = [("r", C.c_float * 9), ("t", C.c_float * 3)]
+
+
+class DepthOptions(C.Structure):
+    _fields_ = [("levels", C.c_uint32), ("depth_scale", C.c_float), ("min_depth", C.c_float),
+                ("max_depth", C.c_float), ("max_normal_depth_jump", C.c_float),
+                ("max_downsample_depth_jump", C.c_float), ("bilateral_filter", C.c_int32),
+                ("bilateral_radius", C.c_int32), ("bilateral_spatial_sigma", C.c_float),
+                ("bilateral_depth_sigma", C.c_float)]
+
+
+class IntegrationOptions(C.Structure):
+    _fields_ = [("depth_scale", C.c_float), ("observation_weight", C.c_float), ("max_weight", C.c_float),
+                ("min_depth", C.c_float), ("max_depth", C.c_float), ("projective_distance", C.c_int32),
+                ("distance_scaled_truncation", C.c_int32), ("truncation_distance_scale", C.c_float),
+                ("mode", C.c_int32)]
+
+
+class RaycastOptions(C.Structure):
+    _fields_ = [("min_depth", C.c_float), ("max_depth", C.c_float), ("step_scale", C.c_float),
+                ("corner_policy", C.c_int32), ("cell_gradient_normals", C.c_int32),
+                ("seed_from_previous", C.c_int32)]
+
+
+class VolumeGeometry(C.Structure):
+    _fields_ = [("res_x", C.c_uint32), ("res_y", C.c_uint32), ("res_z", C.c_uint32), ("voxel_size", C.c_float),
+                ("origin", C.c_float * 3), ("truncation_distance", C.c_float)]
+
+
+class PipelineConfig(C.Structure):
+    _fields_ = [("volume", VolumeGeometry), ("voxel", C.c_int32), ("color", C.c_int32), ("storage", C.c_int32),
+                ("sparse_block_capacity", C.c_uint64), ("tsdf_rule", C.c_int32),
+                ("integration", IntegrationOptions), ("raycast", RaycastOptions), ("raycast_backend", C.c_int32)]
+
+
+class FrameView(C.Structure):
+    _fields_ = [("depth", C.c_void_p), ("color", C.c_void_p), ("normals", C.c_void_p), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("intrinsics", Intrinsics), ("world_to_camera", Rigid),
+                ("memory", C.c_int32)]
+
+
+class RaycastCamera(C.Structure):
+    _fields_ = [("intrinsics", Intrinsics), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("camera_to_world", Rigid)]
+
+
+class SurfaceMapsView(C.Structure):
+    _fields_ = [("points", C.c_void_p), ("normals", C.c_void_p), ("colors", C.c_void_p), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("memory", C.c_int32)]
+
+
+class LevelView(C.Structure):
+    _fields_ = [("depth", C.c_void_p), ("vertices", C.c_void_p), ("normals", C.c_void_p), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("intrinsics", Intrinsics)]
+
+
+class IcpOptions(C.Structure):
+    _fields_ = [("min_correspondences", C.c_uint64), ("max_point_distance", C.c_float),
+                ("min_normal_dot", C.c_float), ("min_update_translation", C.c_float),
+                ("min_update_rotation", C.c_float), ("max_update_translation", C.c_float),
+                ("max_update_rotation", C.c_float), ("min_system_eigenvalue", C.c_float),
+                ("max_condition_number", C.c_float), ("damping_mode", C.c_int32), ("damping_lambda", C.c_float),
+                ("adaptive_damping", C.c_int32), ("lambda_increase", C.c_float), ("lambda_decrease", C.c_float),
+                ("min_lambda", C.c_float), ("max_lambda", C.c_float)]
+
+
+class IcpOutcome(C.Structure):
+    _fields_ = [("pose", Rigid), ("pose_f64", C.c_double * 12), ("status", C.c_int32), ("iterations", C.c_int32),
+                ("correspondences", C.c_uint64), ("mean_point_distance", C.c_float),
+                ("mean_squared_residual", C.c_float), ("min_system_eigenvalue", C.c_float),
+                ("condition_number", C.c_float), ("update_translation", C.c_float),
+                ("update_rotation", C.c_float), ("damping_lambda", C.c_float), ("rejected_steps", C.c_uint64)]
+
+
+class FrameResult(C.Structure):
+    _fields_ = [("camera_to_world", Rigid), ("tracked", C.c_int32), ("status", C.c_int32 * 4),
+                ("iterations", C.c_int32 * 4), ("correspondences", C.c_uint64 * 4)]
+
+
+class Mesh(C.Structure):
+    _fields_ = [("positions", C.POINTER(C.c_float)), ("normals", C.POINTER(C.c_float)),
+                ("colors", C.POINTER(C.c_float)), ("triangles", C.POINTER(C.c_uint32)),
+                ("vertex_count", C.c_uint64), ("triangle_count", C.c_uint64)]
+
+
+P = C.c_void_p
+_PROTOTYPES = {
+    "kf_last_error": (C.c_char_p, []),
+    "kf_abi_version": (C.c_int, []),
+    "kf_device_available": (C.c_int, [C.POINTER(C.c_int32)]),
+    "kf_default_depth_options": (None, [C.POINTER(DepthOptions)]),
+    "kf_default_integration_options": (None, [C.POINTER(IntegrationOptions)]),
+    "kf_default_raycast_options": (None, [C.POINTER(RaycastOptions)]),
+    "kf_default_icp_options": (None, [C.POINTER(IcpOptions)]),
+    "kf_default_pipeline_config": (None, [C.POINTER(PipelineConfig)]),
+    "kf_pyramid_create": (C.c_int, [C.POINTER(DepthOptions), C.POINTER(P)]),
+    "kf_pyramid_destroy": (C.c_int, [P]),
+    "kf_pyramid_build": (C.c_int, [P, P, C.c_uint32, C.c_uint32, Intrinsics, C.c_int32, C.POINTER(C.c_uint32)]),
+    "kf_pyramid_level": (C.c_int, [P, C.c_uint32, C.POINTER(LevelView)]),
+    "kf_pyramid_download_level": (C.c_int, [P, C.c_uint32, P, P, P]),
+    "kf_pipeline_create": (C.c_int, [C.POINTER(PipelineConfig), C.POINTER(P)]),
+    "kf_pipeline_destroy": (C.c_int, [P]),
+    "kf_pipeline_reset": (C.c_int, [P]),
+    "kf_pipeline_integrate": (C.c_int, [P, C.POINTER(FrameView)]),
+    "kf_pipeline_raycast": (C.c_int, [P, C.POINTER(RaycastCamera), C.POINTER(SurfaceMapsView)]),
+    "kf_pipeline_observed_voxel_count": (C.c_int, [P, C.POINTER(C.c_uint64)]),
+    "kf_pipeline_download_volume": (C.c_int, [P, P, P, P]),
+    "kf_pipeline_download_raw": (C.c_int, [P, P, C.c_size_t, P, C.c_size_t]),
+    "kf_pipeline_extract_mesh": (C.c_int, [P, C.c_float, C.POINTER(Mesh)]),
+    "kf_mesh_free": (None, [C.POINTER(Mesh)]),
+    "kf_pipeline_synchronize": (C.c_int, [P]),
+    "kf_tracker_create": (C.c_int, [C.POINTER(IcpOptions), C.POINTER(P)]),
+    "kf_tracker_destroy": (C.c_int, [P]),
+    "kf_pipeline_track": (C.c_int, [P, P, C.POINTER(RaycastCamera), C.POINTER(LevelView), C.c_uint32,
+                                    C.POINTER(IcpOutcome)]),
+    "kf_icp_normal_equations": (C.c_int, [P, C.POINTER(LevelView), P, P, C.c_uint32, C.c_uint32, Intrinsics,
+                                          C.POINTER(Rigid), C.POINTER(Rigid), P, C.POINTER(C.c_uint64)]),
+    "kf_frame_process": (C.c_int, [P, P, P, P, P, C.c_uint32, C.c_uint32, Intrinsics, C.c_int32, P, C.c_int32,
+                                   C.POINTER(Rigid), C.POINTER(FrameResult)]),
+    "kf_frame_enqueue": (C.c_int, [P, P, P, P, P, C.c_uint32, C.c_uint32, Intrinsics, C.c_int32, P, C.c_int32]),
+    "kf_frame_result_fetch": (C.c_int, [P, C.POINTER(FrameResult)]),
+    "kf_frame_set_pose": (C.c_int, [P, P, C.POINTER(Rigid)]),
+}
+
+_lib = None
+
+
+class KfError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"kf status {status}: {message}")
+        self.status = status
+
+
+def load() -> C.CDLL:
+    """Loads libkf_b200.so and declares every prototype; raises if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m kinectfusion_b200.build` "
+                           "(the package has no CPU fallback)")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (restype, argtypes) in _PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.restype = restype
+        fn.argtypes = argtypes
+    _lib = lib
+    return lib
+
+
+def check(status: int) -> None:
+    if status != KF_OK:
+        msg = load().kf_last_error()
+        raise KfError(status, msg.decode() if msg else "")
+
+
+def declared_functions() -> list[str]:
+    """Function names declared in include/kf_b200.h."""
+    import re
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:kf_status|void|const char\*|int)\s+(kf_\w+)\s*\(", text, re.M)))
+
+
+def rigid_from_matrix(m) -> Rigid:
+    import numpy as np
+    m = np.asarray(m, dtype=np.float64)
+    r = Rigid()
+    for i in range(3):
+        for j in range(3):
+            r.r[i * 3 + j] = float(np.float32(m[i, j]))
+        r.t[i] = float(np.float32(m[i, 3]))
+    return r
+
+
+def matrix_from_rigid(r: Rigid):
+    import numpy as np
+    m = np.eye(4, dtype=np.float32)
+    for i in range(3):
+        for j in range(3):
+            m[i, j] = r.r[i * 3 + j]
+        m[i, 3] = r.t[i]
+    return m

@@ -1,0 +1,295 @@
+// kf_frame.cu - the whole per-frame pipeline as one CUDA graph
+// (Reconstruction::process_frame, reconstruction.cpp:184-277):
+//   depth upload -> bilateral + 3-level pyramid -> integration pixel table ->
+//   for level 2, 1, 0: [ICP level begin, model raycast at the current
+//   estimate, N Gauss-Newton steps, level end] -> integrate at the tracked
+//   pose (skipped on a tracking failure) -> result download.
+// One graph launch and at most one host synchronisation per frame.  The
+// reference syncs once per ICP iteration (icp_correspondence.cu:589-596).
+//
+// Also the empty-space block bitmaps of the march skip.
+#include <cstring>
+
+#include "kf_internal.h"
+
+namespace kf {
+namespace {
+
+// One CTA per 8^3 block: the block is free when every voxel is observed with
+// tsdf exactly 1.0 (partial blocks at the volume edge never are).
+template <int Kind>
+__global__ void __launch_bounds__(512) free_blocks_kernel(VolumeDev v, uint32_t* __restrict__ free_bits) {
+  using VT = VoxelTraits<Kind>;
+  const uint32_t block = blockIdx.x;
+  const uint32_t bxi = block % v.bx, byi = (block / v.bx) % v.by, bzi = block / (v.bx * v.by);
+  const uint32_t x = bxi * 8 + (threadIdx.x & 7u);
+  const uint32_t y = byi * 8 + ((threadIdx.x >> 3) & 7u);
+  const uint32_t z = bzi * 8 + (threadIdx.x >> 6);
+  bool free = x < v.rx && y < v.ry && z < v.rz;
+  if (free) {
+    const long long i = storage_index(v, x, y, z);
+    if (i < 0) {
+      free = false;
+    } else {
+      const typename VT::Raw r = reinterpret_cast<const typename VT::Raw*>(v.voxels)[i];
+      free = VT::observed(r) && VT::tsdf(r) == 1.0f;
+    }
+  }
+  if (__syncthreads_and(free) && threadIdx.x == 0) atomicOr(free_bits + (block >> 5), 1u << (block & 31u));
+}
+
+// safe = free block whose 26 neighbours are free and inside the volume.
+__global__ void safe_blocks_kernel(const uint32_t* __restrict__ free_bits, uint32_t* __restrict__ safe_bits,
+                                   uint32_t bx, uint32_t by, uint32_t bz) {
+  const uint32_t block = blockIdx.x * blockDim.x + threadIdx.x;
+  if (block >= bx * by * bz) return;
+  const int x = static_cast<int>(block % bx), y = static_cast<int>((block / bx) % by),
+            z = static_cast<int>(block / (bx * by));
+  bool safe = true;
+  for (int dz = -1; dz <= 1 && safe; ++dz) {
+    for (int dy = -1; dy <= 1 && safe; ++dy) {
+      for (int dx = -1; dx <= 1 && safe; ++dx) {
+        const int nx = x + dx, ny = y + dy, nz = z + dz;
+        if (nx < 0 || ny < 0 || nz < 0 || nx >= static_cast<int>(bx) || ny >= static_cast<int>(by) ||
+            nz >= static_cast<int>(bz)) {
+          safe = false;
+          break;
+        }
+        const uint32_t nb = (static_cast<uint32_t>(nz) * by + static_cast<uint32_t>(ny)) * bx + static_cast<uint32_t>(nx);
+        safe = (free_bits[nb >> 5] >> (nb & 31u)) & 1u;
+      }
+    }
+  }
+  if (safe) atomicOr(safe_bits + (block >> 5), 1u << (block & 31u));
+}
+
+__global__ void frame_begin_kernel(IcpState* st) {
+  if (threadIdx.x != 0) return;
+  st->failed = 0;
+  for (int l = 0; l < 4; ++l) {
+    st->level_status[l] = KF_ICP_NOT_RUN;
+    st->level_iterations[l] = 0;
+    st->level_correspondences[l] = 0;
+  }
+}
+
+}  // namespace
+
+void launch_rebuild_skip(Pipeline& p, cudaStream_t s) {
+  const uint32_t blocks = p.view.bx * p.view.by * p.view.bz;
+  const size_t words = (blocks + 31) / 32;
+  if (p.free_blocks.count != words) {
+    p.free_blocks.resize(words);
+    p.safe_blocks.resize(words);
+  }
+  check(cudaMemsetAsync(p.free_blocks.ptr, 0, p.free_blocks.bytes(), s), "free bits clear");
+  check(cudaMemsetAsync(p.safe_blocks.ptr, 0, p.safe_blocks.bytes(), s), "safe bits clear");
+  switch (p.config.voxel) {
+    case KF_VOXEL_QUANTIZED:
+      free_blocks_kernel<KF_VOXEL_QUANTIZED><<<blocks, 512, 0, s>>>(p.view, p.free_blocks.ptr);
+      break;
+    case KF_VOXEL_BF16:
+      free_blocks_kernel<KF_VOXEL_BF16><<<blocks, 512, 0, s>>>(p.view, p.free_blocks.ptr);
+      break;
+    default:
+      free_blocks_kernel<KF_VOXEL_FLOAT><<<blocks, 512, 0, s>>>(p.view, p.free_blocks.ptr);
+      break;
+  }
+  check(cudaGetLastError(), "free_blocks_kernel launch");
+  safe_blocks_kernel<<<ceil_div(blocks, 256), 256, 0, s>>>(p.free_blocks.ptr, p.safe_blocks.ptr, p.view.bx, p.view.by,
+                                                          p.view.bz);
+  check(cudaGetLastError(), "safe_blocks_kernel launch");
+}
+
+namespace {
+
+// Records the frame's work on `s` (stream capture).
+void record_frame(Pipeline& p, Pyramid& pyr, Tracker& t, const Pipeline::GraphKey& key, bool has_color,
+                  cudaStream_t s) {
+  IcpState* st = t.state.ptr;
+  pyr.launch(s);
+  const PyramidLevelBuffers& l0 = pyr.levels[0];
+  const Intr k0 = intr_from(pyr.intrinsics);
+  launch_pixel_table(pyr.raw.ptr, has_color ? p.frame_color.ptr : nullptr, l0.normals.ptr, pyr.width, pyr.height, k0,
+                     p.config.integration, p.config.tsdf_rule, p.pixel_table.ptr, s);
+  frame_begin_kernel<<<1, 32, 0, s>>>(st);
+  check(cudaGetLastError(), "frame_begin launch");
+  if (!key.first) {
+    const uint32_t iters[4] = {key.it0, key.it1, key.it2, key.it3};
+    for (int level = static_cast<int>(pyr.level_count) - 1; level >= 0; --level) {
+      const PyramidLevelBuffers& b = pyr.levels[level];
+      // AppOptions::raycast_camera (app_options.cpp:94-103)
+      kf_raycast_camera cam;
+      cam.intrinsics = b.intrinsics;
+      cam.width = pyr.width >> level;
+      cam.height = pyr.height >> level;
+      std::memset(&cam.camera_to_world, 0, sizeof(cam.camera_to_world));
+      launch_icp_level_begin(st, t.params.damping_lambda, s);
+      Pipeline::Maps& m = p.maps_for(cam.width, cam.height);
+      launch_raycast(p, cam, m.points.ptr, m.normals.ptr, m.colors.ptr, st, s);
+      IcpLevelArgs a;
+      a.live_vertices = b.vertices.ptr;
+      a.live_normals = b.normals.ptr;
+      a.live_width = b.width;
+      a.live_height = b.height;
+      a.model_points = m.points.ptr;
+      a.model_normals = m.normals.ptr;
+      a.model_width = cam.width;
+      a.model_height = cam.height;
+      a.model_intrinsics = intr_from(cam.intrinsics);
+      for (uint32_t i = 0; i < iters[level]; ++i) launch_icp_iteration(a, st, t.partials.ptr, t.params, 1, 0, s);
+      launch_icp_level_end(st, level, s);
+    }
+  }
+  launch_integrate(p, p.pixel_table.ptr, pyr.width, pyr.height, k0, Rigid{}, has_color, st, s);
+  if (p.config.raycast_backend == KF_RAYCAST_BITMAP_MARCH) launch_rebuild_skip(p, s);
+  check(cudaMemcpyAsync(p.result_staging.ptr, st, sizeof(IcpState), cudaMemcpyDeviceToHost, s), "result download");
+}
+
+void enqueue(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker, const uint16_t* depth,
+             const uint32_t* color, uint32_t width, uint32_t height, kf_intrinsics intrinsics, int32_t memory,
+             const uint32_t* iterations, int32_t first_frame) {
+  require(pipeline && pyramid && tracker && depth, "kf_frame_enqueue: null argument");
+  require(intrinsics.fx > 0.0f && intrinsics.fy > 0.0f, "Depth frame intrinsics must have positive focal lengths");
+  Pipeline& p = pipeline->impl;
+  Pyramid& pyr = pyramid->impl;
+  Tracker& t = tracker->impl;
+  cudaStream_t s = p.stream;
+  const bool size_changed = pyr.width != width || pyr.height != height ||
+                            std::memcmp(&pyr.intrinsics, &intrinsics, sizeof(intrinsics)) != 0;
+  if (p.graph_pyramid != pyramid || p.graph_tracker != tracker || size_changed) {
+    check(cudaStreamSynchronize(s), "graph invalidation");
+    p.clear_graphs();
+    p.graph_pyramid = pyramid;
+    p.graph_tracker = tracker;
+  }
+  pyr.prepare(width, height, intrinsics);
+  const size_t n = static_cast<size_t>(width) * height;
+  if (p.pixel_table.count != n) p.pixel_table.resize(n);
+  if (p.frame_color.count != n) p.frame_color.resize(n);
+  p.result_staging.resize(1);
+  Pipeline::GraphKey key{width, height, 0, 0, 0, 0, first_frame ? 1u : 0u, color != nullptr ? 1u : 0u};
+  uint32_t* its[4] = {&key.it0, &key.it1, &key.it2, &key.it3};
+  for (uint32_t l = 0; l < 4; ++l) *its[l] = (iterations != nullptr && l < pyr.level_count) ? iterations[l] : 0u;
+  if (iterations == nullptr) {
+    // AppOptions::icp_iterations_for_level (app_options.cpp:147-158)
+    key.it0 = 10;
+    key.it1 = 5;
+    key.it2 = key.it3 = 4;
+  }
+  // Inputs into the graph's fixed buffers.
+  if (memory == KF_MEMORY_DEVICE) {
+    check(cudaMemcpyAsync(pyr.raw.ptr, depth, n * sizeof(uint16_t), cudaMemcpyDeviceToDevice, s), "depth copy");
+    if (color) check(cudaMemcpyAsync(p.frame_color.ptr, color, n * 4, cudaMemcpyDeviceToDevice, s), "color copy");
+  } else {
+    // Host buffers go through pinned staging so the copy is a true async DMA;
+    // wait for the previous frame's copy before overwriting the staging.
+    check(cudaStreamSynchronize(s), "staging reuse");
+    p.depth_staging.resize(n);
+    std::memcpy(p.depth_staging.ptr, depth, n * sizeof(uint16_t));
+    check(cudaMemcpyAsync(pyr.raw.ptr, p.depth_staging.ptr, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s),
+          "depth upload");
+    if (color) {
+      p.color_staging.resize(n);
+      std::memcpy(p.color_staging.ptr, color, n * 4);
+      check(cudaMemcpyAsync(p.frame_color.ptr, p.color_staging.ptr, n * 4, cudaMemcpyHostToDevice, s), "color upload");
+    }
+  }
+  auto it = p.graphs.find(key);
+  if (it == p.graphs.end()) {
+    // Size every buffer the graph touches before capture.
+    for (uint32_t level = 0; level < pyr.level_count; ++level) p.maps_for(width >> level, height >> level);
+    if (p.config.raycast_backend == KF_RAYCAST_BITMAP_MARCH && p.free_blocks.count == 0) {
+      const uint32_t blocks = p.view.bx * p.view.by * p.view.bz;
+      p.free_blocks.resize((blocks + 31) / 32);
+      p.safe_blocks.resize((blocks + 31) / 32);
+      check(cudaMemsetAsync(p.free_blocks.ptr, 0, p.free_blocks.bytes(), s), "free bits init");
+      check(cudaMemsetAsync(p.safe_blocks.ptr, 0, p.safe_blocks.bytes(), s), "safe bits init");
+    }
+    check(cudaStreamSynchronize(s), "pre-capture sync");
+    cudaGraph_t graph = nullptr;
+    check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+      record_frame(p, pyr, t, key, color != nullptr, s);
+    } catch (...) {
+      cudaStreamEndCapture(s, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      throw;
+    }
+    check(cudaStreamEndCapture(s, &graph), "end capture");
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t inst = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    check(inst, "graph instantiate");
+    it = p.graphs.emplace(key, exec).first;
+  }
+  check(cudaGraphLaunch(it->second, s), "frame graph launch");
+}
+
+void fill_result(const IcpState& st, int first, kf_frame_result* r) {
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) r->camera_to_world.r[i * 3 + j] = static_cast<float>(st.pose[i * 4 + j]);
+    r->camera_to_world.t[i] = static_cast<float>(st.pose[i * 4 + 3]);
+  }
+  r->tracked = st.failed ? 0 : 1;
+  for (int l = 0; l < 4; ++l) {
+    r->status[l] = first ? KF_ICP_NOT_RUN : st.level_status[l];
+    r->iterations[l] = first ? 0 : st.level_iterations[l];
+    r->correspondences[l] = first ? 0 : st.level_correspondences[l];
+  }
+}
+
+}  // namespace
+}  // namespace kf
+
+using namespace kf;
+
+extern "C" {
+
+kf_status kf_frame_set_pose(kf_pipeline* pipeline, kf_tracker* tracker, const kf_rigid* pose) {
+  return guarded([&] {
+    require(pipeline != nullptr && tracker != nullptr && pose != nullptr, "kf_frame_set_pose: null argument");
+    launch_icp_set_pose(tracker->impl.state.ptr, *pose, 1, pipeline->impl.stream);
+  });
+}
+
+kf_status kf_frame_enqueue(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker, const uint16_t* depth,
+                           const uint32_t* color, uint32_t width, uint32_t height, kf_intrinsics intrinsics,
+                           int32_t memory, const uint32_t* iterations_per_level, int32_t first_frame) {
+  return guarded([&] {
+    enqueue(pipeline, pyramid, tracker, depth, color, width, height, intrinsics, memory, iterations_per_level,
+            first_frame);
+  });
+}
+
+kf_status kf_frame_result_fetch(kf_pipeline* pipeline, kf_frame_result* result) {
+  return guarded([&] {
+    require(pipeline != nullptr && result != nullptr, "kf_frame_result_fetch: null argument");
+    Pipeline& p = pipeline->impl;
+    check(cudaStreamSynchronize(p.stream), "frame");
+    require(p.result_staging.ptr != nullptr, "kf_frame_result_fetch: no frame was processed");
+    fill_result(*p.result_staging.ptr, 0, result);
+  });
+}
+
+kf_status kf_frame_process(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker, const uint16_t* depth,
+                           const uint32_t* color, uint32_t width, uint32_t height, kf_intrinsics intrinsics,
+                           int32_t memory, const uint32_t* iterations_per_level, int32_t first_frame, kf_rigid* pose,
+                           kf_frame_result* result) {
+  return guarded([&] {
+    require(pipeline && tracker && pose, "kf_frame_process: null argument");
+    Pipeline& p = pipeline->impl;
+    require(std::isfinite(pose->t[0]) && std::isfinite(pose->t[1]) && std::isfinite(pose->t[2]),
+            "kf_frame_process: pose must be finite");
+    launch_icp_set_pose(tracker->impl.state.ptr, *pose, 1, p.stream);
+    enqueue(pipeline, pyramid, tracker, depth, color, width, height, intrinsics, memory, iterations_per_level,
+            first_frame);
+    check(cudaStreamSynchronize(p.stream), "frame");
+    kf_frame_result local;
+    fill_result(*p.result_staging.ptr, first_frame, &local);
+    *pose = local.camera_to_world;
+    if (result) *result = local;
+  });
+}
+
+}  // extern "C"

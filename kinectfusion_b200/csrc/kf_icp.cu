@@ -1,0 +1,649 @@
+// kf_icp.cu - projective point-to-plane ICP on the device.
+//
+// One kernel launch per Gauss-Newton step (all steps of a frame are nodes of
+// one CUDA graph).  The kernel:
+//  1. associates every live pixel with the model render
+//     (CorrespondenceSearch::match, icp_correspondence.hpp:244-294) and
+//     accumulates the 29 float sums of IcpNormalEquations::accumulate
+//     (icp_correspondence.hpp:111-129) per thread;
+//  2. reduces them per warp with register shuffles and per CTA through
+//     shared memory in a fixed order, writing one partial slot per CTA;
+//  3. the last CTA to arrive (an atomic ticket, no spinning) combines the
+//     slots in CTA order with Kahan-compensated FP32 sums, and one thread runs
+//     the Gauss-Newton/LM step of ProjectiveIcpTracker::estimate_with
+//     (icp_optimizer.cpp:208-302) in FP64: stability veto, damped LDL^T
+//     solve, Rodrigues increment, pose composition and the convergence test.
+//     The outcome latches in device memory; later steps of the level return at
+//     their first instruction (the reference's device loop does the same,
+//     icp_correspondence.cu:68-78).
+// The reference reduces with FP32 atomics (non-deterministic,
+// icp_correspondence.cu:131-145); this reduction is deterministic.
+#include <cmath>
+
+#include "kf_internal.h"
+
+namespace kf {
+namespace {
+
+__device__ __forceinline__ Rigid rigid_load(const float* c) {
+  return Rigid{{c[0], c[1], c[2]}, {c[3], c[4], c[5]}, {c[6], c[7], c[8]}, {c[9], c[10], c[11]}};
+}
+
+// CorrespondenceSearch::match + IcpCorrespondence::from_match.
+__device__ __forceinline__ bool match(const IcpLevelArgs& a, const Rigid& cam, const Rigid& model,
+                                      float max_d, float min_dot, uint32_t x, uint32_t y, float* j,
+                                      float& residual, float& distance) {
+  const size_t p = static_cast<size_t>(y) * a.live_width + x;
+  const f3 lv = ldg3(a.live_vertices + p * 3);
+  const f3 ln = ldg3(a.live_normals + p * 3);
+  if (!finite3(lv) || !finite3(ln)) return false;
+  const f3 source = apply(cam, lv);
+  const f3 sim = apply(model, source);
+  if (!finite3(sim) || sim.z <= 0.0f) return false;
+  float px, py;
+  project(a.model_intrinsics, sim, px, py);
+  const long mx = lroundf(px), my = lroundf(py);
+  if (mx < 0 || my < 0 || mx >= static_cast<long>(a.model_width) || my >= static_cast<long>(a.model_height)) {
+    return false;
+  }
+  const size_t mi = static_cast<size_t>(my) * a.model_width + static_cast<size_t>(mx);
+  const f3 mv = ldg3(a.model_points + mi * 3);
+  const f3 mn = ldg3(a.model_normals + mi * 3);
+  if (!finite3(mv) || !finite3(mn)) return false;
+  const f3 sn = normalized(rotate(cam, ln));
+  distance = norm(source - mv);
+  if (distance > max_d) return false;
+  if (dot(sn, mn) < min_dot) return false;
+  const f3 rot = cross(source, mn);
+  j[0] = rot.x;
+  j[1] = rot.y;
+  j[2] = rot.z;
+  j[3] = mn.x;
+  j[4] = mn.y;
+  j[5] = mn.z;
+  residual = dot(mn, mv - source);
+  return true;
+}
+
+// ---- FP64 6x6 linear algebra ------------------------------------------------
+// Cholesky A = L L^T; false on a non-positive pivot.
+__device__ bool cholesky6(const double (&a)[6][6], double (&l)[6][6]) {
+  for (int r = 0; r < 6; ++r) {
+    for (int c = 0; c <= r; ++c) {
+      double s = a[r][c];
+      for (int k = 0; k < c; ++k) s -= l[r][k] * l[c][k];
+      if (r == c) {
+        if (!(s > 0.0)) return false;
+        l[r][r] = sqrt(s);
+      } else {
+        l[r][c] = s / l[c][c];
+      }
+    }
+  }
+  return true;
+}
+
+__device__ void cholesky_solve6(const double (&l)[6][6], const double (&b)[6], double (&x)[6]) {
+  double y[6];
+  for (int r = 0; r < 6; ++r) {
+    double s = b[r];
+    for (int k = 0; k < r; ++k) s -= l[r][k] * y[k];
+    y[r] = s / l[r][r];
+  }
+  for (int r = 5; r >= 0; --r) {
+    double s = y[r];
+    for (int k = r + 1; k < 6; ++k) s -= l[k][r] * x[k];
+    x[r] = s / l[r][r];
+  }
+}
+
+// LDL^T solve with symmetric diagonal pivoting (largest remaining diagonal
+// first).  An exactly zero pivot (a rank-deficient system such as a single
+// plane) takes a zero solution component, the minimum-norm convention of the
+// reference's LDLT solve (icp_optimizer.cpp:391).
+__device__ void ldlt_solve6(const double (&in)[6][6], const double (&b)[6], double (&x)[6]) {
+  double a[6][6], l[6][6], d[6];
+  int perm[6];
+  for (int i = 0; i < 6; ++i) {
+    perm[i] = i;
+    for (int j = 0; j < 6; ++j) {
+      a[i][j] = in[i][j];
+      l[i][j] = 0.0;
+    }
+  }
+  for (int k = 0; k < 6; ++k) {
+    int piv = k;
+    double best = fabs(a[k][k]);
+    for (int i = k + 1; i < 6; ++i) {
+      if (fabs(a[i][i]) > best) {
+        best = fabs(a[i][i]);
+        piv = i;
+      }
+    }
+    if (piv != k) {
+      for (int i = 0; i < 6; ++i) {
+        const double t = a[k][i];
+        a[k][i] = a[piv][i];
+        a[piv][i] = t;
+      }
+      for (int i = 0; i < 6; ++i) {
+        const double t = a[i][k];
+        a[i][k] = a[i][piv];
+        a[i][piv] = t;
+      }
+      for (int i = 0; i < k; ++i) {
+        const double t = l[k][i];
+        l[k][i] = l[piv][i];
+        l[piv][i] = t;
+      }
+      const int t = perm[k];
+      perm[k] = perm[piv];
+      perm[piv] = t;
+    }
+    d[k] = a[k][k];
+    l[k][k] = 1.0;
+    for (int i = k + 1; i < 6; ++i) l[i][k] = d[k] != 0.0 ? a[i][k] / d[k] : 0.0;
+    for (int i = k + 1; i < 6; ++i)
+      for (int j = k + 1; j < 6; ++j) a[i][j] -= l[i][k] * d[k] * l[j][k];
+  }
+  double y[6], z[6];
+  for (int i = 0; i < 6; ++i) {
+    double s = b[perm[i]];
+    for (int j = 0; j < i; ++j) s -= l[i][j] * y[j];
+    y[i] = s;
+  }
+  for (int i = 0; i < 6; ++i) y[i] = fabs(d[i]) > 1.17549435e-38 ? y[i] / d[i] : 0.0;
+  for (int i = 5; i >= 0; --i) {
+    double s = y[i];
+    for (int j = i + 1; j < 6; ++j) s -= l[j][i] * z[j];
+    z[i] = s;
+  }
+  for (int i = 0; i < 6; ++i) x[perm[i]] = z[i];
+}
+
+// Symmetric eigenvalues by cyclic Jacobi rotations.
+__device__ bool jacobi6(const double (&in)[6][6], double (&eig)[6]) {
+  double a[6][6];
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) a[i][j] = in[i][j];
+  for (int sweep = 0; sweep < 50; ++sweep) {
+    double off = 0.0, diag = 0.0;
+    for (int p = 0; p < 6; ++p) {
+      diag += a[p][p] * a[p][p];
+      for (int q = p + 1; q < 6; ++q) off += a[p][q] * a[p][q];
+    }
+    if (off <= 1e-30 * diag || off == 0.0) break;
+    for (int p = 0; p < 6; ++p) {
+      for (int q = p + 1; q < 6; ++q) {
+        if (a[p][q] == 0.0) continue;
+        const double theta = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
+        const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        const double c = 1.0 / sqrt(t * t + 1.0);
+        const double s = t * c;
+        for (int k = 0; k < 6; ++k) {
+          const double akp = a[k][p], akq = a[k][q];
+          a[k][p] = c * akp - s * akq;
+          a[k][q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < 6; ++k) {
+          const double apk = a[p][k], aqk = a[q][k];
+          a[p][k] = c * apk - s * aqk;
+          a[q][k] = s * apk + c * aqk;
+        }
+      }
+    }
+  }
+  for (int i = 0; i < 6; ++i) {
+    eig[i] = a[i][i];
+    if (!isfinite(eig[i])) return false;
+  }
+  return true;
+}
+
+struct Stability {
+  bool stable;
+  float min_eigenvalue;
+  float condition_number;
+};
+
+// check_system_stability (icp_optimizer.cpp:319-347).  A Cholesky test of
+// A - min_eig I plus a Frobenius bound on the condition number decides the
+// common well-conditioned case; anything else falls back to the full
+// eigenvalue computation.
+__device__ Stability stability(const double (&a)[6][6], const IcpParams& p, bool want_values) {
+  Stability s{false, 0.0f, 0.0f};
+  if (!want_values) {
+    double shifted[6][6], l[6][6];
+    for (int i = 0; i < 6; ++i)
+      for (int j = 0; j < 6; ++j) shifted[i][j] = a[i][j] - (i == j ? static_cast<double>(p.min_system_eigenvalue) : 0.0);
+    if (cholesky6(shifted, l)) {
+      // ||A||_F * ||A^-1||_F >= cond(A).
+      double la[6][6];
+      if (cholesky6(a, la)) {
+        double fro = 0.0, inv_fro = 0.0;
+        for (int i = 0; i < 6; ++i)
+          for (int j = 0; j < 6; ++j) fro += a[i][j] * a[i][j];
+        for (int c = 0; c < 6; ++c) {
+          double e[6] = {0, 0, 0, 0, 0, 0}, x[6];
+          e[c] = 1.0;
+          cholesky_solve6(la, e, x);
+          for (int i = 0; i < 6; ++i) inv_fro += x[i] * x[i];
+        }
+        const double bound = sqrt(fro) * sqrt(inv_fro);
+        if (bound <= static_cast<double>(p.max_condition_number)) {
+          s.stable = true;
+          return s;
+        }
+      }
+    }
+  }
+  double eig[6];
+  if (!jacobi6(a, eig)) return s;
+  double lo = eig[0], hi = eig[0];
+  for (int i = 1; i < 6; ++i) {
+    lo = fmin(lo, eig[i]);
+    hi = fmax(hi, eig[i]);
+  }
+  const float mn = static_cast<float>(lo), mx = static_cast<float>(hi);
+  s.min_eigenvalue = mn;
+  if (mn <= 0.0f || mx <= 0.0f) return s;
+  s.condition_number = mx / mn;
+  s.stable = mn >= p.min_system_eigenvalue && s.condition_number <= p.max_condition_number;
+  return s;
+}
+
+__device__ float grow(const IcpParams& p, float l) { return fminf(l * p.lambda_increase, p.max_lambda); }
+__device__ float shrink(const IcpParams& p, float l) { return fmaxf(l * p.lambda_decrease, p.min_lambda); }
+
+struct Increment {
+  double r[9];
+  double t[3];
+  float update_translation, update_rotation, lambda;
+  bool solved;
+};
+
+// increment_from_solution (icp_optimizer.cpp:349-365) in FP64:
+// R = c I + s [u]x + (1 - c) u u^T.
+__device__ void increment_from(const double (&x)[6], Increment& inc) {
+  const double angle = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+  for (int i = 0; i < 9; ++i) inc.r[i] = (i % 4 == 0) ? 1.0 : 0.0;
+  if (angle > 1.0e-12) {
+    const double ux = x[0] / angle, uy = x[1] / angle, uz = x[2] / angle;
+    double s, c;
+    sincos(angle, &s, &c);
+    const double oc = 1.0 - c;
+    inc.r[0] = c + ux * ux * oc;
+    inc.r[1] = ux * uy * oc - uz * s;
+    inc.r[2] = ux * uz * oc + uy * s;
+    inc.r[3] = uy * ux * oc + uz * s;
+    inc.r[4] = c + uy * uy * oc;
+    inc.r[5] = uy * uz * oc - ux * s;
+    inc.r[6] = uz * ux * oc - uy * s;
+    inc.r[7] = uz * uy * oc + ux * s;
+    inc.r[8] = c + uz * uz * oc;
+  }
+  inc.t[0] = x[3];
+  inc.t[1] = x[4];
+  inc.t[2] = x[5];
+  inc.update_translation = static_cast<float>(sqrt(x[3] * x[3] + x[4] * x[4] + x[5] * x[5]));
+  inc.update_rotation = static_cast<float>(angle);
+  inc.solved = true;
+}
+
+__device__ bool within_caps(const Increment& inc, const IcpParams& p) {
+  return inc.update_translation <= p.max_update_translation && inc.update_rotation <= p.max_update_rotation;
+}
+
+// solve_increment (icp_optimizer.cpp:370-402) with an FP64 pivoted LDL^T.
+__device__ Increment solve_increment(const float* sums, float lambda, const IcpParams& p) {
+  Increment last;
+  last.solved = false;
+  last.update_translation = last.update_rotation = last.lambda = 0.0f;
+  double base[6][6], rhs[6];
+  int e = 0;
+  for (int r = 0; r < 6; ++r) {
+    for (int c = r; c < 6; ++c) {
+      base[r][c] = base[c][r] = static_cast<double>(sums[e]);
+      ++e;
+    }
+  }
+  for (int r = 0; r < 6; ++r) rhs[r] = static_cast<double>(sums[21 + r]);
+  const bool active = p.damping_mode != KF_DAMPING_NONE;
+  const int attempts = active ? 8 : 1;
+  float scale = lambda;
+  for (int attempt = 0; attempt < attempts; ++attempt) {
+    double damped[6][6], x[6];
+    for (int i = 0; i < 6; ++i)
+      for (int j = 0; j < 6; ++j) damped[i][j] = base[i][j];
+    for (int r = 0; r < 6; ++r) {
+      double off = 0.0;
+      if (p.damping_mode == KF_DAMPING_IDENTITY) off = scale;
+      if (p.damping_mode == KF_DAMPING_DIAGONAL) off = static_cast<double>(scale) * base[r][r];
+      damped[r][r] += off;
+    }
+    ldlt_solve6(damped, rhs, x);
+    bool finite = true;
+    for (int i = 0; i < 6; ++i) finite = finite && isfinite(x[i]);
+    if (finite) {
+      increment_from(x, last);
+      last.lambda = scale;
+      if (!active || within_caps(last, p)) return last;
+    }
+    scale = grow(p, scale);
+  }
+  return last;
+}
+
+// Rigid inverse in FP64, rounded to float ({R^T, -R^T t}).
+__device__ void write_float_inverse(const double* pose, float* out) {
+  // pose is a row-major 3x4 matrix [R | t]
+  double rt[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) rt[i * 3 + j] = pose[j * 4 + i];
+  const double t[3] = {pose[3], pose[7], pose[11]};
+  for (int i = 0; i < 3; ++i) {
+    out[i * 3 + 0] = static_cast<float>(rt[i * 3 + 0]);
+    out[i * 3 + 1] = static_cast<float>(rt[i * 3 + 1]);
+    out[i * 3 + 2] = static_cast<float>(rt[i * 3 + 2]);
+    out[9 + i] = static_cast<float>(-(rt[i * 3 + 0] * t[0] + rt[i * 3 + 1] * t[1] + rt[i * 3 + 2] * t[2]));
+  }
+}
+
+// float kf_rigid layout: r[9] row-major then t[3].  The FP64 pose is a
+// row-major 3x4 matrix.
+__device__ void pose_to_rigid_floats(const double* pose, float* out) {
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) out[i * 3 + j] = static_cast<float>(pose[i * 4 + j]);
+    out[9 + i] = static_cast<float>(pose[i * 4 + 3]);
+  }
+}
+
+// One Gauss-Newton / LM step of estimate_with on the combined sums.
+__device__ void gauss_newton_step(IcpState* st, const float* sums_in, unsigned long long count_in,
+                                  const IcpParams& p, bool want_values) {
+  float sums[kIcpSums];
+  for (int i = 0; i < kIcpSums; ++i) sums[i] = sums_in[i];
+  unsigned long long count = count_in;
+  st->iterations += 1;
+  st->correspondences = count;
+  if (count > 0) st->mean_point_distance = sums[27] / static_cast<float>(count);
+  if (count < p.min_correspondences) {
+    st->status = KF_ICP_TOO_FEW_CORRESPONDENCES;
+    return;
+  }
+  st->mean_squared_residual = sums[28] / static_cast<float>(count);
+  const bool active = p.damping_mode != KF_DAMPING_NONE;
+  bool accepted = true;
+  if (p.adaptive && active) {
+    const float cost = sums[28] / static_cast<float>(count);
+    accepted = !st->have_best || cost <= st->best_cost;
+    if (accepted) {
+      st->have_best = 1;
+      st->best_cost = cost;
+      for (int i = 0; i < 12; ++i) st->best_pose[i] = st->pose[i];
+      for (int i = 0; i < kIcpSums; ++i) st->best_sums[i] = sums[i];
+      st->best_count = count;
+      st->lambda = shrink(p, st->lambda);
+    } else {
+      st->rejected_steps += 1;
+      for (int i = 0; i < 12; ++i) st->pose[i] = st->best_pose[i];
+      for (int i = 0; i < kIcpSums; ++i) sums[i] = st->best_sums[i];
+      count = st->best_count;
+      st->lambda = grow(p, st->lambda);
+    }
+  }
+  double a[6][6];
+  int e = 0;
+  for (int r = 0; r < 6; ++r) {
+    for (int c = r; c < 6; ++c) {
+      a[r][c] = a[c][r] = static_cast<double>(sums[e]);
+      ++e;
+    }
+  }
+  const Stability stab = stability(a, p, want_values);
+  st->min_system_eigenvalue = stab.min_eigenvalue;
+  st->condition_number = stab.condition_number;
+  if (!stab.stable && !active) {
+    st->status = KF_ICP_UNCONSTRAINED_SYSTEM;
+    return;
+  }
+  const Increment inc = solve_increment(sums, st->lambda, p);
+  if (!inc.solved) {
+    st->status = KF_ICP_SOLVE_FAILED;
+    return;
+  }
+  st->lambda = inc.lambda;
+  st->damping_lambda = inc.lambda;
+  st->update_translation = inc.update_translation;
+  st->update_rotation = inc.update_rotation;
+  if (!within_caps(inc, p)) {
+    st->status = KF_ICP_UPDATE_TOO_LARGE;
+    return;
+  }
+  // pose = increment * pose (icp_optimizer.cpp:286)
+  double next[12];
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) {
+      next[i * 4 + j] = inc.r[i * 3 + 0] * st->pose[0 * 4 + j] + inc.r[i * 3 + 1] * st->pose[1 * 4 + j] +
+                        inc.r[i * 3 + 2] * st->pose[2 * 4 + j];
+    }
+    next[i * 4 + 3] = inc.r[i * 3 + 0] * st->pose[3] + inc.r[i * 3 + 1] * st->pose[7] +
+                      inc.r[i * 3 + 2] * st->pose[11] + inc.t[i];
+  }
+  for (int i = 0; i < 12; ++i) st->pose[i] = next[i];
+  pose_to_rigid_floats(st->pose, st->camera);
+  if (accepted && inc.update_translation < p.min_update_translation &&
+      inc.update_rotation < p.min_update_rotation) {
+    st->status = KF_ICP_CONVERGED;
+  }
+}
+
+template <bool Solve>
+__global__ void __launch_bounds__(kIcpBlock)
+    icp_iteration_kernel(IcpLevelArgs a, IcpState* __restrict__ st, float* __restrict__ partials, IcpParams p,
+                         int want_values) {
+  __shared__ int s_flag;
+  __shared__ float s_warp[kIcpBlock / 32][kIcpSlot];
+  __shared__ unsigned s_warp_count[kIcpBlock / 32];
+  __shared__ float s_total[kIcpSlot];
+  __shared__ unsigned long long s_count;
+  if (threadIdx.x == 0) s_flag = (st->status != kIcpRunning);
+  __syncthreads();
+  if (s_flag) return;
+
+  const Rigid cam = rigid_load(st->camera);
+  const Rigid model = rigid_load(st->model);
+  float acc[kIcpSums];
+#pragma unroll
+  for (int i = 0; i < kIcpSums; ++i) acc[i] = 0.0f;
+  unsigned cnt = 0;
+  const uint32_t pixels = a.live_width * a.live_height;
+  for (uint32_t pix = blockIdx.x * kIcpBlock + threadIdx.x; pix < pixels; pix += gridDim.x * kIcpBlock) {
+    float j[6], residual, distance;
+    if (!match(a, cam, model, p.max_point_distance, p.min_normal_dot, pix % a.live_width, pix / a.live_width, j,
+               residual, distance)) {
+      continue;
+    }
+    int e = 0;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+#pragma unroll
+      for (int c = r; c < 6; ++c) {
+        acc[e] += j[r] * j[c];
+        ++e;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 6; ++r) acc[21 + r] += j[r] * residual;
+    acc[27] += distance;
+    acc[28] += residual * residual;
+    ++cnt;
+  }
+  // warp tree (fixed butterfly order)
+#pragma unroll
+  for (int i = 0; i < kIcpSums; ++i) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc[i] += __shfl_xor_sync(0xFFFFFFFFu, acc[i], off);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, off);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < kIcpSums; ++i) s_warp[warp][i] = acc[i];
+    s_warp_count[warp] = cnt;
+  }
+  __syncthreads();
+  if (threadIdx.x < kIcpSums) {
+    float s = 0.0f;
+    for (int w = 0; w < kIcpBlock / 32; ++w) s += s_warp[w][threadIdx.x];
+    partials[blockIdx.x * kIcpSlot + threadIdx.x] = s;
+  } else if (threadIdx.x == kIcpSums) {
+    unsigned c = 0;
+    for (int w = 0; w < kIcpBlock / 32; ++w) c += s_warp_count[w];
+    partials[blockIdx.x * kIcpSlot + kIcpSums] = __uint_as_float(c);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned ticket = atomicAdd(&st->arrived, 1u);
+    s_flag = (ticket == gridDim.x - 1) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s_flag) return;
+  __threadfence();
+  // Last CTA: Kahan-compensated combine in CTA order.
+  if (threadIdx.x < kIcpSums) {
+    float sum = 0.0f, comp = 0.0f;
+    for (unsigned b = 0; b < gridDim.x; ++b) {
+      const float y = __ldcg(partials + b * kIcpSlot + threadIdx.x) - comp;
+      const float t = sum + y;
+      comp = (t - sum) - y;
+      sum = t;
+    }
+    s_total[threadIdx.x] = sum;
+  } else if (threadIdx.x == kIcpSums) {
+    unsigned long long c = 0;
+    for (unsigned b = 0; b < gridDim.x; ++b) c += __float_as_uint(__ldcg(partials + b * kIcpSlot + kIcpSums));
+    s_count = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    st->arrived = 0;
+    for (int i = 0; i < kIcpSums; ++i) st->sums[i] = s_total[i];
+    st->count = s_count;
+    if (Solve) gauss_newton_step(st, s_total, s_count, p, want_values != 0);
+  }
+}
+
+__global__ void icp_level_begin_kernel(IcpState* st, float damping_lambda) {
+  if (threadIdx.x != 0) return;
+  st->arrived = 0;
+  st->iterations = 0;
+  st->have_best = 0;
+  st->lambda = damping_lambda;
+  st->rejected_steps = 0;
+  st->correspondences = 0;
+  st->mean_point_distance = 0.0f;
+  st->mean_squared_residual = 0.0f;
+  st->min_system_eigenvalue = 0.0f;
+  st->condition_number = 0.0f;
+  st->update_translation = 0.0f;
+  st->update_rotation = 0.0f;
+  st->damping_lambda = 0.0f;
+  if (st->failed) {
+    st->status = KF_ICP_NOT_RUN;
+    return;
+  }
+  st->status = kIcpRunning;
+  pose_to_rigid_floats(st->pose, st->camera);
+  write_float_inverse(st->pose, st->model);
+}
+
+__global__ void icp_level_end_kernel(IcpState* st, int level) {
+  if (threadIdx.x != 0) return;
+  if (st->status == kIcpRunning) st->status = KF_ICP_MAX_ITERATIONS;
+  if (level >= 0 && level < 4) {
+    st->level_status[level] = st->status;
+    st->level_iterations[level] = st->iterations;
+    st->level_correspondences[level] = st->correspondences;
+  }
+  if (st->status != KF_ICP_MAX_ITERATIONS && st->status != KF_ICP_CONVERGED) st->failed = 1;
+  pose_to_rigid_floats(st->pose, st->camera);
+  write_float_inverse(st->pose, st->world_to_camera);
+}
+
+__global__ void icp_set_pose_kernel(IcpState* st, kf_rigid pose, int reset_frame) {
+  if (threadIdx.x != 0) return;
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) st->pose[i * 4 + j] = static_cast<double>(pose.r[i * 3 + j]);
+    st->pose[i * 4 + 3] = static_cast<double>(pose.t[i]);
+  }
+  pose_to_rigid_floats(st->pose, st->camera);
+  write_float_inverse(st->pose, st->world_to_camera);
+  if (reset_frame) {
+    st->failed = 0;
+    st->status = KF_ICP_NOT_RUN;
+    for (int l = 0; l < 4; ++l) {
+      st->level_status[l] = KF_ICP_NOT_RUN;
+      st->level_iterations[l] = 0;
+      st->level_correspondences[l] = 0;
+    }
+  }
+}
+
+}  // namespace
+
+IcpParams icp_params_from(const kf_icp_options& o) {
+  IcpParams p;
+  p.min_correspondences = o.min_correspondences;
+  p.max_point_distance = o.max_point_distance;
+  p.min_normal_dot = o.min_normal_dot;
+  p.min_update_translation = o.min_update_translation;
+  p.min_update_rotation = o.min_update_rotation;
+  p.max_update_translation = o.max_update_translation;
+  p.max_update_rotation = o.max_update_rotation;
+  p.min_system_eigenvalue = o.min_system_eigenvalue;
+  p.max_condition_number = o.max_condition_number;
+  p.damping_mode = o.damping_mode;
+  p.damping_lambda = o.damping_lambda;
+  p.adaptive = o.adaptive_damping;
+  p.lambda_increase = o.lambda_increase;
+  p.lambda_decrease = o.lambda_decrease;
+  p.min_lambda = o.min_lambda;
+  p.max_lambda = o.max_lambda;
+  return p;
+}
+
+unsigned icp_grid_for(uint32_t pixels) {
+  const unsigned g = ceil_div(pixels, kIcpBlock);
+  return g < static_cast<unsigned>(kIcpMaxGrid) ? (g == 0 ? 1 : g) : static_cast<unsigned>(kIcpMaxGrid);
+}
+
+void launch_icp_level_begin(IcpState* state, float damping_lambda, cudaStream_t s) {
+  icp_level_begin_kernel<<<1, 32, 0, s>>>(state, damping_lambda);
+  check(cudaGetLastError(), "icp_level_begin launch");
+}
+
+void launch_icp_iteration(const IcpLevelArgs& args, IcpState* state, float* partials, const IcpParams& params,
+                          int solve, int want_values, cudaStream_t s) {
+  const unsigned grid = icp_grid_for(args.live_width * args.live_height);
+  if (solve) {
+    icp_iteration_kernel<true><<<grid, kIcpBlock, 0, s>>>(args, state, partials, params, want_values);
+  } else {
+    icp_iteration_kernel<false><<<grid, kIcpBlock, 0, s>>>(args, state, partials, params, want_values);
+  }
+  check(cudaGetLastError(), "icp_iteration_kernel launch");
+}
+
+void launch_icp_level_end(IcpState* state, int level, cudaStream_t s) {
+  icp_level_end_kernel<<<1, 32, 0, s>>>(state, level);
+  check(cudaGetLastError(), "icp_level_end launch");
+}
+
+void launch_icp_set_pose(IcpState* state, kf_rigid pose, int reset_frame, cudaStream_t s) {
+  icp_set_pose_kernel<<<1, 32, 0, s>>>(state, pose, reset_frame);
+  check(cudaGetLastError(), "icp_set_pose launch");
+}
+
+}  // namespace kf

@@ -1,0 +1,311 @@
+// kf_internal.h - host-side objects behind the C ABI (include/kf_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/kf_b200.h"
+#include "kf_common.cuh"
+
+namespace kf {
+
+// ---- errors ----------------------------------------------------------------
+// Misconfiguration (std::invalid_argument in the reference, validation.hpp:9-13).
+struct InvalidArgument : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+// CUDA failure (std::runtime_error from cuda::check, cuda/check.cuh:11-16).
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct Unsupported : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void set_last_error(const std::string& message);
+void check(cudaError_t status, const char* what);
+void require(bool condition, const char* what);
+
+// Runs `body`, mapping exceptions to kf_status codes and kf_last_error().
+template <typename Body>
+kf_status guarded(Body&& body) {
+  try {
+    body();
+    return KF_OK;
+  } catch (const InvalidArgument& e) {
+    set_last_error(e.what());
+    return KF_ERR_INVALID_ARGUMENT;
+  } catch (const Unsupported& e) {
+    set_last_error(e.what());
+    return KF_ERR_UNSUPPORTED;
+  } catch (const CudaError& e) {
+    set_last_error(e.what());
+    return KF_ERR_CUDA;
+  } catch (const std::bad_alloc&) {
+    set_last_error("host allocation failed");
+    return KF_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return KF_ERR_INVALID_ARGUMENT;
+  }
+}
+
+// Owning device allocation.
+template <typename T>
+struct DeviceArray {
+  T* ptr = nullptr;
+  size_t count = 0;
+  DeviceArray() = default;
+  explicit DeviceArray(size_t n) { resize(n); }
+  DeviceArray(const DeviceArray&) = delete;
+  DeviceArray& operator=(const DeviceArray&) = delete;
+  DeviceArray(DeviceArray&& o) noexcept : ptr(o.ptr), count(o.count) {
+    o.ptr = nullptr;
+    o.count = 0;
+  }
+  DeviceArray& operator=(DeviceArray&& o) noexcept {
+    if (this != &o) {
+      release();
+      ptr = o.ptr;
+      count = o.count;
+      o.ptr = nullptr;
+      o.count = 0;
+    }
+    return *this;
+  }
+  ~DeviceArray() { release(); }
+  void resize(size_t n) {
+    if (n == count) return;
+    release();
+    if (n > 0) {
+      const cudaError_t s = cudaMalloc(reinterpret_cast<void**>(&ptr), n * sizeof(T));
+      if (s != cudaSuccess) {
+        ptr = nullptr;
+        throw CudaError(std::string("cudaMalloc: ") + cudaGetErrorString(s));
+      }
+    }
+    count = n;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    count = 0;
+  }
+  size_t bytes() const { return count * sizeof(T); }
+};
+
+template <typename T>
+struct PinnedArray {
+  T* ptr = nullptr;
+  size_t count = 0;
+  PinnedArray() = default;
+  PinnedArray(const PinnedArray&) = delete;
+  PinnedArray& operator=(const PinnedArray&) = delete;
+  ~PinnedArray() { release(); }
+  void resize(size_t n) {
+    if (n <= count) return;
+    release();
+    check(cudaMallocHost(reinterpret_cast<void**>(&ptr), n * sizeof(T)), "cudaMallocHost");
+    count = n;
+  }
+  void release() {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    count = 0;
+  }
+};
+
+// ---- depth pyramid (PyramidSource, depth_processing.hpp:422-463) -----------
+struct PyramidLevelBuffers {
+  DeviceArray<uint16_t> depth;
+  DeviceArray<float> vertices;
+  DeviceArray<float> normals;
+  uint32_t width = 0, height = 0;
+  kf_intrinsics intrinsics{};
+};
+
+struct Pyramid {
+  kf_depth_options options{};
+  DeviceArray<uint16_t> raw;  // unfiltered input depth (integration reads it)
+  uint32_t width = 0, height = 0;
+  kf_intrinsics intrinsics{};
+  std::vector<PyramidLevelBuffers> levels;
+  uint32_t level_count = 0;
+  cudaStream_t stream = nullptr;  // borrowed from the caller of build
+
+  // Sizes buffers for a width x height frame; returns the level count.
+  uint32_t prepare(uint32_t width, uint32_t height, kf_intrinsics intrinsics);
+  // Launches the pyramid kernels over `raw` on `stream`.
+  void launch(cudaStream_t stream) const;
+};
+
+// ---- ICP device state --------------------------------------------------------
+constexpr int kIcpSums = 29;          // 21 JtJ + 6 Jtr + distance + residual^2
+constexpr int kIcpSlot = 32;          // floats per CTA partial (29 sums + count)
+constexpr int kIcpBlock = 256;
+constexpr int kIcpMaxGrid = 2 * 148;  // two CTAs per SM on a 148-SM B200
+constexpr int kIcpRunning = -1;
+
+// Lives in device memory; one per tracker.  All poses are camera_to_world.
+struct IcpState {
+  double pose[12];       // FP64 pose, row-major 3x4
+  float camera[12];      // float copy used by the correspondence search
+  float model[12];       // model world_to_camera (float), fixed per level
+  float world_to_camera[12];  // float inverse of the pose, for integration
+  double best_pose[12];  // adaptive damping rollback target
+  float best_sums[kIcpSums];
+  unsigned long long best_count;
+  float lambda;
+  float best_cost;
+  int have_best;
+  int status;            // kIcpRunning while iterating, then KF_ICP_*
+  int iterations;        // completed Gauss-Newton steps in this level
+  unsigned arrived;      // CTA arrival ticket of the current sweep
+  int failed;            // a previous level of this frame failed
+  int level_status[4];
+  int level_iterations[4];
+  unsigned long long level_correspondences[4];
+  // diagnostics (IcpDiagnostics, icp_optimizer.hpp:41-51)
+  unsigned long long correspondences;
+  float mean_point_distance;
+  float mean_squared_residual;
+  float min_system_eigenvalue;
+  float condition_number;
+  float update_translation;
+  float update_rotation;
+  float damping_lambda;
+  unsigned long long rejected_steps;
+  // last raw sweep (for kf_icp_normal_equations)
+  float sums[kIcpSums];
+  unsigned long long count;
+};
+
+struct IcpParams {
+  unsigned long long min_correspondences;
+  float max_point_distance, min_normal_dot;
+  float min_update_translation, min_update_rotation;
+  float max_update_translation, max_update_rotation;
+  float min_system_eigenvalue, max_condition_number;
+  int damping_mode;
+  float damping_lambda;
+  int adaptive;
+  float lambda_increase, lambda_decrease, min_lambda, max_lambda;
+};
+
+struct Tracker {
+  kf_icp_options options{};
+  IcpParams params{};
+  DeviceArray<IcpState> state;
+  DeviceArray<float> partials;  // kIcpMaxGrid x kIcpSlot, scratch of the sweep
+  PinnedArray<IcpState> staging;
+};
+
+// Geometry of one correspondence sweep.
+struct IcpLevelArgs {
+  const float* live_vertices;
+  const float* live_normals;
+  uint32_t live_width, live_height;
+  const float* model_points;
+  const float* model_normals;
+  uint32_t model_width, model_height;
+  Intr model_intrinsics;
+};
+
+IcpParams icp_params_from(const kf_icp_options& o);
+unsigned icp_grid_for(uint32_t pixels);
+// Begin a level: model world_to_camera from the current pose, status running,
+// unless a previous level failed (then the level stays skipped).
+void launch_icp_level_begin(IcpState* state, float damping_lambda, cudaStream_t stream);
+// One Gauss-Newton step: sweep + (last CTA) FP64 solve and pose update.
+// `want_values` computes the exact eigenvalue diagnostics every step.
+void launch_icp_iteration(const IcpLevelArgs& args, IcpState* state, float* partials,
+                          const IcpParams& params, int solve, int want_values,
+                          cudaStream_t stream);
+void launch_icp_level_end(IcpState* state, int level, cudaStream_t stream);
+// Set the device pose (FP64 + float) from a float rigid transform.
+void launch_icp_set_pose(IcpState* state, kf_rigid pose, int reset_frame, cudaStream_t stream);
+
+// ---- volume / pipeline --------------------------------------------------------
+struct Pipeline {
+  kf_pipeline_config config{};
+  VolumeDev view{};
+  DeviceArray<uint8_t> voxels;
+  DeviceArray<float4> colors;
+  size_t voxel_bytes = 0;
+  uint64_t voxel_count = 0;
+  // empty-space skip: one bit per 8^3 block that is uniformly free space
+  DeviceArray<uint32_t> free_blocks;   // raw per-block bits
+  DeviceArray<uint32_t> safe_blocks;   // 3x3x3-eroded bits used by the march
+  // integration pixel table (float4 per pixel: depth, lambda, weight, color)
+  DeviceArray<float4> pixel_table;
+  DeviceArray<uint16_t> own_depth;     // upload target when no pyramid supplies one
+  DeviceArray<uint32_t> own_color;
+  DeviceArray<float> own_normals;
+  DeviceArray<uint32_t> frame_color;   // colour of the frame being processed
+  // cached map buffers per extent (device_pipeline.cu:133-136)
+  struct Maps {
+    DeviceArray<float> points, normals;
+    DeviceArray<uint32_t> colors;
+  };
+  std::map<std::pair<uint32_t, uint32_t>, Maps> maps;
+  cudaStream_t stream = nullptr;
+  // whole-frame graphs keyed by (width, height, iterations, first, colour)
+  struct GraphKey {
+    uint32_t w, h, it0, it1, it2, it3, first, color;
+    bool operator<(const GraphKey& o) const {
+      const uint32_t a[8] = {w, h, it0, it1, it2, it3, first, color};
+      const uint32_t b[8] = {o.w, o.h, o.it0, o.it1, o.it2, o.it3, o.first, o.color};
+      for (int i = 0; i < 8; ++i) {
+        if (a[i] != b[i]) return a[i] < b[i];
+      }
+      return false;
+    }
+  };
+  std::map<GraphKey, cudaGraphExec_t> graphs;
+  kf_pyramid* graph_pyramid = nullptr;
+  kf_tracker* graph_tracker = nullptr;
+  PinnedArray<IcpState> result_staging;
+  PinnedArray<uint16_t> depth_staging;
+  PinnedArray<uint32_t> color_staging;
+  int frames_fused = 0;
+
+  Maps& maps_for(uint32_t w, uint32_t h);
+  void clear_graphs();
+};
+
+// Integration pixel table: depth meters (NaN if unusable), lambda, fusion
+// weight and colour, one float4 per pixel.
+void launch_pixel_table(const uint16_t* depth, const uint32_t* color, const float* normals,
+                        uint32_t width, uint32_t height, Intr intrinsics,
+                        const kf_integration_options& options, int rule, float4* table,
+                        cudaStream_t stream);
+// Dense full sweep.  `pose_state` (optional) overrides world_to_camera with
+// the inverse of the tracked pose and skips fusion when tracking failed.
+void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t height,
+                      Intr intrinsics, Rigid world_to_camera, int has_color,
+                      const IcpState* pose_state, cudaStream_t stream);
+void launch_rebuild_skip(Pipeline& p, cudaStream_t stream);
+// Raycast into device maps.  `pose_state` (optional) supplies the
+// camera_to_world from the tracker and skips the render after a failure.
+void launch_raycast(const Pipeline& p, const kf_raycast_camera& camera, float* points,
+                    float* normals, uint32_t* colors, const IcpState* pose_state,
+                    cudaStream_t stream);
+void launch_fill_volume(Pipeline& p, cudaStream_t stream);
+uint64_t count_observed(Pipeline& p);
+
+}  // namespace kf
+
+struct kf_pyramid {
+  kf::Pyramid impl;
+};
+struct kf_tracker {
+  kf::Tracker impl;
+};
+struct kf_pipeline {
+  kf::Pipeline impl;
+};

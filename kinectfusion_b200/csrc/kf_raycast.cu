@@ -1,0 +1,334 @@
+// kf_raycast.cu - per-pixel trilinear ray march (SurfaceRaycast::render_pixel,
+// raycasting.hpp:116-245; TrilinearSampler, volume_sampler.hpp:116-255;
+// trilinear.hpp:85-269).
+//
+// One thread per pixel.  Corner gathers go through the read-only data path
+// (the volume does not change during a render).  Arithmetic is the host
+// expression order, so a render is bit-identical to the CPU raycast of the
+// same volume and camera.
+//
+// Empty-space skip: `safe` holds one bit per 8^3 block whose 3x3x3 block
+// neighbourhood is observed free space (every voxel observed with tsdf
+// exactly 1).  Inside such a block every trilinear sample is exactly 1.0
+// (the blend divides a sum by the identical sum), so the march replays its
+// ray_length additions without sampling; the sequence of sample positions,
+// and therefore the output, is unchanged.
+#include <cmath>
+
+#include "kf_internal.h"
+
+namespace kf {
+namespace {
+
+struct RaycastParams {
+  float min_depth, max_depth, step_scale;
+  int policy;
+  int cell_normals;
+  int seed_previous;
+};
+
+template <int Kind>
+struct Sampler {
+  using VT = VoxelTraits<Kind>;
+  using Raw = typename VT::Raw;
+  VolumeDev v;
+
+  __device__ __forceinline__ f3 grid_of(f3 p) const { return (p - v.origin) * v.inv_voxel_size; }
+
+  __device__ __forceinline__ bool contains(f3 g) const {
+    return g.x >= 0.0f && g.y >= 0.0f && g.z >= 0.0f && g.x < static_cast<float>(v.rx) &&
+           g.y < static_cast<float>(v.ry) && g.z < static_cast<float>(v.rz);
+  }
+
+  // Corner pointer (clipped), nullptr when outside or unallocated.
+  __device__ __forceinline__ const Raw* corner(int x, int y, int z) const {
+    if (x < 0 || y < 0 || z < 0 || x >= static_cast<int>(v.rx) || y >= static_cast<int>(v.ry) ||
+        z >= static_cast<int>(v.rz)) {
+      return nullptr;
+    }
+    const long long i = storage_index(v, static_cast<uint32_t>(x), static_cast<uint32_t>(y), static_cast<uint32_t>(z));
+    if (i < 0) return nullptr;
+    return reinterpret_cast<const Raw*>(v.voxels) + i;
+  }
+
+  __device__ __forceinline__ static float axis_weight(float f, int o) { return o == 0 ? 1.0f - f : f; }
+
+  // TrilinearSampler::tsdf + trilinear::blend_tsdf
+  __device__ bool tsdf(f3 point, int policy, float& out) const {
+    const f3 g = grid_of(point);
+    if (!contains(g)) return false;
+    const f3 gg = make(g.x - 0.5f, g.y - 0.5f, g.z - 0.5f);
+    const f3 fl = make(floorf(gg.x), floorf(gg.y), floorf(gg.z));
+    const int bx = static_cast<int>(fl.x), by = static_cast<int>(fl.y), bz = static_cast<int>(fl.z);
+    const f3 fr = gg - fl;
+    float acc = 0.0f, ws = 0.0f;
+    int valid = 0;
+#pragma unroll
+    for (int oz = 0; oz <= 1; ++oz) {
+#pragma unroll
+      for (int oy = 0; oy <= 1; ++oy) {
+#pragma unroll
+        for (int ox = 0; ox <= 1; ++ox) {
+          const Raw* c = corner(bx + ox, by + oy, bz + oz);
+          if (c == nullptr) continue;
+          const Raw r = __ldg(c);
+          if (!VT::observed(r) || !VT::finite(r)) continue;
+          const float w = axis_weight(fr.x, ox) * axis_weight(fr.y, oy) * axis_weight(fr.z, oz);
+          acc += w * VT::tsdf(r);
+          ws += w;
+          ++valid;
+        }
+      }
+    }
+    if (policy == KF_CORNERS_REQUIRE_ALL && valid < 8) return false;
+    if (ws <= 1.0e-6f) return false;
+    const float d = acc / ws;
+    if (!isfinite(d)) return false;
+    out = d;
+    return true;
+  }
+
+  // TrilinearSampler::color + trilinear::blend_color
+  __device__ bool color(f3 point, f3& out) const {
+    const f3 g = grid_of(point);
+    if (!contains(g)) return false;
+    const f3 gg = make(g.x - 0.5f, g.y - 0.5f, g.z - 0.5f);
+    const f3 fl = make(floorf(gg.x), floorf(gg.y), floorf(gg.z));
+    const int bx = static_cast<int>(fl.x), by = static_cast<int>(fl.y), bz = static_cast<int>(fl.z);
+    const f3 fr = gg - fl;
+    f3 acc = make(0.0f, 0.0f, 0.0f);
+    float ws = 0.0f;
+#pragma unroll
+    for (int oz = 0; oz <= 1; ++oz) {
+#pragma unroll
+      for (int oy = 0; oy <= 1; ++oy) {
+#pragma unroll
+        for (int ox = 0; ox <= 1; ++ox) {
+          const Raw* c = corner(bx + ox, by + oy, bz + oz);
+          if (c == nullptr) continue;
+          const float4 cv = __ldg(v.colors + (c - reinterpret_cast<const Raw*>(v.voxels)));
+          if (cv.w <= 0.0f) continue;
+          const float w = axis_weight(fr.x, ox) * axis_weight(fr.y, oy) * axis_weight(fr.z, oz);
+          acc = acc + make(cv.x, cv.y, cv.z) * w;
+          ws += w;
+        }
+      }
+    }
+    if (ws <= 1.0e-6f) return false;
+    out = acc / ws;
+    return true;
+  }
+
+  // trilinear::central_normal (trilinear.hpp:243-266)
+  __device__ bool central_normal(f3 p, int policy, f3& out) const {
+    const float vs = v.voxel_size;
+    float plus, minus;
+    if (!tsdf(make(p.x + vs, p.y + 0.0f, p.z + 0.0f), policy, plus)) return false;
+    if (!tsdf(make(p.x - vs, p.y - 0.0f, p.z - 0.0f), policy, minus)) return false;
+    const float gx = plus - minus;
+    if (!tsdf(make(p.x + 0.0f, p.y + vs, p.z + 0.0f), policy, plus)) return false;
+    if (!tsdf(make(p.x - 0.0f, p.y - vs, p.z - 0.0f), policy, minus)) return false;
+    const float gy = plus - minus;
+    if (!tsdf(make(p.x + 0.0f, p.y + 0.0f, p.z + vs), policy, plus)) return false;
+    if (!tsdf(make(p.x - 0.0f, p.y - 0.0f, p.z - vs), policy, minus)) return false;
+    const float gz = plus - minus;
+    const f3 d = make(gx, gy, gz);
+    const float length = norm(d);
+    if (length <= 0.0f) return false;
+    out = d / length;
+    return true;
+  }
+
+  // TrilinearSampler::cell_normal (volume_sampler.hpp:189-239)
+  __device__ bool cell_normal(f3 p, f3& out) const {
+    const f3 g = grid_of(p);
+    if (!contains(g)) return false;
+    const f3 gg = make(g.x - 0.5f, g.y - 0.5f, g.z - 0.5f);
+    const f3 fl = make(floorf(gg.x), floorf(gg.y), floorf(gg.z));
+    const int bx = static_cast<int>(fl.x), by = static_cast<int>(fl.y), bz = static_cast<int>(fl.z);
+    const f3 f = gg - fl;
+    float c[2][2][2];
+#pragma unroll
+    for (int oz = 0; oz <= 1; ++oz) {
+#pragma unroll
+      for (int oy = 0; oy <= 1; ++oy) {
+#pragma unroll
+        for (int ox = 0; ox <= 1; ++ox) {
+          const Raw* cp = corner(bx + ox, by + oy, bz + oz);
+          if (cp == nullptr) return central_normal(p, KF_CORNERS_SKIP_MISSING, out);
+          const Raw r = __ldg(cp);
+          if (!VT::observed(r) || !VT::finite(r)) return central_normal(p, KF_CORNERS_SKIP_MISSING, out);
+          c[oz][oy][ox] = VT::tsdf(r);
+        }
+      }
+    }
+    auto lerp = [](float l, float h, float m) { return l + (m * (h - l)); };
+    const float gx = lerp(lerp(c[0][0][1] - c[0][0][0], c[0][1][1] - c[0][1][0], f.y),
+                          lerp(c[1][0][1] - c[1][0][0], c[1][1][1] - c[1][1][0], f.y), f.z);
+    const float gy = lerp(lerp(c[0][1][0] - c[0][0][0], c[0][1][1] - c[0][0][1], f.x),
+                          lerp(c[1][1][0] - c[1][0][0], c[1][1][1] - c[1][0][1], f.x), f.z);
+    const float gz = lerp(lerp(c[1][0][0] - c[0][0][0], c[1][0][1] - c[0][0][1], f.x),
+                          lerp(c[1][1][0] - c[0][1][0], c[1][1][1] - c[0][1][1], f.x), f.y);
+    const f3 gr = make(gx, gy, gz);
+    const float length = norm(gr);
+    if (length <= 0.0f) return false;
+    out = gr / length;
+    return true;
+  }
+};
+
+// True when the sample point lies in a block whose 3x3x3 neighbourhood is
+// uniformly observed free space.
+__device__ __forceinline__ bool in_safe_block(const uint32_t* __restrict__ safe, const VolumeDev& v, f3 point) {
+  const f3 g = (point - v.origin) * v.inv_voxel_size;
+  if (!(g.x >= 0.0f && g.y >= 0.0f && g.z >= 0.0f && g.x < static_cast<float>(v.rx) &&
+        g.y < static_cast<float>(v.ry) && g.z < static_cast<float>(v.rz))) {
+    return false;
+  }
+  const uint32_t block = ((static_cast<uint32_t>(g.z) >> 3) * v.by + (static_cast<uint32_t>(g.y) >> 3)) * v.bx +
+                         (static_cast<uint32_t>(g.x) >> 3);
+  return (__ldg(safe + (block >> 5)) >> (block & 31u)) & 1u;
+}
+
+template <int Kind, bool Color>
+__global__ void __launch_bounds__(256)
+    raycast_kernel(VolumeDev v, const uint32_t* __restrict__ safe, RaycastParams rp, Intr k, uint32_t width,
+                   uint32_t height, Rigid pose, const IcpState* __restrict__ state, float* __restrict__ points,
+                   float* __restrict__ normals, uint32_t* __restrict__ colors) {
+  if (state != nullptr) {
+    if (state->failed) return;
+    const float* c = state->camera;
+    pose = Rigid{{c[0], c[1], c[2]}, {c[3], c[4], c[5]}, {c[6], c[7], c[8]}, {c[9], c[10], c[11]}};
+  }
+  const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t row = blockIdx.y * blockDim.y + threadIdx.y;
+  if (col >= width || row >= height) return;
+  const size_t pix = static_cast<size_t>(row) * width + col;
+  const Sampler<Kind> s{v};
+
+  float seed = rp.min_depth;
+  if (rp.seed_previous) {
+    const f3 previous = load3(points + pix * 3);
+    if (finite3(previous) && dot(previous, previous) > 0.0f) {
+      const float previous_depth = norm(previous - pose.t);
+      const float truncated = previous_depth - (2.0f * v.truncation);
+      seed = rp.min_depth < truncated ? truncated : rp.min_depth;
+    }
+  }
+  f3 out_point = nan3(), out_normal = nan3();
+  uint32_t out_color = 0;
+
+  const f3 translated = back_project(k, static_cast<float>(col), static_cast<float>(row), 1.0f);
+  const f3 direction = rotate(pose, translated);
+  const float dn = norm(direction);
+  if (dn > 0.0f) {
+    const f3 dir = direction / dn;
+    // find_zero_crossing (raycasting.hpp:165-211)
+    const float base_step = v.voxel_size * rp.step_scale;
+    // The step taken after a sample of exactly 1.0 (observed free space).
+    const float precomp_one = 1.0f * v.truncation * rp.step_scale;
+    const float free_step = base_step < precomp_one ? precomp_one : base_step;
+    bool have_prev = false;
+    float prev_tsdf = 0.0f;
+    f3 prev_point = make(0.0f, 0.0f, 0.0f);
+    float ray_length = seed;
+    bool found = false;
+    f3 surface = make(0.0f, 0.0f, 0.0f);
+    while (ray_length <= rp.max_depth) {
+      const f3 point = pose.t + (dir * ray_length);
+      if (safe != nullptr && in_safe_block(safe, v, point)) {
+        // The sample would be exactly 1.0: leaving a surface from behind
+        // ends the march; otherwise it is a positive sample.
+        if (have_prev && prev_tsdf < 0.0f) break;
+        have_prev = true;
+        prev_tsdf = 1.0f;
+        prev_point = point;
+        ray_length += free_step;
+        continue;
+      }
+      float tsdf;
+      if (!s.tsdf(point, rp.policy, tsdf)) {
+        have_prev = false;
+        ray_length += base_step;
+        continue;
+      }
+      if (have_prev && prev_tsdf > 0.0f && tsdf <= 0.0f) {
+        const float gap = prev_tsdf - tsdf;
+        const float alpha = gap != 0.0f ? prev_tsdf / gap : 0.0f;
+        surface = prev_point + ((point - prev_point) * alpha);
+        found = true;
+        break;
+      }
+      if (have_prev && prev_tsdf < 0.0f && tsdf > 0.0f) break;
+      have_prev = true;
+      prev_tsdf = tsdf;
+      prev_point = point;
+      const float precomp = tsdf * v.truncation * rp.step_scale;
+      const float step = base_step < precomp ? precomp : base_step;
+      ray_length += tsdf > 0.0f ? step : base_step;
+    }
+    if (found) {
+      // write_surface_sample (raycasting.hpp:215-245)
+      f3 n;
+      const bool has_normal = rp.cell_normals ? s.cell_normal(surface, n) : s.central_normal(surface, rp.policy, n);
+      if (has_normal) {
+        out_point = surface;
+        out_normal = n;
+        if constexpr (Color) {
+          f3 c;
+          if (s.color(surface, c)) out_color = pixel_from_color(c);
+        } else {
+          const f3 view = normalized(pose.t - surface);
+          const float d = dot(n, view);
+          const float intensity = 255.0f * (0.0f < d ? d : 0.0f);
+          out_color = pixel_from_color(make(intensity, intensity, intensity));
+        }
+      }
+    }
+  }
+  store3(points + pix * 3, out_point);
+  store3(normals + pix * 3, out_normal);
+  colors[pix] = out_color;
+}
+
+template <int Kind, bool Color>
+void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points, float* normals,
+                  uint32_t* colors, const IcpState* state, cudaStream_t s) {
+  RaycastParams rp;
+  rp.min_depth = p.config.raycast.min_depth;
+  rp.max_depth = p.config.raycast.max_depth;
+  rp.step_scale = p.config.raycast.step_scale;
+  rp.policy = p.config.raycast.corner_policy;
+  rp.cell_normals = p.config.raycast.cell_gradient_normals;
+  rp.seed_previous = p.config.raycast.seed_from_previous;
+  const uint32_t* safe = p.safe_blocks.count ? p.safe_blocks.ptr : nullptr;
+  const dim3 block(16, 16);
+  const dim3 grid(ceil_div(cam.width, 16), ceil_div(cam.height, 16));
+  raycast_kernel<Kind, Color><<<grid, block, 0, s>>>(p.view, safe, rp, intr_from(cam.intrinsics), cam.width,
+                                                     cam.height, rigid_from(cam.camera_to_world), state, points,
+                                                     normals, colors);
+  check(cudaGetLastError(), "raycast_kernel launch");
+}
+
+}  // namespace
+
+void launch_raycast(const Pipeline& p, const kf_raycast_camera& cam, float* points, float* normals,
+                    uint32_t* colors, const IcpState* state, cudaStream_t s) {
+  const bool color = p.config.color == KF_COLOR_FLOAT;
+  switch (p.config.voxel) {
+    case KF_VOXEL_QUANTIZED:
+      color ? launch_typed<KF_VOXEL_QUANTIZED, true>(p, cam, points, normals, colors, state, s)
+            : launch_typed<KF_VOXEL_QUANTIZED, false>(p, cam, points, normals, colors, state, s);
+      break;
+    case KF_VOXEL_BF16:
+      color ? launch_typed<KF_VOXEL_BF16, true>(p, cam, points, normals, colors, state, s)
+            : launch_typed<KF_VOXEL_BF16, false>(p, cam, points, normals, colors, state, s);
+      break;
+    default:
+      color ? launch_typed<KF_VOXEL_FLOAT, true>(p, cam, points, normals, colors, state, s)
+            : launch_typed<KF_VOXEL_FLOAT, false>(p, cam, points, normals, colors, state, s);
+      break;
+  }
+}
+
+}  // namespace kf
