@@ -1,0 +1,377 @@
+"""Benchmark of the per-frame pipeline: frames/s at 640x480 into a 512^3 volume.
+
+One step = one frame of the reference's per-frame loop (Reconstruction::
+process_frame, src/app/reconstruction.cpp:184-216): bilateral + 3-level
+pyramid, per level a model raycast at the current pose estimate and the
+ICP iterations [10, 5, 4], then TSDF integration at the tracked pose.
+
+Workload: the 640x480 synthetic scene (seeded box room + spheres + boxes,
+kinectfusion_b200/synthetic.py) through a dense 512^3 float volume at 1 cm
+(8 B/voxel, 1 GiB, colour off), angle-weighted TSDF, truncation 5 cm.
+Frames play forward and back over a 30-frame seeded sequence so that every
+step tracks a real inter-frame motion.  The 1 GiB volume is larger than L2,
+so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: replicas only (each rank tracks its own seeded sequence; the
+path has no exchange step).  Timing is CUDA events on the pipeline's stream,
+barrier + synchronize on both sides, max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "frames/s (640x480, 512^3) and ICP iters/frame, learned vs plain at equal ATE"
+RES, VOXEL, TRUNC = 512, 0.01, 0.05
+ORIGIN = (-0.5 * RES * VOXEL, -0.5 * RES * VOXEL, -0.5)
+SEQ_FRAMES = 30
+KERNELS_PER_FRAME = 4 + 1 + 1 + 3 * 3 + (10 + 5 + 4) + 1  # pyramid, table, frame begin, levels, ICP, integrate
+
+
+def frame_schedule(step: int) -> int:
+    """Triangle wave over the sequence: 0..29, 28..1, 0..29, ..."""
+    period = 2 * (SEQ_FRAMES - 1)
+    s = step % period
+    return s if s < SEQ_FRAMES else period - s
+
+
+def workload_config() -> dict:
+    return {"workload": "640x480 synthetic RGB-D frames tracked and fused into a dense 512^3 float volume "
+                        "(0.01 m voxels, 8 B/voxel, colour off), angle-weighted TSDF, ICP [10,5,4]",
+            "frame": [640, 480], "volume": [RES, RES, RES], "voxel_size_m": VOXEL, "truncation_m": TRUNC,
+            "voxel_bytes": 8, "sequence_frames": SEQ_FRAMES,
+            "l2": "inputs larger than L2 (1 GiB volume re-read every step), no flush"}
+
+
+# ---- clocks ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"hbm_gbs": 6650.0, "fallback": True}
+
+
+def profile_traffic() -> float | None:
+    """DRAM bytes per integrate launch from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "integrate_dense512_cfg2.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ---- our arm ------------------------------------------------------------------------------
+def run_ours(args, rank: int, world: int, dist) -> dict | None:
+    import torch
+
+    import kinectfusion_b200 as kf
+    from kinectfusion_b200 import abi, synthetic
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    lib = abi.load()
+    seq = synthetic.make_sequence(seed=1000 + rank, frames=SEQ_FRAMES)
+    k = abi.Intrinsics(synthetic.FX, synthetic.FY, synthetic.CX, synthetic.CY)
+    cfg = kf.pipeline_config(RES, VOXEL, ORIGIN, TRUNC, color=abi.KF_COLOR_NONE, rule=abi.KF_RULE_ANGLE_WEIGHTED)
+    pipe = kf.Pipeline(cfg)
+    pyr = kf.PyramidSource()
+    tracker = kf.ProjectiveIcpTracker()
+    iters = (C.c_uint32 * 4)(10, 5, 4, 4)
+    stream_ptr = C.c_void_p()
+    abi.check(lib.kf_pipeline_stream(pipe.handle, C.byref(stream_ptr)))
+    stream = torch.cuda.ExternalStream(stream_ptr.value)
+    depth_dev = torch.from_numpy(seq.depth.view(np.int16)).cuda()
+    frame_bytes = 640 * 480 * 2
+    base = depth_dev.data_ptr()
+
+    def enqueue(step: int, first: bool):
+        idx = frame_schedule(step)
+        abi.check(lib.kf_frame_enqueue(pipe.handle, pyr.handle, tracker.handle, C.c_void_p(base + idx * frame_bytes),
+                                       None, 640, 480, k, abi.KF_MEMORY_DEVICE, iters, 1 if first else 0))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # warm-up (the first step fuses the first frame without tracking)
+    enqueue(0, True)
+    for s in range(1, max(args.warmup, 3)):
+        enqueue(s, False)
+    torch.cuda.synchronize()
+    step0 = max(args.warmup, 3)
+
+    # ---- timed region: device-resident inputs ------------------------------------
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    updates0 = C.c_uint64()
+    abi.check(lib.kf_pipeline_update_counts(pipe.handle, C.byref(updates0), None))
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        start.record(stream)
+        for s in range(args.steps):
+            enqueue(step0 + s, False)
+        stop.record(stream)
+        stop.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    elapsed_ms = start.elapsed_time(stop)
+    updates1 = C.c_uint64()
+    abi.check(lib.kf_pipeline_update_counts(pipe.handle, C.byref(updates1), None))
+    last = abi.FrameResult()
+    abi.check(lib.kf_frame_result_fetch(pipe.handle, C.byref(last)))
+    voxel_updates_per_step = (updates1.value - updates0.value) / args.steps
+
+    # ---- end to end through the public API: host depth in, pose out ----------------
+    pipe2 = kf.Pipeline(cfg)
+    loop = kf.Reconstruction(pipe2, k)
+    pinned = torch.from_numpy(seq.depth.view(np.int16)).pin_memory().numpy().view(np.uint16)
+    for s in range(max(args.warmup, 3)):
+        loop.process(pinned[frame_schedule(s)])
+    stream2_ptr = C.c_void_p()
+    abi.check(lib.kf_pipeline_stream(pipe2.handle, C.byref(stream2_ptr)))
+    stream2 = torch.cuda.ExternalStream(stream2_ptr.value)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream2)
+    for s in range(args.steps):
+        loop.process(pinned[frame_schedule(max(args.warmup, 3) + s)])
+    e1.record(stream2)
+    e1.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    result_bytes = C.sizeof(abi.FrameResult)
+
+    # accuracy of the e2e trajectory over the first pass of the sequence
+    ate = None
+    n = min(len(loop.trajectory), SEQ_FRAMES)
+    if n >= 3:
+        est = np.stack(loop.trajectory[:n]).astype(np.float64)
+        ate = synthetic.ate_rmse(est, seq.poses[:n])["rmse"]
+    iters_per_frame = float(np.mean([sum(r.iterations[:3]) for r in loop.results]))
+
+    # ---- dominant kernel: integration, timed alone with events on its stream -------
+    ev_a, ev_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    abi.check(lib.kf_pipeline_set_kernel_events(pipe2.handle, C.c_void_p(ev_a.cuda_event), C.c_void_p(ev_b.cuda_event)))
+    kernel_ms, kernel_updates = [], []
+    pyr_probe = kf.PyramidSource()
+    for s in range(min(args.steps, 20)):
+        idx = frame_schedule(s)
+        pyr_probe.build(seq.depth[idx], k)
+        normals = pyr_probe.download_level(0)["normals"]
+        w2c = np.linalg.inv(seq.poses[idx])
+        u0 = C.c_uint64()
+        abi.check(lib.kf_pipeline_update_counts(pipe2.handle, C.byref(u0), None))
+        pipe2.integrate(seq.depth[idx], k, w2c, normals=normals)
+        u1 = C.c_uint64()
+        abi.check(lib.kf_pipeline_update_counts(pipe2.handle, C.byref(u1), None))
+        kernel_ms.append(ev_a.elapsed_time(ev_b))
+        kernel_updates.append(u1.value - u0.value)
+    abi.check(lib.kf_pipeline_set_kernel_events(pipe2.handle, None, None))
+
+    times = torch.tensor([elapsed_ms, e2e_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    elapsed_ms, e2e_ms = times.tolist()
+    if rank != 0:
+        return None
+
+    fps = args.steps * world / (elapsed_ms / 1e3)
+    e2e_fps = args.steps * world / (e2e_ms / 1e3)
+    peaks = measured_peaks()
+    # algorithmic bytes of one integrate launch: read+write 8 B per fused voxel
+    # plus the frame inputs it reads (depth 2 B + normals 12 B per pixel).
+    frame_inputs = 640 * 480 * (2 + 12)
+    alg_bytes = float(np.mean(kernel_updates)) * 16 + frame_inputs
+    kernel_s = float(np.mean(kernel_ms)) / 1e3
+    achieved = alg_bytes / kernel_s / 1e9
+    traffic = profile_traffic()
+    line = {
+        "metric": METRIC, "value": round(fps, 2), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(elapsed_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded analytic RGB-D scene)",
+        "config": {**workload_config(), "parallelism": f"replicas{world}"},
+        "e2e": {"value": round(e2e_fps, 2), "unit": "frames/s", "h2d_bytes_per_step": frame_bytes,
+                "d2h_bytes_per_step": result_bytes},
+        "gpu_launches": KERNELS_PER_FRAME * args.steps,
+        "voxel_updates_per_s": round(voxel_updates_per_step * fps, 1),
+        "icp_iters_per_frame": iters_per_frame,
+        "ate_rmse_m": ate,
+        "tracked_last_step": bool(last.tracked),
+        "roofline": {"bound": "hbm", "kernel": "integrate_kernel<float,no colour>", "achieved": round(achieved, 1),
+                     "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                     "frac": round(achieved / peaks.get("hbm_gbs", 6650.0), 4),
+                     "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                     "launch_ms": round(kernel_s * 1e3, 4),
+                     "peak_source": "measured" if not peaks.get("fallback") else "fallback"},
+        "clocks": clocks.summary(),
+    }
+    if args.cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(seq)
+    return line
+
+
+# ---- CPU baseline (the oracle port, bounded sample) -----------------------------------------
+def cpu_baseline(seq, threads: int = 1, frames: int = 2) -> dict:
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import kf_oracle as ko
+    from kinectfusion_b200 import abi, synthetic
+
+    k = abi.Intrinsics(synthetic.FX, synthetic.FY, synthetic.CX, synthetic.CY)
+    vol = ko.OracleVolume(RES, VOXEL, ORIGIN, TRUNC)
+    pose = np.eye(4, dtype=np.float32)
+    args = (ko.depth_options(), ko.integration_options(), ko.raycast_options(), ko.icp_options())
+    ko.track_frame(vol, seq.depth[0], k, pose, *args, threads=threads, first=True)
+    t0 = time.perf_counter()
+    for f in range(1, 1 + frames):
+        pose, _, _ = ko.track_frame(vol, seq.depth[f], k, pose, *args, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": round(frames / dt, 4), "unit": "frames/s", "cores": threads, "kind": "port",
+            "host_cores": os.cpu_count(),
+            "sample": f"{frames} tracked frames of the same 512^3 workload (after one fused first frame) "
+                      f"on the CPU oracle, {threads} thread(s)"}
+
+
+# ---- reference arm -----------------------------------------------------------------------------
+def run_reference(args, rank: int) -> dict | None:
+    """The reference's CPU implementation of the path (the oracle port: the
+    reference itself does not build here) on all host cores."""
+    if rank != 0:
+        return None
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import kf_oracle as ko
+    from kinectfusion_b200 import abi, synthetic
+
+    threads = os.cpu_count() or 1
+    seq = synthetic.make_sequence(seed=1000, frames=SEQ_FRAMES)
+    k = abi.Intrinsics(synthetic.FX, synthetic.FY, synthetic.CX, synthetic.CY)
+    vol = ko.OracleVolume(RES, VOXEL, ORIGIN, TRUNC)
+    pose = np.eye(4, dtype=np.float32)
+    opts = (ko.depth_options(), ko.integration_options(), ko.raycast_options(), ko.icp_options())
+    ko.track_frame(vol, seq.depth[0], k, pose, *opts, threads=threads, first=True)
+    steps, warmup = args.steps, args.warmup
+    # bound the run to a few minutes: one frame is ~1-2 s on 8 cores
+    budget = int(os.environ.get("KF_REFERENCE_MAX_FRAMES", "40"))
+    if steps + warmup > budget:
+        warmup = min(warmup, 3)
+        steps = max(1, budget - warmup)
+    for s in range(1, 1 + warmup):
+        pose, _, _ = ko.track_frame(vol, seq.depth[frame_schedule(s)], k, pose, *opts, threads=threads)
+    t0 = time.perf_counter()
+    for s in range(steps):
+        pose, _, _ = ko.track_frame(vol, seq.depth[frame_schedule(1 + warmup + s)], k, pose, *opts, threads=threads)
+    dt = time.perf_counter() - t0
+    fps = steps / dt
+    return {"impl": "reference", "metric": METRIC, "value": round(fps, 4), "unit": "frames/s", "n_gpus": 0,
+            "steps": steps, "warmup": warmup, "ms_per_step": round(dt / steps * 1e3, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded analytic RGB-D scene)",
+            "config": {**workload_config(), "parallelism": f"cpu{threads}"},
+            "cpu_baseline": {"value": round(fps, 4), "unit": "frames/s", "cores": threads, "kind": "port",
+                             "sample": f"{steps} tracked frames of the 512^3 workload on the CPU oracle "
+                                       f"({threads} OpenMP threads)"},
+            "e2e": {"value": round(fps, 4), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        line = run_reference(args, rank)
+    else:
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as tdist
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+            tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            dist = tdist
+        line = run_ours(args, rank, world, dist)
+        if dist is not None:
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -283,6 +283,16 @@ kf_status kf_pipeline_extract_mesh(kf_pipeline* pipeline, float min_weight, kf_m
 void kf_mesh_free(kf_mesh* mesh);
 /* Waits for the pipeline's stream. */
 kf_status kf_pipeline_synchronize(kf_pipeline* pipeline);
+/* The pipeline's CUDA stream (a cudaStream_t) for callers that order or time
+ * their own work against it. */
+kf_status kf_pipeline_stream(kf_pipeline* pipeline, void** stream);
+/* Two cudaEvent_t handles (or NULL) recorded on the pipeline's stream right
+ * before and after each standalone integration kernel launch. */
+kf_status kf_pipeline_set_kernel_events(kf_pipeline* pipeline, void* start, void* stop);
+/* Cumulative fused voxel updates and colour updates since creation/reset
+ * (the unit of the voxel-updates/s metric). */
+kf_status kf_pipeline_update_counts(kf_pipeline* pipeline, uint64_t* voxel_updates,
+                                    uint64_t* color_updates);
 
 /* ---- tracker: ProjectiveIcpTracker::estimate_pose(DeviceTrackingRequest)
  * (icp_optimizer.hpp:115-116, icp_optimizer.cpp:58-76) with the device solve. */

@@ -165,6 +165,9 @@ _PROTOTYPES = {
     "kf_pipeline_extract_mesh": (C.c_int, [P, C.c_float, C.POINTER(Mesh)]),
     "kf_mesh_free": (None, [C.POINTER(Mesh)]),
     "kf_pipeline_synchronize": (C.c_int, [P]),
+    "kf_pipeline_stream": (C.c_int, [P, C.POINTER(P)]),
+    "kf_pipeline_set_kernel_events": (C.c_int, [P, P, P]),
+    "kf_pipeline_update_counts": (C.c_int, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "kf_tracker_create": (C.c_int, [C.POINTER(IcpOptions), C.POINTER(P)]),
     "kf_tracker_destroy": (C.c_int, [P]),
     "kf_pipeline_track": (C.c_int, [P, P, C.POINTER(RaycastCamera), C.POINTER(LevelView), C.c_uint32,

@@ -250,6 +250,8 @@ kf_status kf_pipeline_create(const kf_pipeline_config* config, kf_pipeline** out
       v.origin = make(g.origin[0], g.origin[1], g.origin[2]);
       v.truncation = g.truncation_distance;
       launch_fill_volume(p, p.stream);
+      p.counters.resize(2);
+      check(cudaMemsetAsync(p.counters.ptr, 0, p.counters.bytes(), p.stream), "counter init");
       check(cudaStreamSynchronize(p.stream), "volume fill");
     } catch (...) {
       delete h;
@@ -275,6 +277,7 @@ kf_status kf_pipeline_reset(kf_pipeline* pipeline) {
     require(pipeline != nullptr, "kf_pipeline_reset: null pipeline");
     Pipeline& p = pipeline->impl;
     launch_fill_volume(p, p.stream);
+    check(cudaMemsetAsync(p.counters.ptr, 0, p.counters.bytes(), p.stream), "counter reset");
     if (p.free_blocks.count) check(cudaMemsetAsync(p.free_blocks.ptr, 0, p.free_blocks.bytes(), p.stream), "skip reset");
     if (p.safe_blocks.count) check(cudaMemsetAsync(p.safe_blocks.ptr, 0, p.safe_blocks.bytes(), p.stream), "skip reset");
     check(cudaStreamSynchronize(p.stream), "volume reset");
@@ -411,6 +414,33 @@ kf_status kf_pipeline_synchronize(kf_pipeline* pipeline) {
   return guarded([&] {
     require(pipeline != nullptr, "kf_pipeline_synchronize: null pipeline");
     check(cudaStreamSynchronize(pipeline->impl.stream), "pipeline synchronize");
+  });
+}
+
+kf_status kf_pipeline_stream(kf_pipeline* pipeline, void** stream) {
+  return guarded([&] {
+    require(pipeline != nullptr && stream != nullptr, "kf_pipeline_stream: null argument");
+    *stream = reinterpret_cast<void*>(pipeline->impl.stream);
+  });
+}
+
+kf_status kf_pipeline_set_kernel_events(kf_pipeline* pipeline, void* start, void* stop) {
+  return guarded([&] {
+    require(pipeline != nullptr, "kf_pipeline_set_kernel_events: null pipeline");
+    pipeline->impl.kernel_start = reinterpret_cast<cudaEvent_t>(start);
+    pipeline->impl.kernel_stop = reinterpret_cast<cudaEvent_t>(stop);
+  });
+}
+
+kf_status kf_pipeline_update_counts(kf_pipeline* pipeline, uint64_t* voxel_updates, uint64_t* color_updates) {
+  return guarded([&] {
+    require(pipeline != nullptr, "kf_pipeline_update_counts: null pipeline");
+    Pipeline& p = pipeline->impl;
+    unsigned long long host[2] = {0, 0};
+    check(cudaMemcpyAsync(host, p.counters.ptr, sizeof(host), cudaMemcpyDeviceToHost, p.stream), "counter read");
+    check(cudaStreamSynchronize(p.stream), "counter read");
+    if (voxel_updates) *voxel_updates = host[0];
+    if (color_updates) *color_updates = host[1];
   });
 }
 

@@ -105,7 +105,8 @@ __device__ __forceinline__ bool column_range(f3 a, f3 b, const Intr& k, float wi
 template <int Kind, bool Color>
 __global__ void __launch_bounds__(256)
     integrate_kernel(VolumeDev v, const float4* __restrict__ table, uint32_t width, uint32_t height,
-                     Intr k, Rigid T, IntegParams ip, const IcpState* __restrict__ state) {
+                     Intr k, Rigid T, IntegParams ip, const IcpState* __restrict__ state,
+                     unsigned long long* __restrict__ counters) {
   using VT = VoxelTraits<Kind>;
   using Raw = typename VT::Raw;
   if (state != nullptr) {
@@ -130,12 +131,11 @@ __global__ void __launch_bounds__(256)
   const f3 a = make((hx + T.rx.z * w0) + T.t.x, (hy + T.ry.z * w0) + T.t.y, (hz + T.rz.z * w0) + T.t.z);
   const f3 b = make(T.rx.z * v.voxel_size, T.ry.z * v.voxel_size, T.rz.z * v.voxel_size);
   float lo, hi;
-  if (!column_range(a, b, k, static_cast<float>(width), static_cast<float>(height),
-                    static_cast<float>(v.rz - 1), lo, hi)) {
-    return;
-  }
-  const uint32_t z_first = static_cast<uint32_t>(lo);
-  const uint32_t z_last = static_cast<uint32_t>(hi);
+  const bool visible = column_range(a, b, k, static_cast<float>(width), static_cast<float>(height),
+                                    static_cast<float>(v.rz - 1), lo, hi);
+  const uint32_t z_first = visible ? static_cast<uint32_t>(lo) : 1u;
+  const uint32_t z_last = visible ? static_cast<uint32_t>(hi) : 0u;
+  unsigned updates = 0, color_updates = 0;
 
   Raw* __restrict__ voxels = reinterpret_cast<Raw*>(v.voxels);
   const size_t column = static_cast<size_t>(y) * v.rx + x;
@@ -170,8 +170,10 @@ __global__ void __launch_bounds__(256)
     const float avg = ((t0 * w0v) + (tsdf * ow)) / (w0v + ow);
     const float sum_w = w0v + ow;
     voxels[index] = VT::encode(avg, ip.max_weight < sum_w ? ip.max_weight : sum_w);
+    ++updates;
     if constexpr (Color) {
       if (ip.has_color && sdf <= truncation * 0.5f) {
+        ++color_updates;
         // ColorVoxel::fused (volume.hpp:160-170)
         const float4 cv = v.colors[index];
         const f3 c = color_from_pixel(__float_as_uint(tb.w));
@@ -180,6 +182,14 @@ __global__ void __launch_bounds__(256)
         v.colors[index] = make_float4(avgc.x, avgc.y, avgc.z, ip.max_weight < cw ? ip.max_weight : cw);
       }
     }
+  }
+  // One atomic per warp for the voxel-update counters.
+  const unsigned mask = __activemask();
+  const unsigned total = __reduce_add_sync(mask, updates);
+  const unsigned total_color = __reduce_add_sync(mask, color_updates);
+  if ((threadIdx.x & 31u) == static_cast<unsigned>(__ffs(mask) - 1) && counters != nullptr) {
+    if (total) atomicAdd(counters, static_cast<unsigned long long>(total));
+    if (total_color) atomicAdd(counters + 1, static_cast<unsigned long long>(total_color));
   }
 }
 
@@ -220,8 +230,11 @@ void launch_integrate_typed(Pipeline& p, const float4* table, uint32_t width, ui
   ip.has_color = has_color;
   const dim3 block(32, 8);
   const dim3 grid(ceil_div(p.view.rx, 32), ceil_div(p.view.ry, 8));
-  integrate_kernel<Kind, Color><<<grid, block, 0, s>>>(p.view, table, width, height, k, T, ip, state);
+  if (state == nullptr && p.kernel_start != nullptr) check(cudaEventRecord(p.kernel_start, s), "event record");
+  integrate_kernel<Kind, Color><<<grid, block, 0, s>>>(p.view, table, width, height, k, T, ip, state,
+                                                       p.counters.ptr);
   check(cudaGetLastError(), "integrate_kernel launch");
+  if (state == nullptr && p.kernel_stop != nullptr) check(cudaEventRecord(p.kernel_stop, s), "event record");
 }
 
 }  // namespace

@@ -254,6 +254,8 @@ struct Pipeline {
   };
   std::map<std::pair<uint32_t, uint32_t>, Maps> maps;
   cudaStream_t stream = nullptr;
+  DeviceArray<unsigned long long> counters;  // [0] voxel updates, [1] colour updates
+  cudaEvent_t kernel_start = nullptr, kernel_stop = nullptr;  // borrowed
   // whole-frame graphs keyed by (width, height, iterations, first, colour)
   struct GraphKey {
     uint32_t w, h, it0, it1, it2, it3, first, color;

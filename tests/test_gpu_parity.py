@@ -232,7 +232,9 @@ def pose_error(a, b):
     b = np.asarray(b, dtype=np.float64)
     dt = np.linalg.norm(a[:3, 3] - b[:3, 3])
     r = a[:3, :3].T @ b[:3, :3]
-    ang = np.arccos(np.clip((np.trace(r) - 1) / 2, -1, 1))
+    # atan2 form: arccos of the trace has a sqrt(eps) floor near identity
+    skew = np.array([r[2, 1] - r[1, 2], r[0, 2] - r[2, 0], r[1, 0] - r[0, 1]]) / 2
+    ang = np.arctan2(np.linalg.norm(skew), (np.trace(r) - 1) / 2)
     return dt, ang
 
 
