@@ -224,6 +224,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
 
     # ---- dominant kernel: integration, timed alone with events on its stream -------
     ev_a, ev_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev_a.record(stream2)  # torch creates the CUDA events lazily, on first record
+    ev_b.record(stream2)
     abi.check(lib.kf_pipeline_set_kernel_events(pipe2.handle, C.c_void_p(ev_a.cuda_event), C.c_void_p(ev_b.cuda_event)))
     kernel_ms, kernel_updates = [], []
     pyr_probe = kf.PyramidSource()
