@@ -278,8 +278,6 @@ kf_status kf_pipeline_reset(kf_pipeline* pipeline) {
     Pipeline& p = pipeline->impl;
     launch_fill_volume(p, p.stream);
     check(cudaMemsetAsync(p.counters.ptr, 0, p.counters.bytes(), p.stream), "counter reset");
-    if (p.free_blocks.count) check(cudaMemsetAsync(p.free_blocks.ptr, 0, p.free_blocks.bytes(), p.stream), "skip reset");
-    if (p.safe_blocks.count) check(cudaMemsetAsync(p.safe_blocks.ptr, 0, p.safe_blocks.bytes(), p.stream), "skip reset");
     check(cudaStreamSynchronize(p.stream), "volume reset");
   });
 }
@@ -300,7 +298,6 @@ kf_status kf_pipeline_integrate(kf_pipeline* pipeline, const kf_frame_view* fram
                        p.pixel_table.ptr, p.stream);
     launch_integrate(p, p.pixel_table.ptr, f.width, f.height, k, rigid_from(f.world_to_camera),
                      color != nullptr, nullptr, p.stream);
-    if (p.config.raycast_backend == KF_RAYCAST_BITMAP_MARCH) launch_rebuild_skip(p, p.stream);
     check(cudaStreamSynchronize(p.stream), "integrate");
   });
 }

@@ -6,62 +6,12 @@
 //   pose (skipped on a tracking failure) -> result download.
 // One graph launch and at most one host synchronisation per frame.  The
 // reference syncs once per ICP iteration (icp_correspondence.cu:589-596).
-//
-// Also the empty-space block bitmaps of the march skip.
 #include <cstring>
 
 #include "kf_internal.h"
 
 namespace kf {
 namespace {
-
-// One CTA per 8^3 block: the block is free when every voxel is observed with
-// tsdf exactly 1.0 (partial blocks at the volume edge never are).
-template <int Kind>
-__global__ void __launch_bounds__(512) free_blocks_kernel(VolumeDev v, uint32_t* __restrict__ free_bits) {
-  using VT = VoxelTraits<Kind>;
-  const uint32_t block = blockIdx.x;
-  const uint32_t bxi = block % v.bx, byi = (block / v.bx) % v.by, bzi = block / (v.bx * v.by);
-  const uint32_t x = bxi * 8 + (threadIdx.x & 7u);
-  const uint32_t y = byi * 8 + ((threadIdx.x >> 3) & 7u);
-  const uint32_t z = bzi * 8 + (threadIdx.x >> 6);
-  bool free = x < v.rx && y < v.ry && z < v.rz;
-  if (free) {
-    const long long i = storage_index(v, x, y, z);
-    if (i < 0) {
-      free = false;
-    } else {
-      const typename VT::Raw r = reinterpret_cast<const typename VT::Raw*>(v.voxels)[i];
-      free = VT::observed(r) && VT::tsdf(r) == 1.0f;
-    }
-  }
-  if (__syncthreads_and(free) && threadIdx.x == 0) atomicOr(free_bits + (block >> 5), 1u << (block & 31u));
-}
-
-// safe = free block whose 26 neighbours are free and inside the volume.
-__global__ void safe_blocks_kernel(const uint32_t* __restrict__ free_bits, uint32_t* __restrict__ safe_bits,
-                                   uint32_t bx, uint32_t by, uint32_t bz) {
-  const uint32_t block = blockIdx.x * blockDim.x + threadIdx.x;
-  if (block >= bx * by * bz) return;
-  const int x = static_cast<int>(block % bx), y = static_cast<int>((block / bx) % by),
-            z = static_cast<int>(block / (bx * by));
-  bool safe = true;
-  for (int dz = -1; dz <= 1 && safe; ++dz) {
-    for (int dy = -1; dy <= 1 && safe; ++dy) {
-      for (int dx = -1; dx <= 1 && safe; ++dx) {
-        const int nx = x + dx, ny = y + dy, nz = z + dz;
-        if (nx < 0 || ny < 0 || nz < 0 || nx >= static_cast<int>(bx) || ny >= static_cast<int>(by) ||
-            nz >= static_cast<int>(bz)) {
-          safe = false;
-          break;
-        }
-        const uint32_t nb = (static_cast<uint32_t>(nz) * by + static_cast<uint32_t>(ny)) * bx + static_cast<uint32_t>(nx);
-        safe = (free_bits[nb >> 5] >> (nb & 31u)) & 1u;
-      }
-    }
-  }
-  if (safe) atomicOr(safe_bits + (block >> 5), 1u << (block & 31u));
-}
 
 __global__ void frame_begin_kernel(IcpState* st) {
   if (threadIdx.x != 0) return;
@@ -74,32 +24,6 @@ __global__ void frame_begin_kernel(IcpState* st) {
 }
 
 }  // namespace
-
-void launch_rebuild_skip(Pipeline& p, cudaStream_t s) {
-  const uint32_t blocks = p.view.bx * p.view.by * p.view.bz;
-  const size_t words = (blocks + 31) / 32;
-  if (p.free_blocks.count != words) {
-    p.free_blocks.resize(words);
-    p.safe_blocks.resize(words);
-  }
-  check(cudaMemsetAsync(p.free_blocks.ptr, 0, p.free_blocks.bytes(), s), "free bits clear");
-  check(cudaMemsetAsync(p.safe_blocks.ptr, 0, p.safe_blocks.bytes(), s), "safe bits clear");
-  switch (p.config.voxel) {
-    case KF_VOXEL_QUANTIZED:
-      free_blocks_kernel<KF_VOXEL_QUANTIZED><<<blocks, 512, 0, s>>>(p.view, p.free_blocks.ptr);
-      break;
-    case KF_VOXEL_BF16:
-      free_blocks_kernel<KF_VOXEL_BF16><<<blocks, 512, 0, s>>>(p.view, p.free_blocks.ptr);
-      break;
-    default:
-      free_blocks_kernel<KF_VOXEL_FLOAT><<<blocks, 512, 0, s>>>(p.view, p.free_blocks.ptr);
-      break;
-  }
-  check(cudaGetLastError(), "free_blocks_kernel launch");
-  safe_blocks_kernel<<<ceil_div(blocks, 256), 256, 0, s>>>(p.free_blocks.ptr, p.safe_blocks.ptr, p.view.bx, p.view.by,
-                                                          p.view.bz);
-  check(cudaGetLastError(), "safe_blocks_kernel launch");
-}
 
 namespace {
 
@@ -142,7 +66,6 @@ void record_frame(Pipeline& p, Pyramid& pyr, Tracker& t, const Pipeline::GraphKe
     }
   }
   launch_integrate(p, p.pixel_table.ptr, pyr.width, pyr.height, k0, Rigid{}, has_color, st, s);
-  if (p.config.raycast_backend == KF_RAYCAST_BITMAP_MARCH) launch_rebuild_skip(p, s);
   check(cudaMemcpyAsync(p.result_staging.ptr, st, sizeof(IcpState), cudaMemcpyDeviceToHost, s), "result download");
 }
 
@@ -199,13 +122,7 @@ void enqueue(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker, co
   if (it == p.graphs.end()) {
     // Size every buffer the graph touches before capture.
     for (uint32_t level = 0; level < pyr.level_count; ++level) p.maps_for(width >> level, height >> level);
-    if (p.config.raycast_backend == KF_RAYCAST_BITMAP_MARCH && p.free_blocks.count == 0) {
-      const uint32_t blocks = p.view.bx * p.view.by * p.view.bz;
-      p.free_blocks.resize((blocks + 31) / 32);
-      p.safe_blocks.resize((blocks + 31) / 32);
-      check(cudaMemsetAsync(p.free_blocks.ptr, 0, p.free_blocks.bytes(), s), "free bits init");
-      check(cudaMemsetAsync(p.safe_blocks.ptr, 0, p.safe_blocks.bytes(), s), "safe bits init");
-    }
+    prepare_blocks(p, width, height, s);
     check(cudaStreamSynchronize(s), "pre-capture sync");
     cudaGraph_t graph = nullptr;
     check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");

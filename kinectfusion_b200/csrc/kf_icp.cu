@@ -66,34 +66,79 @@ __device__ __forceinline__ bool match(const IcpLevelArgs& a, const Rigid& cam, c
 }
 
 // ---- FP64 6x6 linear algebra ------------------------------------------------
-// Cholesky A = L L^T; false on a non-positive pivot.
-__device__ bool cholesky6(const double (&a)[6][6], double (&l)[6][6]) {
-  for (int r = 0; r < 6; ++r) {
-    for (int c = 0; c <= r; ++c) {
-      double s = a[r][c];
-      for (int k = 0; k < c; ++k) s -= l[r][k] * l[c][k];
-      if (r == c) {
-        if (!(s > 0.0)) return false;
-        l[r][r] = sqrt(s);
-      } else {
-        l[r][c] = s / l[c][c];
+// Every loop has constant bounds and is unrolled, so the matrices live in
+// registers (the solve runs on one thread of the last CTA).
+// Cholesky A = L L^T; false on a non-positive pivot.  rinv[c] = 1 / L[c][c].
+__device__ __forceinline__ bool cholesky6(const double (&a)[6][6], double (&l)[6][6], double (&rinv)[6]) {
+  bool ok = true;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    double d = a[c][c];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      if (k < c) d -= l[c][k] * l[c][k];
+    }
+    ok = ok && (d > 0.0);
+    const double lc = sqrt(fmax(d, 1e-300));
+    l[c][c] = lc;
+    rinv[c] = 1.0 / lc;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      if (r <= c) {
+        if (r < c) l[r][c] = 0.0;
+        continue;
       }
+      double s = a[r][c];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        if (k < c) s -= l[r][k] * l[c][k];
+      }
+      l[r][c] = s * rinv[c];
     }
   }
-  return true;
+  return ok;
 }
 
-__device__ void cholesky_solve6(const double (&l)[6][6], const double (&b)[6], double (&x)[6]) {
-  double y[6];
-  for (int r = 0; r < 6; ++r) {
-    double s = b[r];
-    for (int k = 0; k < r; ++k) s -= l[r][k] * y[k];
-    y[r] = s / l[r][r];
+// L^-1 of a lower triangular factor (no divisions: rinv holds 1 / L[c][c]).
+__device__ __forceinline__ void lower_inverse6(const double (&l)[6][6], const double (&rinv)[6], double (&inv)[6][6]) {
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+      if (r < c) {
+        inv[r][c] = 0.0;
+        continue;
+      }
+      double s = (r == c) ? 1.0 : 0.0;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        if (k >= c && k < r) s -= l[r][k] * inv[k][c];
+      }
+      inv[r][c] = s * rinv[r];
+    }
   }
-  for (int r = 5; r >= 0; --r) {
-    double s = y[r];
-    for (int k = r + 1; k < 6; ++k) s -= l[k][r] * x[k];
-    x[r] = s / l[r][r];
+}
+
+// x = A^-1 b = L^-T (L^-1 b).
+__device__ __forceinline__ void inverse_solve6(const double (&inv)[6][6], const double (&b)[6], double (&x)[6]) {
+  double y[6];
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      if (k <= r) s += inv[r][k] * b[k];
+    }
+    y[r] = s;
+  }
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      if (k >= r) s += inv[k][r] * y[k];
+    }
+    x[r] = s;
   }
 }
 
@@ -206,35 +251,32 @@ struct Stability {
   float condition_number;
 };
 
-// check_system_stability (icp_optimizer.cpp:319-347).  A Cholesky test of
-// A - min_eig I plus a Frobenius bound on the condition number decides the
-// common well-conditioned case; anything else falls back to the full
-// eigenvalue computation.
-__device__ Stability stability(const double (&a)[6][6], const IcpParams& p, bool want_values) {
+// check_system_stability (icp_optimizer.cpp:319-347).  The common
+// well-conditioned case is decided without eigenvalues: with A = L L^T,
+// s = ||L^-1||_F^2 >= ||A^-1||_2, so lambda_min >= 1/s and
+// lambda_max / lambda_min <= ||A||_F * s; when both bounds meet the limits
+// the system is stable.  Any other case computes the spectrum.  `inv`
+// receives L^-1 when A factorises.
+__device__ Stability stability(const double (&a)[6][6], const IcpParams& p, bool want_values, double (&inv)[6][6],
+                               bool& chol_ok) {
   Stability s{false, 0.0f, 0.0f};
-  if (!want_values) {
-    double shifted[6][6], l[6][6];
-    for (int i = 0; i < 6; ++i)
-      for (int j = 0; j < 6; ++j) shifted[i][j] = a[i][j] - (i == j ? static_cast<double>(p.min_system_eigenvalue) : 0.0);
-    if (cholesky6(shifted, l)) {
-      // ||A||_F * ||A^-1||_F >= cond(A).
-      double la[6][6];
-      if (cholesky6(a, la)) {
-        double fro = 0.0, inv_fro = 0.0;
-        for (int i = 0; i < 6; ++i)
-          for (int j = 0; j < 6; ++j) fro += a[i][j] * a[i][j];
-        for (int c = 0; c < 6; ++c) {
-          double e[6] = {0, 0, 0, 0, 0, 0}, x[6];
-          e[c] = 1.0;
-          cholesky_solve6(la, e, x);
-          for (int i = 0; i < 6; ++i) inv_fro += x[i] * x[i];
-        }
-        const double bound = sqrt(fro) * sqrt(inv_fro);
-        if (bound <= static_cast<double>(p.max_condition_number)) {
-          s.stable = true;
-          return s;
-        }
+  double l[6][6], rinv[6];
+  chol_ok = cholesky6(a, l, rinv);
+  if (chol_ok) lower_inverse6(l, rinv, inv);
+  if (!want_values && chol_ok) {
+    double fro = 0.0, inv2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        fro += a[i][j] * a[i][j];
+        inv2 += inv[i][j] * inv[i][j];
       }
+    }
+    if (1.0 >= static_cast<double>(p.min_system_eigenvalue) * inv2 &&
+        sqrt(fro) * inv2 <= static_cast<double>(p.max_condition_number)) {
+      s.stable = true;
+      return s;
     }
   }
   double eig[6];
@@ -294,8 +336,11 @@ __device__ bool within_caps(const Increment& inc, const IcpParams& p) {
   return inc.update_translation <= p.max_update_translation && inc.update_rotation <= p.max_update_rotation;
 }
 
-// solve_increment (icp_optimizer.cpp:370-402) with an FP64 pivoted LDL^T.
-__device__ Increment solve_increment(const float* sums, float lambda, const IcpParams& p) {
+// solve_increment (icp_optimizer.cpp:370-402) in FP64: a Cholesky solve for
+// positive definite systems (the factor of the undamped system is reused),
+// the pivoted LDL^T for the rank-deficient ones.
+__device__ Increment solve_increment(const float* sums, float lambda, const IcpParams& p,
+                                     const double (&inv)[6][6], bool chol_ok) {
   Increment last;
   last.solved = false;
   last.update_translation = last.update_rotation = last.lambda = 0.0f;
@@ -321,7 +366,15 @@ __device__ Increment solve_increment(const float* sums, float lambda, const IcpP
       if (p.damping_mode == KF_DAMPING_DIAGONAL) off = static_cast<double>(scale) * base[r][r];
       damped[r][r] += off;
     }
-    ldlt_solve6(damped, rhs, x);
+    double l[6][6], rinv[6], dinv[6][6];
+    if (p.damping_mode == KF_DAMPING_NONE && chol_ok) {
+      inverse_solve6(inv, rhs, x);
+    } else if (cholesky6(damped, l, rinv)) {
+      lower_inverse6(l, rinv, dinv);
+      inverse_solve6(dinv, rhs, x);
+    } else {
+      ldlt_solve6(damped, rhs, x);
+    }
     bool finite = true;
     for (int i = 0; i < 6; ++i) finite = finite && isfinite(x[i]);
     if (finite) {
@@ -400,14 +453,16 @@ __device__ void gauss_newton_step(IcpState* st, const float* sums_in, unsigned l
       ++e;
     }
   }
-  const Stability stab = stability(a, p, want_values);
+  double inv[6][6];
+  bool chol_ok = false;
+  const Stability stab = stability(a, p, want_values, inv, chol_ok);
   st->min_system_eigenvalue = stab.min_eigenvalue;
   st->condition_number = stab.condition_number;
   if (!stab.stable && !active) {
     st->status = KF_ICP_UNCONSTRAINED_SYSTEM;
     return;
   }
-  const Increment inc = solve_increment(sums, st->lambda, p);
+  const Increment inc = solve_increment(sums, st->lambda, p, inv, chol_ok);
   if (!inc.solved) {
     st->status = KF_ICP_SOLVE_FAILED;
     return;
@@ -438,8 +493,10 @@ __device__ void gauss_newton_step(IcpState* st, const float* sums_in, unsigned l
   }
 }
 
+// Two CTAs per SM so that a 296-CTA level-0 sweep runs in one wave; the
+// rarely taken FP64 paths of the solve spill instead.
 template <bool Solve>
-__global__ void __launch_bounds__(kIcpBlock)
+__global__ void __launch_bounds__(kIcpBlock, 2)
     icp_iteration_kernel(IcpLevelArgs a, IcpState* __restrict__ st, float* __restrict__ partials, IcpParams p,
                          int want_values) {
   __shared__ int s_flag;
@@ -512,11 +569,34 @@ __global__ void __launch_bounds__(kIcpBlock)
   __syncthreads();
   if (!s_flag) return;
   __threadfence();
-  // Last CTA: Kahan-compensated combine in CTA order.
+  // Last CTA: deterministic Kahan-compensated combine of the CTA partials.
+  // Thread (sum i, segment g) compensates over CTAs g, g+8, g+16, ... then
+  // the eight segment results of each sum are combined in segment order.
+  __shared__ float s_seg_sum[8][kIcpSlot];
+  __shared__ float s_seg_comp[8][kIcpSlot];
+  {
+    const unsigned i = threadIdx.x % kIcpSlot, g = threadIdx.x / kIcpSlot;  // 8 x 32 threads
+    if (i < kIcpSums) {
+      float sum = 0.0f, comp = 0.0f;
+      for (unsigned b = g; b < gridDim.x; b += 8) {
+        const float y = __ldcg(partials + b * kIcpSlot + i) - comp;
+        const float t = sum + y;
+        comp = (t - sum) - y;
+        sum = t;
+      }
+      s_seg_sum[g][i] = sum;
+      s_seg_comp[g][i] = comp;
+    } else if (i == kIcpSums) {
+      unsigned c = 0;
+      for (unsigned b = g; b < gridDim.x; b += 8) c += __float_as_uint(__ldcg(partials + b * kIcpSlot + kIcpSums));
+      s_seg_sum[g][i] = __uint_as_float(c);
+    }
+  }
+  __syncthreads();
   if (threadIdx.x < kIcpSums) {
     float sum = 0.0f, comp = 0.0f;
-    for (unsigned b = 0; b < gridDim.x; ++b) {
-      const float y = __ldcg(partials + b * kIcpSlot + threadIdx.x) - comp;
+    for (int g = 0; g < 8; ++g) {
+      const float y = (s_seg_sum[g][threadIdx.x] - s_seg_comp[g][threadIdx.x]) - comp;
       const float t = sum + y;
       comp = (t - sum) - y;
       sum = t;
@@ -524,7 +604,7 @@ __global__ void __launch_bounds__(kIcpBlock)
     s_total[threadIdx.x] = sum;
   } else if (threadIdx.x == kIcpSums) {
     unsigned long long c = 0;
-    for (unsigned b = 0; b < gridDim.x; ++b) c += __float_as_uint(__ldcg(partials + b * kIcpSlot + kIcpSums));
+    for (int g = 0; g < 8; ++g) c += __float_as_uint(s_seg_sum[g][kIcpSums]);
     s_count = c;
   }
   __syncthreads();

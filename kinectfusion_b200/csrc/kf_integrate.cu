@@ -2,20 +2,28 @@
 // (IntegrationContext::observe/fuse + ClassicTsdf/AngleWeightedTsdf,
 // tsdf_integration.hpp:127-342; reference device sweep tsdf_integration.cu:61-107).
 //
-// Design:
-//  * A per-frame pixel table (one float4 per depth pixel: depth in metres or
-//    NaN, |K^-1 [u v 1]|, the rule's observation weight, RGBA8 colour) holds
-//    everything of observe() that depends on the pixel only.  It is the same
-//    float expression as the per-voxel host code, evaluated once per pixel.
-//  * One thread per (x, y) column of voxels streams z.  The world point's x/y
-//    part of each row of world_to_camera is constant along a column and is
-//    hoisted; the per-voxel remainder is the host expression verbatim.
-//  * Each column's z range is clipped to the camera frustum with a one-voxel
-//    and two-pixel margin (conservative: a skipped voxel provably projects
-//    outside the image or behind the camera); inside it every voxel runs the
-//    exact host test, so results are bit-identical to the host sweep.
-//  * Voxels are read and written with one 8-byte (float) or 4-byte
-//    (int16/bf16) access each, coalesced along x across the warp.
+// The reference sweeps every (x, y) column of the volume and tests every voxel
+// of a column that projects into the image.  Almost all of that work is in
+// voxels that cannot fuse: behind the measured surface or outside the image.
+// Here the full sweep runs in three steps, with the same result:
+//
+//  1. pixel table: one float4 per depth pixel - depth in metres (NaN when
+//     unusable), |K^-1 [u v 1]|, the rule's observation weight, RGBA8 colour.
+//     These are the per-pixel parts of observe(), the same float expressions
+//     evaluated once per pixel instead of once per voxel.
+//  2. block culling: a max-depth pyramid over 8x8 pixel tiles, then one
+//     thread per 8^3 block bounds the block's projection and camera depth.
+//     A block is dropped only when no voxel of it can fuse: it lies behind
+//     the camera, projects outside the image (1.5-pixel margin), or is
+//     farther than (max depth of its footprint + truncation) * (1 + 2/f)
+//     (a fused voxel has |p|/lambda <= depth + truncation, and |p|/lambda >=
+//     p.z * (1 - 0.71/f) since the pixel ray is rounded by half a pixel).
+//  3. listed-block integration: one CTA per surviving block, every voxel
+//     runs the exact host observe/fuse; the CTA also maintains the per-block
+//     bits of the raycast's empty-space skip (free space / observed).
+//
+// Voxel reads and writes are 8 B (float) or 4 B (int16/bf16) per voxel, a
+// warp covering four 64-byte block rows.
 #include <algorithm>
 #include <cmath>
 
@@ -25,13 +33,15 @@ namespace kf {
 namespace {
 
 struct IntegParams {
-  float observation_weight_unused;
   float max_weight;
   int projective_distance;
   int distance_scaled_truncation;
   float truncation_distance_scale;
   int has_color;
 };
+
+constexpr int kTile = 8;          // pixels per depth tile edge
+constexpr int kBlockThreads = 128;
 
 // Per-pixel part of IntegrationContext::observe and the rule weight
 // (tsdf_integration.hpp:196-212, 329-342).
@@ -63,50 +73,136 @@ __global__ void pixel_table_kernel(const uint16_t* __restrict__ depth, const uin
   table[pix] = make_float4(valid ? sd : kNaN, lambda, weight, __uint_as_float(c));
 }
 
-// Conservative z interval [lo, hi] (in voxel steps) of a column whose camera
-// point is affine in z: P(z) = a + b z.  Keeps every z where P.z > 0 and the
-// projection may land inside the image (two-pixel margin).
-__device__ __forceinline__ bool column_range(f3 a, f3 b, const Intr& k, float width, float height,
-                                             float zmax, float& lo, float& hi) {
-  lo = 0.0f;
-  hi = zmax;
-  // constraint alpha + beta z > 0
-  auto clip = [&](float alpha, float beta) {
-    if (fabsf(beta) < 1e-20f) {
-      if (!(alpha > -1e-6f)) {
-        lo = 1.0f;
-        hi = 0.0f;
-      }
-      return;
+// Level 0 of the depth-tile pyramid: the largest usable depth of each 8x8
+// pixel tile (0 when the tile has none).
+__global__ void tile_max_kernel(const float4* __restrict__ table, uint32_t width, uint32_t height,
+                                uint32_t tiles_x, uint32_t tiles_y, float* __restrict__ out) {
+  const uint32_t tx = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t ty = blockIdx.y * blockDim.y + threadIdx.y;
+  if (tx >= tiles_x || ty >= tiles_y) return;
+  float m = 0.0f;
+  for (uint32_t y = ty * kTile; y < min((ty + 1) * kTile, height); ++y) {
+    for (uint32_t x = tx * kTile; x < min((tx + 1) * kTile, width); ++x) {
+      const float d = __ldg(&table[static_cast<size_t>(y) * width + x].x);
+      if (d > m) m = d;  // NaN compares false
     }
-    const float root = -alpha / beta;
-    if (beta > 0.0f) {
-      lo = fmaxf(lo, root);
-    } else {
-      hi = fminf(hi, root);
-    }
-  };
-  // depth in front of the camera plane
-  clip(a.z, b.z);
-  const float m = 2.0f;
-  // fx x + (cx - (-0.5 - m)) z > 0   (left edge)
-  clip(k.fx * a.x + (k.cx + 0.5f + m) * a.z, k.fx * b.x + (k.cx + 0.5f + m) * b.z);
-  // (W - 0.5 + m - cx) z - fx x > 0  (right edge)
-  clip((width - 0.5f + m - k.cx) * a.z - k.fx * a.x, (width - 0.5f + m - k.cx) * b.z - k.fx * b.x);
-  clip(k.fy * a.y + (k.cy + 0.5f + m) * a.z, k.fy * b.y + (k.cy + 0.5f + m) * b.z);
-  clip((height - 0.5f + m - k.cy) * a.z - k.fy * a.y, (height - 0.5f + m - k.cy) * b.z - k.fy * b.y);
-  lo = floorf(lo) - 1.0f;
-  hi = ceilf(hi) + 1.0f;
-  lo = fmaxf(lo, 0.0f);
-  hi = fminf(hi, zmax);
-  return lo <= hi;
+  }
+  out[ty * tiles_x + tx] = m;
 }
 
+struct TileLevels {
+  uint32_t count;
+  uint32_t w[12], h[12], off[12];
+};
+
+// Coarser levels by 2x2 max, one CTA (the pyramid is a few thousand values).
+__global__ void tile_pyramid_kernel(float* __restrict__ tiles, TileLevels lv) {
+  for (uint32_t l = 1; l < lv.count; ++l) {
+    const float* src = tiles + lv.off[l - 1];
+    float* dst = tiles + lv.off[l];
+    const uint32_t n = lv.w[l] * lv.h[l];
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+      const uint32_t x = i % lv.w[l], y = i / lv.w[l];
+      float m = 0.0f;
+      for (uint32_t dy = 0; dy < 2; ++dy) {
+        for (uint32_t dx = 0; dx < 2; ++dx) {
+          const uint32_t sx = x * 2 + dx, sy = y * 2 + dy;
+          if (sx < lv.w[l - 1] && sy < lv.h[l - 1]) m = fmaxf(m, src[sy * lv.w[l - 1] + sx]);
+        }
+      }
+      dst[i] = m;
+    }
+    __syncthreads();
+  }
+}
+
+struct CullParams {
+  float trunc_base, trunc_scale;
+  int distance_scaled;
+  float slack;  // 1 / (1 - 2/f)
+  uint32_t width, height;
+};
+
+// Step 2: one thread per 8^3 block; survivors are appended to `list`.
+__global__ void cull_blocks_kernel(VolumeDev v, Rigid T, Intr k, const float* __restrict__ tiles, TileLevels lv,
+                                   CullParams cp, const IcpState* __restrict__ state, uint32_t* __restrict__ list,
+                                   unsigned* __restrict__ count) {
+  if (state != nullptr) {
+    if (state->failed) return;
+    const float* w = state->world_to_camera;
+    T = Rigid{{w[0], w[1], w[2]}, {w[3], w[4], w[5]}, {w[6], w[7], w[8]}, {w[9], w[10], w[11]}};
+  }
+  const uint32_t block = blockIdx.x * blockDim.x + threadIdx.x;
+  bool keep = false;
+  if (block < v.bx * v.by * v.bz) {
+    const uint32_t bxi = block % v.bx, byi = (block / v.bx) % v.by, bzi = block / (v.bx * v.by);
+    const float x0 = static_cast<float>(bxi * 8) + 0.5f, x1 = static_cast<float>(min(bxi * 8 + 8, v.rx) - 1) + 0.5f;
+    const float y0 = static_cast<float>(byi * 8) + 0.5f, y1 = static_cast<float>(min(byi * 8 + 8, v.ry) - 1) + 0.5f;
+    const float z0 = static_cast<float>(bzi * 8) + 0.5f, z1 = static_cast<float>(min(bzi * 8 + 8, v.rz) - 1) + 0.5f;
+    float zmin = 1e30f, zmax = -1e30f, umin = 1e30f, umax = -1e30f, vmin = 1e30f, vmax = -1e30f;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const f3 w = v.origin + make(c & 1 ? x1 : x0, c & 2 ? y1 : y0, c & 4 ? z1 : z0) * v.voxel_size;
+      const f3 p = apply(T, w);
+      zmin = fminf(zmin, p.z);
+      zmax = fmaxf(zmax, p.z);
+      if (p.z > 1e-4f) {
+        const float u = (k.fx * p.x) / p.z + k.cx, vv = (k.fy * p.y) / p.z + k.cy;
+        umin = fminf(umin, u);
+        umax = fmaxf(umax, u);
+        vmin = fminf(vmin, vv);
+        vmax = fmaxf(vmax, vv);
+      }
+    }
+    const float fw = static_cast<float>(cp.width), fh = static_cast<float>(cp.height);
+    if (zmax > 0.0f) {
+      if (zmin <= 1e-4f) {
+        keep = true;  // straddles the camera plane: the projection is unbounded
+      } else if (umax >= -2.0f && vmax >= -2.0f && umin <= fw + 1.0f && vmin <= fh + 1.0f) {
+        const int u0 = max(0, static_cast<int>(floorf(umin - 1.5f)));
+        const int u1 = min(static_cast<int>(cp.width) - 1, static_cast<int>(ceilf(umax + 1.5f)));
+        const int v0 = max(0, static_cast<int>(floorf(vmin - 1.5f)));
+        const int v1 = min(static_cast<int>(cp.height) - 1, static_cast<int>(ceilf(vmax + 1.5f)));
+        if (u0 <= u1 && v0 <= v1) {
+          // level whose tiles cover the rectangle with at most 2x2 texels
+          int tx0 = u0 / kTile, tx1 = u1 / kTile, ty0 = v0 / kTile, ty1 = v1 / kTile;
+          uint32_t l = 0;
+          while (l + 1 < lv.count && (tx1 - tx0 > 1 || ty1 - ty0 > 1)) {
+            tx0 >>= 1;
+            tx1 >>= 1;
+            ty0 >>= 1;
+            ty1 >>= 1;
+            ++l;
+          }
+          float maxd = 0.0f;
+          for (int ty = ty0; ty <= ty1; ++ty)
+            for (int tx = tx0; tx <= tx1; ++tx) maxd = fmaxf(maxd, __ldg(tiles + lv.off[l] + ty * lv.w[l] + tx));
+          if (maxd > 0.0f) {
+            const float trunc = cp.distance_scaled ? cp.trunc_base + cp.trunc_scale * maxd : cp.trunc_base;
+            keep = zmin <= (maxd + trunc) * cp.slack + 1e-3f;
+          }
+        }
+      }
+    }
+  }
+  // warp-aggregated append
+  const unsigned ballot = __ballot_sync(0xFFFFFFFFu, keep);
+  if (ballot == 0) return;
+  const int lane = threadIdx.x & 31;
+  unsigned base = 0;
+  if (lane == __ffs(ballot) - 1) base = atomicAdd(count, static_cast<unsigned>(__popc(ballot)));
+  base = __shfl_sync(0xFFFFFFFFu, base, __ffs(ballot) - 1);
+  if (keep) list[base + __popc(ballot & ((1u << lane) - 1u))] = block;
+}
+
+// Step 3: one CTA per listed block, four voxels (along z) per thread.
 template <int Kind, bool Color>
-__global__ void __launch_bounds__(256)
-    integrate_kernel(VolumeDev v, const float4* __restrict__ table, uint32_t width, uint32_t height,
-                     Intr k, Rigid T, IntegParams ip, const IcpState* __restrict__ state,
-                     unsigned long long* __restrict__ counters) {
+__global__ void __launch_bounds__(kBlockThreads)
+    integrate_blocks_kernel(VolumeDev v, const float4* __restrict__ table, uint32_t width, uint32_t height, Intr k,
+                            Rigid T, IntegParams ip, const IcpState* __restrict__ state,
+                            const uint32_t* __restrict__ list, const unsigned* __restrict__ count,
+                            uint32_t* __restrict__ free_bits, uint32_t* __restrict__ observed_bits,
+                            unsigned long long* __restrict__ counters) {
   using VT = VoxelTraits<Kind>;
   using Raw = typename VT::Raw;
   if (state != nullptr) {
@@ -114,82 +210,133 @@ __global__ void __launch_bounds__(256)
     const float* w = state->world_to_camera;
     T = Rigid{{w[0], w[1], w[2]}, {w[3], w[4], w[5]}, {w[6], w[7], w[8]}, {w[9], w[10], w[11]}};
   }
-  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= v.rx || y >= v.ry) return;
-
-  // World x/y of the column and the hoisted first two terms of each dot
-  // product: dot(row, p) = (row.x * p.x + row.y * p.y) + row.z * p.z.
-  const float wx = v.origin.x + ((static_cast<float>(x) + 0.5f) * v.voxel_size);
-  const float wy = v.origin.y + ((static_cast<float>(y) + 0.5f) * v.voxel_size);
-  const float hx = (T.rx.x * wx) + (T.rx.y * wy);
-  const float hy = (T.ry.x * wx) + (T.ry.y * wy);
-  const float hz = (T.rz.x * wx) + (T.rz.y * wy);
-
-  // Affine model of the camera point along z for the frustum clip.
-  const float w0 = v.origin.z + (0.5f * v.voxel_size);
-  const f3 a = make((hx + T.rx.z * w0) + T.t.x, (hy + T.ry.z * w0) + T.t.y, (hz + T.rz.z * w0) + T.t.z);
-  const f3 b = make(T.rx.z * v.voxel_size, T.ry.z * v.voxel_size, T.rz.z * v.voxel_size);
-  float lo, hi;
-  const bool visible = column_range(a, b, k, static_cast<float>(width), static_cast<float>(height),
-                                    static_cast<float>(v.rz - 1), lo, hi);
-  const uint32_t z_first = visible ? static_cast<uint32_t>(lo) : 1u;
-  const uint32_t z_last = visible ? static_cast<uint32_t>(hi) : 0u;
-  unsigned updates = 0, color_updates = 0;
-
   Raw* __restrict__ voxels = reinterpret_cast<Raw*>(v.voxels);
-  const size_t column = static_cast<size_t>(y) * v.rx + x;
   const size_t slice = static_cast<size_t>(v.rx) * v.ry;
-  const float trunc_base = v.truncation;
+  const unsigned n = *count;
+  const uint32_t lx = threadIdx.x & 7u, ly = (threadIdx.x >> 3) & 7u, lz = (threadIdx.x >> 6) * 4u;
+  unsigned updates = 0, color_updates = 0;
+  for (unsigned item = blockIdx.x; item < n; item += gridDim.x) {
+    const uint32_t block = list[item];
+    const uint32_t bxi = block % v.bx, byi = (block / v.bx) % v.by, bzi = block / (v.bx * v.by);
+    const uint32_t x = bxi * 8 + lx, y = byi * 8 + ly;
+    const bool full = bxi * 8 + 8 <= v.rx && byi * 8 + 8 <= v.ry && bzi * 8 + 8 <= v.rz;
+    bool all_one = true, any_other = false, any_fused = false;
+#pragma unroll
+    for (uint32_t i = 0; i < 4; ++i) {
+      const uint32_t z = bzi * 8 + lz + i;
+      bool fused_one = false;
+      if (x < v.rx && y < v.ry && z < v.rz) {
+        // IntegrationContext::observe (tsdf_integration.hpp:183-224)
+        const f3 cp = apply(T, cell_center(v, x, y, z));
+        if (cp.z > 0.0f) {
+          float px, py;
+          project(k, cp, px, py);
+          const long rx = lroundf(px), ry = lroundf(py);
+          if (rx >= 0 && ry >= 0 && rx < static_cast<long>(width) && ry < static_cast<long>(height)) {
+            const float4 tb = __ldg(table + (static_cast<size_t>(ry) * width + static_cast<size_t>(rx)));
+            const float sd = tb.x;
+            if (!isnan(sd)) {
+              const float truncation =
+                  ip.distance_scaled_truncation ? v.truncation + (ip.truncation_distance_scale * sd) : v.truncation;
+              const float sdf = ip.projective_distance ? sd - (norm(cp) / tb.y) : sd - cp.z;
+              const float ow = tb.z;
+              if (!(sdf < -truncation) && ow > 0.0f) {
+                const float tsdf = clampf(sdf / truncation, -1.0f, 1.0f);
+                // BasicVoxel::fused (volume.hpp:137-146)
+                const size_t index = static_cast<size_t>(z) * slice + static_cast<size_t>(y) * v.rx + x;
+                const Raw old = voxels[index];
+                const float t0 = VT::tsdf(old);
+                const float w0 = VT::weight(old);
+                const float avg = ((t0 * w0) + (tsdf * ow)) / (w0 + ow);
+                const float sum_w = w0 + ow;
+                const Raw fused = VT::encode(avg, ip.max_weight < sum_w ? ip.max_weight : sum_w);
+                voxels[index] = fused;
+                ++updates;
+                any_fused = true;
+                if (VT::tsdf(fused) == 1.0f) {
+                  fused_one = true;
+                } else {
+                  any_other = true;
+                }
+                if constexpr (Color) {
+                  if (ip.has_color && sdf <= truncation * 0.5f) {
+                    // ColorVoxel::fused (volume.hpp:160-170)
+                    ++color_updates;
+                    const float4 cv = v.colors[index];
+                    const f3 c = color_from_pixel(__float_as_uint(tb.w));
+                    const f3 avgc = ((make(cv.x, cv.y, cv.z) * cv.w) + (c * ow)) / (cv.w + ow);
+                    const float cw = cv.w + ow;
+                    v.colors[index] = make_float4(avgc.x, avgc.y, avgc.z, ip.max_weight < cw ? ip.max_weight : cw);
+                  }
+                }
+              }
+            }
+          }
+        }
+      }
+      all_one = all_one && fused_one;
+    }
+    // Skip bits: free when this frame fused every voxel to exactly 1; not free
+    // when it wrote anything else; unchanged otherwise.  Observed is sticky.
+    const bool block_one = __syncthreads_and(all_one) && full;
+    const bool block_other = __syncthreads_or(any_other);
+    const bool block_fused = __syncthreads_or(any_fused);
+    if (threadIdx.x == 0) {
+      const uint32_t bit = 1u << (block & 31u);
+      if (block_one) {
+        atomicOr(free_bits + (block >> 5), bit);
+      } else if (block_other) {
+        atomicAnd(free_bits + (block >> 5), ~bit);
+      }
+      if (block_fused) atomicOr(observed_bits + (block >> 5), bit);
+    }
+  }
+  const unsigned total = __reduce_add_sync(0xFFFFFFFFu, updates);
+  const unsigned total_color = __reduce_add_sync(0xFFFFFFFFu, color_updates);
+  if ((threadIdx.x & 31u) == 0 && counters != nullptr) {
+    if (total) atomicAdd(counters, static_cast<unsigned long long>(total));
+    if (total_color) atomicAdd(counters + 1, static_cast<unsigned long long>(total_color));
+  }
+}
 
-  for (uint32_t z = z_first; z <= z_last; ++z) {
-    const float wz = v.origin.z + ((static_cast<float>(z) + 0.5f) * v.voxel_size);
-    const f3 cp = make((hx + (T.rx.z * wz)) + T.t.x, (hy + (T.ry.z * wz)) + T.t.y,
-                       (hz + (T.rz.z * wz)) + T.t.z);
-    if (cp.z <= 0.0f) continue;
-    float px, py;
-    project(k, cp, px, py);
-    const long rx = lroundf(px);
-    const long ry = lroundf(py);
-    if (rx < 0 || ry < 0 || rx >= static_cast<long>(width) || ry >= static_cast<long>(height)) continue;
-    const float4 tb = __ldg(table + (static_cast<size_t>(ry) * width + static_cast<size_t>(rx)));
-    const float sd = tb.x;
-    if (isnan(sd)) continue;
-    const float truncation =
-        ip.distance_scaled_truncation ? trunc_base + (ip.truncation_distance_scale * sd) : trunc_base;
-    const float sdf = ip.projective_distance ? sd - (norm(cp) / tb.y) : sd - cp.z;
-    if (sdf < -truncation) continue;
-    const float tsdf = clampf(sdf / truncation, -1.0f, 1.0f);
-    const float ow = tb.z;
-    if (ow <= 0.0f) continue;
-    // BasicVoxel::fused (volume.hpp:137-146)
-    const size_t index = static_cast<size_t>(z) * slice + column;
-    const Raw old = voxels[index];
-    const float t0 = VT::tsdf(old);
-    const float w0v = VT::weight(old);
-    const float avg = ((t0 * w0v) + (tsdf * ow)) / (w0v + ow);
-    const float sum_w = w0v + ow;
-    voxels[index] = VT::encode(avg, ip.max_weight < sum_w ? ip.max_weight : sum_w);
-    ++updates;
-    if constexpr (Color) {
-      if (ip.has_color && sdf <= truncation * 0.5f) {
-        ++color_updates;
-        // ColorVoxel::fused (volume.hpp:160-170)
-        const float4 cv = v.colors[index];
-        const f3 c = color_from_pixel(__float_as_uint(tb.w));
-        const f3 avgc = ((make(cv.x, cv.y, cv.z) * cv.w) + (c * ow)) / (cv.w + ow);
-        const float cw = cv.w + ow;
-        v.colors[index] = make_float4(avgc.x, avgc.y, avgc.z, ip.max_weight < cw ? ip.max_weight : cw);
+// The march's skip bits from the per-block bits: free blocks whose 26
+// neighbours are free (and inside the volume); blocks whose 3x3x3
+// neighbourhood holds no observed voxel (outside neighbours hold none).
+__global__ void skip_bits_kernel(const uint32_t* __restrict__ free_bits, const uint32_t* __restrict__ observed_bits,
+                                 uint32_t* __restrict__ free_safe, uint32_t* __restrict__ empty_safe, uint32_t bx,
+                                 uint32_t by, uint32_t bz, const IcpState* __restrict__ state) {
+  if (state != nullptr && state->failed) return;
+  const uint32_t block = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t total = bx * by * bz;
+  bool fs = false, es = false;
+  if (block < total) {
+    const int x = static_cast<int>(block % bx), y = static_cast<int>((block / bx) % by),
+              z = static_cast<int>(block / (bx * by));
+    fs = true;
+    es = true;
+    for (int dz = -1; dz <= 1; ++dz) {
+      for (int dy = -1; dy <= 1; ++dy) {
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int nx = x + dx, ny = y + dy, nz = z + dz;
+          if (nx < 0 || ny < 0 || nz < 0 || nx >= static_cast<int>(bx) || ny >= static_cast<int>(by) ||
+              nz >= static_cast<int>(bz)) {
+            fs = false;
+            continue;
+          }
+          const uint32_t nb = (static_cast<uint32_t>(nz) * by + static_cast<uint32_t>(ny)) * bx + static_cast<uint32_t>(nx);
+          const uint32_t bit = 1u << (nb & 31u);
+          if (!(__ldg(free_bits + (nb >> 5)) & bit)) fs = false;
+          if (__ldg(observed_bits + (nb >> 5)) & bit) es = false;
+        }
       }
     }
   }
-  // One atomic per warp for the voxel-update counters.
-  const unsigned mask = __activemask();
-  const unsigned total = __reduce_add_sync(mask, updates);
-  const unsigned total_color = __reduce_add_sync(mask, color_updates);
-  if ((threadIdx.x & 31u) == static_cast<unsigned>(__ffs(mask) - 1) && counters != nullptr) {
-    if (total) atomicAdd(counters, static_cast<unsigned long long>(total));
-    if (total_color) atomicAdd(counters + 1, static_cast<unsigned long long>(total_color));
+  // 32 consecutive blocks share a word: assemble it in the warp, one store.
+  const unsigned fw = __ballot_sync(0xFFFFFFFFu, fs);
+  const unsigned ew = __ballot_sync(0xFFFFFFFFu, es);
+  if ((threadIdx.x & 31u) == 0 && block < total) {
+    free_safe[block >> 5] = fw;
+    empty_safe[block >> 5] = ew;
   }
 }
 
@@ -217,27 +364,68 @@ __global__ void count_observed_kernel(const void* voxels, size_t count, unsigned
   if ((threadIdx.x & 31) == 0 && local) atomicAdd(result, local);
 }
 
+TileLevels tile_levels_of(const Pipeline& p) {
+  TileLevels lv;
+  lv.count = p.tile_levels;
+  for (uint32_t l = 0; l < 12; ++l) {
+    lv.w[l] = p.tile_w[l];
+    lv.h[l] = p.tile_h[l];
+    lv.off[l] = p.tile_off[l];
+  }
+  return lv;
+}
+
 template <int Kind, bool Color>
-void launch_integrate_typed(Pipeline& p, const float4* table, uint32_t width, uint32_t height, Intr k,
-                            Rigid T, int has_color, const IcpState* state, cudaStream_t s) {
-  const kf_integration_options& o = p.config.integration;
-  IntegParams ip;
-  ip.observation_weight_unused = o.observation_weight;
-  ip.max_weight = o.max_weight;
-  ip.projective_distance = o.projective_distance;
-  ip.distance_scaled_truncation = o.distance_scaled_truncation;
-  ip.truncation_distance_scale = o.truncation_distance_scale;
-  ip.has_color = has_color;
-  const dim3 block(32, 8);
-  const dim3 grid(ceil_div(p.view.rx, 32), ceil_div(p.view.ry, 8));
+void launch_blocks_typed(Pipeline& p, const float4* table, uint32_t width, uint32_t height, Intr k, Rigid T,
+                         const IntegParams& ip, const IcpState* state, cudaStream_t s) {
   if (state == nullptr && p.kernel_start != nullptr) check(cudaEventRecord(p.kernel_start, s), "event record");
-  integrate_kernel<Kind, Color><<<grid, block, 0, s>>>(p.view, table, width, height, k, T, ip, state,
-                                                       p.counters.ptr);
-  check(cudaGetLastError(), "integrate_kernel launch");
+  integrate_blocks_kernel<Kind, Color><<<148 * 12, kBlockThreads, 0, s>>>(
+      p.view, table, width, height, k, T, ip, state, p.block_list.ptr, p.block_count.ptr, p.free_blocks.ptr,
+      p.observed_blocks.ptr, p.counters.ptr);
+  check(cudaGetLastError(), "integrate_blocks_kernel launch");
   if (state == nullptr && p.kernel_stop != nullptr) check(cudaEventRecord(p.kernel_stop, s), "event record");
 }
 
 }  // namespace
+
+void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t s) {
+  const uint32_t blocks = p.view.bx * p.view.by * p.view.bz;
+  const size_t words = (blocks + 31) / 32;
+  if (p.free_blocks.count != words) {
+    p.free_blocks.resize(words);
+    p.observed_blocks.resize(words);
+    p.safe_blocks.resize(words);
+    p.empty_safe.resize(words);
+    p.block_list.resize(blocks);
+    p.block_count.resize(1);
+    reset_blocks(p, s);
+  }
+  // depth-tile pyramid geometry for this frame size
+  uint32_t w = ceil_div(width, kTile), h = ceil_div(height, kTile), off = 0, l = 0;
+  if (p.tile_levels == 0 || p.tile_w[0] != w || p.tile_h[0] != h) {
+    while (true) {
+      p.tile_w[l] = w;
+      p.tile_h[l] = h;
+      p.tile_off[l] = off;
+      off += w * h;
+      ++l;
+      if ((w == 1 && h == 1) || l == 12) break;
+      w = (w + 1) / 2;
+      h = (h + 1) / 2;
+    }
+    p.tile_levels = l;
+    p.depth_tiles.resize(off);
+  }
+}
+
+void reset_blocks(Pipeline& p, cudaStream_t s) {
+  if (p.free_blocks.count == 0) return;
+  check(cudaMemsetAsync(p.free_blocks.ptr, 0, p.free_blocks.bytes(), s), "skip bits reset");
+  check(cudaMemsetAsync(p.observed_blocks.ptr, 0, p.observed_blocks.bytes(), s), "skip bits reset");
+  check(cudaMemsetAsync(p.safe_blocks.ptr, 0, p.safe_blocks.bytes(), s), "skip bits reset");
+  // nothing observed: every block is empty-safe
+  check(cudaMemsetAsync(p.empty_safe.ptr, 0xFF, p.empty_safe.bytes(), s), "skip bits reset");
+}
 
 void launch_pixel_table(const uint16_t* depth, const uint32_t* color, const float* normals, uint32_t width,
                         uint32_t height, Intr k, const kf_integration_options& o, int rule, float4* table,
@@ -252,21 +440,54 @@ void launch_pixel_table(const uint16_t* depth, const uint32_t* color, const floa
 
 void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t height, Intr k, Rigid T,
                       int has_color, const IcpState* state, cudaStream_t s) {
+  prepare_blocks(p, width, height, s);
+  const kf_integration_options& o = p.config.integration;
+  // depth-tile pyramid
+  const TileLevels lv = tile_levels_of(p);
+  tile_max_kernel<<<dim3(ceil_div(lv.w[0], 16), ceil_div(lv.h[0], 16)), dim3(16, 16), 0, s>>>(
+      table, width, height, lv.w[0], lv.h[0], p.depth_tiles.ptr);
+  check(cudaGetLastError(), "tile_max_kernel launch");
+  tile_pyramid_kernel<<<1, 1024, 0, s>>>(p.depth_tiles.ptr, lv);
+  check(cudaGetLastError(), "tile_pyramid_kernel launch");
+  // block culling
+  CullParams cp;
+  cp.trunc_base = p.view.truncation;
+  cp.trunc_scale = o.truncation_distance_scale;
+  cp.distance_scaled = o.distance_scaled_truncation;
+  cp.slack = 1.0f / (1.0f - 2.0f / fminf(k.fx, k.fy));
+  cp.width = width;
+  cp.height = height;
+  check(cudaMemsetAsync(p.block_count.ptr, 0, sizeof(unsigned), s), "block count clear");
+  const uint32_t blocks = p.view.bx * p.view.by * p.view.bz;
+  cull_blocks_kernel<<<ceil_div(blocks, 256), 256, 0, s>>>(p.view, T, k, p.depth_tiles.ptr, lv, cp, state,
+                                                           p.block_list.ptr, p.block_count.ptr);
+  check(cudaGetLastError(), "cull_blocks_kernel launch");
+  // listed blocks
+  IntegParams ip;
+  ip.max_weight = o.max_weight;
+  ip.projective_distance = o.projective_distance;
+  ip.distance_scaled_truncation = o.distance_scaled_truncation;
+  ip.truncation_distance_scale = o.truncation_distance_scale;
+  ip.has_color = has_color;
   const bool color = p.config.color == KF_COLOR_FLOAT;
   switch (p.config.voxel) {
     case KF_VOXEL_QUANTIZED:
-      color ? launch_integrate_typed<KF_VOXEL_QUANTIZED, true>(p, table, width, height, k, T, has_color, state, s)
-            : launch_integrate_typed<KF_VOXEL_QUANTIZED, false>(p, table, width, height, k, T, has_color, state, s);
+      color ? launch_blocks_typed<KF_VOXEL_QUANTIZED, true>(p, table, width, height, k, T, ip, state, s)
+            : launch_blocks_typed<KF_VOXEL_QUANTIZED, false>(p, table, width, height, k, T, ip, state, s);
       break;
     case KF_VOXEL_BF16:
-      color ? launch_integrate_typed<KF_VOXEL_BF16, true>(p, table, width, height, k, T, has_color, state, s)
-            : launch_integrate_typed<KF_VOXEL_BF16, false>(p, table, width, height, k, T, has_color, state, s);
+      color ? launch_blocks_typed<KF_VOXEL_BF16, true>(p, table, width, height, k, T, ip, state, s)
+            : launch_blocks_typed<KF_VOXEL_BF16, false>(p, table, width, height, k, T, ip, state, s);
       break;
     default:
-      color ? launch_integrate_typed<KF_VOXEL_FLOAT, true>(p, table, width, height, k, T, has_color, state, s)
-            : launch_integrate_typed<KF_VOXEL_FLOAT, false>(p, table, width, height, k, T, has_color, state, s);
+      color ? launch_blocks_typed<KF_VOXEL_FLOAT, true>(p, table, width, height, k, T, ip, state, s)
+            : launch_blocks_typed<KF_VOXEL_FLOAT, false>(p, table, width, height, k, T, ip, state, s);
       break;
   }
+  // raycast skip bits
+  skip_bits_kernel<<<ceil_div(blocks, 256), 256, 0, s>>>(p.free_blocks.ptr, p.observed_blocks.ptr, p.safe_blocks.ptr,
+                                                         p.empty_safe.ptr, p.view.bx, p.view.by, p.view.bz, state);
+  check(cudaGetLastError(), "skip_bits_kernel launch");
 }
 
 void launch_fill_volume(Pipeline& p, cudaStream_t s) {
@@ -284,6 +505,7 @@ void launch_fill_volume(Pipeline& p, cudaStream_t s) {
       break;
   }
   check(cudaGetLastError(), "fill_kernel launch");
+  reset_blocks(p, s);
 }
 
 uint64_t count_observed(Pipeline& p) {

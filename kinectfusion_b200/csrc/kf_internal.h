@@ -238,9 +238,16 @@ struct Pipeline {
   DeviceArray<float4> colors;
   size_t voxel_bytes = 0;
   uint64_t voxel_count = 0;
-  // empty-space skip: one bit per 8^3 block that is uniformly free space
-  DeviceArray<uint32_t> free_blocks;   // raw per-block bits
-  DeviceArray<uint32_t> safe_blocks;   // 3x3x3-eroded bits used by the march
+  // Exact empty-space skip, one bit per 8^3 block (x-major block order):
+  DeviceArray<uint32_t> free_blocks;     // every voxel observed with tsdf exactly 1
+  DeviceArray<uint32_t> observed_blocks; // some voxel observed
+  DeviceArray<uint32_t> safe_blocks;     // free, with all 26 neighbours free
+  DeviceArray<uint32_t> empty_safe;      // no observed voxel in the 3x3x3 neighbourhood
+  // Block culling of the full sweep
+  DeviceArray<float> depth_tiles;        // max depth per 8x8 pixel tile, then coarser levels
+  DeviceArray<uint32_t> block_list;
+  DeviceArray<unsigned> block_count;
+  uint32_t tile_levels = 0, tile_w[12] = {}, tile_h[12] = {}, tile_off[12] = {};
   // integration pixel table (float4 per pixel: depth, lambda, weight, color)
   DeviceArray<float4> pixel_table;
   DeviceArray<uint16_t> own_depth;     // upload target when no pyramid supplies one
@@ -291,7 +298,10 @@ void launch_pixel_table(const uint16_t* depth, const uint32_t* color, const floa
 void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t height,
                       Intr intrinsics, Rigid world_to_camera, int has_color,
                       const IcpState* pose_state, cudaStream_t stream);
-void launch_rebuild_skip(Pipeline& p, cudaStream_t stream);
+// Allocates and clears the per-block skip and culling buffers.
+void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t stream);
+// Clears the skip bits (a freshly filled volume: nothing observed).
+void reset_blocks(Pipeline& p, cudaStream_t stream);
 // Raycast into device maps.  `pose_state` (optional) supplies the
 // camera_to_world from the tracker and skips the render after a failure.
 void launch_raycast(const Pipeline& p, const kf_raycast_camera& camera, float* points,

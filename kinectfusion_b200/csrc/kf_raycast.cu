@@ -7,12 +7,15 @@
 // expression order, so a render is bit-identical to the CPU raycast of the
 // same volume and camera.
 //
-// Empty-space skip: `safe` holds one bit per 8^3 block whose 3x3x3 block
-// neighbourhood is observed free space (every voxel observed with tsdf
-// exactly 1).  Inside such a block every trilinear sample is exactly 1.0
-// (the blend divides a sum by the identical sum), so the march replays its
-// ray_length additions without sampling; the sequence of sample positions,
-// and therefore the output, is unchanged.
+// Empty-space skip, exact: one bit per 8^3 block marks blocks whose 3x3x3
+// block neighbourhood is (a) observed free space - every voxel observed with
+// tsdf exactly 1, so every trilinear sample there is exactly 1.0 (the blend
+// divides a sum by the identical sum) - or (b) wholly unobserved, so every
+// sample there is nullopt.  The march replays its ray_length additions
+// through such blocks without gathering corners; the sample positions, and
+// therefore the output, are those of the plain march.  Samples before the
+// volume box are replayed the same way, and the march ends once the ray has
+// left the box.
 #include <cmath>
 
 #include "kf_internal.h"
@@ -177,22 +180,74 @@ struct Sampler {
   }
 };
 
-// True when the sample point lies in a block whose 3x3x3 neighbourhood is
-// uniformly observed free space.
-__device__ __forceinline__ bool in_safe_block(const uint32_t* __restrict__ safe, const VolumeDev& v, f3 point) {
+// Block class of a sample point: 1 = its 3x3x3 block neighbourhood is
+// observed free space (every voxel tsdf exactly 1), 2 = the neighbourhood
+// holds no observed voxel, 0 = anything else or outside the grid.
+__device__ __forceinline__ int skip_class(const uint32_t* __restrict__ free_safe,
+                                          const uint32_t* __restrict__ empty_safe, const VolumeDev& v, f3 point,
+                                          uint32_t& bxi, uint32_t& byi, uint32_t& bzi) {
   const f3 g = (point - v.origin) * v.inv_voxel_size;
   if (!(g.x >= 0.0f && g.y >= 0.0f && g.z >= 0.0f && g.x < static_cast<float>(v.rx) &&
         g.y < static_cast<float>(v.ry) && g.z < static_cast<float>(v.rz))) {
-    return false;
+    return 0;
   }
-  const uint32_t block = ((static_cast<uint32_t>(g.z) >> 3) * v.by + (static_cast<uint32_t>(g.y) >> 3)) * v.bx +
-                         (static_cast<uint32_t>(g.x) >> 3);
-  return (__ldg(safe + (block >> 5)) >> (block & 31u)) & 1u;
+  bxi = static_cast<uint32_t>(g.x) >> 3;
+  byi = static_cast<uint32_t>(g.y) >> 3;
+  bzi = static_cast<uint32_t>(g.z) >> 3;
+  const uint32_t block = (bzi * v.by + byi) * v.bx + bxi;
+  const uint32_t bit = 1u << (block & 31u);
+  if (__ldg(free_safe + (block >> 5)) & bit) return 1;
+  if (__ldg(empty_safe + (block >> 5)) & bit) return 2;
+  return 0;
+}
+
+// Ray parameter where the ray leaves block (bxi, byi, bzi).  Approximate:
+// samples within rounding distance of the face still lie in the block's
+// one-block safety neighbourhood.
+__device__ __forceinline__ float block_exit(const VolumeDev& v, f3 o, f3 inv_dir, uint32_t bxi, uint32_t byi,
+                                            uint32_t bzi) {
+  const float edge = 8.0f * v.voxel_size;
+  const f3 lo = v.origin + make(static_cast<float>(bxi), static_cast<float>(byi), static_cast<float>(bzi)) * edge;
+  const float tx = ((inv_dir.x >= 0.0f ? lo.x + edge : lo.x) - o.x) * inv_dir.x;
+  const float ty = ((inv_dir.y >= 0.0f ? lo.y + edge : lo.y) - o.y) * inv_dir.y;
+  const float tz = ((inv_dir.z >= 0.0f ? lo.z + edge : lo.z) - o.z) * inv_dir.z;
+  return fminf(tx, fminf(ty, tz));
+}
+
+// Ray parameters where the ray enters and leaves the volume box, widened by
+// two voxels (FP64: the samples' own rounding stays far inside the margin).
+__device__ __forceinline__ void box_range(const VolumeDev& v, f3 o, f3 d, float& t_in, float& t_out) {
+  double lo = -1e300, hi = 1e300;
+  const double org[3] = {o.x, o.y, o.z}, dir[3] = {d.x, d.y, d.z};
+  const double bmin[3] = {v.origin.x, v.origin.y, v.origin.z};
+  const double ext[3] = {static_cast<double>(v.rx) * v.voxel_size, static_cast<double>(v.ry) * v.voxel_size,
+                         static_cast<double>(v.rz) * v.voxel_size};
+  for (int a = 0; a < 3; ++a) {
+    if (dir[a] == 0.0) {
+      if (org[a] < bmin[a] || org[a] > bmin[a] + ext[a]) {
+        lo = 1e300;
+        hi = -1e300;
+      }
+      continue;
+    }
+    const double t0 = (bmin[a] - org[a]) / dir[a];
+    const double t1 = (bmin[a] + ext[a] - org[a]) / dir[a];
+    lo = fmax(lo, fmin(t0, t1));
+    hi = fmin(hi, fmax(t0, t1));
+  }
+  const double margin = 2.0 * v.voxel_size;
+  t_in = static_cast<float>(lo - margin);
+  t_out = static_cast<float>(hi + margin);
+  if (!(lo <= hi)) {
+    t_in = 1e30f;
+    t_out = -1e30f;
+  }
 }
 
 template <int Kind, bool Color>
 __global__ void __launch_bounds__(256)
-    raycast_kernel(VolumeDev v, const uint32_t* __restrict__ safe, RaycastParams rp, Intr k, uint32_t width,
+    raycast_kernel(VolumeDev v, const uint32_t* __restrict__ free_safe, const uint32_t* __restrict__ empty_safe,
+                   RaycastParams rp, Intr k, uint32_t width,
                    uint32_t height, Rigid pose, const IcpState* __restrict__ state, float* __restrict__ points,
                    float* __restrict__ normals, uint32_t* __restrict__ colors) {
   if (state != nullptr) {
@@ -234,17 +289,43 @@ __global__ void __launch_bounds__(256)
     float ray_length = seed;
     bool found = false;
     f3 surface = make(0.0f, 0.0f, 0.0f);
+    // Samples outside the volume box are nullopt: replay the base steps up
+    // to the box, and stop once the ray has left it (a box is convex).
+    float t_in, t_out;
+    box_range(v, pose.t, dir, t_in, t_out);
+    const f3 inv_dir = make(dir.x != 0.0f ? 1.0f / dir.x : 1e30f, dir.y != 0.0f ? 1.0f / dir.y : 1e30f,
+                            dir.z != 0.0f ? 1.0f / dir.z : 1e30f);
+    while (ray_length < t_in && ray_length <= rp.max_depth) ray_length += base_step;
     while (ray_length <= rp.max_depth) {
+      if (ray_length > t_out) break;
       const f3 point = pose.t + (dir * ray_length);
-      if (safe != nullptr && in_safe_block(safe, v, point)) {
-        // The sample would be exactly 1.0: leaving a surface from behind
-        // ends the march; otherwise it is a positive sample.
-        if (have_prev && prev_tsdf < 0.0f) break;
-        have_prev = true;
-        prev_tsdf = 1.0f;
-        prev_point = point;
-        ray_length += free_step;
-        continue;
+      if (free_safe != nullptr) {
+        uint32_t bxi, byi, bzi;
+        const int cls = skip_class(free_safe, empty_safe, v, point, bxi, byi, bzi);
+        if (cls != 0) {
+          // Replay the plain march's additions up to the block exit.
+          const float t_exit = block_exit(v, pose.t, inv_dir, bxi, byi, bzi);
+          if (cls == 1) {
+            // Samples are exactly 1.0: leaving a surface from behind ends
+            // the march at the first one; after it every step is free_step.
+            if (have_prev && prev_tsdf < 0.0f) break;
+            float last = ray_length;
+            do {
+              last = ray_length;
+              ray_length += free_step;
+            } while (ray_length < t_exit && ray_length <= rp.max_depth);
+            have_prev = true;
+            prev_tsdf = 1.0f;
+            prev_point = pose.t + (dir * last);
+          } else {
+            // No observed corner anywhere near: every sample is nullopt.
+            have_prev = false;
+            do {
+              ray_length += base_step;
+            } while (ray_length < t_exit && ray_length <= rp.max_depth);
+          }
+          continue;
+        }
       }
       float tsdf;
       if (!s.tsdf(point, rp.policy, tsdf)) {
@@ -301,10 +382,11 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
   rp.policy = p.config.raycast.corner_policy;
   rp.cell_normals = p.config.raycast.cell_gradient_normals;
   rp.seed_previous = p.config.raycast.seed_from_previous;
-  const uint32_t* safe = p.safe_blocks.count ? p.safe_blocks.ptr : nullptr;
+  const uint32_t* free_safe = p.safe_blocks.count ? p.safe_blocks.ptr : nullptr;
+  const uint32_t* empty_safe = p.safe_blocks.count ? p.empty_safe.ptr : nullptr;
   const dim3 block(16, 16);
   const dim3 grid(ceil_div(cam.width, 16), ceil_div(cam.height, 16));
-  raycast_kernel<Kind, Color><<<grid, block, 0, s>>>(p.view, safe, rp, intr_from(cam.intrinsics), cam.width,
+  raycast_kernel<Kind, Color><<<grid, block, 0, s>>>(p.view, free_safe, empty_safe, rp, intr_from(cam.intrinsics), cam.width,
                                                      cam.height, rigid_from(cam.camera_to_world), state, points,
                                                      normals, colors);
   check(cudaGetLastError(), "raycast_kernel launch");
