@@ -574,12 +574,19 @@ __global__ void __launch_bounds__(kIcpBlock, 2)
   // the eight segment results of each sum are combined in segment order.
   __shared__ float s_seg_sum[8][kIcpSlot];
   __shared__ float s_seg_comp[8][kIcpSlot];
+  __shared__ float s_parts[kIcpMaxGrid * kIcpSlot];
+  {
+    // stage every partial in shared memory with independent coalesced loads
+    const unsigned n = gridDim.x * kIcpSlot;
+    for (unsigned e = threadIdx.x; e < n; e += kIcpBlock) s_parts[e] = __ldcg(partials + e);
+  }
+  __syncthreads();
   {
     const unsigned i = threadIdx.x % kIcpSlot, g = threadIdx.x / kIcpSlot;  // 8 x 32 threads
     if (i < kIcpSums) {
       float sum = 0.0f, comp = 0.0f;
       for (unsigned b = g; b < gridDim.x; b += 8) {
-        const float y = __ldcg(partials + b * kIcpSlot + i) - comp;
+        const float y = s_parts[b * kIcpSlot + i] - comp;
         const float t = sum + y;
         comp = (t - sum) - y;
         sum = t;
@@ -588,7 +595,7 @@ __global__ void __launch_bounds__(kIcpBlock, 2)
       s_seg_comp[g][i] = comp;
     } else if (i == kIcpSums) {
       unsigned c = 0;
-      for (unsigned b = g; b < gridDim.x; b += 8) c += __float_as_uint(__ldcg(partials + b * kIcpSlot + kIcpSums));
+      for (unsigned b = g; b < gridDim.x; b += 8) c += __float_as_uint(s_parts[b * kIcpSlot + kIcpSums]);
       s_seg_sum[g][i] = __uint_as_float(c);
     }
   }

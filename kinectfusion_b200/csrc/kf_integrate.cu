@@ -202,7 +202,9 @@ __global__ void __launch_bounds__(kBlockThreads)
                             Rigid T, IntegParams ip, const IcpState* __restrict__ state,
                             const uint32_t* __restrict__ list, const unsigned* __restrict__ count,
                             uint32_t* __restrict__ free_bits, uint32_t* __restrict__ observed_bits,
+                            uint32_t* __restrict__ observed_cells, uint32_t cells_x, uint32_t cells_y,
                             unsigned long long* __restrict__ counters) {
+  __shared__ uint32_t s_cells[16];  // this block's 4x4x4 cells: [z][y] rows of 4 x-bits
   using VT = VoxelTraits<Kind>;
   using Raw = typename VT::Raw;
   if (state != nullptr) {
@@ -221,6 +223,9 @@ __global__ void __launch_bounds__(kBlockThreads)
     const uint32_t x = bxi * 8 + lx, y = byi * 8 + ly;
     const bool full = bxi * 8 + 8 <= v.rx && byi * 8 + 8 <= v.ry && bzi * 8 + 8 <= v.rz;
     bool all_one = true, any_other = false, any_fused = false;
+    if (threadIdx.x < 16) s_cells[threadIdx.x] = 0u;
+    __syncthreads();
+    uint32_t fused_z = 0;  // bit i: voxel z = lz + i fused
 #pragma unroll
     for (uint32_t i = 0; i < 4; ++i) {
       const uint32_t z = bzi * 8 + lz + i;
@@ -253,6 +258,7 @@ __global__ void __launch_bounds__(kBlockThreads)
                 voxels[index] = fused;
                 ++updates;
                 any_fused = true;
+                fused_z |= 1u << i;
                 if (VT::tsdf(fused) == 1.0f) {
                   fused_one = true;
                 } else {
@@ -276,6 +282,9 @@ __global__ void __launch_bounds__(kBlockThreads)
       }
       all_one = all_one && fused_one;
     }
+    // Observed 2x2x2 cells of this block (sticky bits, merged in shared memory).
+    if (fused_z & 3u) atomicOr(&s_cells[((lz >> 1) + 0) * 4 + (ly >> 1)], 1u << (lx >> 1));
+    if (fused_z & 12u) atomicOr(&s_cells[((lz >> 1) + 1) * 4 + (ly >> 1)], 1u << (lx >> 1));
     // Skip bits: free when this frame fused every voxel to exactly 1; not free
     // when it wrote anything else; unchanged otherwise.  Observed is sticky.
     const bool block_one = __syncthreads_and(all_one) && full;
@@ -290,6 +299,12 @@ __global__ void __launch_bounds__(kBlockThreads)
       }
       if (block_fused) atomicOr(observed_bits + (block >> 5), bit);
     }
+    if (threadIdx.x < 16 && s_cells[threadIdx.x] != 0u) {
+      const uint32_t cz = bzi * 4 + (threadIdx.x >> 2), cy = byi * 4 + (threadIdx.x & 3u), cx = bxi * 4;
+      const size_t cell = (static_cast<size_t>(cz) * cells_y + cy) * cells_x + cx;
+      atomicOr(observed_cells + (cell >> 5), s_cells[threadIdx.x] << (cell & 31u));
+    }
+    __syncthreads();
   }
   const unsigned total = __reduce_add_sync(0xFFFFFFFFu, updates);
   const unsigned total_color = __reduce_add_sync(0xFFFFFFFFu, color_updates);
@@ -381,7 +396,7 @@ void launch_blocks_typed(Pipeline& p, const float4* table, uint32_t width, uint3
   if (state == nullptr && p.kernel_start != nullptr) check(cudaEventRecord(p.kernel_start, s), "event record");
   integrate_blocks_kernel<Kind, Color><<<148 * 12, kBlockThreads, 0, s>>>(
       p.view, table, width, height, k, T, ip, state, p.block_list.ptr, p.block_count.ptr, p.free_blocks.ptr,
-      p.observed_blocks.ptr, p.counters.ptr);
+      p.observed_blocks.ptr, p.observed_cells.ptr, p.cx, p.cy, p.counters.ptr);
   check(cudaGetLastError(), "integrate_blocks_kernel launch");
   if (state == nullptr && p.kernel_stop != nullptr) check(cudaEventRecord(p.kernel_stop, s), "event record");
 }
@@ -398,6 +413,11 @@ void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t s
     p.empty_safe.resize(words);
     p.block_list.resize(blocks);
     p.block_count.resize(1);
+    // cells padded to whole blocks (4 per block edge), rows of 32-bit words
+    p.cx = p.view.bx * 4;
+    p.cy = p.view.by * 4;
+    p.cz = p.view.bz * 4;
+    p.observed_cells.resize((static_cast<size_t>(p.cx) * p.cy * p.cz + 31) / 32);
     reset_blocks(p, s);
   }
   // depth-tile pyramid geometry for this frame size
@@ -423,6 +443,7 @@ void reset_blocks(Pipeline& p, cudaStream_t s) {
   check(cudaMemsetAsync(p.free_blocks.ptr, 0, p.free_blocks.bytes(), s), "skip bits reset");
   check(cudaMemsetAsync(p.observed_blocks.ptr, 0, p.observed_blocks.bytes(), s), "skip bits reset");
   check(cudaMemsetAsync(p.safe_blocks.ptr, 0, p.safe_blocks.bytes(), s), "skip bits reset");
+  check(cudaMemsetAsync(p.observed_cells.ptr, 0, p.observed_cells.bytes(), s), "skip bits reset");
   // nothing observed: every block is empty-safe
   check(cudaMemsetAsync(p.empty_safe.ptr, 0xFF, p.empty_safe.bytes(), s), "skip bits reset");
 }

@@ -201,6 +201,32 @@ __device__ __forceinline__ int skip_class(const uint32_t* __restrict__ free_safe
   return 0;
 }
 
+// True when no corner of the trilinear stencil at `point` is observed (the
+// sample is nullopt), decided from the 2x2x2-cell observed bits alone.
+__device__ __forceinline__ bool cells_unobserved(const uint32_t* __restrict__ cells, const VolumeDev& v, uint32_t cx,
+                                                 uint32_t cy, f3 point) {
+  const f3 g = (point - v.origin) * v.inv_voxel_size;
+  if (!(g.x >= 0.0f && g.y >= 0.0f && g.z >= 0.0f && g.x < static_cast<float>(v.rx) &&
+        g.y < static_cast<float>(v.ry) && g.z < static_cast<float>(v.rz))) {
+    return false;  // outside the grid: the sampler itself rejects it cheaply
+  }
+  const int bx = static_cast<int>(floorf(g.x - 0.5f)), by = static_cast<int>(floorf(g.y - 0.5f)),
+            bz = static_cast<int>(floorf(g.z - 0.5f));
+  const int x0 = max(bx, 0) >> 1, x1 = min(bx + 1, static_cast<int>(v.rx) - 1) >> 1;
+  const int y0 = max(by, 0) >> 1, y1 = min(by + 1, static_cast<int>(v.ry) - 1) >> 1;
+  const int z0 = max(bz, 0) >> 1, z1 = min(bz + 1, static_cast<int>(v.rz) - 1) >> 1;
+  for (int z = z0; z <= z1; ++z) {
+    for (int y = y0; y <= y1; ++y) {
+      const size_t row = (static_cast<size_t>(z) * cy + static_cast<size_t>(y)) * cx;
+      for (int x = x0; x <= x1; ++x) {
+        const size_t c = row + static_cast<size_t>(x);
+        if ((__ldg(cells + (c >> 5)) >> (c & 31u)) & 1u) return false;
+      }
+    }
+  }
+  return true;
+}
+
 // Ray parameter where the ray leaves block (bxi, byi, bzi).  Approximate:
 // samples within rounding distance of the face still lie in the block's
 // one-block safety neighbourhood.
@@ -247,6 +273,7 @@ __device__ __forceinline__ void box_range(const VolumeDev& v, f3 o, f3 d, float&
 template <int Kind, bool Color>
 __global__ void __launch_bounds__(256)
     raycast_kernel(VolumeDev v, const uint32_t* __restrict__ free_safe, const uint32_t* __restrict__ empty_safe,
+                   const uint32_t* __restrict__ cells, uint32_t cells_x, uint32_t cells_y,
                    RaycastParams rp, Intr k, uint32_t width,
                    uint32_t height, Rigid pose, const IcpState* __restrict__ state, float* __restrict__ points,
                    float* __restrict__ normals, uint32_t* __restrict__ colors) {
@@ -327,6 +354,11 @@ __global__ void __launch_bounds__(256)
           continue;
         }
       }
+      if (cells != nullptr && cells_unobserved(cells, v, cells_x, cells_y, point)) {
+        have_prev = false;
+        ray_length += base_step;
+        continue;
+      }
       float tsdf;
       if (!s.tsdf(point, rp.policy, tsdf)) {
         have_prev = false;
@@ -386,7 +418,8 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
   const uint32_t* empty_safe = p.safe_blocks.count ? p.empty_safe.ptr : nullptr;
   const dim3 block(16, 16);
   const dim3 grid(ceil_div(cam.width, 16), ceil_div(cam.height, 16));
-  raycast_kernel<Kind, Color><<<grid, block, 0, s>>>(p.view, free_safe, empty_safe, rp, intr_from(cam.intrinsics), cam.width,
+  const uint32_t* cells = p.safe_blocks.count ? p.observed_cells.ptr : nullptr;
+  raycast_kernel<Kind, Color><<<grid, block, 0, s>>>(p.view, free_safe, empty_safe, cells, p.cx, p.cy, rp, intr_from(cam.intrinsics), cam.width,
                                                      cam.height, rigid_from(cam.camera_to_world), state, points,
                                                      normals, colors);
   check(cudaGetLastError(), "raycast_kernel launch");
