@@ -202,9 +202,11 @@ __global__ void __launch_bounds__(kBlockThreads)
                             Rigid T, IntegParams ip, const IcpState* __restrict__ state,
                             const uint32_t* __restrict__ list, const unsigned* __restrict__ count,
                             uint32_t* __restrict__ free_bits, uint32_t* __restrict__ observed_bits,
-                            uint32_t* __restrict__ observed_cells, uint32_t cells_x, uint32_t cells_y,
-                            unsigned long long* __restrict__ counters) {
-  __shared__ uint32_t s_cells[16];  // this block's 4x4x4 cells: [z][y] rows of 4 x-bits
+                            uint32_t* __restrict__ free_cells, uint32_t* __restrict__ observed_cells,
+                            uint32_t cells_x, uint32_t cells_y, unsigned long long* __restrict__ counters) {
+  // this block's 4x4x4 cells as [z][y] rows of four x-bits
+  __shared__ uint32_t s_touch[16];
+  __shared__ uint32_t s_free[16];
   using VT = VoxelTraits<Kind>;
   using Raw = typename VT::Raw;
   if (state != nullptr) {
@@ -221,15 +223,16 @@ __global__ void __launch_bounds__(kBlockThreads)
     const uint32_t block = list[item];
     const uint32_t bxi = block % v.bx, byi = (block / v.bx) % v.by, bzi = block / (v.bx * v.by);
     const uint32_t x = bxi * 8 + lx, y = byi * 8 + ly;
-    const bool full = bxi * 8 + 8 <= v.rx && byi * 8 + 8 <= v.ry && bzi * 8 + 8 <= v.rz;
-    bool all_one = true, any_other = false, any_fused = false;
-    if (threadIdx.x < 16) s_cells[threadIdx.x] = 0u;
+    if (threadIdx.x < 16) {
+      s_touch[threadIdx.x] = 0u;
+      s_free[threadIdx.x] = 0u;
+    }
     __syncthreads();
-    uint32_t fused_z = 0;  // bit i: voxel z = lz + i fused
+    uint32_t fused_z = 0;  // bit i: voxel z = lz + i fused this frame
+    uint32_t one_z = 0;    // bit i: voxel z = lz + i now observed with tsdf exactly 1
 #pragma unroll
     for (uint32_t i = 0; i < 4; ++i) {
       const uint32_t z = bzi * 8 + lz + i;
-      bool fused_one = false;
       if (x < v.rx && y < v.ry && z < v.rz) {
         // IntegrationContext::observe (tsdf_integration.hpp:183-224)
         const f3 cp = apply(T, cell_center(v, x, y, z));
@@ -257,13 +260,8 @@ __global__ void __launch_bounds__(kBlockThreads)
                 const Raw fused = VT::encode(avg, ip.max_weight < sum_w ? ip.max_weight : sum_w);
                 voxels[index] = fused;
                 ++updates;
-                any_fused = true;
                 fused_z |= 1u << i;
-                if (VT::tsdf(fused) == 1.0f) {
-                  fused_one = true;
-                } else {
-                  any_other = true;
-                }
+                if (VT::tsdf(fused) == 1.0f) one_z |= 1u << i;
                 if constexpr (Color) {
                   if (ip.has_color && sdf <= truncation * 0.5f) {
                     // ColorVoxel::fused (volume.hpp:160-170)
@@ -280,31 +278,67 @@ __global__ void __launch_bounds__(kBlockThreads)
           }
         }
       }
-      all_one = all_one && fused_one;
     }
-    // Observed 2x2x2 cells of this block (sticky bits, merged in shared memory).
-    if (fused_z & 3u) atomicOr(&s_cells[((lz >> 1) + 0) * 4 + (ly >> 1)], 1u << (lx >> 1));
-    if (fused_z & 12u) atomicOr(&s_cells[((lz >> 1) + 1) * 4 + (ly >> 1)], 1u << (lx >> 1));
-    // Skip bits: free when this frame fused every voxel to exactly 1; not free
-    // when it wrote anything else; unchanged otherwise.  Observed is sticky.
-    const bool block_one = __syncthreads_and(all_one) && full;
-    const bool block_other = __syncthreads_or(any_other);
-    const bool block_fused = __syncthreads_or(any_fused);
-    if (threadIdx.x == 0) {
-      const uint32_t bit = 1u << (block & 31u);
-      if (block_one) {
-        atomicOr(free_bits + (block >> 5), bit);
-      } else if (block_other) {
-        atomicAnd(free_bits + (block >> 5), ~bit);
+    // ---- skip bits of the raycast ---------------------------------------
+    // Per 2x2x2-voxel cell: free (all eight voxels observed with tsdf exactly
+    // 1) and observed (some voxel observed).  A cell is re-evaluated when this
+    // frame fused any of its voxels; its other voxels are then read.  The
+    // four threads of a cell are lanes {a, a^1, a^8, a^9} of one warp.
+    uint32_t pair_fused = ((fused_z & 3u) ? 1u : 0u) | ((fused_z & 12u) ? 2u : 0u);
+    pair_fused |= __shfl_xor_sync(0xFFFFFFFFu, pair_fused, 1);
+    pair_fused |= __shfl_xor_sync(0xFFFFFFFFu, pair_fused, 8);
+#pragma unroll
+    for (uint32_t i = 0; i < 4; ++i) {
+      const uint32_t z = bzi * 8 + lz + i;
+      if (!(fused_z & (1u << i)) && (pair_fused & (1u << (i >> 1))) && x < v.rx && y < v.ry && z < v.rz) {
+        const Raw r = voxels[static_cast<size_t>(z) * slice + static_cast<size_t>(y) * v.rx + x];
+        if (VT::observed(r) && VT::tsdf(r) == 1.0f) one_z |= 1u << i;
       }
-      if (block_fused) atomicOr(observed_bits + (block >> 5), bit);
     }
-    if (threadIdx.x < 16 && s_cells[threadIdx.x] != 0u) {
-      const uint32_t cz = bzi * 4 + (threadIdx.x >> 2), cy = byi * 4 + (threadIdx.x & 3u), cx = bxi * 4;
-      const size_t cell = (static_cast<size_t>(cz) * cells_y + cy) * cells_x + cx;
-      atomicOr(observed_cells + (cell >> 5), s_cells[threadIdx.x] << (cell & 31u));
+    uint32_t pair_one = ((one_z & 3u) == 3u ? 1u : 0u) | ((one_z & 12u) == 12u ? 2u : 0u);
+    pair_one &= __shfl_xor_sync(0xFFFFFFFFu, pair_one, 1);
+    pair_one &= __shfl_xor_sync(0xFFFFFFFFu, pair_one, 8);
+    if (!(lx & 1u) && !(ly & 1u)) {
+#pragma unroll
+      for (uint32_t q = 0; q < 2; ++q) {
+        if (pair_fused & (1u << q)) {
+          const uint32_t row = ((lz >> 1) + q) * 4u + (ly >> 1);
+          atomicOr(&s_touch[row], 1u << (lx >> 1));
+          if (pair_one & (1u << q)) atomicOr(&s_free[row], 1u << (lx >> 1));
+        }
+      }
     }
     __syncthreads();
+    // Apply the cell bits (threads 0..15, one row of four x-cells each) and
+    // derive the block bits: a block is free when its 64 cells are.
+    if (threadIdx.x < 16) {
+      const uint32_t row = threadIdx.x;
+      const uint32_t cz = bzi * 4 + (row >> 2), cy = byi * 4 + (row & 3u);
+      const size_t cell = (static_cast<size_t>(cz) * cells_y + cy) * cells_x + bxi * 4;
+      const size_t word = cell >> 5;
+      const uint32_t sh = static_cast<uint32_t>(cell & 31u);
+      const uint32_t touch = s_touch[row], fr = s_free[row];
+      uint32_t old_word;
+      if (touch) {
+        old_word = atomicAnd(free_cells + word, ~(touch << sh));
+        if (fr) atomicOr(free_cells + word, fr << sh);
+        atomicOr(observed_cells + word, touch << sh);
+      } else {
+        old_word = __ldcg(free_cells + word);
+      }
+      const uint32_t now = (((old_word >> sh) & 0xFu) & ~touch) | fr;
+      const bool block_free = __all_sync(0x0000FFFFu, now == 0xFu);
+      if (threadIdx.x == 0) {
+        const uint32_t bit = 1u << (block & 31u);
+        if (block_free) {
+          atomicOr(free_bits + (block >> 5), bit);
+        } else {
+          atomicAnd(free_bits + (block >> 5), ~bit);
+        }
+      }
+    }
+    const bool block_fused = __syncthreads_or(fused_z != 0u);
+    if (threadIdx.x == 0 && block_fused) atomicOr(observed_bits + (block >> 5), 1u << (block & 31u));
   }
   const unsigned total = __reduce_add_sync(0xFFFFFFFFu, updates);
   const unsigned total_color = __reduce_add_sync(0xFFFFFFFFu, color_updates);
@@ -396,7 +430,7 @@ void launch_blocks_typed(Pipeline& p, const float4* table, uint32_t width, uint3
   if (state == nullptr && p.kernel_start != nullptr) check(cudaEventRecord(p.kernel_start, s), "event record");
   integrate_blocks_kernel<Kind, Color><<<148 * 12, kBlockThreads, 0, s>>>(
       p.view, table, width, height, k, T, ip, state, p.block_list.ptr, p.block_count.ptr, p.free_blocks.ptr,
-      p.observed_blocks.ptr, p.observed_cells.ptr, p.cx, p.cy, p.counters.ptr);
+      p.observed_blocks.ptr, p.free_cells.ptr, p.observed_cells.ptr, p.cx, p.cy, p.counters.ptr);
   check(cudaGetLastError(), "integrate_blocks_kernel launch");
   if (state == nullptr && p.kernel_stop != nullptr) check(cudaEventRecord(p.kernel_stop, s), "event record");
 }
@@ -418,6 +452,7 @@ void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t s
     p.cy = p.view.by * 4;
     p.cz = p.view.bz * 4;
     p.observed_cells.resize((static_cast<size_t>(p.cx) * p.cy * p.cz + 31) / 32);
+    p.free_cells.resize(p.observed_cells.count);
     reset_blocks(p, s);
   }
   // depth-tile pyramid geometry for this frame size
@@ -444,6 +479,7 @@ void reset_blocks(Pipeline& p, cudaStream_t s) {
   check(cudaMemsetAsync(p.observed_blocks.ptr, 0, p.observed_blocks.bytes(), s), "skip bits reset");
   check(cudaMemsetAsync(p.safe_blocks.ptr, 0, p.safe_blocks.bytes(), s), "skip bits reset");
   check(cudaMemsetAsync(p.observed_cells.ptr, 0, p.observed_cells.bytes(), s), "skip bits reset");
+  check(cudaMemsetAsync(p.free_cells.ptr, 0, p.free_cells.bytes(), s), "skip bits reset");
   // nothing observed: every block is empty-safe
   check(cudaMemsetAsync(p.empty_safe.ptr, 0xFF, p.empty_safe.bytes(), s), "skip bits reset");
 }

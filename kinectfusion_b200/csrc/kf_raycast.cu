@@ -7,15 +7,17 @@
 // expression order, so a render is bit-identical to the CPU raycast of the
 // same volume and camera.
 //
-// Empty-space skip, exact: one bit per 8^3 block marks blocks whose 3x3x3
-// block neighbourhood is (a) observed free space - every voxel observed with
-// tsdf exactly 1, so every trilinear sample there is exactly 1.0 (the blend
-// divides a sum by the identical sum) - or (b) wholly unobserved, so every
-// sample there is nullopt.  The march replays its ray_length additions
-// through such blocks without gathering corners; the sample positions, and
-// therefore the output, are those of the plain march.  Samples before the
-// volume box are replayed the same way, and the march ends once the ray has
-// left the box.
+// Empty-space skip, exact, at two granularities.  A sample whose eight
+// corners are all observed with tsdf exactly 1 is exactly 1.0 (the blend
+// divides a sum by the identical sum); a sample with no observed corner is
+// nullopt.  Neither needs the corner gather:
+//  * 8^3 blocks whose 3x3x3 block neighbourhood is entirely free space (or
+//    entirely unobserved) are crossed in one go, replaying the march's
+//    ray_length additions up to the block exit;
+//  * otherwise 2x2x2-voxel cell bits decide single samples.
+// The sample positions, and therefore the output, are those of the plain
+// march.  Samples before the volume box are replayed the same way, and the
+// march ends once the ray has left the box.
 #include <cmath>
 
 #include "kf_internal.h"
@@ -201,30 +203,38 @@ __device__ __forceinline__ int skip_class(const uint32_t* __restrict__ free_safe
   return 0;
 }
 
-// True when no corner of the trilinear stencil at `point` is observed (the
-// sample is nullopt), decided from the 2x2x2-cell observed bits alone.
-__device__ __forceinline__ bool cells_unobserved(const uint32_t* __restrict__ cells, const VolumeDev& v, uint32_t cx,
-                                                 uint32_t cy, f3 point) {
+// Class of the trilinear stencil at `point` from the 2x2x2-cell bits alone:
+// 1 = every corner lies in a free cell (the sample is exactly 1.0), 2 = no
+// corner lies in an observed cell (the sample is nullopt), 0 = undecided.
+__device__ __forceinline__ int cell_class(const uint32_t* __restrict__ free_cells,
+                                          const uint32_t* __restrict__ observed_cells, const VolumeDev& v,
+                                          uint32_t cx, uint32_t cy, f3 point) {
   const f3 g = (point - v.origin) * v.inv_voxel_size;
   if (!(g.x >= 0.0f && g.y >= 0.0f && g.z >= 0.0f && g.x < static_cast<float>(v.rx) &&
         g.y < static_cast<float>(v.ry) && g.z < static_cast<float>(v.rz))) {
-    return false;  // outside the grid: the sampler itself rejects it cheaply
+    return 0;  // outside the grid: the sampler itself rejects it cheaply
   }
   const int bx = static_cast<int>(floorf(g.x - 0.5f)), by = static_cast<int>(floorf(g.y - 0.5f)),
             bz = static_cast<int>(floorf(g.z - 0.5f));
+  // all eight corners inside the volume (a missing corner is never "free")
+  const bool inside = bx >= 0 && by >= 0 && bz >= 0 && bx + 1 < static_cast<int>(v.rx) &&
+                      by + 1 < static_cast<int>(v.ry) && bz + 1 < static_cast<int>(v.rz);
   const int x0 = max(bx, 0) >> 1, x1 = min(bx + 1, static_cast<int>(v.rx) - 1) >> 1;
   const int y0 = max(by, 0) >> 1, y1 = min(by + 1, static_cast<int>(v.ry) - 1) >> 1;
   const int z0 = max(bz, 0) >> 1, z1 = min(bz + 1, static_cast<int>(v.rz) - 1) >> 1;
+  bool all_free = inside, none_observed = true;
   for (int z = z0; z <= z1; ++z) {
     for (int y = y0; y <= y1; ++y) {
       const size_t row = (static_cast<size_t>(z) * cy + static_cast<size_t>(y)) * cx;
       for (int x = x0; x <= x1; ++x) {
         const size_t c = row + static_cast<size_t>(x);
-        if ((__ldg(cells + (c >> 5)) >> (c & 31u)) & 1u) return false;
+        const uint32_t bit = 1u << (c & 31u);
+        if (!(__ldg(free_cells + (c >> 5)) & bit)) all_free = false;
+        if (__ldg(observed_cells + (c >> 5)) & bit) none_observed = false;
       }
     }
   }
-  return true;
+  return all_free ? 1 : (none_observed ? 2 : 0);
 }
 
 // Ray parameter where the ray leaves block (bxi, byi, bzi).  Approximate:
@@ -273,7 +283,8 @@ __device__ __forceinline__ void box_range(const VolumeDev& v, f3 o, f3 d, float&
 template <int Kind, bool Color>
 __global__ void __launch_bounds__(256)
     raycast_kernel(VolumeDev v, const uint32_t* __restrict__ free_safe, const uint32_t* __restrict__ empty_safe,
-                   const uint32_t* __restrict__ cells, uint32_t cells_x, uint32_t cells_y,
+                   const uint32_t* __restrict__ free_cells, const uint32_t* __restrict__ observed_cells,
+                   uint32_t cells_x, uint32_t cells_y,
                    RaycastParams rp, Intr k, uint32_t width,
                    uint32_t height, Rigid pose, const IcpState* __restrict__ state, float* __restrict__ points,
                    float* __restrict__ normals, uint32_t* __restrict__ colors) {
@@ -354,10 +365,21 @@ __global__ void __launch_bounds__(256)
           continue;
         }
       }
-      if (cells != nullptr && cells_unobserved(cells, v, cells_x, cells_y, point)) {
-        have_prev = false;
-        ray_length += base_step;
-        continue;
+      if (free_cells != nullptr) {
+        const int cls = cell_class(free_cells, observed_cells, v, cells_x, cells_y, point);
+        if (cls == 1) {
+          if (have_prev && prev_tsdf < 0.0f) break;
+          have_prev = true;
+          prev_tsdf = 1.0f;
+          prev_point = point;
+          ray_length += free_step;
+          continue;
+        }
+        if (cls == 2) {
+          have_prev = false;
+          ray_length += base_step;
+          continue;
+        }
       }
       float tsdf;
       if (!s.tsdf(point, rp.policy, tsdf)) {
@@ -418,8 +440,10 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
   const uint32_t* empty_safe = p.safe_blocks.count ? p.empty_safe.ptr : nullptr;
   const dim3 block(16, 16);
   const dim3 grid(ceil_div(cam.width, 16), ceil_div(cam.height, 16));
-  const uint32_t* cells = p.safe_blocks.count ? p.observed_cells.ptr : nullptr;
-  raycast_kernel<Kind, Color><<<grid, block, 0, s>>>(p.view, free_safe, empty_safe, cells, p.cx, p.cy, rp, intr_from(cam.intrinsics), cam.width,
+  const uint32_t* free_cells = p.safe_blocks.count ? p.free_cells.ptr : nullptr;
+  const uint32_t* observed_cells = p.safe_blocks.count ? p.observed_cells.ptr : nullptr;
+  raycast_kernel<Kind, Color><<<grid, block, 0, s>>>(p.view, free_safe, empty_safe, free_cells, observed_cells,
+                                                     p.cx, p.cy, rp, intr_from(cam.intrinsics), cam.width,
                                                      cam.height, rigid_from(cam.camera_to_world), state, points,
                                                      normals, colors);
   check(cudaGetLastError(), "raycast_kernel launch");
