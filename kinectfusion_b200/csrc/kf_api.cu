@@ -1,5 +1,6 @@
 // kf_api.cu - C ABI entry points (include/kf_b200.h) for pipelines, trackers
 // and the whole-frame CUDA graph.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -231,7 +232,8 @@ kf_status kf_pipeline_create(const kf_pipeline_config* config, kf_pipeline** out
       p.config = c;
       check(cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking), "cudaStreamCreate");
       const kf_volume_geometry& g = c.volume;
-      p.voxel_count = static_cast<uint64_t>(g.res_x) * g.res_y * g.res_z;
+      // bricked storage: whole 8^3 bricks (edge blocks padded)
+      p.voxel_count = static_cast<uint64_t>((g.res_x + 7) / 8) * ((g.res_y + 7) / 8) * ((g.res_z + 7) / 8) * 512;
       p.voxel_bytes = voxel_bytes_of(c.voxel);
       p.voxels.resize(p.voxel_count * p.voxel_bytes);
       if (c.color == KF_COLOR_FLOAT) p.colors.resize(p.voxel_count);
@@ -339,20 +341,43 @@ kf_status kf_pipeline_observed_voxel_count(kf_pipeline* pipeline, uint64_t* coun
   });
 }
 
+namespace {
+// Copies the bricked device volume to the host in the reference's x-fastest
+// order (Size3::flatten, vector.hpp:61-67): elem_bytes per voxel.
+void download_dense(const void* device, size_t elem_bytes, const kf_volume_geometry& g, void* out) {
+  const uint64_t bx = (g.res_x + 7) / 8, by = (g.res_y + 7) / 8, bz = (g.res_z + 7) / 8;
+  std::vector<uint8_t> raw(bx * by * bz * 512 * elem_bytes);
+  check(cudaMemcpy(raw.data(), device, raw.size(), cudaMemcpyDeviceToHost), "volume download");
+  uint8_t* dst = static_cast<uint8_t*>(out);
+  for (uint64_t z = 0; z < g.res_z; ++z) {
+    for (uint64_t y = 0; y < g.res_y; ++y) {
+      for (uint64_t x0 = 0; x0 < g.res_x; x0 += 8) {
+        const uint64_t block = ((z / 8) * by + (y / 8)) * bx + (x0 / 8);
+        const uint64_t src = (block * 512 + ((z % 8) * 8 + (y % 8)) * 8) * elem_bytes;
+        const uint64_t n = std::min<uint64_t>(8, g.res_x - x0);
+        std::memcpy(dst + ((z * g.res_y + y) * g.res_x + x0) * elem_bytes, raw.data() + src, n * elem_bytes);
+      }
+    }
+  }
+}
+}  // namespace
+
 kf_status kf_pipeline_download_raw(kf_pipeline* pipeline, void* voxels, size_t voxel_bytes, void* colors,
                                    size_t color_bytes) {
   return guarded([&] {
     require(pipeline != nullptr, "kf_pipeline_download_raw: null pipeline");
     Pipeline& p = pipeline->impl;
     check(cudaStreamSynchronize(p.stream), "download sync");
+    const kf_volume_geometry& g = p.config.volume;
+    const uint64_t dense = static_cast<uint64_t>(g.res_x) * g.res_y * g.res_z;
     if (voxels) {
-      require(voxel_bytes == p.voxels.bytes(), "kf_pipeline_download_raw: voxel buffer size mismatch");
-      check(cudaMemcpy(voxels, p.voxels.ptr, voxel_bytes, cudaMemcpyDeviceToHost), "voxel download");
+      require(voxel_bytes == dense * p.voxel_bytes, "kf_pipeline_download_raw: voxel buffer size mismatch");
+      download_dense(p.voxels.ptr, p.voxel_bytes, g, voxels);
     }
     if (colors) {
       require(p.colors.count != 0, "kf_pipeline_download_raw: the pipeline stores no colour");
-      require(color_bytes == p.colors.bytes(), "kf_pipeline_download_raw: colour buffer size mismatch");
-      check(cudaMemcpy(colors, p.colors.ptr, color_bytes, cudaMemcpyDeviceToHost), "colour download");
+      require(color_bytes == dense * sizeof(float4), "kf_pipeline_download_raw: colour buffer size mismatch");
+      download_dense(p.colors.ptr, sizeof(float4), g, colors);
     }
   });
 }
@@ -362,10 +387,12 @@ kf_status kf_pipeline_download_volume(kf_pipeline* pipeline, float* tsdf, float*
     require(pipeline != nullptr && tsdf != nullptr && weight != nullptr, "kf_pipeline_download_volume: null argument");
     Pipeline& p = pipeline->impl;
     check(cudaStreamSynchronize(p.stream), "download sync");
-    std::vector<uint8_t> raw(p.voxels.bytes());
-    check(cudaMemcpy(raw.data(), p.voxels.ptr, raw.size(), cudaMemcpyDeviceToHost), "voxel download");
-    // BlockRep/DenseRep::host_dense_view decode (volume.hpp:28-100)
-    for (uint64_t i = 0; i < p.voxel_count; ++i) {
+    const kf_volume_geometry& g = p.config.volume;
+    const uint64_t dense = static_cast<uint64_t>(g.res_x) * g.res_y * g.res_z;
+    std::vector<uint8_t> raw(dense * p.voxel_bytes);
+    download_dense(p.voxels.ptr, p.voxel_bytes, g, raw.data());
+    // host_dense_view decode (volume.hpp:28-100)
+    for (uint64_t i = 0; i < dense; ++i) {
       if (p.config.voxel == KF_VOXEL_FLOAT) {
         std::memcpy(tsdf + i, raw.data() + i * 8, 4);
         std::memcpy(weight + i, raw.data() + i * 8 + 4, 4);
@@ -384,7 +411,7 @@ kf_status kf_pipeline_download_volume(kf_pipeline* pipeline, float* tsdf, float*
     }
     if (color != nullptr) {
       require(p.colors.count != 0, "kf_pipeline_download_volume: the pipeline stores no colour");
-      check(cudaMemcpy(color, p.colors.ptr, p.colors.bytes(), cudaMemcpyDeviceToHost), "colour download");
+      download_dense(p.colors.ptr, sizeof(float4), g, color);
     }
   });
 }

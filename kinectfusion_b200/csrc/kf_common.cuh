@@ -170,15 +170,26 @@ struct VolumeDev {
 
 constexpr uint32_t kUnallocated = 0xFFFFFFFFu;
 
+// Voxel storage is bricked: 8x8x8 bricks of 512 contiguous voxels, voxel
+// (x, y, z) at brick slot * 512 + ((z & 7) * 8 + (y & 7)) * 8 + (x & 7) (the
+// intra-block order of BlockGrid::intra_of_voxel, grid.hpp:54-69).  Dense
+// volumes place brick b (x-major block index) at slot b; sparse volumes look
+// the slot up in `grid`.  A trilinear stencil or an 8-voxel walk along any
+// axis stays inside one or two 4 KB bricks, where the reference's
+// x-fastest layout puts z-neighbours a whole slice (2 MB at 512^3) apart.
+__device__ __forceinline__ uint32_t brick_offset(uint32_t x, uint32_t y, uint32_t z) {
+  return ((z & 7u) * 8u + (y & 7u)) * 8u + (x & 7u);
+}
+
 // Storage index of an in-bounds voxel, or -1 when its block is not allocated.
 __device__ __forceinline__ long long storage_index(const VolumeDev& v, uint32_t x, uint32_t y, uint32_t z) {
-  if (v.grid == nullptr) {
-    return (static_cast<long long>(z) * v.ry + y) * v.rx + x;
-  }
   const uint32_t block = ((z >> 3) * v.by + (y >> 3)) * v.bx + (x >> 3);
+  if (v.grid == nullptr) {
+    return static_cast<long long>(block) * 512 + brick_offset(x, y, z);
+  }
   const uint32_t slot = __ldg(v.grid + block);
   if (slot == kUnallocated) return -1;
-  return static_cast<long long>(slot) * 512 + (((z & 7u) * 8u + (y & 7u)) * 8u + (x & 7u));
+  return static_cast<long long>(slot) * 512 + brick_offset(x, y, z);
 }
 
 // VolumeGeometry::cell_center (volume.hpp:276-283)

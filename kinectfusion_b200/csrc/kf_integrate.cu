@@ -22,8 +22,8 @@
 //     runs the exact host observe/fuse; the CTA also maintains the per-block
 //     bits of the raycast's empty-space skip (free space / observed).
 //
-// Voxel reads and writes are 8 B (float) or 4 B (int16/bf16) per voxel, a
-// warp covering four 64-byte block rows.
+// Voxels are bricked (kf_common.cuh): a CTA's block is 512 contiguous
+// voxels and a warp reads and writes 32 consecutive ones (256 B for float).
 #include <algorithm>
 #include <cmath>
 
@@ -215,7 +215,6 @@ __global__ void __launch_bounds__(kBlockThreads)
     T = Rigid{{w[0], w[1], w[2]}, {w[3], w[4], w[5]}, {w[6], w[7], w[8]}, {w[9], w[10], w[11]}};
   }
   Raw* __restrict__ voxels = reinterpret_cast<Raw*>(v.voxels);
-  const size_t slice = static_cast<size_t>(v.rx) * v.ry;
   const unsigned n = *count;
   const uint32_t lx = threadIdx.x & 7u, ly = (threadIdx.x >> 3) & 7u, lz = (threadIdx.x >> 6) * 4u;
   unsigned updates = 0, color_updates = 0;
@@ -251,7 +250,7 @@ __global__ void __launch_bounds__(kBlockThreads)
               if (!(sdf < -truncation) && ow > 0.0f) {
                 const float tsdf = clampf(sdf / truncation, -1.0f, 1.0f);
                 // BasicVoxel::fused (volume.hpp:137-146)
-                const size_t index = static_cast<size_t>(z) * slice + static_cast<size_t>(y) * v.rx + x;
+                const size_t index = static_cast<size_t>(block) * 512 + brick_offset(x, y, z);
                 const Raw old = voxels[index];
                 const float t0 = VT::tsdf(old);
                 const float w0 = VT::weight(old);
@@ -291,7 +290,7 @@ __global__ void __launch_bounds__(kBlockThreads)
     for (uint32_t i = 0; i < 4; ++i) {
       const uint32_t z = bzi * 8 + lz + i;
       if (!(fused_z & (1u << i)) && (pair_fused & (1u << (i >> 1))) && x < v.rx && y < v.ry && z < v.rz) {
-        const Raw r = voxels[static_cast<size_t>(z) * slice + static_cast<size_t>(y) * v.rx + x];
+        const Raw r = voxels[static_cast<size_t>(block) * 512 + brick_offset(x, y, z)];
         if (VT::observed(r) && VT::tsdf(r) == 1.0f) one_z |= 1u << i;
       }
     }
