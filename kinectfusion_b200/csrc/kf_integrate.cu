@@ -388,6 +388,41 @@ __global__ void skip_bits_kernel(const uint32_t* __restrict__ free_bits, const u
   }
 }
 
+// Per-cell pair bits of the raycast (one thread per 32-cell word): cell c
+// gets free2 when the eight cells {c, c+1}^3 are free, empty2 when none of
+// them is observed.  The corners of a trilinear stencil whose base voxel
+// lies in cell c all lie in those eight cells.
+__global__ void cell_pairs_kernel(const uint32_t* __restrict__ free_cells, const uint32_t* __restrict__ observed_cells,
+                                  uint32_t* __restrict__ free2, uint32_t* __restrict__ empty2, uint32_t words_per_row,
+                                  uint32_t rows_y, uint32_t rows_z, const IcpState* __restrict__ state) {
+  if (state != nullptr && state->failed) return;
+  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t total = words_per_row * rows_y * rows_z;
+  if (w >= total) return;
+  const uint32_t xw = w % words_per_row, row = w / words_per_row;
+  const uint32_t y = row % rows_y, z = row / rows_y;
+  uint32_t f = 0xFFFFFFFFu, o = 0u;
+#pragma unroll
+  for (uint32_t dz = 0; dz < 2; ++dz) {
+#pragma unroll
+    for (uint32_t dy = 0; dy < 2; ++dy) {
+      if (y + dy >= rows_y || z + dz >= rows_z) {
+        f = 0u;
+        continue;
+      }
+      const size_t base = (static_cast<size_t>(z + dz) * rows_y + (y + dy)) * words_per_row;
+      const uint32_t fa = __ldg(free_cells + base + xw);
+      const uint32_t fb = xw + 1 < words_per_row ? __ldg(free_cells + base + xw + 1) : 0u;
+      const uint32_t oa = __ldg(observed_cells + base + xw);
+      const uint32_t ob = xw + 1 < words_per_row ? __ldg(observed_cells + base + xw + 1) : 0u;
+      f &= fa & ((fa >> 1) | (fb << 31));
+      o |= oa | ((oa >> 1) | (ob << 31));
+    }
+  }
+  free2[w] = f;
+  empty2[w] = ~o;
+}
+
 template <int Kind>
 __global__ void fill_kernel(void* voxels, float4* colors, size_t count) {
   using VT = VoxelTraits<Kind>;
@@ -447,11 +482,13 @@ void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t s
     p.block_list.resize(blocks);
     p.block_count.resize(1);
     // cells padded to whole blocks (4 per block edge), rows of 32-bit words
-    p.cx = p.view.bx * 4;
+    p.cx = (p.view.bx * 4 + 31) / 32 * 32;  // rows of whole 32-bit words
     p.cy = p.view.by * 4;
     p.cz = p.view.bz * 4;
-    p.observed_cells.resize((static_cast<size_t>(p.cx) * p.cy * p.cz + 31) / 32);
+    p.observed_cells.resize(static_cast<size_t>(p.cx) * p.cy * p.cz / 32);
     p.free_cells.resize(p.observed_cells.count);
+    p.free2.resize(p.observed_cells.count);
+    p.empty2.resize(p.observed_cells.count);
     reset_blocks(p, s);
   }
   // depth-tile pyramid geometry for this frame size
@@ -479,6 +516,8 @@ void reset_blocks(Pipeline& p, cudaStream_t s) {
   check(cudaMemsetAsync(p.safe_blocks.ptr, 0, p.safe_blocks.bytes(), s), "skip bits reset");
   check(cudaMemsetAsync(p.observed_cells.ptr, 0, p.observed_cells.bytes(), s), "skip bits reset");
   check(cudaMemsetAsync(p.free_cells.ptr, 0, p.free_cells.bytes(), s), "skip bits reset");
+  check(cudaMemsetAsync(p.free2.ptr, 0, p.free2.bytes(), s), "skip bits reset");
+  check(cudaMemsetAsync(p.empty2.ptr, 0xFF, p.empty2.bytes(), s), "skip bits reset");
   // nothing observed: every block is empty-safe
   check(cudaMemsetAsync(p.empty_safe.ptr, 0xFF, p.empty_safe.bytes(), s), "skip bits reset");
 }
@@ -544,6 +583,10 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
   skip_bits_kernel<<<ceil_div(blocks, 256), 256, 0, s>>>(p.free_blocks.ptr, p.observed_blocks.ptr, p.safe_blocks.ptr,
                                                          p.empty_safe.ptr, p.view.bx, p.view.by, p.view.bz, state);
   check(cudaGetLastError(), "skip_bits_kernel launch");
+  const uint32_t words = static_cast<uint32_t>(p.free2.count);
+  cell_pairs_kernel<<<ceil_div(words, 256), 256, 0, s>>>(p.free_cells.ptr, p.observed_cells.ptr, p.free2.ptr,
+                                                         p.empty2.ptr, p.cx / 32, p.cy, p.cz, state);
+  check(cudaGetLastError(), "cell_pairs_kernel launch");
 }
 
 void launch_fill_volume(Pipeline& p, cudaStream_t s) {

@@ -68,6 +68,24 @@ struct Sampler {
     const f3 fr = gg - fl;
     float acc = 0.0f, ws = 0.0f;
     int valid = 0;
+    if (v.grid == nullptr && bx >= 0 && by >= 0 && bz >= 0 && (bx & 7) != 7 && (by & 7) != 7 && (bz & 7) != 7 &&
+        bx + 1 < static_cast<int>(v.rx) && by + 1 < static_cast<int>(v.ry) && bz + 1 < static_cast<int>(v.rz)) {
+      // Dense, all eight corners in one brick: fixed offsets from the base
+      // voxel, loads issued together, blended in the reference corner order.
+      const Raw* b = reinterpret_cast<const Raw*>(v.voxels) +
+                     storage_index(v, static_cast<uint32_t>(bx), static_cast<uint32_t>(by), static_cast<uint32_t>(bz));
+      Raw r[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) r[c] = __ldg(b + ((c >> 2) * 64 + ((c >> 1) & 1) * 8 + (c & 1)));
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (!VT::observed(r[c]) || !VT::finite(r[c])) continue;
+        const float w = axis_weight(fr.x, c & 1) * axis_weight(fr.y, (c >> 1) & 1) * axis_weight(fr.z, c >> 2);
+        acc += w * VT::tsdf(r[c]);
+        ws += w;
+        ++valid;
+      }
+    } else {
 #pragma unroll
     for (int oz = 0; oz <= 1; ++oz) {
 #pragma unroll
@@ -84,6 +102,7 @@ struct Sampler {
           ++valid;
         }
       }
+    }
     }
     if (policy == KF_CORNERS_REQUIRE_ALL && valid < 8) return false;
     if (ws <= 1.0e-6f) return false;
@@ -182,61 +201,6 @@ struct Sampler {
   }
 };
 
-// Block class of a sample point: 1 = its 3x3x3 block neighbourhood is
-// observed free space (every voxel tsdf exactly 1), 2 = the neighbourhood
-// holds no observed voxel, 0 = anything else or outside the grid.
-__device__ __forceinline__ int skip_class(const uint32_t* __restrict__ free_safe,
-                                          const uint32_t* __restrict__ empty_safe, const VolumeDev& v, f3 point,
-                                          uint32_t& bxi, uint32_t& byi, uint32_t& bzi) {
-  const f3 g = (point - v.origin) * v.inv_voxel_size;
-  if (!(g.x >= 0.0f && g.y >= 0.0f && g.z >= 0.0f && g.x < static_cast<float>(v.rx) &&
-        g.y < static_cast<float>(v.ry) && g.z < static_cast<float>(v.rz))) {
-    return 0;
-  }
-  bxi = static_cast<uint32_t>(g.x) >> 3;
-  byi = static_cast<uint32_t>(g.y) >> 3;
-  bzi = static_cast<uint32_t>(g.z) >> 3;
-  const uint32_t block = (bzi * v.by + byi) * v.bx + bxi;
-  const uint32_t bit = 1u << (block & 31u);
-  if (__ldg(free_safe + (block >> 5)) & bit) return 1;
-  if (__ldg(empty_safe + (block >> 5)) & bit) return 2;
-  return 0;
-}
-
-// Class of the trilinear stencil at `point` from the 2x2x2-cell bits alone:
-// 1 = every corner lies in a free cell (the sample is exactly 1.0), 2 = no
-// corner lies in an observed cell (the sample is nullopt), 0 = undecided.
-__device__ __forceinline__ int cell_class(const uint32_t* __restrict__ free_cells,
-                                          const uint32_t* __restrict__ observed_cells, const VolumeDev& v,
-                                          uint32_t cx, uint32_t cy, f3 point) {
-  const f3 g = (point - v.origin) * v.inv_voxel_size;
-  if (!(g.x >= 0.0f && g.y >= 0.0f && g.z >= 0.0f && g.x < static_cast<float>(v.rx) &&
-        g.y < static_cast<float>(v.ry) && g.z < static_cast<float>(v.rz))) {
-    return 0;  // outside the grid: the sampler itself rejects it cheaply
-  }
-  const int bx = static_cast<int>(floorf(g.x - 0.5f)), by = static_cast<int>(floorf(g.y - 0.5f)),
-            bz = static_cast<int>(floorf(g.z - 0.5f));
-  // all eight corners inside the volume (a missing corner is never "free")
-  const bool inside = bx >= 0 && by >= 0 && bz >= 0 && bx + 1 < static_cast<int>(v.rx) &&
-                      by + 1 < static_cast<int>(v.ry) && bz + 1 < static_cast<int>(v.rz);
-  const int x0 = max(bx, 0) >> 1, x1 = min(bx + 1, static_cast<int>(v.rx) - 1) >> 1;
-  const int y0 = max(by, 0) >> 1, y1 = min(by + 1, static_cast<int>(v.ry) - 1) >> 1;
-  const int z0 = max(bz, 0) >> 1, z1 = min(bz + 1, static_cast<int>(v.rz) - 1) >> 1;
-  bool all_free = inside, none_observed = true;
-  for (int z = z0; z <= z1; ++z) {
-    for (int y = y0; y <= y1; ++y) {
-      const size_t row = (static_cast<size_t>(z) * cy + static_cast<size_t>(y)) * cx;
-      for (int x = x0; x <= x1; ++x) {
-        const size_t c = row + static_cast<size_t>(x);
-        const uint32_t bit = 1u << (c & 31u);
-        if (!(__ldg(free_cells + (c >> 5)) & bit)) all_free = false;
-        if (__ldg(observed_cells + (c >> 5)) & bit) none_observed = false;
-      }
-    }
-  }
-  return all_free ? 1 : (none_observed ? 2 : 0);
-}
-
 // Ray parameter where the ray leaves block (bxi, byi, bzi).  Approximate:
 // samples within rounding distance of the face still lie in the block's
 // one-block safety neighbourhood.
@@ -281,10 +245,10 @@ __device__ __forceinline__ void box_range(const VolumeDev& v, f3 o, f3 d, float&
 }
 
 template <int Kind, bool Color>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(64)
     raycast_kernel(VolumeDev v, const uint32_t* __restrict__ free_safe, const uint32_t* __restrict__ empty_safe,
-                   const uint32_t* __restrict__ free_cells, const uint32_t* __restrict__ observed_cells,
-                   uint32_t cells_x, uint32_t cells_y,
+                   const uint32_t* __restrict__ free2, const uint32_t* __restrict__ empty2, uint32_t cells_x,
+                   uint32_t cells_y,
                    RaycastParams rp, Intr k, uint32_t width,
                    uint32_t height, Rigid pose, const IcpState* __restrict__ state, float* __restrict__ points,
                    float* __restrict__ normals, uint32_t* __restrict__ colors) {
@@ -337,15 +301,39 @@ __global__ void __launch_bounds__(256)
     while (ray_length <= rp.max_depth) {
       if (ray_length > t_out) break;
       const f3 point = pose.t + (dir * ray_length);
-      if (free_safe != nullptr) {
-        uint32_t bxi, byi, bzi;
-        const int cls = skip_class(free_safe, empty_safe, v, point, bxi, byi, bzi);
+      if (free2 != nullptr) {
+        // Exact skip (see the file comment): decide the sample from the cell
+        // pair bits of its stencil's base cell, and cross whole safe blocks.
+        const f3 g = (point - v.origin) * v.inv_voxel_size;
+        if (!(g.x >= 0.0f && g.y >= 0.0f && g.z >= 0.0f && g.x < static_cast<float>(v.rx) &&
+              g.y < static_cast<float>(v.ry) && g.z < static_cast<float>(v.rz))) {
+          have_prev = false;  // outside the grid: nullopt
+          ray_length += base_step;
+          continue;
+        }
+        const int sx = static_cast<int>(floorf(g.x - 0.5f)), sy = static_cast<int>(floorf(g.y - 0.5f)),
+                  sz = static_cast<int>(floorf(g.z - 0.5f));
+        const size_t cell = (static_cast<size_t>(max(sz, 0) >> 1) * cells_y + static_cast<size_t>(max(sy, 0) >> 1)) *
+                                cells_x + static_cast<size_t>(max(sx, 0) >> 1);
+        const uint32_t cbit = 1u << (cell & 31u);
+        const bool stencil_inside = sx >= 0 && sy >= 0 && sz >= 0 && sx + 1 < static_cast<int>(v.rx) &&
+                                    sy + 1 < static_cast<int>(v.ry) && sz + 1 < static_cast<int>(v.rz);
+        int cls = 0;
+        if (stencil_inside && (__ldg(free2 + (cell >> 5)) & cbit)) {
+          cls = 1;
+        } else if (__ldg(empty2 + (cell >> 5)) & cbit) {
+          cls = 2;
+        }
         if (cls != 0) {
-          // Replay the plain march's additions up to the block exit.
-          const float t_exit = block_exit(v, pose.t, inv_dir, bxi, byi, bzi);
+          const uint32_t bxi = static_cast<uint32_t>(g.x) >> 3, byi = static_cast<uint32_t>(g.y) >> 3,
+                         bzi = static_cast<uint32_t>(g.z) >> 3;
+          const uint32_t block = (bzi * v.by + byi) * v.bx + bxi;
+          const uint32_t bbit = 1u << (block & 31u);
+          const bool block_safe = (__ldg((cls == 1 ? free_safe : empty_safe) + (block >> 5)) & bbit) != 0u;
+          const float t_exit = block_safe ? block_exit(v, pose.t, inv_dir, bxi, byi, bzi) : 0.0f;
           if (cls == 1) {
-            // Samples are exactly 1.0: leaving a surface from behind ends
-            // the march at the first one; after it every step is free_step.
+            // Exactly 1.0: leaving a surface from behind ends the march at
+            // the first such sample; after it every step is free_step.
             if (have_prev && prev_tsdf < 0.0f) break;
             float last = ray_length;
             do {
@@ -354,30 +342,13 @@ __global__ void __launch_bounds__(256)
             } while (ray_length < t_exit && ray_length <= rp.max_depth);
             have_prev = true;
             prev_tsdf = 1.0f;
-            prev_point = pose.t + (dir * last);
+            prev_point = last == ray_length ? point : pose.t + (dir * last);
           } else {
-            // No observed corner anywhere near: every sample is nullopt.
-            have_prev = false;
+            have_prev = false;  // nullopt
             do {
               ray_length += base_step;
             } while (ray_length < t_exit && ray_length <= rp.max_depth);
           }
-          continue;
-        }
-      }
-      if (free_cells != nullptr) {
-        const int cls = cell_class(free_cells, observed_cells, v, cells_x, cells_y, point);
-        if (cls == 1) {
-          if (have_prev && prev_tsdf < 0.0f) break;
-          have_prev = true;
-          prev_tsdf = 1.0f;
-          prev_point = point;
-          ray_length += free_step;
-          continue;
-        }
-        if (cls == 2) {
-          have_prev = false;
-          ray_length += base_step;
           continue;
         }
       }
@@ -438,12 +409,11 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
   rp.seed_previous = p.config.raycast.seed_from_previous;
   const uint32_t* free_safe = p.safe_blocks.count ? p.safe_blocks.ptr : nullptr;
   const uint32_t* empty_safe = p.safe_blocks.count ? p.empty_safe.ptr : nullptr;
-  const dim3 block(16, 16);
-  const dim3 grid(ceil_div(cam.width, 16), ceil_div(cam.height, 16));
-  const uint32_t* free_cells = p.safe_blocks.count ? p.free_cells.ptr : nullptr;
-  const uint32_t* observed_cells = p.safe_blocks.count ? p.observed_cells.ptr : nullptr;
-  raycast_kernel<Kind, Color><<<grid, block, 0, s>>>(p.view, free_safe, empty_safe, free_cells, observed_cells,
-                                                     p.cx, p.cy, rp, intr_from(cam.intrinsics), cam.width,
+  const dim3 block(8, 8);
+  const dim3 grid(ceil_div(cam.width, 8), ceil_div(cam.height, 8));
+  const uint32_t* free2 = p.safe_blocks.count ? p.free2.ptr : nullptr;
+  const uint32_t* empty2 = p.safe_blocks.count ? p.empty2.ptr : nullptr;
+  raycast_kernel<Kind, Color><<<grid, block, 0, s>>>(p.view, free_safe, empty_safe, free2, empty2, p.cx, p.cy, rp, intr_from(cam.intrinsics), cam.width,
                                                      cam.height, rigid_from(cam.camera_to_world), state, points,
                                                      normals, colors);
   check(cudaGetLastError(), "raycast_kernel launch");
