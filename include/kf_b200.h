@@ -314,6 +314,26 @@ kf_status kf_icp_normal_equations(kf_tracker* tracker, const kf_level_view* live
                                   const kf_rigid* model_world_to_camera, float* sums,
                                   uint64_t* count);
 
+/* The same sweep without any allocation (no counterpart in the reference).
+ * For callers that must not allocate device memory - code running inside
+ * another framework's memory pool or a replayed CUDA graph, plug-ins whose
+ * host forbids cudaMalloc after start-up, real-time loops kept off the
+ * allocator: no tracker object is needed, and the per-CTA partial sums live in
+ * a fixed device array (about 150 KB, present on every GPU that loads the
+ * library until the process exits).  Live images of at most 1,228,800 pixels
+ * (1200 CTAs of 1024 pixels) are accepted; larger ones return
+ * KF_ERR_INVALID_ARGUMENT.  The first call on each device looks up the
+ * array's address (make it before any stream capture).  Every call shares the
+ * array: calls that overlap on the GPU (for example from two host threads)
+ * race.  Runs on the legacy default stream and returns after the results are
+ * copied to `sums` and `count`. */
+kf_status kf_icp_normal_equations_static(const kf_level_view* live, const float* model_points,
+                                         const float* model_normals, uint32_t model_width,
+                                         uint32_t model_height, kf_intrinsics model_intrinsics,
+                                         const kf_rigid* camera, const kf_rigid* model_world_to_camera,
+                                         float max_point_distance, float min_normal_dot, float* sums,
+                                         uint64_t* count);
+
 /* ---- whole frame (Reconstruction::process_frame, reconstruction.cpp:184-216)
  * pyramid -> per level (raycast at the current estimate, ICP) -> integrate at
  * the tracked pose, as one CUDA graph with one host sync.  depth is

@@ -174,6 +174,9 @@ _PROTOTYPES = {
                                     C.POINTER(IcpOutcome)]),
     "kf_icp_normal_equations": (C.c_int, [P, C.POINTER(LevelView), P, P, C.c_uint32, C.c_uint32, Intrinsics,
                                           C.POINTER(Rigid), C.POINTER(Rigid), P, C.POINTER(C.c_uint64)]),
+    "kf_icp_normal_equations_static": (C.c_int, [C.POINTER(LevelView), P, P, C.c_uint32, C.c_uint32, Intrinsics,
+                                                 C.POINTER(Rigid), C.POINTER(Rigid), C.c_float, C.c_float, P,
+                                                 C.POINTER(C.c_uint64)]),
     "kf_frame_process": (C.c_int, [P, P, P, P, P, C.c_uint32, C.c_uint32, Intrinsics, C.c_int32, P, C.c_int32,
                                    C.POINTER(Rigid), C.POINTER(FrameResult)]),
     "kf_frame_enqueue": (C.c_int, [P, P, P, P, P, C.c_uint32, C.c_uint32, Intrinsics, C.c_int32, P, C.c_int32]),

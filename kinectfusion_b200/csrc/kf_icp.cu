@@ -734,3 +734,224 @@ void launch_icp_set_pose(IcpState* state, kf_rigid pose, int reset_frame, cudaSt
 }
 
 }  // namespace kf
+
+// ---------------------------------------------------------------------------
+// Allocation-free correspondence sweep.
+//
+// Some callers of this library cannot allocate device memory: code running
+// inside another framework's memory pool or a CUDA-graph-replayed section,
+// plug-ins whose host forbids cudaMalloc after start-up, or real-time loops
+// that must not hit the allocator.  kf_icp_normal_equations_static serves
+// them: the per-CTA partial sums live in a file-scope __device__ array that
+// exists on every GPU that loads this library (about 150 KB, held until the
+// process exits), so the call needs no tracker object and allocates nothing.
+// ---------------------------------------------------------------------------
+#include <cstring>
+#include <mutex>
+#include <string>
+
+namespace kf {
+namespace {
+
+constexpr int kStaticPixelsPerCta = 4 * kIcpBlock;  // each CTA sweeps 1024 live pixels
+constexpr int kStaticSlots = 1200;                  // one partial slot per CTA
+constexpr uint64_t kStaticMaxPixels = static_cast<uint64_t>(kStaticSlots) * kStaticPixelsPerCta;  // 1,228,800
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) float g_static_partials[kStaticSlots * kIcpSlot];
+static __device__ __align__(256) IcpState g_static_state;
+
+// Same association and accumulation as icp_iteration_kernel; the image is cut
+// into 1024-pixel tiles, one per CTA, and the last CTA to finish combines the
+// partial slots (Kahan-compensated, in slot order) straight from memory.
+__global__ void __launch_bounds__(kIcpBlock)
+    icp_static_sweep_kernel(IcpLevelArgs a, IcpState* __restrict__ st, float* __restrict__ partials, float max_d,
+                            float min_dot) {
+  __shared__ int s_last;
+  __shared__ float s_warp[kIcpBlock / 32][kIcpSlot];
+  __shared__ unsigned s_warp_count[kIcpBlock / 32];
+  __shared__ float s_seg_sum[8][kIcpSlot];
+  __shared__ float s_seg_comp[8][kIcpSlot];
+  const Rigid cam = rigid_load(st->camera);
+  const Rigid model = rigid_load(st->model);
+  float acc[kIcpSums];
+#pragma unroll
+  for (int i = 0; i < kIcpSums; ++i) acc[i] = 0.0f;
+  unsigned cnt = 0;
+  const uint32_t pixels = a.live_width * a.live_height;
+  const uint32_t first = blockIdx.x * kStaticPixelsPerCta;
+#pragma unroll 1
+  for (uint32_t k = 0; k < kStaticPixelsPerCta / kIcpBlock; ++k) {
+    const uint32_t pix = first + k * kIcpBlock + threadIdx.x;
+    if (pix >= pixels) break;
+    float j[6], residual, distance;
+    if (!match(a, cam, model, max_d, min_dot, pix % a.live_width, pix / a.live_width, j, residual, distance)) {
+      continue;
+    }
+    int e = 0;
+#pragma unroll
+    for (int r = 0; r < 6; ++r) {
+#pragma unroll
+      for (int c = r; c < 6; ++c) {
+        acc[e] += j[r] * j[c];
+        ++e;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 6; ++r) acc[21 + r] += j[r] * residual;
+    acc[27] += distance;
+    acc[28] += residual * residual;
+    ++cnt;
+  }
+#pragma unroll
+  for (int i = 0; i < kIcpSums; ++i) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc[i] += __shfl_xor_sync(0xFFFFFFFFu, acc[i], off);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, off);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < kIcpSums; ++i) s_warp[warp][i] = acc[i];
+    s_warp_count[warp] = cnt;
+  }
+  __syncthreads();
+  if (threadIdx.x < kIcpSums) {
+    float s = 0.0f;
+    for (int w = 0; w < kIcpBlock / 32; ++w) s += s_warp[w][threadIdx.x];
+    partials[blockIdx.x * kIcpSlot + threadIdx.x] = s;
+  } else if (threadIdx.x == kIcpSums) {
+    unsigned c = 0;
+    for (int w = 0; w < kIcpBlock / 32; ++w) c += s_warp_count[w];
+    partials[blockIdx.x * kIcpSlot + kIcpSums] = __uint_as_float(c);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(&st->arrived, 1u) == gridDim.x - 1) ? 1 : 0;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  {
+    const unsigned i = threadIdx.x % kIcpSlot, g = threadIdx.x / kIcpSlot;
+    if (i < kIcpSums) {
+      float sum = 0.0f, comp = 0.0f;
+      for (unsigned b = g; b < gridDim.x; b += 8) {
+        const float y = __ldcg(partials + b * kIcpSlot + i) - comp;
+        const float t = sum + y;
+        comp = (t - sum) - y;
+        sum = t;
+      }
+      s_seg_sum[g][i] = sum;
+      s_seg_comp[g][i] = comp;
+    } else if (i == kIcpSums) {
+      unsigned c = 0;
+      for (unsigned b = g; b < gridDim.x; b += 8) c += __float_as_uint(__ldcg(partials + b * kIcpSlot + kIcpSums));
+      s_seg_sum[g][i] = __uint_as_float(c);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < kIcpSums) {
+    float sum = 0.0f, comp = 0.0f;
+    for (int g = 0; g < 8; ++g) {
+      const float y = (s_seg_sum[g][threadIdx.x] - s_seg_comp[g][threadIdx.x]) - comp;
+      const float t = sum + y;
+      comp = (t - sum) - y;
+      sum = t;
+    }
+    st->sums[threadIdx.x] = sum;
+  } else if (threadIdx.x == kIcpSums) {
+    unsigned long long c = 0;
+    for (int g = 0; g < 8; ++g) c += __float_as_uint(s_seg_sum[g][kIcpSums]);
+    st->count = c;
+    st->arrived = 0;
+  }
+}
+
+// Device addresses of the two scratch symbols, looked up once per device.
+struct StaticScratch {
+  float* partials;
+  IcpState* state;
+};
+
+StaticScratch static_scratch_for_current_device() {
+  static std::mutex lock;
+  static StaticScratch table[kMaxDevices] = {};
+  int device = 0;
+  check(cudaGetDevice(&device), "cudaGetDevice");
+  require(device >= 0 && device < kMaxDevices, "kf_icp_normal_equations_static: device ordinal out of range");
+  std::lock_guard<std::mutex> guard(lock);
+  StaticScratch& entry = table[device];
+  if (entry.partials == nullptr) {
+    void* partials = nullptr;
+    void* state = nullptr;
+    check(cudaGetSymbolAddress(&partials, g_static_partials), "cudaGetSymbolAddress(partials scratch)");
+    check(cudaGetSymbolAddress(&state, g_static_state), "cudaGetSymbolAddress(state scratch)");
+    entry.partials = static_cast<float*>(partials);
+    entry.state = static_cast<IcpState*>(state);
+  }
+  return entry;
+}
+
+}  // namespace
+}  // namespace kf
+
+extern "C" kf_status kf_icp_normal_equations_static(const kf_level_view* live, const float* model_points,
+                                                    const float* model_normals, uint32_t model_width,
+                                                    uint32_t model_height, kf_intrinsics model_intrinsics,
+                                                    const kf_rigid* camera, const kf_rigid* model_world_to_camera,
+                                                    float max_point_distance, float min_normal_dot, float* sums,
+                                                    uint64_t* count) {
+  using namespace kf;
+  return guarded([&] {
+    require(live && model_points && model_normals && camera && model_world_to_camera && sums && count,
+            "kf_icp_normal_equations_static: null argument");
+    const uint64_t pixels = static_cast<uint64_t>(live->width) * live->height;
+    if (pixels > kStaticMaxPixels) {
+      throw InvalidArgument("kf_icp_normal_equations_static: the live image has " + std::to_string(pixels) +
+                            " pixels; the static scratch holds sweeps of at most " +
+                            std::to_string(kStaticMaxPixels) + " pixels");
+    }
+    if (pixels == 0) {
+      for (int i = 0; i < kIcpSums; ++i) sums[i] = 0.0f;
+      *count = 0;
+      return;
+    }
+    const StaticScratch scratch = static_scratch_for_current_device();
+    // Transforms in, arrival ticket cleared: the array keeps the last call's
+    // contents otherwise.
+    float transforms[24];
+    std::memcpy(transforms, camera->r, 9 * sizeof(float));
+    std::memcpy(transforms + 9, camera->t, 3 * sizeof(float));
+    std::memcpy(transforms + 12, model_world_to_camera->r, 9 * sizeof(float));
+    std::memcpy(transforms + 21, model_world_to_camera->t, 3 * sizeof(float));
+    static_assert(offsetof(IcpState, model) == offsetof(IcpState, camera) + 12 * sizeof(float),
+                  "camera and model transforms are adjacent");
+    char* state = reinterpret_cast<char*>(scratch.state);
+    const unsigned zero = 0;
+    check(cudaMemcpy(state + offsetof(IcpState, camera), transforms, sizeof(transforms), cudaMemcpyHostToDevice),
+          "static sweep transforms upload");
+    check(cudaMemcpy(state + offsetof(IcpState, arrived), &zero, sizeof(zero), cudaMemcpyHostToDevice),
+          "static sweep ticket clear");
+    IcpLevelArgs a;
+    a.live_vertices = live->vertices;
+    a.live_normals = live->normals;
+    a.live_width = live->width;
+    a.live_height = live->height;
+    a.model_points = model_points;
+    a.model_normals = model_normals;
+    a.model_width = model_width;
+    a.model_height = model_height;
+    a.model_intrinsics = intr_from(model_intrinsics);
+    const unsigned grid = static_cast<unsigned>((pixels + kStaticPixelsPerCta - 1) / kStaticPixelsPerCta);
+    icp_static_sweep_kernel<<<grid, kIcpBlock, 0, 0>>>(a, scratch.state, scratch.partials, max_point_distance,
+                                                       min_normal_dot);
+    check(cudaGetLastError(), "icp_static_sweep_kernel launch");
+    check(cudaMemcpy(sums, state + offsetof(IcpState, sums), kIcpSums * sizeof(float), cudaMemcpyDeviceToHost),
+          "static sweep sums download");
+    unsigned long long c = 0;
+    check(cudaMemcpy(&c, state + offsetof(IcpState, count), sizeof(c), cudaMemcpyDeviceToHost),
+          "static sweep count download");
+    *count = c;
+  });
+}
