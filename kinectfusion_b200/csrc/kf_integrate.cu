@@ -19,8 +19,8 @@
 //     (a fused voxel has |p|/lambda <= depth + truncation, and |p|/lambda >=
 //     p.z * (1 - 0.71/f) since the pixel ray is rounded by half a pixel).
 //  3. listed-block integration: one CTA per surviving block, every voxel
-//     runs the exact host observe/fuse; the CTA also maintains the per-block
-//     bits of the raycast's empty-space skip (free space / observed).
+//     runs the exact host observe/fuse; the CTA also maintains the raycast's
+//     skip bits (per voxel: observed / exactly 1; per block: free / observed).
 //
 // Voxels are bricked (kf_common.cuh): a CTA's block is 512 contiguous
 // voxels and a warp reads and writes 32 consecutive ones (256 B for float).
@@ -202,11 +202,8 @@ __global__ void __launch_bounds__(kBlockThreads)
                             Rigid T, IntegParams ip, const IcpState* __restrict__ state,
                             const uint32_t* __restrict__ list, const unsigned* __restrict__ count,
                             uint32_t* __restrict__ free_bits, uint32_t* __restrict__ observed_bits,
-                            uint32_t* __restrict__ free_cells, uint32_t* __restrict__ observed_cells,
-                            uint32_t cells_x, uint32_t cells_y, unsigned long long* __restrict__ counters) {
-  // this block's 4x4x4 cells as [z][y] rows of four x-bits
-  __shared__ uint32_t s_touch[16];
-  __shared__ uint32_t s_free[16];
+                            uint32_t* __restrict__ voxel_bits, unsigned long long* __restrict__ counters) {
+  __shared__ uint32_t s_one[16];
   using VT = VoxelTraits<Kind>;
   using Raw = typename VT::Raw;
   if (state != nullptr) {
@@ -222,11 +219,6 @@ __global__ void __launch_bounds__(kBlockThreads)
     const uint32_t block = list[item];
     const uint32_t bxi = block % v.bx, byi = (block / v.bx) % v.by, bzi = block / (v.bx * v.by);
     const uint32_t x = bxi * 8 + lx, y = byi * 8 + ly;
-    if (threadIdx.x < 16) {
-      s_touch[threadIdx.x] = 0u;
-      s_free[threadIdx.x] = 0u;
-    }
-    __syncthreads();
     uint32_t fused_z = 0;  // bit i: voxel z = lz + i fused this frame
     uint32_t one_z = 0;    // bit i: voxel z = lz + i now observed with tsdf exactly 1
 #pragma unroll
@@ -279,65 +271,44 @@ __global__ void __launch_bounds__(kBlockThreads)
       }
     }
     // ---- skip bits of the raycast ---------------------------------------
-    // Per 2x2x2-voxel cell: free (all eight voxels observed with tsdf exactly
-    // 1) and observed (some voxel observed).  A cell is re-evaluated when this
-    // frame fused any of its voxels; its other voxels are then read.  The
-    // four threads of a cell are lanes {a, a^1, a^8, a^9} of one warp.
-    uint32_t pair_fused = ((fused_z & 3u) ? 1u : 0u) | ((fused_z & 12u) ? 2u : 0u);
-    pair_fused |= __shfl_xor_sync(0xFFFFFFFFu, pair_fused, 1);
-    pair_fused |= __shfl_xor_sync(0xFFFFFFFFu, pair_fused, 8);
+    // Per voxel: `one` (observed with tsdf exactly 1) and `observed`, 512 +
+    // 512 bits per brick stored as 16 + 16 words (one 128-byte line).  A warp
+    // holds 32 consecutive voxels of the brick for each of its four z, i.e.
+    // exactly one word: ballots give the new bits of the voxels fused this
+    // frame, the other bits are kept.
+    uint32_t* bits = voxel_bits + static_cast<size_t>(block) * 32u;
+    const uint32_t half = (threadIdx.x >> 5) & 1u;
+    uint32_t any_observed = 0u;
 #pragma unroll
     for (uint32_t i = 0; i < 4; ++i) {
-      const uint32_t z = bzi * 8 + lz + i;
-      if (!(fused_z & (1u << i)) && (pair_fused & (1u << (i >> 1))) && x < v.rx && y < v.ry && z < v.rz) {
-        const Raw r = voxels[static_cast<size_t>(block) * 512 + brick_offset(x, y, z)];
-        if (VT::observed(r) && VT::tsdf(r) == 1.0f) one_z |= 1u << i;
+      const uint32_t fused = __ballot_sync(0xFFFFFFFFu, (fused_z >> i) & 1u);
+      const uint32_t ones = __ballot_sync(0xFFFFFFFFu, (one_z >> i) & 1u);
+      if ((threadIdx.x & 31u) == 0) {
+        const uint32_t w = 2u * (lz + i) + half;
+        const uint32_t one = (__ldcg(bits + w) & ~fused) | (ones & fused);
+        const uint32_t obs = __ldcg(bits + 16u + w) | fused;
+        if (fused) {
+          bits[w] = one;
+          bits[16u + w] = obs;
+        }
+        s_one[w] = one;
+        any_observed |= obs;
       }
     }
-    uint32_t pair_one = ((one_z & 3u) == 3u ? 1u : 0u) | ((one_z & 12u) == 12u ? 2u : 0u);
-    pair_one &= __shfl_xor_sync(0xFFFFFFFFu, pair_one, 1);
-    pair_one &= __shfl_xor_sync(0xFFFFFFFFu, pair_one, 8);
-    if (!(lx & 1u) && !(ly & 1u)) {
+    const bool block_observed = __syncthreads_or(any_observed != 0u);
+    if (threadIdx.x == 0) {
+      uint32_t all = 0xFFFFFFFFu;
 #pragma unroll
-      for (uint32_t q = 0; q < 2; ++q) {
-        if (pair_fused & (1u << q)) {
-          const uint32_t row = ((lz >> 1) + q) * 4u + (ly >> 1);
-          atomicOr(&s_touch[row], 1u << (lx >> 1));
-          if (pair_one & (1u << q)) atomicOr(&s_free[row], 1u << (lx >> 1));
-        }
+      for (int w = 0; w < 16; ++w) all &= s_one[w];
+      const uint32_t bit = 1u << (block & 31u);
+      if (all == 0xFFFFFFFFu) {
+        atomicOr(free_bits + (block >> 5), bit);
+      } else {
+        atomicAnd(free_bits + (block >> 5), ~bit);
       }
+      if (block_observed) atomicOr(observed_bits + (block >> 5), bit);
     }
     __syncthreads();
-    // Apply the cell bits (threads 0..15, one row of four x-cells each) and
-    // derive the block bits: a block is free when its 64 cells are.
-    if (threadIdx.x < 16) {
-      const uint32_t row = threadIdx.x;
-      const uint32_t cz = bzi * 4 + (row >> 2), cy = byi * 4 + (row & 3u);
-      const size_t cell = (static_cast<size_t>(cz) * cells_y + cy) * cells_x + bxi * 4;
-      const size_t word = cell >> 5;
-      const uint32_t sh = static_cast<uint32_t>(cell & 31u);
-      const uint32_t touch = s_touch[row], fr = s_free[row];
-      uint32_t old_word;
-      if (touch) {
-        old_word = atomicAnd(free_cells + word, ~(touch << sh));
-        if (fr) atomicOr(free_cells + word, fr << sh);
-        atomicOr(observed_cells + word, touch << sh);
-      } else {
-        old_word = __ldcg(free_cells + word);
-      }
-      const uint32_t now = (((old_word >> sh) & 0xFu) & ~touch) | fr;
-      const bool block_free = __all_sync(0x0000FFFFu, now == 0xFu);
-      if (threadIdx.x == 0) {
-        const uint32_t bit = 1u << (block & 31u);
-        if (block_free) {
-          atomicOr(free_bits + (block >> 5), bit);
-        } else {
-          atomicAnd(free_bits + (block >> 5), ~bit);
-        }
-      }
-    }
-    const bool block_fused = __syncthreads_or(fused_z != 0u);
-    if (threadIdx.x == 0 && block_fused) atomicOr(observed_bits + (block >> 5), 1u << (block & 31u));
   }
   const unsigned total = __reduce_add_sync(0xFFFFFFFFu, updates);
   const unsigned total_color = __reduce_add_sync(0xFFFFFFFFu, color_updates);
@@ -388,41 +359,6 @@ __global__ void skip_bits_kernel(const uint32_t* __restrict__ free_bits, const u
   }
 }
 
-// Per-cell pair bits of the raycast (one thread per 32-cell word): cell c
-// gets free2 when the eight cells {c, c+1}^3 are free, empty2 when none of
-// them is observed.  The corners of a trilinear stencil whose base voxel
-// lies in cell c all lie in those eight cells.
-__global__ void cell_pairs_kernel(const uint32_t* __restrict__ free_cells, const uint32_t* __restrict__ observed_cells,
-                                  uint32_t* __restrict__ free2, uint32_t* __restrict__ empty2, uint32_t words_per_row,
-                                  uint32_t rows_y, uint32_t rows_z, const IcpState* __restrict__ state) {
-  if (state != nullptr && state->failed) return;
-  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t total = words_per_row * rows_y * rows_z;
-  if (w >= total) return;
-  const uint32_t xw = w % words_per_row, row = w / words_per_row;
-  const uint32_t y = row % rows_y, z = row / rows_y;
-  uint32_t f = 0xFFFFFFFFu, o = 0u;
-#pragma unroll
-  for (uint32_t dz = 0; dz < 2; ++dz) {
-#pragma unroll
-    for (uint32_t dy = 0; dy < 2; ++dy) {
-      if (y + dy >= rows_y || z + dz >= rows_z) {
-        f = 0u;
-        continue;
-      }
-      const size_t base = (static_cast<size_t>(z + dz) * rows_y + (y + dy)) * words_per_row;
-      const uint32_t fa = __ldg(free_cells + base + xw);
-      const uint32_t fb = xw + 1 < words_per_row ? __ldg(free_cells + base + xw + 1) : 0u;
-      const uint32_t oa = __ldg(observed_cells + base + xw);
-      const uint32_t ob = xw + 1 < words_per_row ? __ldg(observed_cells + base + xw + 1) : 0u;
-      f &= fa & ((fa >> 1) | (fb << 31));
-      o |= oa | ((oa >> 1) | (ob << 31));
-    }
-  }
-  free2[w] = f;
-  empty2[w] = ~o;
-}
-
 template <int Kind>
 __global__ void fill_kernel(void* voxels, float4* colors, size_t count) {
   using VT = VoxelTraits<Kind>;
@@ -464,7 +400,7 @@ void launch_blocks_typed(Pipeline& p, const float4* table, uint32_t width, uint3
   if (state == nullptr && p.kernel_start != nullptr) check(cudaEventRecord(p.kernel_start, s), "event record");
   integrate_blocks_kernel<Kind, Color><<<148 * 12, kBlockThreads, 0, s>>>(
       p.view, table, width, height, k, T, ip, state, p.block_list.ptr, p.block_count.ptr, p.free_blocks.ptr,
-      p.observed_blocks.ptr, p.free_cells.ptr, p.observed_cells.ptr, p.cx, p.cy, p.counters.ptr);
+      p.observed_blocks.ptr, p.voxel_bits.ptr, p.counters.ptr);
   check(cudaGetLastError(), "integrate_blocks_kernel launch");
   if (state == nullptr && p.kernel_stop != nullptr) check(cudaEventRecord(p.kernel_stop, s), "event record");
 }
@@ -481,14 +417,7 @@ void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t s
     p.empty_safe.resize(words);
     p.block_list.resize(blocks);
     p.block_count.resize(1);
-    // cells padded to whole blocks (4 per block edge), rows of 32-bit words
-    p.cx = (p.view.bx * 4 + 31) / 32 * 32;  // rows of whole 32-bit words
-    p.cy = p.view.by * 4;
-    p.cz = p.view.bz * 4;
-    p.observed_cells.resize(static_cast<size_t>(p.cx) * p.cy * p.cz / 32);
-    p.free_cells.resize(p.observed_cells.count);
-    p.free2.resize(p.observed_cells.count);
-    p.empty2.resize(p.observed_cells.count);
+    p.voxel_bits.resize(static_cast<size_t>(blocks) * 32u);
     reset_blocks(p, s);
   }
   // depth-tile pyramid geometry for this frame size
@@ -514,10 +443,7 @@ void reset_blocks(Pipeline& p, cudaStream_t s) {
   check(cudaMemsetAsync(p.free_blocks.ptr, 0, p.free_blocks.bytes(), s), "skip bits reset");
   check(cudaMemsetAsync(p.observed_blocks.ptr, 0, p.observed_blocks.bytes(), s), "skip bits reset");
   check(cudaMemsetAsync(p.safe_blocks.ptr, 0, p.safe_blocks.bytes(), s), "skip bits reset");
-  check(cudaMemsetAsync(p.observed_cells.ptr, 0, p.observed_cells.bytes(), s), "skip bits reset");
-  check(cudaMemsetAsync(p.free_cells.ptr, 0, p.free_cells.bytes(), s), "skip bits reset");
-  check(cudaMemsetAsync(p.free2.ptr, 0, p.free2.bytes(), s), "skip bits reset");
-  check(cudaMemsetAsync(p.empty2.ptr, 0xFF, p.empty2.bytes(), s), "skip bits reset");
+  check(cudaMemsetAsync(p.voxel_bits.ptr, 0, p.voxel_bits.bytes(), s), "skip bits reset");
   // nothing observed: every block is empty-safe
   check(cudaMemsetAsync(p.empty_safe.ptr, 0xFF, p.empty_safe.bytes(), s), "skip bits reset");
 }
@@ -583,10 +509,6 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
   skip_bits_kernel<<<ceil_div(blocks, 256), 256, 0, s>>>(p.free_blocks.ptr, p.observed_blocks.ptr, p.safe_blocks.ptr,
                                                          p.empty_safe.ptr, p.view.bx, p.view.by, p.view.bz, state);
   check(cudaGetLastError(), "skip_bits_kernel launch");
-  const uint32_t words = static_cast<uint32_t>(p.free2.count);
-  cell_pairs_kernel<<<ceil_div(words, 256), 256, 0, s>>>(p.free_cells.ptr, p.observed_cells.ptr, p.free2.ptr,
-                                                         p.empty2.ptr, p.cx / 32, p.cy, p.cz, state);
-  check(cudaGetLastError(), "cell_pairs_kernel launch");
 }
 
 void launch_fill_volume(Pipeline& p, cudaStream_t s) {

@@ -243,11 +243,7 @@ struct Pipeline {
   DeviceArray<uint32_t> observed_blocks; // some voxel observed
   DeviceArray<uint32_t> safe_blocks;     // free, with all 26 neighbours free
   DeviceArray<uint32_t> empty_safe;      // no observed voxel in the 3x3x3 neighbourhood
-  DeviceArray<uint32_t> observed_cells;  // one bit per 2x2x2 voxel cell: some voxel observed
-  DeviceArray<uint32_t> free_cells;      // one bit per cell: all eight voxels observed, tsdf exactly 1
-  DeviceArray<uint32_t> free2;           // cell c: the cells {c, c+1}^3 are all free
-  DeviceArray<uint32_t> empty2;          // cell c: none of the cells {c, c+1}^3 is observed
-  uint32_t cx = 0, cy = 0, cz = 0;       // cell extent
+  DeviceArray<uint32_t> voxel_bits;      // per brick: 16 words "tsdf exactly 1", 16 words "observed"
   // Block culling of the full sweep
   DeviceArray<float> depth_tiles;        // max depth per 8x8 pixel tile, then coarser levels
   DeviceArray<uint32_t> block_list;

@@ -14,7 +14,7 @@
 //  * 8^3 blocks whose 3x3x3 block neighbourhood is entirely free space (or
 //    entirely unobserved) are crossed in one go, replaying the march's
 //    ray_length additions up to the block exit;
-//  * otherwise 2x2x2-voxel cell bits decide single samples.
+//  * otherwise per-voxel bits (observed / exactly 1) decide single samples.
 // The sample positions, and therefore the output, are those of the plain
 // march.  Samples before the volume box are replayed the same way, and the
 // march ends once the ray has left the box.
@@ -201,6 +201,73 @@ struct Sampler {
   }
 };
 
+// Corner masks of the trilinear stencil with base voxel (sx, sy, sz), read
+// from the per-voxel skip bits (16 words "tsdf exactly 1" + 16 words
+// "observed" per brick).  Bit c of each mask is corner (c & 1, (c >> 1) & 1,
+// c >> 2), the sampler's blend order.  A corner outside the volume is missing:
+// neither "one" nor "observed".
+__device__ __forceinline__ void stencil_masks(const uint32_t* __restrict__ bits, const VolumeDev& v, int sx, int sy,
+                                              int sz, uint32_t& observed, uint32_t& one) {
+  if (sx >= 0 && sy >= 0 && sz >= 0 && (sx & 7) != 7 && (sy & 7) != 7 && (sz & 7) != 7 &&
+      sx + 1 < static_cast<int>(v.rx) && sy + 1 < static_cast<int>(v.ry) && sz + 1 < static_cast<int>(v.rz)) {
+    const uint32_t brick = ((static_cast<uint32_t>(sz) >> 3) * v.by + (static_cast<uint32_t>(sy) >> 3)) * v.bx +
+                           (static_cast<uint32_t>(sx) >> 3);
+    // one z-layer of a brick is 64 bits (two words); the stencil's four
+    // corners in a layer sit at bits y*8+x + {0, 1, 8, 9}
+    const uint2* b = reinterpret_cast<const uint2*>(bits + static_cast<size_t>(brick) * 32u);
+    const uint32_t lz = static_cast<uint32_t>(sz) & 7u;
+    const uint32_t shift = (static_cast<uint32_t>(sy) & 7u) * 8u + (static_cast<uint32_t>(sx) & 7u);
+    const uint2 n0 = __ldg(b + lz), n1 = __ldg(b + lz + 1u), o0 = __ldg(b + 8u + lz), o1 = __ldg(b + 9u + lz);
+    auto quad = [shift](uint2 layer) {
+      const uint64_t l = ((static_cast<uint64_t>(layer.y) << 32) | layer.x) >> shift;
+      return static_cast<uint32_t>((l & 3u) | ((l >> 6) & 0xCu));
+    };
+    one = quad(n0) | (quad(n1) << 4);
+    observed = quad(o0) | (quad(o1) << 4);
+    return;
+  }
+  one = 0u;
+  observed = 0u;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int x = sx + (c & 1), y = sy + ((c >> 1) & 1), z = sz + (c >> 2);
+    if (x < 0 || y < 0 || z < 0 || x >= static_cast<int>(v.rx) || y >= static_cast<int>(v.ry) ||
+        z >= static_cast<int>(v.rz)) {
+      continue;
+    }
+    const uint32_t brick = ((static_cast<uint32_t>(z) >> 3) * v.by + (static_cast<uint32_t>(y) >> 3)) * v.bx +
+                           (static_cast<uint32_t>(x) >> 3);
+    const uint32_t idx = brick_offset(static_cast<uint32_t>(x), static_cast<uint32_t>(y), static_cast<uint32_t>(z));
+    const uint32_t* w = bits + static_cast<size_t>(brick) * 32u;
+    one |= ((__ldg(w + (idx >> 5)) >> (idx & 31u)) & 1u) << c;
+    observed |= ((__ldg(w + 16u + (idx >> 5)) >> (idx & 31u)) & 1u) << c;
+  }
+}
+
+// What the sampler returns for a stencil, decided from its corner masks
+// without reading a voxel: 1 = exactly 1.0, 2 = nullopt, 0 = needs the
+// gather.  With every observed corner exactly 1, the blend's numerator and
+// denominator are the same sum of weights, so the value is 1.0 whenever the
+// weight sum passes the sampler's 1e-6 test (the sum is recomputed here from
+// the fractional position, in the sampler's order).
+__device__ __forceinline__ int stencil_class(uint32_t observed, uint32_t one, int policy, f3 g) {
+  if (observed == 0u) return 2;
+  if (policy == KF_CORNERS_REQUIRE_ALL && observed != 0xFFu) return 2;
+  if (one != observed) return 0;
+  if (observed == 0xFFu) return 1;  // the eight weights sum to 1 within rounding
+  const f3 gg = make(g.x - 0.5f, g.y - 0.5f, g.z - 0.5f);
+  const f3 fr = gg - make(floorf(gg.x), floorf(gg.y), floorf(gg.z));
+  float ws = 0.0f;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    if (!((observed >> c) & 1u)) continue;
+    const float w = ((c & 1) ? fr.x : 1.0f - fr.x) * (((c >> 1) & 1) ? fr.y : 1.0f - fr.y) *
+                    ((c >> 2) ? fr.z : 1.0f - fr.z);
+    ws += w;
+  }
+  return ws <= 1.0e-6f ? 2 : 1;
+}
+
 // Ray parameter where the ray leaves block (bxi, byi, bzi).  Approximate:
 // samples within rounding distance of the face still lie in the block's
 // one-block safety neighbourhood.
@@ -247,8 +314,7 @@ __device__ __forceinline__ void box_range(const VolumeDev& v, f3 o, f3 d, float&
 template <int Kind, bool Color>
 __global__ void __launch_bounds__(64)
     raycast_kernel(VolumeDev v, const uint32_t* __restrict__ free_safe, const uint32_t* __restrict__ empty_safe,
-                   const uint32_t* __restrict__ free2, const uint32_t* __restrict__ empty2, uint32_t cells_x,
-                   uint32_t cells_y,
+                   const uint32_t* __restrict__ voxel_bits,
                    RaycastParams rp, Intr k, uint32_t width,
                    uint32_t height, Rigid pose, const IcpState* __restrict__ state, float* __restrict__ points,
                    float* __restrict__ normals, uint32_t* __restrict__ colors) {
@@ -301,9 +367,9 @@ __global__ void __launch_bounds__(64)
     while (ray_length <= rp.max_depth) {
       if (ray_length > t_out) break;
       const f3 point = pose.t + (dir * ray_length);
-      if (free2 != nullptr) {
-        // Exact skip (see the file comment): decide the sample from the cell
-        // pair bits of its stencil's base cell, and cross whole safe blocks.
+      if (voxel_bits != nullptr) {
+        // Exact skip (see the file comment): decide the sample from the
+        // per-voxel bits of its stencil, and cross whole safe blocks.
         const f3 g = (point - v.origin) * v.inv_voxel_size;
         if (!(g.x >= 0.0f && g.y >= 0.0f && g.z >= 0.0f && g.x < static_cast<float>(v.rx) &&
               g.y < static_cast<float>(v.ry) && g.z < static_cast<float>(v.rz))) {
@@ -313,17 +379,9 @@ __global__ void __launch_bounds__(64)
         }
         const int sx = static_cast<int>(floorf(g.x - 0.5f)), sy = static_cast<int>(floorf(g.y - 0.5f)),
                   sz = static_cast<int>(floorf(g.z - 0.5f));
-        const size_t cell = (static_cast<size_t>(max(sz, 0) >> 1) * cells_y + static_cast<size_t>(max(sy, 0) >> 1)) *
-                                cells_x + static_cast<size_t>(max(sx, 0) >> 1);
-        const uint32_t cbit = 1u << (cell & 31u);
-        const bool stencil_inside = sx >= 0 && sy >= 0 && sz >= 0 && sx + 1 < static_cast<int>(v.rx) &&
-                                    sy + 1 < static_cast<int>(v.ry) && sz + 1 < static_cast<int>(v.rz);
-        int cls = 0;
-        if (stencil_inside && (__ldg(free2 + (cell >> 5)) & cbit)) {
-          cls = 1;
-        } else if (__ldg(empty2 + (cell >> 5)) & cbit) {
-          cls = 2;
-        }
+        uint32_t observed, one;
+        stencil_masks(voxel_bits, v, sx, sy, sz, observed, one);
+        const int cls = stencil_class(observed, one, rp.policy, g);
         if (cls != 0) {
           const uint32_t bxi = static_cast<uint32_t>(g.x) >> 3, byi = static_cast<uint32_t>(g.y) >> 3,
                          bzi = static_cast<uint32_t>(g.z) >> 3;
@@ -411,9 +469,8 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
   const uint32_t* empty_safe = p.safe_blocks.count ? p.empty_safe.ptr : nullptr;
   const dim3 block(8, 8);
   const dim3 grid(ceil_div(cam.width, 8), ceil_div(cam.height, 8));
-  const uint32_t* free2 = p.safe_blocks.count ? p.free2.ptr : nullptr;
-  const uint32_t* empty2 = p.safe_blocks.count ? p.empty2.ptr : nullptr;
-  raycast_kernel<Kind, Color><<<grid, block, 0, s>>>(p.view, free_safe, empty_safe, free2, empty2, p.cx, p.cy, rp, intr_from(cam.intrinsics), cam.width,
+  const uint32_t* voxel_bits = p.safe_blocks.count && p.view.grid == nullptr ? p.voxel_bits.ptr : nullptr;
+  raycast_kernel<Kind, Color><<<grid, block, 0, s>>>(p.view, free_safe, empty_safe, voxel_bits, rp, intr_from(cam.intrinsics), cam.width,
                                                      cam.height, rigid_from(cam.camera_to_world), state, points,
                                                      normals, colors);
   check(cudaGetLastError(), "raycast_kernel launch");
