@@ -201,9 +201,8 @@ __global__ void __launch_bounds__(kBlockThreads)
     integrate_blocks_kernel(VolumeDev v, const float4* __restrict__ table, uint32_t width, uint32_t height, Intr k,
                             Rigid T, IntegParams ip, const IcpState* __restrict__ state,
                             const uint32_t* __restrict__ list, const unsigned* __restrict__ count,
-                            uint32_t* __restrict__ free_bits, uint32_t* __restrict__ observed_bits,
-                            uint32_t* __restrict__ voxel_bits, unsigned long long* __restrict__ counters) {
-  __shared__ uint32_t s_one[16];
+                            uint32_t* __restrict__ voxel_bits, uint32_t* __restrict__ dirty_bits,
+                            unsigned long long* __restrict__ counters) {
   using VT = VoxelTraits<Kind>;
   using Raw = typename VT::Raw;
   if (state != nullptr) {
@@ -271,44 +270,34 @@ __global__ void __launch_bounds__(kBlockThreads)
       }
     }
     // ---- skip bits of the raycast ---------------------------------------
-    // Per voxel: `one` (observed with tsdf exactly 1) and `observed`, 512 +
-    // 512 bits per brick stored as 16 + 16 words (one 128-byte line).  A warp
-    // holds 32 consecutive voxels of the brick for each of its four z, i.e.
+    // Per voxel: `one` (observed with tsdf exactly 1) and `observed`.  A
+    // brick layer z is 16 bytes: words 4z, 4z+1 hold `one`, 4z+2, 4z+3 hold
+    // `observed`, bit (y & 3) * 8 + x of word (y >> 2).  A warp holds 32
+    // consecutive voxels of one layer half for each of its four z, i.e.
     // exactly one word: ballots give the new bits of the voxels fused this
     // frame, the other bits are kept.
     uint32_t* bits = voxel_bits + static_cast<size_t>(block) * 32u;
     const uint32_t half = (threadIdx.x >> 5) & 1u;
-    uint32_t any_observed = 0u;
+    uint32_t changed = 0u;
 #pragma unroll
     for (uint32_t i = 0; i < 4; ++i) {
       const uint32_t fused = __ballot_sync(0xFFFFFFFFu, (fused_z >> i) & 1u);
       const uint32_t ones = __ballot_sync(0xFFFFFFFFu, (one_z >> i) & 1u);
-      if ((threadIdx.x & 31u) == 0) {
-        const uint32_t w = 2u * (lz + i) + half;
-        const uint32_t one = (__ldcg(bits + w) & ~fused) | (ones & fused);
-        const uint32_t obs = __ldcg(bits + 16u + w) | fused;
-        if (fused) {
+      if ((threadIdx.x & 31u) == 0 && fused != 0u) {
+        const uint32_t w = 4u * (lz + i) + half;
+        const uint32_t old_one = __ldcg(bits + w), old_obs = __ldcg(bits + w + 2u);
+        const uint32_t one = (old_one & ~fused) | (ones & fused);
+        const uint32_t obs = old_obs | fused;
+        if (one != old_one || obs != old_obs) {
           bits[w] = one;
-          bits[16u + w] = obs;
+          bits[w + 2u] = obs;
+          changed = 1u;
         }
-        s_one[w] = one;
-        any_observed |= obs;
       }
     }
-    const bool block_observed = __syncthreads_or(any_observed != 0u);
-    if (threadIdx.x == 0) {
-      uint32_t all = 0xFFFFFFFFu;
-#pragma unroll
-      for (int w = 0; w < 16; ++w) all &= s_one[w];
-      const uint32_t bit = 1u << (block & 31u);
-      if (all == 0xFFFFFFFFu) {
-        atomicOr(free_bits + (block >> 5), bit);
-      } else {
-        atomicAnd(free_bits + (block >> 5), ~bit);
-      }
-      if (block_observed) atomicOr(observed_bits + (block >> 5), bit);
+    if (__syncthreads_or(changed != 0u) && threadIdx.x == 0) {
+      atomicOr(dirty_bits + (block >> 5), 1u << (block & 31u));
     }
-    __syncthreads();
   }
   const unsigned total = __reduce_add_sync(0xFFFFFFFFu, updates);
   const unsigned total_color = __reduce_add_sync(0xFFFFFFFFu, color_updates);
@@ -318,44 +307,79 @@ __global__ void __launch_bounds__(kBlockThreads)
   }
 }
 
-// The march's skip bits from the per-block bits: free blocks whose 26
-// neighbours are free (and inside the volume); blocks whose 3x3x3
-// neighbourhood holds no observed voxel (outside neighbours hold none).
-__global__ void skip_bits_kernel(const uint32_t* __restrict__ free_bits, const uint32_t* __restrict__ observed_bits,
-                                 uint32_t* __restrict__ free_safe, uint32_t* __restrict__ empty_safe, uint32_t bx,
-                                 uint32_t by, uint32_t bz, const IcpState* __restrict__ state) {
+// Stencil bits of one brick layer from the per-voxel bits of the brick and
+// its +x, +y, +z neighbours (missing neighbours: no voxel observed).  Bit
+// y*8+x of the result describes the trilinear stencil whose base corner is
+// voxel (x, y, z) of the brick, i.e. corners (x..x+1, y..y+1, z..z+1).  Only
+// bricks whose stencils reach a brick changed this frame are rewritten.
+__device__ __forceinline__ uint64_t lo64(uint4 l) { return (static_cast<uint64_t>(l.y) << 32) | l.x; }
+__device__ __forceinline__ uint64_t hi64(uint4 l) { return (static_cast<uint64_t>(l.w) << 32) | l.z; }
+// value at (x+1, y) for every (x, y); column x = 7 from the +x neighbour's column 0
+__device__ __forceinline__ uint64_t next_x(uint64_t a, uint64_t ax) {
+  return ((a >> 1) & 0x7F7F7F7F7F7F7F7Full) | ((ax & 0x0101010101010101ull) << 7);
+}
+// value at (x, y+1); row y = 7 from the +y neighbour's row 0
+__device__ __forceinline__ uint64_t next_y(uint64_t a, uint64_t ay) { return (a >> 8) | (ay << 56); }
+
+__global__ void stencil_bits_kernel(const uint4* __restrict__ voxel_bits, uint4* __restrict__ stencil_bits,
+                                    uint8_t* __restrict__ brick_class, const uint32_t* __restrict__ dirty,
+                                    uint32_t bx, uint32_t by, uint32_t bz, int require_all,
+                                    const IcpState* __restrict__ state) {
   if (state != nullptr && state->failed) return;
-  const uint32_t block = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t total = bx * by * bz;
-  bool fs = false, es = false;
-  if (block < total) {
-    const int x = static_cast<int>(block % bx), y = static_cast<int>((block / bx) % by),
-              z = static_cast<int>(block / (bx * by));
-    fs = true;
-    es = true;
-    for (int dz = -1; dz <= 1; ++dz) {
-      for (int dy = -1; dy <= 1; ++dy) {
-        for (int dx = -1; dx <= 1; ++dx) {
-          const int nx = x + dx, ny = y + dy, nz = z + dz;
-          if (nx < 0 || ny < 0 || nz < 0 || nx >= static_cast<int>(bx) || ny >= static_cast<int>(by) ||
-              nz >= static_cast<int>(bz)) {
-            fs = false;
-            continue;
-          }
-          const uint32_t nb = (static_cast<uint32_t>(nz) * by + static_cast<uint32_t>(ny)) * bx + static_cast<uint32_t>(nx);
-          const uint32_t bit = 1u << (nb & 31u);
-          if (!(__ldg(free_bits + (nb >> 5)) & bit)) fs = false;
-          if (__ldg(observed_bits + (nb >> 5)) & bit) es = false;
-        }
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t brick = t >> 3, z = t & 7u;
+  bool work = false;
+  const uint32_t x0 = brick % bx, y0 = (brick / bx) % by, z0 = brick / (bx * by);
+  if (brick < bx * by * bz) {
+#pragma unroll
+    for (uint32_t c = 0; c < 8; ++c) {
+      const uint32_t nx = x0 + (c & 1u), ny = y0 + ((c >> 1) & 1u), nz = z0 + (c >> 2);
+      if (nx < bx && ny < by && nz < bz) {
+        const uint32_t nb = (nz * by + ny) * bx + nx;
+        work |= ((__ldg(dirty + (nb >> 5)) >> (nb & 31u)) & 1u) != 0u;
       }
     }
   }
-  // 32 consecutive blocks share a word: assemble it in the warp, one store.
-  const unsigned fw = __ballot_sync(0xFFFFFFFFu, fs);
-  const unsigned ew = __ballot_sync(0xFFFFFFFFu, es);
-  if ((threadIdx.x & 31u) == 0 && block < total) {
-    free_safe[block >> 5] = fw;
-    empty_safe[block >> 5] = ew;
+  uint64_t undecided = 0u, one = 0u;
+  if (work) {
+    uint64_t any_obs = 0u, all_obs = ~0ull, no_bad = ~0ull;
+#pragma unroll
+    for (uint32_t dz = 0; dz < 2; ++dz) {
+      const uint32_t lz = z + dz, nz = z0 + (lz >> 3);
+      uint4 q[4];  // (x, y), (x+1, y), (x, y+1), (x+1, y+1) bricks, this layer
+#pragma unroll
+      for (uint32_t c = 0; c < 4; ++c) {
+        const uint32_t nx = x0 + (c & 1u), ny = y0 + (c >> 1);
+        q[c] = nx < bx && ny < by && nz < bz
+                   ? __ldg(voxel_bits + static_cast<size_t>((nz * by + ny) * bx + nx) * 8u + (lz & 7u))
+                   : make_uint4(0u, 0u, 0u, 0u);
+      }
+      // observed
+      const uint64_t o = hi64(q[0]), ox = hi64(q[1]), oy = hi64(q[2]), oxy = hi64(q[3]);
+      const uint64_t o1 = next_x(o, ox), o2 = next_y(o, oy), o3 = next_y(o1, next_x(oy, oxy));
+      any_obs |= o | o1 | o2 | o3;
+      all_obs &= o & o1 & o2 & o3;
+      // observed implies exactly 1
+      const uint64_t b = lo64(q[0]) | ~o, bxn = lo64(q[1]) | ~ox, byn = lo64(q[2]) | ~oy, bxy = lo64(q[3]) | ~oxy;
+      const uint64_t b1 = next_x(b, bxn), b2 = next_y(b, byn), b3 = next_y(b1, next_x(byn, bxy));
+      no_bad &= b & b1 & b2 & b3;
+    }
+    one = all_obs & no_bad;
+    // REQUIRE_ALL: a missing corner gives nullopt; otherwise only a stencil
+    // without any observed corner does
+    const uint64_t decided = require_all ? (~all_obs | no_bad) : (~any_obs | one);
+    undecided = ~decided;
+    stencil_bits[static_cast<size_t>(brick) * 8u + z] =
+        make_uint4(static_cast<uint32_t>(undecided), static_cast<uint32_t>(undecided >> 32),
+                   static_cast<uint32_t>(one), static_cast<uint32_t>(one >> 32));
+  }
+  // brick summary from its eight layers (eight consecutive lanes)
+  const uint32_t all_null = __ballot_sync(0xFFFFFFFFu, undecided == 0u && one == 0u);
+  const uint32_t all_one = __ballot_sync(0xFFFFFFFFu, one == ~0ull);
+  if (work && z == 0) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t n8 = (all_null >> lane) & 0xFFu, o8 = (all_one >> lane) & 0xFFu;
+    brick_class[brick] = static_cast<uint8_t>(n8 == 0xFFu ? 1u : (o8 == 0xFFu ? 2u : 0u));
   }
 }
 
@@ -399,8 +423,8 @@ void launch_blocks_typed(Pipeline& p, const float4* table, uint32_t width, uint3
                          const IntegParams& ip, const IcpState* state, cudaStream_t s) {
   if (state == nullptr && p.kernel_start != nullptr) check(cudaEventRecord(p.kernel_start, s), "event record");
   integrate_blocks_kernel<Kind, Color><<<148 * 12, kBlockThreads, 0, s>>>(
-      p.view, table, width, height, k, T, ip, state, p.block_list.ptr, p.block_count.ptr, p.free_blocks.ptr,
-      p.observed_blocks.ptr, p.voxel_bits.ptr, p.counters.ptr);
+      p.view, table, width, height, k, T, ip, state, p.block_list.ptr, p.block_count.ptr, p.voxel_bits.ptr,
+      p.brick_dirty.ptr, p.counters.ptr);
   check(cudaGetLastError(), "integrate_blocks_kernel launch");
   if (state == nullptr && p.kernel_stop != nullptr) check(cudaEventRecord(p.kernel_stop, s), "event record");
 }
@@ -410,14 +434,13 @@ void launch_blocks_typed(Pipeline& p, const float4* table, uint32_t width, uint3
 void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t s) {
   const uint32_t blocks = p.view.bx * p.view.by * p.view.bz;
   const size_t words = (blocks + 31) / 32;
-  if (p.free_blocks.count != words) {
-    p.free_blocks.resize(words);
-    p.observed_blocks.resize(words);
-    p.safe_blocks.resize(words);
-    p.empty_safe.resize(words);
+  if (p.brick_dirty.count != words) {
     p.block_list.resize(blocks);
     p.block_count.resize(1);
     p.voxel_bits.resize(static_cast<size_t>(blocks) * 32u);
+    p.stencil_bits.resize(static_cast<size_t>(blocks) * 32u);
+    p.brick_dirty.resize(words);
+    p.brick_class.resize(blocks);
     reset_blocks(p, s);
   }
   // depth-tile pyramid geometry for this frame size
@@ -439,13 +462,12 @@ void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t s
 }
 
 void reset_blocks(Pipeline& p, cudaStream_t s) {
-  if (p.free_blocks.count == 0) return;
-  check(cudaMemsetAsync(p.free_blocks.ptr, 0, p.free_blocks.bytes(), s), "skip bits reset");
-  check(cudaMemsetAsync(p.observed_blocks.ptr, 0, p.observed_blocks.bytes(), s), "skip bits reset");
-  check(cudaMemsetAsync(p.safe_blocks.ptr, 0, p.safe_blocks.bytes(), s), "skip bits reset");
+  if (p.brick_dirty.count == 0) return;
+  // nothing observed: every stencil is decided nullopt
   check(cudaMemsetAsync(p.voxel_bits.ptr, 0, p.voxel_bits.bytes(), s), "skip bits reset");
-  // nothing observed: every block is empty-safe
-  check(cudaMemsetAsync(p.empty_safe.ptr, 0xFF, p.empty_safe.bytes(), s), "skip bits reset");
+  check(cudaMemsetAsync(p.stencil_bits.ptr, 0, p.stencil_bits.bytes(), s), "skip bits reset");
+  check(cudaMemsetAsync(p.brick_class.ptr, 1, p.brick_class.bytes(), s), "skip bits reset");
+  check(cudaMemsetAsync(p.brick_dirty.ptr, 0, p.brick_dirty.bytes(), s), "skip bits reset");
 }
 
 void launch_pixel_table(const uint16_t* depth, const uint32_t* color, const float* normals, uint32_t width,
@@ -479,6 +501,7 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
   cp.width = width;
   cp.height = height;
   check(cudaMemsetAsync(p.block_count.ptr, 0, sizeof(unsigned), s), "block count clear");
+  check(cudaMemsetAsync(p.brick_dirty.ptr, 0, p.brick_dirty.bytes(), s), "dirty bits clear");
   const uint32_t blocks = p.view.bx * p.view.by * p.view.bz;
   cull_blocks_kernel<<<ceil_div(blocks, 256), 256, 0, s>>>(p.view, T, k, p.depth_tiles.ptr, lv, cp, state,
                                                            p.block_list.ptr, p.block_count.ptr);
@@ -506,9 +529,11 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
       break;
   }
   // raycast skip bits
-  skip_bits_kernel<<<ceil_div(blocks, 256), 256, 0, s>>>(p.free_blocks.ptr, p.observed_blocks.ptr, p.safe_blocks.ptr,
-                                                         p.empty_safe.ptr, p.view.bx, p.view.by, p.view.bz, state);
-  check(cudaGetLastError(), "skip_bits_kernel launch");
+  stencil_bits_kernel<<<ceil_div(blocks * 8u, 256), 256, 0, s>>>(
+      reinterpret_cast<const uint4*>(p.voxel_bits.ptr), reinterpret_cast<uint4*>(p.stencil_bits.ptr),
+      p.brick_class.ptr, p.brick_dirty.ptr, p.view.bx, p.view.by, p.view.bz, p.config.raycast.corner_policy == KF_CORNERS_REQUIRE_ALL,
+      state);
+  check(cudaGetLastError(), "stencil_bits_kernel launch");
 }
 
 void launch_fill_volume(Pipeline& p, cudaStream_t s) {

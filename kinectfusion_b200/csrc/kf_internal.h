@@ -238,12 +238,18 @@ struct Pipeline {
   DeviceArray<float4> colors;
   size_t voxel_bytes = 0;
   uint64_t voxel_count = 0;
-  // Exact empty-space skip, one bit per 8^3 block (x-major block order):
-  DeviceArray<uint32_t> free_blocks;     // every voxel observed with tsdf exactly 1
-  DeviceArray<uint32_t> observed_blocks; // some voxel observed
-  DeviceArray<uint32_t> safe_blocks;     // free, with all 26 neighbours free
-  DeviceArray<uint32_t> empty_safe;      // no observed voxel in the 3x3x3 neighbourhood
-  DeviceArray<uint32_t> voxel_bits;      // per brick: 16 words "tsdf exactly 1", 16 words "observed"
+  // Exact empty-space skip of the raycast (8^3 bricks, x-major order).
+  // Per-voxel bits, per brick 8 layers (z) of 16 bytes: 64 bits "observed
+  // with tsdf exactly 1" then 64 bits "observed", bit y*8+x.
+  DeviceArray<uint32_t> voxel_bits;
+  // Per stencil base voxel, same layout: 64 bits "undecided" then 64 bits
+  // "exactly 1.0" (when decided and clear: nullopt), for the trilinear
+  // stencil based at that voxel under the pipeline's corner policy.
+  DeviceArray<uint32_t> stencil_bits;
+  DeviceArray<uint32_t> brick_dirty;     // per brick: voxel bits changed this frame
+  // Per brick: 1 = every stencil based in the brick is nullopt, 2 = every
+  // one is exactly 1.0 (all eight corners observed with tsdf exactly 1).
+  DeviceArray<uint8_t> brick_class;
   // Block culling of the full sweep
   DeviceArray<float> depth_tiles;        // max depth per 8x8 pixel tile, then coarser levels
   DeviceArray<uint32_t> block_list;

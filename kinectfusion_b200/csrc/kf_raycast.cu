@@ -7,14 +7,19 @@
 // expression order, so a render is bit-identical to the CPU raycast of the
 // same volume and camera.
 //
-// Empty-space skip, exact, at two granularities.  A sample whose eight
-// corners are all observed with tsdf exactly 1 is exactly 1.0 (the blend
-// divides a sum by the identical sum); a sample with no observed corner is
-// nullopt.  Neither needs the corner gather:
-//  * 8^3 blocks whose 3x3x3 block neighbourhood is entirely free space (or
-//    entirely unobserved) are crossed in one go, replaying the march's
-//    ray_length additions up to the block exit;
-//  * otherwise per-voxel bits (observed / exactly 1) decide single samples.
+// Empty-space skip, exact.  A sample whose eight corners are all observed
+// with tsdf exactly 1 is exactly 1.0 (the blend divides a sum by the
+// identical sum), and so is one whose observed corners are all exactly 1
+// when their weights pass the sampler's 1e-6 test; a sample with no observed
+// corner (or, under REQUIRE_ALL, a missing one) is nullopt.  None of these
+// needs the corner gather.  The integration pass keeps, per stencil base
+// voxel, bits that decide this class where the corners alone settle it, and
+// per 8^3 brick whether every stencil based in it is nullopt or exactly 1.0:
+//  * a sample in such a brick and of that class crosses the brick in one go,
+//    replaying the march's ray_length additions while the samples' bases
+//    stay in the brick;
+//  * otherwise the per-base bits decide single samples, and the per-voxel
+//    bits settle the partially observed ones.
 // The sample positions, and therefore the output, are those of the plain
 // march.  Samples before the volume box are replayed the same way, and the
 // march ends once the ray has left the box.
@@ -24,6 +29,9 @@
 
 namespace kf {
 namespace {
+
+// Rays left in a warp at or below which they march cooperatively.
+constexpr int kCoopLanes = 8;
 
 struct RaycastParams {
   float min_depth, max_depth, step_scale;
@@ -143,20 +151,20 @@ struct Sampler {
     return true;
   }
 
-  // trilinear::central_normal (trilinear.hpp:243-266)
+  // trilinear::central_normal (trilinear.hpp:243-266).  The six samples
+  // are independent reads of an unchanging volume, so all are taken before
+  // any is tested: the result is that of the reference's early-exit order.
   __device__ bool central_normal(f3 p, int policy, f3& out) const {
     const float vs = v.voxel_size;
-    float plus, minus;
-    if (!tsdf(make(p.x + vs, p.y + 0.0f, p.z + 0.0f), policy, plus)) return false;
-    if (!tsdf(make(p.x - vs, p.y - 0.0f, p.z - 0.0f), policy, minus)) return false;
-    const float gx = plus - minus;
-    if (!tsdf(make(p.x + 0.0f, p.y + vs, p.z + 0.0f), policy, plus)) return false;
-    if (!tsdf(make(p.x - 0.0f, p.y - vs, p.z - 0.0f), policy, minus)) return false;
-    const float gy = plus - minus;
-    if (!tsdf(make(p.x + 0.0f, p.y + 0.0f, p.z + vs), policy, plus)) return false;
-    if (!tsdf(make(p.x - 0.0f, p.y - 0.0f, p.z - vs), policy, minus)) return false;
-    const float gz = plus - minus;
-    const f3 d = make(gx, gy, gz);
+    float xp = 0.0f, xm = 0.0f, yp = 0.0f, ym = 0.0f, zp = 0.0f, zm = 0.0f;
+    const bool ok = tsdf(make(p.x + vs, p.y + 0.0f, p.z + 0.0f), policy, xp) &
+                    tsdf(make(p.x - vs, p.y - 0.0f, p.z - 0.0f), policy, xm) &
+                    tsdf(make(p.x + 0.0f, p.y + vs, p.z + 0.0f), policy, yp) &
+                    tsdf(make(p.x - 0.0f, p.y - vs, p.z - 0.0f), policy, ym) &
+                    tsdf(make(p.x + 0.0f, p.y + 0.0f, p.z + vs), policy, zp) &
+                    tsdf(make(p.x - 0.0f, p.y - 0.0f, p.z - vs), policy, zm);
+    if (!ok) return false;
+    const f3 d = make(xp - xm, yp - ym, zp - zm);
     const float length = norm(d);
     if (length <= 0.0f) return false;
     out = d / length;
@@ -202,28 +210,27 @@ struct Sampler {
 };
 
 // Corner masks of the trilinear stencil with base voxel (sx, sy, sz), read
-// from the per-voxel skip bits (16 words "tsdf exactly 1" + 16 words
-// "observed" per brick).  Bit c of each mask is corner (c & 1, (c >> 1) & 1,
-// c >> 2), the sampler's blend order.  A corner outside the volume is missing:
-// neither "one" nor "observed".
+// from the per-voxel bits (per brick layer z, 16 bytes: 64 bits "tsdf
+// exactly 1", 64 bits "observed", bit y*8+x).  Bit c of each mask is corner
+// (c & 1, (c >> 1) & 1, c >> 2), the sampler's blend order.  A corner outside
+// the volume is missing: neither "one" nor "observed".
 __device__ __forceinline__ void stencil_masks(const uint32_t* __restrict__ bits, const VolumeDev& v, int sx, int sy,
                                               int sz, uint32_t& observed, uint32_t& one) {
   if (sx >= 0 && sy >= 0 && sz >= 0 && (sx & 7) != 7 && (sy & 7) != 7 && (sz & 7) != 7 &&
       sx + 1 < static_cast<int>(v.rx) && sy + 1 < static_cast<int>(v.ry) && sz + 1 < static_cast<int>(v.rz)) {
     const uint32_t brick = ((static_cast<uint32_t>(sz) >> 3) * v.by + (static_cast<uint32_t>(sy) >> 3)) * v.bx +
                            (static_cast<uint32_t>(sx) >> 3);
-    // one z-layer of a brick is 64 bits (two words); the stencil's four
-    // corners in a layer sit at bits y*8+x + {0, 1, 8, 9}
-    const uint2* b = reinterpret_cast<const uint2*>(bits + static_cast<size_t>(brick) * 32u);
+    // the stencil's four corners in a layer sit at bits y*8+x + {0, 1, 8, 9}
+    const uint4* b = reinterpret_cast<const uint4*>(bits) + static_cast<size_t>(brick) * 8u;
     const uint32_t lz = static_cast<uint32_t>(sz) & 7u;
     const uint32_t shift = (static_cast<uint32_t>(sy) & 7u) * 8u + (static_cast<uint32_t>(sx) & 7u);
-    const uint2 n0 = __ldg(b + lz), n1 = __ldg(b + lz + 1u), o0 = __ldg(b + 8u + lz), o1 = __ldg(b + 9u + lz);
-    auto quad = [shift](uint2 layer) {
-      const uint64_t l = ((static_cast<uint64_t>(layer.y) << 32) | layer.x) >> shift;
+    const uint4 l0 = __ldg(b + lz), l1 = __ldg(b + lz + 1u);
+    auto quad = [shift](uint32_t lo, uint32_t hi) {
+      const uint64_t l = ((static_cast<uint64_t>(hi) << 32) | lo) >> shift;
       return static_cast<uint32_t>((l & 3u) | ((l >> 6) & 0xCu));
     };
-    one = quad(n0) | (quad(n1) << 4);
-    observed = quad(o0) | (quad(o1) << 4);
+    one = quad(l0.x, l0.y) | (quad(l1.x, l1.y) << 4);
+    observed = quad(l0.z, l0.w) | (quad(l1.z, l1.w) << 4);
     return;
   }
   one = 0u;
@@ -237,10 +244,11 @@ __device__ __forceinline__ void stencil_masks(const uint32_t* __restrict__ bits,
     }
     const uint32_t brick = ((static_cast<uint32_t>(z) >> 3) * v.by + (static_cast<uint32_t>(y) >> 3)) * v.bx +
                            (static_cast<uint32_t>(x) >> 3);
-    const uint32_t idx = brick_offset(static_cast<uint32_t>(x), static_cast<uint32_t>(y), static_cast<uint32_t>(z));
-    const uint32_t* w = bits + static_cast<size_t>(brick) * 32u;
-    one |= ((__ldg(w + (idx >> 5)) >> (idx & 31u)) & 1u) << c;
-    observed |= ((__ldg(w + 16u + (idx >> 5)) >> (idx & 31u)) & 1u) << c;
+    const size_t word = static_cast<size_t>(brick) * 32u + (static_cast<uint32_t>(z) & 7u) * 4u +
+                          ((static_cast<uint32_t>(y) >> 2) & 1u);
+    const uint32_t bit = (static_cast<uint32_t>(y) & 3u) * 8u + (static_cast<uint32_t>(x) & 7u);
+    one |= ((__ldg(bits + word) >> bit) & 1u) << c;
+    observed |= ((__ldg(bits + word + 2u) >> bit) & 1u) << c;
   }
 }
 
@@ -268,17 +276,122 @@ __device__ __forceinline__ int stencil_class(uint32_t observed, uint32_t one, in
   return ws <= 1.0e-6f ? 2 : 1;
 }
 
-// Ray parameter where the ray leaves block (bxi, byi, bzi).  Approximate:
-// samples within rounding distance of the face still lie in the block's
-// one-block safety neighbourhood.
-__device__ __forceinline__ float block_exit(const VolumeDev& v, f3 o, f3 inv_dir, uint32_t bxi, uint32_t byi,
-                                            uint32_t bzi) {
-  const float edge = 8.0f * v.voxel_size;
-  const f3 lo = v.origin + make(static_cast<float>(bxi), static_cast<float>(byi), static_cast<float>(bzi)) * edge;
-  const float tx = ((inv_dir.x >= 0.0f ? lo.x + edge : lo.x) - o.x) * inv_dir.x;
-  const float ty = ((inv_dir.y >= 0.0f ? lo.y + edge : lo.y) - o.y) * inv_dir.y;
-  const float tz = ((inv_dir.z >= 0.0f ? lo.z + edge : lo.z) - o.z) * inv_dir.z;
-  return fminf(tx, fminf(ty, tz));
+// The grid position of a sample is inside the volume (TrilinearSampler's
+// bounds test; outside, the sample is nullopt).
+__device__ __forceinline__ bool in_grid(const VolumeDev& v, f3 g) {
+  return g.x >= 0.0f && g.y >= 0.0f && g.z >= 0.0f && g.x < static_cast<float>(v.rx) &&
+         g.y < static_cast<float>(v.ry) && g.z < static_cast<float>(v.rz);
+}
+
+// Record of the per-base stencil bits holding the stencil of grid position
+// g, the bit of that stencil in the record's 64-bit halves, and the brick
+// of the base voxel.  Returns false when the base voxel lies below the
+// volume (g < 0.5 on an axis); there is no record then.
+struct Slot {
+  uint32_t record, bit, bx, by, bz;
+};
+__device__ __forceinline__ bool stencil_slot(const VolumeDev& v, f3 g, Slot& s) {
+  const int sx = static_cast<int>(floorf(g.x - 0.5f)), sy = static_cast<int>(floorf(g.y - 0.5f)),
+            sz = static_cast<int>(floorf(g.z - 0.5f));
+  if (sx < 0 || sy < 0 || sz < 0) return false;
+  const uint32_t ux = static_cast<uint32_t>(sx), uy = static_cast<uint32_t>(sy), uz = static_cast<uint32_t>(sz);
+  s.bx = ux >> 3;
+  s.by = uy >> 3;
+  s.bz = uz >> 3;
+  s.record = ((s.bz * v.by + s.by) * v.bx + s.bx) * 8u + (uz & 7u);
+  s.bit = (uy & 7u) * 8u + (ux & 7u);
+  return true;
+}
+
+// Class of a stencil from its record: 1 = exactly 1.0, 2 = nullopt, 0 = not
+// decided by the stencil bits.
+__device__ __forceinline__ int record_class(uint4 r, uint32_t bit) {
+  const uint32_t undecided = bit < 32u ? r.x >> bit : r.y >> (bit - 32u);
+  const uint32_t one = bit < 32u ? r.z >> bit : r.w >> (bit - 32u);
+  if (undecided & 1u) return 0;
+  return (one & 1u) ? 1 : 2;
+}
+
+// Ray parameter up to which the samples' stencil bases stay in brick
+// (bxi, byi, bzi): the sample's grid position stays in the brick shifted by
+// half a voxel, [8b + 0.5, 8b + 8.5) per axis, clipped to the volume when
+// `clip` is set.  The ray is taken as g0 + gdir * t in grid units; `margin`
+// (voxels) shrinks the box by more than the rounding that separates this
+// line from the march's own sample positions, so every sample before the
+// returned parameter has its base in the brick.
+__device__ __forceinline__ float brick_exit(const VolumeDev& v, f3 g0, f3 inv_gdir, uint32_t bxi, uint32_t byi,
+                                            uint32_t bzi, bool clip, float margin) {
+  auto axis = [margin, clip](float g, float inv, uint32_t b, uint32_t extent) {
+    const float lo = static_cast<float>(b * 8u) + 0.5f + margin;
+    float hi = static_cast<float>(b * 8u) + 8.5f - margin;
+    if (clip) hi = fminf(hi, static_cast<float>(extent) - margin);
+    return ((inv >= 0.0f ? hi : lo) - g) * inv;
+  };
+  return fminf(axis(g0.x, inv_gdir.x, bxi, v.rx), fminf(axis(g0.y, inv_gdir.y, byi, v.ry),
+                                                          axis(g0.z, inv_gdir.z, bzi, v.rz)));
+}
+
+// A march sample: nullopt, a value, or past the march's end.
+enum : int { kNull = 0, kValue = 1, kEnd = 2 };
+// What a sample does to the march: nothing, a zero crossing, the end.
+enum : int { kNone = 0, kFound = 1, kStop = 2 };
+
+// The sample at `point` (find_zero_crossing's volume.tsdf, raycasting.hpp:
+// 176-205): kNull or kValue with its value in `tsdf`.  With the skip
+// structures, a sample the stencil bits decide needs no corner gather, and
+// `jump` gets its brick (bit 31 | x | y << 10 | z << 20) when every stencil
+// of that brick has the sample's class.
+template <int Kind>
+__device__ __forceinline__ int march_sample(const Sampler<Kind>& s, const VolumeDev& v,
+                                            const uint32_t* __restrict__ voxel_bits,
+                                            const uint4* __restrict__ stencil_bits,
+                                            const uint8_t* __restrict__ brick_class, int policy, f3 point,
+                                            float& tsdf, uint32_t& jump) {
+  jump = 0u;
+  if (voxel_bits != nullptr) {
+    const f3 g = (point - v.origin) * v.inv_voxel_size;
+    if (!in_grid(v, g)) return kNull;
+    Slot slot;
+    int cls = 0, summary = 0;
+    if (stencil_slot(v, g, slot)) {
+      const uint4 rec = __ldg(stencil_bits + slot.record);
+      summary = __ldg(brick_class + (slot.record >> 3));
+      cls = record_class(rec, slot.bit);
+    }
+    if (cls == 0) {
+      uint32_t observed, one;
+      stencil_masks(voxel_bits, v, static_cast<int>(floorf(g.x - 0.5f)), static_cast<int>(floorf(g.y - 0.5f)),
+                    static_cast<int>(floorf(g.z - 0.5f)), observed, one);
+      cls = stencil_class(observed, one, policy, g);
+    }
+    if (cls != 0) {
+      if (summary == (cls == 1 ? 2 : 1) && slot.bx < 1024u && slot.by < 1024u && slot.bz < 1024u) {
+        jump = 0x80000000u | slot.bx | (slot.by << 10) | (slot.bz << 20);
+      }
+      if (cls == 2) return kNull;
+      tsdf = 1.0f;
+      return kValue;
+    }
+  }
+  return s.tsdf(point, policy, tsdf) ? kValue : kNull;
+}
+
+// find_zero_crossing's tests of a sample against the previous one
+// (raycasting.hpp:186-203): a crossing from positive to non-positive gives
+// the interpolated surface; a rise from negative to positive ends the march.
+__device__ __forceinline__ int sample_event(int kind, float tsdf, f3 point, bool p_have, float p_tsdf, f3 p_point,
+                                            f3& surf) {
+  if (kind == kEnd) return kStop;
+  if (kind == kValue && p_have) {
+    if (p_tsdf > 0.0f && tsdf <= 0.0f) {
+      const float gap = p_tsdf - tsdf;
+      const float alpha = gap != 0.0f ? p_tsdf / gap : 0.0f;
+      surf = p_point + ((point - p_point) * alpha);
+      return kFound;
+    }
+    if (p_tsdf < 0.0f && tsdf > 0.0f) return kStop;
+  }
+  return kNone;
 }
 
 // Ray parameters where the ray enters and leaves the volume box, widened by
@@ -311,26 +424,29 @@ __device__ __forceinline__ void box_range(const VolumeDev& v, f3 o, f3 d, float&
   }
 }
 
-template <int Kind, bool Color>
+template <int Kind>
 __global__ void __launch_bounds__(64)
-    raycast_kernel(VolumeDev v, const uint32_t* __restrict__ free_safe, const uint32_t* __restrict__ empty_safe,
-                   const uint32_t* __restrict__ voxel_bits,
+    raycast_kernel(VolumeDev v, const uint32_t* __restrict__ voxel_bits, const uint4* __restrict__ stencil_bits,
+                   const uint8_t* __restrict__ brick_class,
                    RaycastParams rp, Intr k, uint32_t width,
-                   uint32_t height, Rigid pose, const IcpState* __restrict__ state, float* __restrict__ points,
-                   float* __restrict__ normals, uint32_t* __restrict__ colors) {
+                   uint32_t height, Rigid pose, const IcpState* __restrict__ state, float* __restrict__ points) {
   if (state != nullptr) {
     if (state->failed) return;
     const float* c = state->camera;
     pose = Rigid{{c[0], c[1], c[2]}, {c[3], c[4], c[5]}, {c[6], c[7], c[8]}, {c[9], c[10], c[11]}};
   }
+  // Every lane of a warp takes part in the march's rounds (lanes without a
+  // ray are done from the start), so that the warp reconverges at each
+  // sample instead of running its lanes' divergent marches one after
+  // another.
   const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t row = blockIdx.y * blockDim.y + threadIdx.y;
-  if (col >= width || row >= height) return;
-  const size_t pix = static_cast<size_t>(row) * width + col;
+  const bool in_image = col < width && row < height;
+  const size_t pix = in_image ? static_cast<size_t>(row) * width + col : 0;
   const Sampler<Kind> s{v};
 
   float seed = rp.min_depth;
-  if (rp.seed_previous) {
+  if (rp.seed_previous && in_image) {
     const f3 previous = load3(points + pix * 3);
     if (finite3(previous) && dot(previous, previous) > 0.0f) {
       const float previous_depth = norm(previous - pose.t);
@@ -338,115 +454,206 @@ __global__ void __launch_bounds__(64)
       seed = rp.min_depth < truncated ? truncated : rp.min_depth;
     }
   }
-  f3 out_point = nan3(), out_normal = nan3();
-  uint32_t out_color = 0;
 
   const f3 translated = back_project(k, static_cast<float>(col), static_cast<float>(row), 1.0f);
   const f3 direction = rotate(pose, translated);
   const float dn = norm(direction);
-  if (dn > 0.0f) {
-    const f3 dir = direction / dn;
-    // find_zero_crossing (raycasting.hpp:165-211)
-    const float base_step = v.voxel_size * rp.step_scale;
-    // The step taken after a sample of exactly 1.0 (observed free space).
-    const float precomp_one = 1.0f * v.truncation * rp.step_scale;
-    const float free_step = base_step < precomp_one ? precomp_one : base_step;
-    bool have_prev = false;
-    float prev_tsdf = 0.0f;
-    f3 prev_point = make(0.0f, 0.0f, 0.0f);
-    float ray_length = seed;
-    bool found = false;
-    f3 surface = make(0.0f, 0.0f, 0.0f);
-    // Samples outside the volume box are nullopt: replay the base steps up
-    // to the box, and stop once the ray has left it (a box is convex).
-    float t_in, t_out;
-    box_range(v, pose.t, dir, t_in, t_out);
-    const f3 inv_dir = make(dir.x != 0.0f ? 1.0f / dir.x : 1e30f, dir.y != 0.0f ? 1.0f / dir.y : 1e30f,
-                            dir.z != 0.0f ? 1.0f / dir.z : 1e30f);
+  bool done = !(in_image && dn > 0.0f);
+  const f3 dir = done ? make(0.0f, 0.0f, 1.0f) : direction / dn;
+  // find_zero_crossing (raycasting.hpp:165-211)
+  const float base_step = v.voxel_size * rp.step_scale;
+  // The step taken after a sample of exactly 1.0 (observed free space).
+  const float precomp_one = 1.0f * v.truncation * rp.step_scale;
+  const float free_step = base_step < precomp_one ? precomp_one : base_step;
+  bool have_prev = false;
+  float prev_tsdf = 0.0f;
+  f3 prev_point = make(0.0f, 0.0f, 0.0f);
+  float ray_length = seed;
+  bool found = false;
+  f3 surface = make(0.0f, 0.0f, 0.0f);
+  // Samples outside the volume box are nullopt: replay the base steps up
+  // to the box, and stop once the ray has left it (a box is convex).
+  float t_in, t_out;
+  box_range(v, pose.t, dir, t_in, t_out);
+  // The ray in grid units for brick exits, and the margin that covers the
+  // rounding of the samples' own positions (grows with the coordinates).
+  const f3 g0 = (pose.t - v.origin) * v.inv_voxel_size;
+  const f3 gdir = dir * v.inv_voxel_size;
+  const f3 inv_gdir = make(gdir.x != 0.0f ? 1.0f / gdir.x : 1e30f, gdir.y != 0.0f ? 1.0f / gdir.y : 1e30f,
+                           gdir.z != 0.0f ? 1.0f / gdir.z : 1e30f);
+  const float reach = fmaxf(fabsf(g0.x), fmaxf(fabsf(g0.y), fabsf(g0.z))) +
+                      fmaxf(fabsf(gdir.x), fmaxf(fabsf(gdir.y), fabsf(gdir.z))) * fmaxf(fabsf(t_out), 1.0f) +
+                      static_cast<float>(max(v.rx, max(v.ry, v.rz)));
+  const float margin = (1.0f / 64.0f) + reach * 4.0e-6f;
+  if (!done) {
     while (ray_length < t_in && ray_length <= rp.max_depth) ray_length += base_step;
-    while (ray_length <= rp.max_depth) {
-      if (ray_length > t_out) break;
-      const f3 point = pose.t + (dir * ray_length);
-      if (voxel_bits != nullptr) {
-        // Exact skip (see the file comment): decide the sample from the
-        // per-voxel bits of its stencil, and cross whole safe blocks.
-        const f3 g = (point - v.origin) * v.inv_voxel_size;
-        if (!(g.x >= 0.0f && g.y >= 0.0f && g.z >= 0.0f && g.x < static_cast<float>(v.rx) &&
-              g.y < static_cast<float>(v.ry) && g.z < static_cast<float>(v.rz))) {
-          have_prev = false;  // outside the grid: nullopt
-          ray_length += base_step;
-          continue;
-        }
-        const int sx = static_cast<int>(floorf(g.x - 0.5f)), sy = static_cast<int>(floorf(g.y - 0.5f)),
-                  sz = static_cast<int>(floorf(g.z - 0.5f));
-        uint32_t observed, one;
-        stencil_masks(voxel_bits, v, sx, sy, sz, observed, one);
-        const int cls = stencil_class(observed, one, rp.policy, g);
-        if (cls != 0) {
-          const uint32_t bxi = static_cast<uint32_t>(g.x) >> 3, byi = static_cast<uint32_t>(g.y) >> 3,
-                         bzi = static_cast<uint32_t>(g.z) >> 3;
-          const uint32_t block = (bzi * v.by + byi) * v.bx + bxi;
-          const uint32_t bbit = 1u << (block & 31u);
-          const bool block_safe = (__ldg((cls == 1 ? free_safe : empty_safe) + (block >> 5)) & bbit) != 0u;
-          const float t_exit = block_safe ? block_exit(v, pose.t, inv_dir, bxi, byi, bzi) : 0.0f;
-          if (cls == 1) {
-            // Exactly 1.0: leaving a surface from behind ends the march at
-            // the first such sample; after it every step is free_step.
-            if (have_prev && prev_tsdf < 0.0f) break;
-            float last = ray_length;
-            do {
-              last = ray_length;
-              ray_length += free_step;
-            } while (ray_length < t_exit && ray_length <= rp.max_depth);
-            have_prev = true;
-            prev_tsdf = 1.0f;
-            prev_point = last == ray_length ? point : pose.t + (dir * last);
-          } else {
-            have_prev = false;  // nullopt
-            do {
-              ray_length += base_step;
-            } while (ray_length < t_exit && ray_length <= rp.max_depth);
-          }
-          continue;
-        }
-      }
-      float tsdf;
-      if (!s.tsdf(point, rp.policy, tsdf)) {
-        have_prev = false;
-        ray_length += base_step;
-        continue;
-      }
-      if (have_prev && prev_tsdf > 0.0f && tsdf <= 0.0f) {
-        const float gap = prev_tsdf - tsdf;
-        const float alpha = gap != 0.0f ? prev_tsdf / gap : 0.0f;
-        surface = prev_point + ((point - prev_point) * alpha);
-        found = true;
-        break;
-      }
-      if (have_prev && prev_tsdf < 0.0f && tsdf > 0.0f) break;
-      have_prev = true;
-      prev_tsdf = tsdf;
-      prev_point = point;
+  }
+  float spec = free_step;  // the step the ray's last sample implies
+  // The step after a sample (find_zero_crossing's advance, raycasting.hpp:
+  // 204-209): nullopt and non-positive values take the base step.
+  auto step_after = [&](int kind, float tsdf) {
+    if (kind == kValue && tsdf > 0.0f) {
       const float precomp = tsdf * v.truncation * rp.step_scale;
-      const float step = base_step < precomp ? precomp : base_step;
-      ray_length += tsdf > 0.0f ? step : base_step;
+      return base_step < precomp ? precomp : base_step;
     }
-    if (found) {
-      // write_surface_sample (raycasting.hpp:215-245)
-      f3 n;
-      const bool has_normal = rp.cell_normals ? s.cell_normal(surface, n) : s.central_normal(surface, rp.policy, n);
-      if (has_normal) {
-        out_point = surface;
-        out_normal = n;
-        if constexpr (Color) {
-          f3 c;
-          if (s.color(surface, c)) out_color = pixel_from_color(c);
-        } else {
-          const f3 view = normalized(pose.t - surface);
-          const float d = dot(n, view);
-          const float intensity = 255.0f * (0.0f < d ? d : 0.0f);
-          out_color = pixel_from_color(make(intensity, intensity, intensity));
+    return base_step;
+  };
+  // Take a sample (known kind and event) into the march state; a decided
+  // sample whose brick holds only its class also takes every following
+  // sample up to the brick exit.
+  auto apply = [&](int event, int kind, float tsdf, f3 point, float r, uint32_t jump, f3 surf) {
+    if (event == kFound) {
+      found = true;
+      surface = surf;
+      done = true;
+      return;
+    }
+    if (event == kStop) {
+      done = true;
+      return;
+    }
+    const float step = step_after(kind, tsdf);
+    float last = r, next = r + step;
+    if (jump != 0u) {
+      const float t_exit = brick_exit(v, g0, inv_gdir, jump & 1023u, (jump >> 10) & 1023u, (jump >> 20) & 1023u,
+                                      kind == kValue, margin);
+      while (next < t_exit && next <= rp.max_depth && !(next > t_out)) {
+        last = next;
+        next += step;
+      }
+    }
+    have_prev = kind == kValue;
+    prev_tsdf = tsdf;
+    prev_point = last == r ? point : pose.t + (dir * last);
+    ray_length = next;
+    spec = step;
+  };
+
+  const unsigned lane = (threadIdx.y * blockDim.x + threadIdx.x) & 31u;
+  unsigned live;
+  while ((live = __ballot_sync(0xFFFFFFFFu, !done)) != 0u) {
+    const int n = __popc(live);
+    if (n > kCoopLanes) {
+      // every live lane takes the next sample of its own ray
+      if (!done) {
+        const float r = ray_length;
+        int kind = kEnd;
+        float tsdf = 0.0f;
+        uint32_t jump = 0u;
+        f3 point = make(0.0f, 0.0f, 0.0f);
+        if (r <= rp.max_depth && !(r > t_out)) {
+          point = pose.t + (dir * r);
+          kind = march_sample(s, v, voxel_bits, stencil_bits, brick_class, rp.policy, point, tsdf, jump);
         }
+        f3 surf = make(0.0f, 0.0f, 0.0f);
+        const int event = sample_event(kind, tsdf, point, have_prev, prev_tsdf, prev_point, surf);
+        apply(event, kind, tsdf, point, r, jump, surf);
+      }
+      continue;
+    }
+    // Few rays left: each live ray gets a segment of G lanes, lane `off` of
+    // which takes the sample `off` steps ahead, assuming every step until
+    // then equals the ray's last one.  The samples up to the first one that
+    // ends the march or takes another step are exactly the march's next
+    // samples; the ray takes them all in this round.
+    const int lg = n > 8 ? 1 : (n > 4 ? 2 : (n > 2 ? 3 : (n > 1 ? 4 : 5)));
+    const unsigned G = 1u << lg;
+    const unsigned seg = lane >> lg, off = lane & (G - 1u);
+    const bool active = seg < static_cast<unsigned>(n);
+    unsigned owner = lane;
+    if (active) {
+      unsigned m = live;
+      for (unsigned i = 0; i < seg; ++i) m &= m - 1u;
+      owner = static_cast<unsigned>(__ffs(m) - 1);
+    }
+    const float o_r = __shfl_sync(0xFFFFFFFFu, ray_length, owner);
+    const float o_s = __shfl_sync(0xFFFFFFFFu, spec, owner);
+    const float o_tout = __shfl_sync(0xFFFFFFFFu, t_out, owner);
+    const f3 o_dir = make(__shfl_sync(0xFFFFFFFFu, dir.x, owner), __shfl_sync(0xFFFFFFFFu, dir.y, owner),
+                          __shfl_sync(0xFFFFFFFFu, dir.z, owner));
+    const bool o_hp = __shfl_sync(0xFFFFFFFFu, have_prev ? 1 : 0, owner) != 0;
+    const float o_pt = __shfl_sync(0xFFFFFFFFu, prev_tsdf, owner);
+    const f3 o_pp = make(__shfl_sync(0xFFFFFFFFu, prev_point.x, owner),
+                         __shfl_sync(0xFFFFFFFFu, prev_point.y, owner),
+                         __shfl_sync(0xFFFFFFFFu, prev_point.z, owner));
+    float r = o_r;
+    for (unsigned i = 0; i < off; ++i) r += o_s;
+    int kind = kEnd;
+    float tsdf = 0.0f;
+    uint32_t jump = 0u;
+    f3 point = make(0.0f, 0.0f, 0.0f);
+    if (active && r <= rp.max_depth && !(r > o_tout)) {
+      point = pose.t + (o_dir * r);
+      kind = march_sample(s, v, voxel_bits, stencil_bits, brick_class, rp.policy, point, tsdf, jump);
+    }
+    // the state before this sample: the previous lane's sample, or the ray's
+    const int up_kind = __shfl_up_sync(0xFFFFFFFFu, kind, 1);
+    const float up_tsdf = __shfl_up_sync(0xFFFFFFFFu, tsdf, 1);
+    const f3 up_point = make(__shfl_up_sync(0xFFFFFFFFu, point.x, 1), __shfl_up_sync(0xFFFFFFFFu, point.y, 1),
+                             __shfl_up_sync(0xFFFFFFFFu, point.z, 1));
+    f3 surf = make(0.0f, 0.0f, 0.0f);
+    const int event = off == 0 ? sample_event(kind, tsdf, point, o_hp, o_pt, o_pp, surf)
+                               : sample_event(kind, tsdf, point, up_kind == kValue, up_tsdf, up_point, surf);
+    const bool stop = !active || event != kNone || !(step_after(kind, tsdf) == o_s);
+    const unsigned stops = __ballot_sync(0xFFFFFFFFu, stop);
+    // each live lane reads the last sample its segment took
+    unsigned src = lane;
+    if (!done) {
+      const unsigned base = static_cast<unsigned>(__popc(live & ((1u << lane) - 1u))) << lg;
+      const unsigned mine = (stops >> base) & (G == 32u ? 0xFFFFFFFFu : ((1u << G) - 1u));
+      src = base + (mine != 0u ? static_cast<unsigned>(__ffs(mine) - 1) : G - 1u);
+    }
+    const int m_event = __shfl_sync(0xFFFFFFFFu, event, src);
+    const int m_kind = __shfl_sync(0xFFFFFFFFu, kind, src);
+    const float m_r = __shfl_sync(0xFFFFFFFFu, r, src);
+    const float m_tsdf = __shfl_sync(0xFFFFFFFFu, tsdf, src);
+    const uint32_t m_jump = __shfl_sync(0xFFFFFFFFu, jump, src);
+    const f3 m_point = make(__shfl_sync(0xFFFFFFFFu, point.x, src), __shfl_sync(0xFFFFFFFFu, point.y, src),
+                            __shfl_sync(0xFFFFFFFFu, point.z, src));
+    const f3 m_surf = make(__shfl_sync(0xFFFFFFFFu, surf.x, src), __shfl_sync(0xFFFFFFFFu, surf.y, src),
+                           __shfl_sync(0xFFFFFFFFu, surf.z, src));
+    if (!done) apply(m_event, m_kind, m_tsdf, m_point, m_r, m_jump, m_surf);
+  }
+  if (in_image) store3(points + pix * 3, found ? surface : nan3());
+}
+
+// write_surface_sample (raycasting.hpp:215-245) for every pixel whose march
+// found a zero crossing (its point is finite): the normal, then the colour
+// or the shading; without a normal the pixel has no surface.
+template <int Kind, bool Color>
+__global__ void __launch_bounds__(128)
+    surface_kernel(VolumeDev v, RaycastParams rp, uint32_t width, uint32_t height, Rigid pose,
+                   const IcpState* __restrict__ state, float* __restrict__ points, float* __restrict__ normals,
+                   uint32_t* __restrict__ colors) {
+  if (state != nullptr) {
+    if (state->failed) return;
+    if constexpr (!Color) {  // the shading needs the camera position
+      const float* c = state->camera;
+      pose = Rigid{{c[0], c[1], c[2]}, {c[3], c[4], c[5]}, {c[6], c[7], c[8]}, {c[9], c[10], c[11]}};
+    }
+  }
+  const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t row = blockIdx.y * blockDim.y + threadIdx.y;
+  if (col >= width || row >= height) return;
+  const size_t pix = static_cast<size_t>(row) * width + col;
+  const Sampler<Kind> s{v};
+  const f3 surface = load3(points + pix * 3);
+  f3 out_point = nan3(), out_normal = nan3();
+  uint32_t out_color = 0;
+  if (finite3(surface)) {
+    f3 n;
+    const bool has_normal = rp.cell_normals ? s.cell_normal(surface, n) : s.central_normal(surface, rp.policy, n);
+    if (has_normal) {
+      out_point = surface;
+      out_normal = n;
+      if constexpr (Color) {
+        f3 c;
+        if (s.color(surface, c)) out_color = pixel_from_color(c);
+      } else {
+        const f3 view = normalized(pose.t - surface);
+        const float d = dot(n, view);
+        const float intensity = 255.0f * (0.0f < d ? d : 0.0f);
+        out_color = pixel_from_color(make(intensity, intensity, intensity));
       }
     }
   }
@@ -465,15 +672,20 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
   rp.policy = p.config.raycast.corner_policy;
   rp.cell_normals = p.config.raycast.cell_gradient_normals;
   rp.seed_previous = p.config.raycast.seed_from_previous;
-  const uint32_t* free_safe = p.safe_blocks.count ? p.safe_blocks.ptr : nullptr;
-  const uint32_t* empty_safe = p.safe_blocks.count ? p.empty_safe.ptr : nullptr;
   const dim3 block(8, 8);
   const dim3 grid(ceil_div(cam.width, 8), ceil_div(cam.height, 8));
-  const uint32_t* voxel_bits = p.safe_blocks.count && p.view.grid == nullptr ? p.voxel_bits.ptr : nullptr;
-  raycast_kernel<Kind, Color><<<grid, block, 0, s>>>(p.view, free_safe, empty_safe, voxel_bits, rp, intr_from(cam.intrinsics), cam.width,
-                                                     cam.height, rigid_from(cam.camera_to_world), state, points,
-                                                     normals, colors);
+  // the skip structures exist once a full-sweep integration prepared them
+  const uint32_t* voxel_bits = p.brick_class.count && p.view.grid == nullptr ? p.voxel_bits.ptr : nullptr;
+  const uint4* stencil_bits = reinterpret_cast<const uint4*>(p.stencil_bits.ptr);
+  const Rigid pose = rigid_from(cam.camera_to_world);
+  raycast_kernel<Kind><<<grid, block, 0, s>>>(p.view, voxel_bits, stencil_bits, p.brick_class.ptr, rp,
+                                              intr_from(cam.intrinsics), cam.width, cam.height, pose, state, points);
   check(cudaGetLastError(), "raycast_kernel launch");
+  const dim3 sblock(32, 4);
+  const dim3 sgrid(ceil_div(cam.width, 32), ceil_div(cam.height, 4));
+  surface_kernel<Kind, Color><<<sgrid, sblock, 0, s>>>(p.view, rp, cam.width, cam.height, pose, state, points,
+                                                       normals, colors);
+  check(cudaGetLastError(), "surface_kernel launch");
 }
 
 }  // namespace
