@@ -481,6 +481,7 @@ kf_status kf_tracker_create(const kf_icp_options* options, kf_tracker** out) {
       t->impl.state.resize(1);
       t->impl.partials.resize(static_cast<size_t>(kIcpMaxGrid) * kIcpSlot);
       t->impl.staging.resize(1);
+      prepare_icp_kernels();
       check(cudaMemset(t->impl.state.ptr, 0, sizeof(IcpState)), "tracker state init");
       const kf_rigid identity = {{1, 0, 0, 0, 1, 0, 0, 0, 1}, {0, 0, 0}};
       launch_icp_set_pose(t->impl.state.ptr, identity, 1, 0);

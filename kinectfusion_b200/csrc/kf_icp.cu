@@ -29,6 +29,28 @@ __device__ __forceinline__ Rigid rigid_load(const float* c) {
   return Rigid{{c[0], c[1], c[2]}, {c[3], c[4], c[5]}, {c[6], c[7], c[8]}, {c[9], c[10], c[11]}};
 }
 
+// The model half of CorrespondenceSearch::match and
+// IcpCorrespondence::from_match (icp_correspondence.hpp:270-294, 52-74):
+// `source` is the live vertex in world coordinates, (mv, mn) the model
+// point and normal the live pixel projects to.
+__device__ __forceinline__ bool finish_match(f3 source, f3 ln, f3 mv, f3 mn, const Rigid& cam, float max_d,
+                                             float min_dot, float* j, float& residual, float& distance) {
+  if (!finite3(mv) || !finite3(mn)) return false;
+  const f3 sn = normalized(rotate(cam, ln));
+  distance = norm(source - mv);
+  if (distance > max_d) return false;
+  if (dot(sn, mn) < min_dot) return false;
+  const f3 rot = cross(source, mn);
+  j[0] = rot.x;
+  j[1] = rot.y;
+  j[2] = rot.z;
+  j[3] = mn.x;
+  j[4] = mn.y;
+  j[5] = mn.z;
+  residual = dot(mn, mv - source);
+  return true;
+}
+
 // CorrespondenceSearch::match + IcpCorrespondence::from_match.
 __device__ __forceinline__ bool match(const IcpLevelArgs& a, const Rigid& cam, const Rigid& model,
                                       float max_d, float min_dot, uint32_t x, uint32_t y, float* j,
@@ -47,22 +69,8 @@ __device__ __forceinline__ bool match(const IcpLevelArgs& a, const Rigid& cam, c
     return false;
   }
   const size_t mi = static_cast<size_t>(my) * a.model_width + static_cast<size_t>(mx);
-  const f3 mv = ldg3(a.model_points + mi * 3);
-  const f3 mn = ldg3(a.model_normals + mi * 3);
-  if (!finite3(mv) || !finite3(mn)) return false;
-  const f3 sn = normalized(rotate(cam, ln));
-  distance = norm(source - mv);
-  if (distance > max_d) return false;
-  if (dot(sn, mn) < min_dot) return false;
-  const f3 rot = cross(source, mn);
-  j[0] = rot.x;
-  j[1] = rot.y;
-  j[2] = rot.z;
-  j[3] = mn.x;
-  j[4] = mn.y;
-  j[5] = mn.z;
-  residual = dot(mn, mv - source);
-  return true;
+  return finish_match(source, ln, ldg3(a.model_points + mi * 3), ldg3(a.model_normals + mi * 3), cam, max_d,
+                      min_dot, j, residual, distance);
 }
 
 // ---- FP64 6x6 linear algebra ------------------------------------------------
@@ -412,7 +420,7 @@ __device__ void pose_to_rigid_floats(const double* pose, float* out) {
 }
 
 // One Gauss-Newton / LM step of estimate_with on the combined sums.
-__device__ void gauss_newton_step(IcpState* st, const float* sums_in, unsigned long long count_in,
+__device__ __noinline__ void gauss_newton_step(IcpState* st, const float* sums_in, unsigned long long count_in,
                                   const IcpParams& p, bool want_values) {
   float sums[kIcpSums];
   for (int i = 0; i < kIcpSums; ++i) sums[i] = sums_in[i];
@@ -493,15 +501,14 @@ __device__ void gauss_newton_step(IcpState* st, const float* sums_in, unsigned l
   }
 }
 
-// Two CTAs per SM so that a 296-CTA level-0 sweep runs in one wave; the
-// rarely taken FP64 paths of the solve spill instead.
-template <bool Solve>
+// Two CTAs per SM (the FP64 solve is a separate function and spills there,
+// not here).  Pix live pixels per thread and grid step.
+template <bool Solve, int Pix>
 __global__ void __launch_bounds__(kIcpBlock, 2)
     icp_iteration_kernel(IcpLevelArgs a, IcpState* __restrict__ st, float* __restrict__ partials, IcpParams p,
                          int want_values) {
   __shared__ int s_flag;
   __shared__ float s_warp[kIcpBlock / 32][kIcpSlot];
-  __shared__ unsigned s_warp_count[kIcpBlock / 32];
   __shared__ float s_total[kIcpSlot];
   __shared__ unsigned long long s_count;
   if (threadIdx.x == 0) s_flag = (st->status != kIcpRunning);
@@ -510,57 +517,97 @@ __global__ void __launch_bounds__(kIcpBlock, 2)
 
   const Rigid cam = rigid_load(st->camera);
   const Rigid model = rigid_load(st->model);
-  float acc[kIcpSums];
+  // acc[0..28]: the 29 sums, acc[29]: matched pixels, acc[30..31]: padding
+  float acc[32];
 #pragma unroll
-  for (int i = 0; i < kIcpSums; ++i) acc[i] = 0.0f;
-  unsigned cnt = 0;
+  for (int i = 0; i < 32; ++i) acc[i] = 0.0f;
   const uint32_t pixels = a.live_width * a.live_height;
-  for (uint32_t pix = blockIdx.x * kIcpBlock + threadIdx.x; pix < pixels; pix += gridDim.x * kIcpBlock) {
-    float j[6], residual, distance;
-    if (!match(a, cam, model, p.max_point_distance, p.min_normal_dot, pix % a.live_width, pix / a.live_width, j,
-               residual, distance)) {
-      continue;
+  const uint32_t stride = gridDim.x * kIcpBlock;
+  for (uint32_t first = blockIdx.x * kIcpBlock + threadIdx.x; first < pixels; first += stride * Pix) {
+    // Pix pixels per thread, each step of the association issued for all of
+    // them before the next, so their memory latencies overlap
+    f3 src[Pix], lnr[Pix];
+    long mi[Pix];
+#pragma unroll
+    for (int q = 0; q < Pix; ++q) {
+      const uint32_t pix = first + q * stride;
+      mi[q] = -1;
+      src[q] = lnr[q] = make(0.0f, 0.0f, 0.0f);
+      if (pix < pixels) {
+        const f3 lv = ldg3(a.live_vertices + static_cast<size_t>(pix) * 3);
+        const f3 ln = ldg3(a.live_normals + static_cast<size_t>(pix) * 3);
+        if (finite3(lv) && finite3(ln)) {
+          const f3 source = apply(cam, lv);
+          const f3 sim = apply(model, source);
+          if (finite3(sim) && sim.z > 0.0f) {
+            float px, py;
+            project(a.model_intrinsics, sim, px, py);
+            const long mx = lroundf(px), my = lroundf(py);
+            if (mx >= 0 && my >= 0 && mx < static_cast<long>(a.model_width) &&
+                my < static_cast<long>(a.model_height)) {
+              mi[q] = my * static_cast<long>(a.model_width) + mx;
+              src[q] = source;
+              lnr[q] = ln;
+            }
+          }
+        }
+      }
     }
-    int e = 0;
+    f3 mv[Pix], mn[Pix];
 #pragma unroll
-    for (int r = 0; r < 6; ++r) {
-#pragma unroll
-      for (int c = r; c < 6; ++c) {
-        acc[e] += j[r] * j[c];
-        ++e;
+    for (int q = 0; q < Pix; ++q) {
+      mv[q] = mn[q] = make(kNaN, kNaN, kNaN);
+      if (mi[q] >= 0) {
+        mv[q] = ldg3(a.model_points + static_cast<size_t>(mi[q]) * 3);
+        mn[q] = ldg3(a.model_normals + static_cast<size_t>(mi[q]) * 3);
       }
     }
 #pragma unroll
-    for (int r = 0; r < 6; ++r) acc[21 + r] += j[r] * residual;
-    acc[27] += distance;
-    acc[28] += residual * residual;
-    ++cnt;
+    for (int q = 0; q < Pix; ++q) {
+      float j[6], residual, distance;
+      if (mi[q] < 0 || !finish_match(src[q], lnr[q], mv[q], mn[q], cam, p.max_point_distance, p.min_normal_dot, j,
+                                     residual, distance)) {
+        continue;
+      }
+      int e = 0;
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+#pragma unroll
+        for (int c = r; c < 6; ++c) {
+          acc[e] += j[r] * j[c];
+          ++e;
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 6; ++r) acc[21 + r] += j[r] * residual;
+      acc[27] += distance;
+      acc[28] += residual * residual;
+      acc[29] += 1.0f;
+    }
   }
-  // warp tree (fixed butterfly order)
-#pragma unroll
-  for (int i = 0; i < kIcpSums; ++i) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) acc[i] += __shfl_xor_sync(0xFFFFFFFFu, acc[i], off);
-  }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, off);
+  // Warp: recursive halving, 31 shuffles; lane L ends with the warp's sum of
+  // value L (a fixed order).
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) {
 #pragma unroll
-    for (int i = 0; i < kIcpSums; ++i) s_warp[warp][i] = acc[i];
-    s_warp_count[warp] = cnt;
+  for (int k = 16; k >= 1; k >>= 1) {
+    const bool upper = (lane & k) != 0;
+#pragma unroll
+    for (int i = 0; i < k; ++i) {
+      const float give = upper ? acc[i] : acc[i + k];
+      const float keep = upper ? acc[i + k] : acc[i];
+      acc[i] = keep + __shfl_xor_sync(0xFFFFFFFFu, give, k);
+    }
   }
+  s_warp[warp][lane] = acc[0];
   __syncthreads();
-  if (threadIdx.x < kIcpSums) {
-    float s = 0.0f;
-    for (int w = 0; w < kIcpBlock / 32; ++w) s += s_warp[w][threadIdx.x];
-    partials[blockIdx.x * kIcpSlot + threadIdx.x] = s;
-  } else if (threadIdx.x == kIcpSums) {
-    unsigned c = 0;
-    for (int w = 0; w < kIcpBlock / 32; ++w) c += s_warp_count[w];
-    partials[blockIdx.x * kIcpSlot + kIcpSums] = __uint_as_float(c);
+  if (threadIdx.x < kIcpSlot) {
+    float sum = 0.0f;
+    for (int w = 0; w < kIcpBlock / 32; ++w) sum += s_warp[w][threadIdx.x];
+    // the count travels as integer bits in slot kIcpSums
+    partials[blockIdx.x * kIcpSlot + threadIdx.x] =
+        threadIdx.x == kIcpSums ? __uint_as_float(static_cast<unsigned>(sum)) : sum;
+    __threadfence();
   }
-  __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned ticket = atomicAdd(&st->arrived, 1u);
@@ -574,11 +621,24 @@ __global__ void __launch_bounds__(kIcpBlock, 2)
   // the eight segment results of each sum are combined in segment order.
   __shared__ float s_seg_sum[8][kIcpSlot];
   __shared__ float s_seg_comp[8][kIcpSlot];
-  __shared__ float s_parts[kIcpMaxGrid * kIcpSlot];
+  // Stage every partial in shared memory: independent coalesced loads, eight
+  // in flight per thread.
+  extern __shared__ float s_parts[];
   {
-    // stage every partial in shared memory with independent coalesced loads
     const unsigned n = gridDim.x * kIcpSlot;
-    for (unsigned e = threadIdx.x; e < n; e += kIcpBlock) s_parts[e] = __ldcg(partials + e);
+    for (unsigned e0 = threadIdx.x; e0 < n; e0 += 8 * kIcpBlock) {
+      float v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const unsigned e = e0 + u * kIcpBlock;
+        v[u] = e < n ? __ldcg(partials + e) : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const unsigned e = e0 + u * kIcpBlock;
+        if (e < n) s_parts[e] = v[u];
+      }
+    }
   }
   __syncthreads();
   {
@@ -703,8 +763,17 @@ IcpParams icp_params_from(const kf_icp_options& o) {
 }
 
 unsigned icp_grid_for(uint32_t pixels) {
-  const unsigned g = ceil_div(pixels, kIcpBlock);
+  const unsigned g = ceil_div(pixels, kIcpBlock * kIcpPixels);
   return g < static_cast<unsigned>(kIcpMaxGrid) ? (g == 0 ? 1 : g) : static_cast<unsigned>(kIcpMaxGrid);
+}
+
+void prepare_icp_kernels() {
+  const int bytes = kIcpMaxGrid * kIcpSlot * static_cast<int>(sizeof(float));
+  check(cudaFuncSetAttribute(icp_iteration_kernel<true, kIcpPixels>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+        "icp kernel attribute");
+  check(cudaFuncSetAttribute(icp_iteration_kernel<false, kIcpPixels>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             bytes),
+        "icp kernel attribute");
 }
 
 void launch_icp_level_begin(IcpState* state, float damping_lambda, cudaStream_t s) {
@@ -714,11 +783,14 @@ void launch_icp_level_begin(IcpState* state, float damping_lambda, cudaStream_t 
 
 void launch_icp_iteration(const IcpLevelArgs& args, IcpState* state, float* partials, const IcpParams& params,
                           int solve, int want_values, cudaStream_t s) {
-  const unsigned grid = icp_grid_for(args.live_width * args.live_height);
+  const uint32_t pixels = args.live_width * args.live_height;
+  const unsigned grid = icp_grid_for(pixels);
+  // dynamic shared memory: the last CTA's staging of every partial
+  const size_t smem = static_cast<size_t>(grid) * kIcpSlot * sizeof(float);
   if (solve) {
-    icp_iteration_kernel<true><<<grid, kIcpBlock, 0, s>>>(args, state, partials, params, want_values);
+    icp_iteration_kernel<true, kIcpPixels><<<grid, kIcpBlock, smem, s>>>(args, state, partials, params, want_values);
   } else {
-    icp_iteration_kernel<false><<<grid, kIcpBlock, 0, s>>>(args, state, partials, params, want_values);
+    icp_iteration_kernel<false, kIcpPixels><<<grid, kIcpBlock, smem, s>>>(args, state, partials, params, want_values);
   }
   check(cudaGetLastError(), "icp_iteration_kernel launch");
 }

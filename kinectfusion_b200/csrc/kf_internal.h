@@ -148,6 +148,7 @@ struct Pyramid {
 constexpr int kIcpSums = 29;          // 21 JtJ + 6 Jtr + distance + residual^2
 constexpr int kIcpSlot = 32;          // floats per CTA partial (29 sums + count)
 constexpr int kIcpBlock = 256;
+constexpr int kIcpPixels = 1;         // live pixels per thread and grid step of a sweep
 constexpr int kIcpMaxGrid = 2 * 148;  // two CTAs per SM on a 148-SM B200
 constexpr int kIcpRunning = -1;
 
@@ -218,6 +219,8 @@ struct IcpLevelArgs {
 
 IcpParams icp_params_from(const kf_icp_options& o);
 unsigned icp_grid_for(uint32_t pixels);
+// Per-device kernel attributes of the sweep (its shared-memory staging).
+void prepare_icp_kernels();
 // Begin a level: model world_to_camera from the current pose, status running,
 // unless a previous level failed (then the level stays skipped).
 void launch_icp_level_begin(IcpState* state, float damping_lambda, cudaStream_t stream);
