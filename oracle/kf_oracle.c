@@ -1378,3 +1378,196 @@ void kfo_icp_estimate(const float* lv, const float* ln, uint32_t lw, uint32_t lh
     out->pose_f64[i * 4 + 3] = pose.t[i];
   }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Marching cubes (MarchingCubes::extract / MeshBuilder,                    */
+/* marching_cubes.cpp:311-485) with this project's triangulation table      */
+/* (kf_mc_tables.h); every other step follows the reference.               */
+/* ------------------------------------------------------------------------ */
+#include "kf_mc_tables.h"
+
+typedef struct {
+  uint64_t* keys;
+  uint32_t* values;
+  uint64_t capacity; /* power of two */
+  uint64_t count;
+} weld_map;
+
+static uint64_t weld_hash(uint64_t k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdULL;
+  k ^= k >> 33;
+  return k;
+}
+
+static void weld_grow(weld_map* m) {
+  const uint64_t old_cap = m->capacity;
+  uint64_t* old_keys = m->keys;
+  uint32_t* old_values = m->values;
+  m->capacity = old_cap ? old_cap * 2 : 1024;
+  m->keys = (uint64_t*)malloc(m->capacity * sizeof(uint64_t));
+  m->values = (uint32_t*)malloc(m->capacity * sizeof(uint32_t));
+  for (uint64_t i = 0; i < m->capacity; ++i) m->keys[i] = UINT64_MAX;
+  for (uint64_t i = 0; i < old_cap; ++i) {
+    if (old_keys[i] == UINT64_MAX) continue;
+    uint64_t h = weld_hash(old_keys[i]) & (m->capacity - 1);
+    while (m->keys[h] != UINT64_MAX) h = (h + 1) & (m->capacity - 1);
+    m->keys[h] = old_keys[i];
+    m->values[h] = old_values[i];
+  }
+  free(old_keys);
+  free(old_values);
+}
+
+/* Returns the slot for `key`; *found tells whether it already held a vertex. */
+static uint64_t weld_slot(weld_map* m, uint64_t key, int* found) {
+  if ((m->count + 1) * 2 > m->capacity) weld_grow(m);
+  uint64_t h = weld_hash(key) & (m->capacity - 1);
+  while (m->keys[h] != UINT64_MAX) {
+    if (m->keys[h] == key) {
+      *found = 1;
+      return h;
+    }
+    h = (h + 1) & (m->capacity - 1);
+  }
+  *found = 0;
+  m->keys[h] = key;
+  ++m->count;
+  return h;
+}
+
+typedef struct {
+  const kfo_volume* v;
+  sampler s;
+  float min_weight;
+  weld_map weld;
+  float *pos, *nrm, *col;
+  uint64_t nv, cap_v;
+  uint32_t* tri;
+  uint64_t nt, cap_t;
+} mesh_builder;
+
+/* MeshBuilder::vertex_on_edge (marching_cubes.cpp:403-437) */
+static uint32_t vertex_on_edge(mesh_builder* b, uint64_t x, uint64_t y, uint64_t z, const float values[8], int edge) {
+  const kf_volume_geometry* g = &b->v->geometry;
+  const int near = kMcEdge[edge][0], far = kMcEdge[edge][1], axis = kMcEdge[edge][2];
+  const uint64_t nx = x + kMcCorner[near][0], ny = y + kMcCorner[near][1], nz = z + kMcCorner[near][2];
+  const uint64_t key = ((nz * g->res_y + ny) * g->res_x + nx) * 3u + (uint64_t)axis;
+  int found;
+  const uint64_t slot = weld_slot(&b->weld, key, &found);
+  if (found) return b->weld.values[slot];
+  const uint32_t index = (uint32_t)b->nv;
+  b->weld.values[slot] = index;
+  const float near_value = values[near], far_value = values[far];
+  const v3 near_point = cell_center(g, nx, ny, nz);
+  const v3 far_point = cell_center(g, x + kMcCorner[far][0], y + kMcCorner[far][1], z + kMcCorner[far][2]);
+  const float fraction = -near_value / (far_value - near_value);
+  const v3 position = v3add(near_point, v3mul(v3sub(far_point, near_point), fraction));
+  v3 normal = v3m(0.0f, 0.0f, 0.0f);
+  if (!central_normal(&b->s, position, KF_CORNERS_SKIP_MISSING, &normal)) normal = v3m(0.0f, 0.0f, 0.0f);
+  v3 color;
+  if (!sample_color(&b->s, position, &color)) color = v3m(255.0f, 255.0f, 255.0f);
+  if (b->nv == b->cap_v) {
+    b->cap_v = b->cap_v ? b->cap_v * 2 : 1024;
+    b->pos = (float*)realloc(b->pos, b->cap_v * 3 * sizeof(float));
+    b->nrm = (float*)realloc(b->nrm, b->cap_v * 3 * sizeof(float));
+    b->col = (float*)realloc(b->col, b->cap_v * 3 * sizeof(float));
+  }
+  v3store(b->pos + b->nv * 3, position);
+  v3store(b->nrm + b->nv * 3, normal);
+  v3store(b->col + b->nv * 3, color);
+  ++b->nv;
+  return index;
+}
+
+/* MeshBuilder::add_cell (marching_cubes.cpp:369-400); a corner that is
+ * missing, unobserved, non-finite or lighter than min_weight skips the cell */
+static void add_cell(mesh_builder* b, uint64_t x, uint64_t y, uint64_t z) {
+  float values[8];
+  unsigned cube = 0;
+  for (int c = 0; c < 8; ++c) {
+    const int64_t i = storage_index(b->v, x + kMcCorner[c][0], y + kMcCorner[c][1], z + kMcCorner[c][2]);
+    if (i < 0) return;
+    const decoded_voxel d = decode_voxel(b->v->voxel, b->v->voxels, (size_t)i);
+    if (!d.observed || !d.finite || d.weight < b->min_weight) return;
+    values[c] = d.tsdf;
+    if (values[c] < 0.0f) cube |= 1u << c;
+  }
+  if (kMcEdgeMask[cube] == 0) return;
+  for (int k = 0; kMcTriangles[cube][k] >= 0; k += 3) {
+    const uint32_t a = vertex_on_edge(b, x, y, z, values, kMcTriangles[cube][k]);
+    const uint32_t bb = vertex_on_edge(b, x, y, z, values, kMcTriangles[cube][k + 1]);
+    const uint32_t c = vertex_on_edge(b, x, y, z, values, kMcTriangles[cube][k + 2]);
+    if (b->nt == b->cap_t) {
+      b->cap_t = b->cap_t ? b->cap_t * 2 : 1024;
+      b->tri = (uint32_t*)realloc(b->tri, b->cap_t * 3 * sizeof(uint32_t));
+    }
+    b->tri[b->nt * 3] = a;
+    b->tri[b->nt * 3 + 1] = bb;
+    b->tri[b->nt * 3 + 2] = c;
+    ++b->nt;
+  }
+}
+
+/* MeshBuilder::fill_missing_normals (marching_cubes.cpp:441-456): a vertex
+ * without a gradient normal takes the normalised sum of its face normals. */
+static void fill_missing_normals(mesh_builder* b) {
+  uint8_t* missing = (uint8_t*)calloc(b->nv ? b->nv : 1, 1);
+  float* acc = (float*)calloc((b->nv ? b->nv : 1) * 3, sizeof(float));
+  for (uint64_t i = 0; i < b->nv; ++i) {
+    missing[i] = b->nrm[i * 3] == 0.0f && b->nrm[i * 3 + 1] == 0.0f && b->nrm[i * 3 + 2] == 0.0f;
+  }
+  for (uint64_t t = 0; t < b->nt; ++t) {
+    const uint32_t* tr = b->tri + t * 3;
+    const v3 p0 = v3load(b->pos + (size_t)tr[0] * 3), p1 = v3load(b->pos + (size_t)tr[1] * 3),
+             p2 = v3load(b->pos + (size_t)tr[2] * 3);
+    const v3 face = v3cross(v3sub(p1, p0), v3sub(p2, p0));
+    for (int k = 0; k < 3; ++k) {
+      if (!missing[tr[k]]) continue;
+      v3store(acc + (size_t)tr[k] * 3, v3add(v3load(acc + (size_t)tr[k] * 3), face));
+    }
+  }
+  for (uint64_t i = 0; i < b->nv; ++i) {
+    if (missing[i]) v3store(b->nrm + i * 3, v3normalized(v3load(acc + i * 3)));
+  }
+  free(missing);
+  free(acc);
+}
+
+kf_status kfo_marching_cubes(const kfo_volume* volume, float min_weight, kf_mesh* out) {
+  memset(out, 0, sizeof(*out));
+  const kf_volume_geometry* g = &volume->geometry;
+  if (g->res_x < 2 || g->res_y < 2 || g->res_z < 2) return KF_OK;
+  mesh_builder b;
+  memset(&b, 0, sizeof(b));
+  b.v = volume;
+  b.s.v = volume;
+  b.s.inv_voxel = 1.0f / g->voxel_size;
+  b.min_weight = min_weight;
+  const uint64_t cx = g->res_x - 1, cy = g->res_y - 1, cz = g->res_z - 1;
+  if (!is_sparse(volume)) {
+    for (uint64_t z = 0; z < cz; ++z)
+      for (uint64_t y = 0; y < cy; ++y)
+        for (uint64_t x = 0; x < cx; ++x) add_cell(&b, x, y, z);
+  } else {
+    /* only allocated blocks can hold the zero crossing (marching_cubes.cpp:475-485) */
+    const uint64_t bx = blocks_along(g->res_x), by = blocks_along(g->res_y), bz = blocks_along(g->res_z);
+    for (uint64_t block = 0; block < bx * by * bz; ++block) {
+      if (volume->grid[block] == 0xFFFFFFFFu) continue;
+      const uint64_t x0 = (block % bx) * 8, y0 = ((block / bx) % by) * 8, z0 = (block / (bx * by)) * 8;
+      for (uint64_t z = z0; z < z0 + 8 && z < cz; ++z)
+        for (uint64_t y = y0; y < y0 + 8 && y < cy; ++y)
+          for (uint64_t x = x0; x < x0 + 8 && x < cx; ++x) add_cell(&b, x, y, z);
+    }
+  }
+  fill_missing_normals(&b);
+  free(b.weld.keys);
+  free(b.weld.values);
+  out->positions = b.pos;
+  out->normals = b.nrm;
+  out->colors = b.col;
+  out->triangles = b.tri;
+  out->vertex_count = b.nv;
+  out->triangle_count = b.nt;
+  return KF_OK;
+}

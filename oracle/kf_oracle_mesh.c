@@ -1,5 +1,6 @@
 /*
- * kf_oracle_mesh.c - marching cubes of the oracle (filled in with the mesher).
+ * kf_oracle_mesh.c - mesh storage helpers of the oracle (the marching cubes
+ * themselves are in kf_oracle.c, next to the sampler they use).
  *
  * TEST INFRASTRUCTURE ONLY.
  */
@@ -7,13 +8,7 @@
 #include <string.h>
 
 #include "kf_oracle.h"
-
-kf_status kfo_marching_cubes(const kfo_volume* volume, float min_weight, kf_mesh* out) {
-  (void)volume;
-  (void)min_weight;
-  memset(out, 0, sizeof(*out));
-  return KF_ERR_UNSUPPORTED;
-}
+#include "kf_mc_tables.h"
 
 void kfo_mesh_free(kf_mesh* mesh) {
   free(mesh->positions);
@@ -23,6 +18,11 @@ void kfo_mesh_free(kf_mesh* mesh) {
   memset(mesh, 0, sizeof(*mesh));
 }
 
+/* Triangles per sign case of the triangulation table. */
 void kfo_mc_case_triangle_counts(int32_t* counts) {
-  for (int i = 0; i < 256; ++i) counts[i] = 0;
+  for (int i = 0; i < 256; ++i) {
+    int n = 0;
+    while (n < 5 && kMcTriangles[i][3 * n] >= 0) ++n;
+    counts[i] = n;
+  }
 }

@@ -103,3 +103,31 @@ def compare_maps(p_points, p_normals, r_points, r_normals):
             "only_reference": int((rv & ~pv).sum()),
             "max_point_distance": float(d.max()) if d.size else 0.0,
             "max_normal_angle": float(ang.max()) if ang.size else 0.0}
+
+
+def sphere_volume(vol, radius_fraction=0.3):
+    """Writes the clamped signed distance of a sphere at the volume centre into
+    a dense float oracle volume, weight 1 (tests.cpp:320-337)."""
+    g = vol.geometry
+    rx, ry, rz = vol.res
+    extent = np.float32(rx) * np.float32(g.voxel_size)
+    origin = np.array(g.origin[:], dtype=np.float32)
+    center = origin + np.float32(0.5) * extent
+    radius = np.float32(radius_fraction) * extent
+    z, y, x = np.meshgrid(np.arange(rz), np.arange(ry), np.arange(rx), indexing="ij")
+    cells = (np.stack([x, y, z], -1).astype(np.float32) + np.float32(0.5)) * np.float32(g.voxel_size) + origin
+    distance = np.linalg.norm(cells - center, axis=-1).astype(np.float32) - radius
+    tsdf = np.clip(distance / np.float32(g.truncation_distance), -1.0, 1.0).astype(np.float32)
+    vol.voxels[:, 0] = tsdf.reshape(-1)
+    vol.voxels[:, 1] = 1.0
+    return center, radius
+
+
+def mesh_edge_uses(triangles):
+    """Undirected edge -> number of triangles using it."""
+    uses = {}
+    for t in np.asarray(triangles, dtype=np.int64):
+        for a, b in ((t[0], t[1]), (t[1], t[2]), (t[2], t[0])):
+            key = (min(a, b), max(a, b))
+            uses[key] = uses.get(key, 0) + 1
+    return uses

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import kf_oracle as ko
-from fixtures import (DEPTH_1M, DEPTH_1P4M, SYNTH_IMAGE, compare_maps, compare_volumes, flat_depth,
+from fixtures import (DEPTH_1M, DEPTH_1P4M, SYNTH_IMAGE, SYNTH_VOXEL, compare_maps, compare_volumes, flat_depth,
                       identical_surface, perturbed_initial, planar_surface, synth_intrinsics, synth_volume)
 from kinectfusion_b200 import abi
 
@@ -199,3 +199,73 @@ def test_icp_f64_sums_agree_with_f32():
     s64, c64 = ko.icp_equations(v, n, v, n, k, np.eye(4), np.eye(4), 0.1, 0.9, f64=True)
     assert c32 == c64 == 9
     assert np.allclose(s32, s64, rtol=1e-5, atol=1e-7)
+
+
+# ---- marching cubes (tests.cpp:320-452) -------------------------------------------------
+def test_marching_cubes_sphere_is_closed_and_outward():
+    # tests.cpp:320-385
+    from fixtures import mesh_edge_uses, sphere_volume
+    vol = synth_volume()
+    center, radius = sphere_volume(vol)
+    mesh = ko.marching_cubes(vol)
+    p, n, t = mesh["positions"], mesh["normals"], mesh["triangles"].astype(np.int64)
+    assert len(p) > 0 and len(t) > 0 and len(n) == len(p) == len(mesh["colors"])
+    radial = p - center
+    assert (np.abs(np.linalg.norm(radial, axis=1) - radius) < vol.geometry.voxel_size).all()
+    assert ((n * radial).sum(1) > 0).all()
+    face = np.cross(p[t[:, 1]] - p[t[:, 0]], p[t[:, 2]] - p[t[:, 0]])
+    centroid = (p[t[:, 0]] + p[t[:, 1]] + p[t[:, 2]]) / 3
+    assert ((face * (centroid - center)).sum(1) > 0).all()
+    uses = mesh_edge_uses(t)
+    assert set(uses.values()) == {2}
+    assert len(p) - len(uses) + len(t) == 2  # Euler characteristic of a sphere
+    assert (mesh["colors"] == 255.0).all()   # no colour facet: white
+
+
+def test_marching_cubes_plane_at_one_metre():
+    # tests.cpp:387-400
+    mesh = ko.marching_cubes(_plane_volume(rule=abi.KF_RULE_CLASSIC))
+    assert len(mesh["triangles"]) > 0
+    assert (np.abs(mesh["positions"][:, 2] - 1.0) < SYNTH_VOXEL).all()
+
+
+def test_marching_cubes_unobserved_is_empty():
+    # tests.cpp:402-407
+    mesh = ko.marching_cubes(synth_volume())
+    assert len(mesh["positions"]) == 0 and len(mesh["triangles"]) == 0
+
+
+def test_sparse_marching_cubes_matches_dense_band_mesh():
+    # tests.cpp:409-437
+    o = ko.integration_options(mode=abi.KF_INTEGRATION_BAND)
+    dense = synth_volume()
+    ko.integrate(dense, flat_depth(DEPTH_1M), synth_intrinsics(), np.eye(4), o)
+    sparse = synth_volume(sparse=True)
+    ko.integrate(sparse, flat_depth(DEPTH_1M), synth_intrinsics(), np.eye(4), o)
+    a, b = ko.marching_cubes(sparse), ko.marching_cubes(dense)
+    assert len(a["triangles"]) > 0
+    assert len(a["triangles"]) == len(b["triangles"]) and len(a["positions"]) == len(b["positions"])
+    key = lambda p: p[np.lexsort((p[:, 2], p[:, 1], p[:, 0]))]
+    assert np.array_equal(key(a["positions"]), key(b["positions"]))
+
+
+def test_marching_cubes_weight_threshold():
+    # tests.cpp:439-452: one classic frame leaves every weight at 1
+    vol = _plane_volume(rule=abi.KF_RULE_CLASSIC)
+    assert len(ko.marching_cubes(vol, 2.0)["triangles"]) == 0
+    assert len(ko.marching_cubes(vol, 1.0)["triangles"]) > 0
+
+
+def test_marching_cubes_table_is_the_generated_one():
+    # the committed header is what the generator writes
+    import importlib.util
+    import pathlib
+    here = pathlib.Path(__file__).resolve().parent.parent / "kinectfusion_b200" / "csrc"
+    spec = importlib.util.spec_from_file_location("mc_tables", here / "mc_tables.py")
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    masks, table = gen.build()
+    counts = ko.mc_case_triangle_counts()
+    assert counts[0] == 0 and counts[255] == 0
+    assert [sum(1 for v in row if v >= 0) // 3 for row in table] == counts.tolist()
+    assert all(bin(m).count("1") >= 3 for m in masks[1:255])
