@@ -419,9 +419,9 @@ kf_status kf_pipeline_download_volume(kf_pipeline* pipeline, float* tsdf, float*
 kf_status kf_pipeline_extract_mesh(kf_pipeline* pipeline, float min_weight, kf_mesh* out) {
   return guarded([&] {
     require(pipeline != nullptr && out != nullptr, "kf_pipeline_extract_mesh: null argument");
-    (void)min_weight;
     std::memset(out, 0, sizeof(*out));
-    throw Unsupported("the device mesher is not built yet");
+    require(std::isfinite(min_weight), "kf_pipeline_extract_mesh: min_weight must be finite");
+    extract_mesh(pipeline->impl, min_weight, *out);
   });
 }
 

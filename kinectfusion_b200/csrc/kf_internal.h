@@ -309,6 +309,8 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
                       Intr intrinsics, Rigid world_to_camera, int has_color,
                       const IcpState* pose_state, cudaStream_t stream);
 // Allocates and clears the per-block skip and culling buffers.
+// MarchingCubes::extract on the device (dense volumes); fills a host mesh.
+void extract_mesh(Pipeline& p, float min_weight, kf_mesh& out);
 void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t stream);
 // Clears the skip bits (a freshly filled volume: nothing observed).
 void reset_blocks(Pipeline& p, cudaStream_t stream);

@@ -317,3 +317,43 @@ def test_device_plane_matches_oracle_fixture():
     assert d["max_distance_delta"] == 0.0 and d["max_weight_delta"] == 0.0
     maps = gpu.raycast(synth_intrinsics(), SYNTH_IMAGE, SYNTH_IMAGE, np.eye(4))
     assert compare_maps(maps.points, maps.normals, maps.points, maps.normals)["compared"] > 0
+
+
+# ---- marching cubes ----------------------------------------------------------------------
+def _same_mesh(a, b):
+    assert a["positions"].shape == b["positions"].shape and a["triangles"].shape == b["triangles"].shape
+    for key in ("positions", "normals", "colors"):
+        assert a[key].tobytes() == b[key].tobytes(), key
+    assert np.array_equal(a["triangles"], b["triangles"])
+
+
+@pytest.mark.parametrize("voxel,color,min_weight", [(abi.KF_VOXEL_FLOAT, True, 0.0), (abi.KF_VOXEL_FLOAT, False, 2.0),
+                                                    (abi.KF_VOXEL_QUANTIZED, False, 0.0),
+                                                    (abi.KF_VOXEL_BF16, True, 1.0)])
+def test_mesh_identical_to_oracle(seq, voxel, color, min_weight):
+    # MarchingCubes::extract (marching_cubes.cpp:461-485): same cells, welded
+    # vertices in first-use order, same positions, normals and colours
+    gpu, ref = _integrated_pair(seq, 3, voxel=voxel, color=color)
+    got = gpu.extract_mesh(min_weight)
+    want = ko.marching_cubes(ref, min_weight)
+    assert len(want["triangles"]) > 1000
+    _same_mesh(got, want)
+
+
+def test_mesh_of_unobserved_volume_is_empty():
+    # tests.cpp:402-407
+    res, vs, origin, trunc = cfg1_geometry()
+    gpu = kf.Pipeline(kf.pipeline_config(res, vs, origin, trunc))
+    mesh = gpu.extract_mesh()
+    assert len(mesh["positions"]) == 0 and len(mesh["triangles"]) == 0
+
+
+def test_mesh_weight_threshold_and_closed_edges(seq):
+    # tests.cpp:439-452 plus the welded-edge property of tests.cpp:368-384:
+    # inside the volume every mesh edge has at most two triangles
+    from fixtures import mesh_edge_uses
+    gpu, _ = _integrated_pair(seq, 1, color=False)
+    assert len(gpu.extract_mesh(1e9)["triangles"]) == 0
+    mesh = gpu.extract_mesh(0.0)
+    assert len(mesh["triangles"]) > 0
+    assert max(mesh_edge_uses(mesh["triangles"]).values()) <= 2
