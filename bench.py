@@ -14,6 +14,9 @@ so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+The default 1000 steps keep the timed region (about 1.3 s) long enough for
+the clock sampler to see it.
+
 Multi-GPU: replicas only (each rank tracks its own seeded sequence; the
 path has no exchange step).  Timing is CUDA events on the pipeline's stream,
 barrier + synchronize on both sides, max over ranks.
@@ -41,7 +44,6 @@ METRIC = "frames/s (640x480, 512^3) and ICP iters/frame, learned vs plain at equ
 RES, VOXEL, TRUNC = 512, 0.01, 0.05
 ORIGIN = (-0.5 * RES * VOXEL, -0.5 * RES * VOXEL, -0.5)
 SEQ_FRAMES = 30
-KERNELS_PER_FRAME = 4 + 1 + 1 + 3 * 3 + (10 + 5 + 4) + 1  # pyramid, table, frame begin, levels, ICP, integrate
 
 
 def frame_schedule(step: int) -> int:
@@ -73,7 +75,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -84,6 +86,14 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+
+    def wait_started(self, timeout: float = 5.0):
+        # nvidia-smi needs a moment before its first sample; the timed region
+        # starts once it reports
+        t0 = time.time()
+        while self.proc is not None and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.02)
+        self.skip = len(self.lines)
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -96,7 +106,7 @@ class ClockSampler:
     def summary(self) -> dict:
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for line in self.lines[getattr(self, "skip", 0):]:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -179,6 +189,7 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(torch.cuda.current_device()) as clocks:
+        clocks.wait_started()
         start.record(stream)
         for s in range(args.steps):
             enqueue(step0 + s, False)
@@ -191,6 +202,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     abi.check(lib.kf_pipeline_update_counts(pipe.handle, C.byref(updates1), None))
     last = abi.FrameResult()
     abi.check(lib.kf_frame_result_fetch(pipe.handle, C.byref(last)))
+    kernels_per_frame = C.c_uint32()
+    abi.check(lib.kf_frame_kernel_count(pipe.handle, C.byref(kernels_per_frame)))
     voxel_updates_per_step = (updates1.value - updates0.value) / args.steps
 
     # ---- end to end through the public API: host depth in, pose out ----------------
@@ -267,7 +280,8 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "config": {**workload_config(), "parallelism": f"replicas{world}"},
         "e2e": {"value": round(e2e_fps, 2), "unit": "frames/s", "h2d_bytes_per_step": frame_bytes,
                 "d2h_bytes_per_step": result_bytes},
-        "gpu_launches": KERNELS_PER_FRAME * args.steps,
+        "gpu_launches": int(kernels_per_frame.value) * args.steps,
+        "gpu_launches_per_frame": int(kernels_per_frame.value),
         "voxel_updates_per_s": round(voxel_updates_per_step * fps, 1),
         "icp_iters_per_frame": iters_per_frame,
         "ate_rmse_m": ate,
@@ -349,7 +363,7 @@ def run_reference(args, rank: int) -> dict | None:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")

@@ -353,6 +353,12 @@ kf_status kf_frame_enqueue(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracke
                            uint32_t height, kf_intrinsics intrinsics, int32_t memory,
                            const uint32_t* iterations_per_level, int32_t first_frame);
 kf_status kf_frame_result_fetch(kf_pipeline* pipeline, kf_frame_result* result);
+/* Kernel launches in one frame graph: the kernel nodes of the graph that the
+ * last kf_frame_enqueue / kf_frame_process launched (this library's kernels;
+ * copies, memsets and event records are not kernels).  No counterpart in the
+ * reference, which launches frame by frame from the host. */
+kf_status kf_frame_kernel_count(kf_pipeline* pipeline, uint32_t* kernels);
+
 /* Sets the device-resident camera_to_world that the next enqueued frame
  * starts from (ordered on the pipeline's stream). */
 kf_status kf_frame_set_pose(kf_pipeline* pipeline, kf_tracker* tracker, const kf_rigid* pose);

@@ -163,6 +163,7 @@ _PROTOTYPES = {
     "kf_pipeline_download_volume": (C.c_int, [P, P, P, P]),
     "kf_pipeline_download_raw": (C.c_int, [P, P, C.c_size_t, P, C.c_size_t]),
     "kf_pipeline_extract_mesh": (C.c_int, [P, C.c_float, C.POINTER(Mesh)]),
+    "kf_frame_kernel_count": (C.c_int, [P, C.POINTER(C.c_uint32)]),
     "kf_mesh_free": (None, [C.POINTER(Mesh)]),
     "kf_pipeline_synchronize": (C.c_int, [P]),
     "kf_pipeline_stream": (C.c_int, [P, C.POINTER(P)]),

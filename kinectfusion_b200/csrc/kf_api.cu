@@ -122,7 +122,7 @@ Pipeline::Maps& Pipeline::maps_for(uint32_t w, uint32_t h) {
 }
 
 void Pipeline::clear_graphs() {
-  for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+  for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
   graphs.clear();
 }
 

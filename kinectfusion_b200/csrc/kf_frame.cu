@@ -8,6 +8,8 @@
 // reference syncs once per ICP iteration (icp_correspondence.cu:589-596).
 #include <cstring>
 
+#include <vector>
+
 #include "kf_internal.h"
 
 namespace kf {
@@ -134,13 +136,25 @@ void enqueue(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker, co
       throw;
     }
     check(cudaStreamEndCapture(s, &graph), "end capture");
-    cudaGraphExec_t exec = nullptr;
-    const cudaError_t inst = cudaGraphInstantiate(&exec, graph, 0);
+    Pipeline::FrameGraph fg;
+    size_t nodes = 0;
+    cudaError_t e = cudaGraphGetNodes(graph, nullptr, &nodes);
+    if (e == cudaSuccess && nodes > 0) {
+      std::vector<cudaGraphNode_t> list(nodes);
+      e = cudaGraphGetNodes(graph, list.data(), &nodes);
+      for (size_t i = 0; e == cudaSuccess && i < nodes; ++i) {
+        cudaGraphNodeType type;
+        e = cudaGraphNodeGetType(list[i], &type);
+        if (e == cudaSuccess && type == cudaGraphNodeTypeKernel) ++fg.kernels;
+      }
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&fg.exec, graph, 0);
     cudaGraphDestroy(graph);
-    check(inst, "graph instantiate");
-    it = p.graphs.emplace(key, exec).first;
+    check(e, "graph instantiate");
+    it = p.graphs.emplace(key, fg).first;
   }
-  check(cudaGraphLaunch(it->second, s), "frame graph launch");
+  check(cudaGraphLaunch(it->second.exec, s), "frame graph launch");
+  p.last_frame_kernels = it->second.kernels;
 }
 
 void fill_result(const IcpState& st, int first, kf_frame_result* r) {
@@ -162,6 +176,13 @@ void fill_result(const IcpState& st, int first, kf_frame_result* r) {
 using namespace kf;
 
 extern "C" {
+
+kf_status kf_frame_kernel_count(kf_pipeline* pipeline, uint32_t* kernels) {
+  return guarded([&] {
+    require(pipeline != nullptr && kernels != nullptr, "kf_frame_kernel_count: null argument");
+    *kernels = pipeline->impl.last_frame_kernels;
+  });
+}
 
 kf_status kf_frame_set_pose(kf_pipeline* pipeline, kf_tracker* tracker, const kf_rigid* pose) {
   return guarded([&] {

@@ -285,7 +285,12 @@ struct Pipeline {
       return false;
     }
   };
-  std::map<GraphKey, cudaGraphExec_t> graphs;
+  struct FrameGraph {
+    cudaGraphExec_t exec = nullptr;
+    uint32_t kernels = 0;  // kernel nodes of the captured frame
+  };
+  std::map<GraphKey, FrameGraph> graphs;
+  uint32_t last_frame_kernels = 0;
   kf_pyramid* graph_pyramid = nullptr;
   kf_tracker* graph_tracker = nullptr;
   PinnedArray<IcpState> result_staging;
