@@ -220,7 +220,6 @@ kf_status kf_pipeline_create(const kf_pipeline_config* config, kf_pipeline** out
     require(c.color == KF_COLOR_FLOAT || c.color == KF_COLOR_NONE, "Unknown color store");
     require(c.tsdf_rule == KF_RULE_CLASSIC || c.tsdf_rule == KF_RULE_ANGLE_WEIGHTED, "Unknown TSDF rule");
     if (c.storage == KF_STORAGE_SPARSE) throw Unsupported("sparse storage is not built yet");
-    if (c.integration.mode == KF_INTEGRATION_BAND) throw Unsupported("band integration is not built yet");
     if (c.raycast_backend == KF_RAYCAST_BAND_MARCH) throw Unsupported("band-march raycast is not built yet");
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {

@@ -383,6 +383,74 @@ __global__ void stencil_bits_kernel(const uint4* __restrict__ voxel_bits, uint4*
   }
 }
 
+// ---- band integration (BandIntegrationSweep<kDevice>, tsdf_integration.cu:
+// 240-291; TruncationBandWalk::visit_pixel, tsdf_integration.hpp:384-426) ----
+// One thread per pixel walks its truncation band [d - band, d + band] along
+// the pixel ray at half-block steps and marks every block a sample falls in
+// (consecutive samples in one block mark it once).  The pixel table holds the
+// depth that depth_in_range accepted (NaN otherwise; with finite, non-zero
+// focal lengths the table's other NaN cause, an unusable ray, cannot occur).
+__global__ void band_mark_kernel(const float4* __restrict__ table, uint32_t width, uint32_t height, Intr k,
+                                 Rigid T, float trunc_base, float trunc_scale, int distance_scaled,
+                                 VolumeDev v, const IcpState* __restrict__ state, uint32_t* __restrict__ bits) {
+  if (state != nullptr) {
+    if (state->failed) return;
+    const float* w = state->world_to_camera;
+    T = Rigid{{w[0], w[1], w[2]}, {w[3], w[4], w[5]}, {w[6], w[7], w[8]}, {w[9], w[10], w[11]}};
+  }
+  const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t row = blockIdx.y * blockDim.y + threadIdx.y;
+  if (col >= width || row >= height) return;
+  const float measured = __ldg(&table[static_cast<size_t>(row) * width + col].x);
+  if (isnan(measured)) return;
+  // camera_to_world = inverse(world_to_camera) (vector.hpp:219-229)
+  const f3 c0 = make(T.rx.x, T.ry.x, T.rz.x), c1 = make(T.rx.y, T.ry.y, T.rz.y), c2 = make(T.rx.z, T.ry.z, T.rz.z);
+  const Rigid inv{c0, c1, c2, -make(dot(c0, T.t), dot(c1, T.t), dot(c2, T.t))};
+  const float band = distance_scaled ? trunc_base + (trunc_scale * measured) : trunc_base;
+  const float step = 0.5f * 8.0f * v.voxel_size;  // TruncationBandWalk::half_block_step
+  const float inv_voxel = 1.0f / v.voxel_size;
+  const int samples = static_cast<int>((2.0f * band) / step) + 1;
+  uint32_t previous = 0xFFFFFFFFu;
+  for (int i = 0; i <= samples; ++i) {
+    const float depth = (measured - band) + (static_cast<float>(i) * step);
+    const f3 world = apply(inv, back_project(k, static_cast<float>(col), static_cast<float>(row), depth));
+    const f3 g = (world - v.origin) * inv_voxel;
+    if (!(g.x >= 0.0f && g.y >= 0.0f && g.z >= 0.0f && g.x < static_cast<float>(v.rx) &&
+          g.y < static_cast<float>(v.ry) && g.z < static_cast<float>(v.rz))) {
+      continue;
+    }
+    const uint32_t block = ((static_cast<uint32_t>(g.z) >> 3) * v.by + (static_cast<uint32_t>(g.y) >> 3)) * v.bx +
+                           (static_cast<uint32_t>(g.x) >> 3);
+    if (block == previous) continue;
+    previous = block;
+    // lanes hitting the same word merge their bits into one atomic
+    const uint32_t word = block >> 5, bit = 1u << (block & 31u);
+    const unsigned peers = __match_any_sync(__activemask(), word);
+    const uint32_t merged = __reduce_or_sync(peers, bit);
+    if ((threadIdx.x + threadIdx.y * blockDim.x) % 32u == static_cast<unsigned>(__ffs(peers) - 1)) {
+      atomicOr(bits + word, merged);
+    }
+  }
+}
+
+// Marked blocks into the work list (order does not matter: each listed block
+// is fused once, independently of the others).
+__global__ void band_compact_kernel(const uint32_t* __restrict__ bits, uint32_t words, uint32_t* __restrict__ list,
+                                    unsigned* __restrict__ count, const IcpState* __restrict__ state) {
+  if (state != nullptr && state->failed) return;
+  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= words) return;
+  uint32_t word = bits[w];
+  if (word == 0u) return;
+  const unsigned base = atomicAdd(count, static_cast<unsigned>(__popc(word)));
+  unsigned n = 0;
+  while (word != 0u) {
+    const uint32_t b = static_cast<uint32_t>(__ffs(word) - 1);
+    word &= word - 1u;
+    list[base + n++] = w * 32u + b;
+  }
+}
+
 template <int Kind>
 __global__ void fill_kernel(void* voxels, float4* colors, size_t count) {
   using VT = VoxelTraits<Kind>;
@@ -441,6 +509,7 @@ void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t s
     p.stencil_bits.resize(static_cast<size_t>(blocks) * 32u);
     p.brick_dirty.resize(words);
     p.brick_class.resize(blocks);
+    p.band_bits.resize(words);
     reset_blocks(p, s);
   }
   // depth-tile pyramid geometry for this frame size
@@ -485,27 +554,40 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
                       int has_color, const IcpState* state, cudaStream_t s) {
   prepare_blocks(p, width, height, s);
   const kf_integration_options& o = p.config.integration;
-  // depth-tile pyramid
-  const TileLevels lv = tile_levels_of(p);
-  tile_max_kernel<<<dim3(ceil_div(lv.w[0], 16), ceil_div(lv.h[0], 16)), dim3(16, 16), 0, s>>>(
-      table, width, height, lv.w[0], lv.h[0], p.depth_tiles.ptr);
-  check(cudaGetLastError(), "tile_max_kernel launch");
-  tile_pyramid_kernel<<<1, 1024, 0, s>>>(p.depth_tiles.ptr, lv);
-  check(cudaGetLastError(), "tile_pyramid_kernel launch");
-  // block culling
-  CullParams cp;
-  cp.trunc_base = p.view.truncation;
-  cp.trunc_scale = o.truncation_distance_scale;
-  cp.distance_scaled = o.distance_scaled_truncation;
-  cp.slack = 1.0f / (1.0f - 2.0f / fminf(k.fx, k.fy));
-  cp.width = width;
-  cp.height = height;
+  const uint32_t blocks = p.view.bx * p.view.by * p.view.bz;
   check(cudaMemsetAsync(p.block_count.ptr, 0, sizeof(unsigned), s), "block count clear");
   check(cudaMemsetAsync(p.brick_dirty.ptr, 0, p.brick_dirty.bytes(), s), "dirty bits clear");
-  const uint32_t blocks = p.view.bx * p.view.by * p.view.bz;
-  cull_blocks_kernel<<<ceil_div(blocks, 256), 256, 0, s>>>(p.view, T, k, p.depth_tiles.ptr, lv, cp, state,
-                                                           p.block_list.ptr, p.block_count.ptr);
-  check(cudaGetLastError(), "cull_blocks_kernel launch");
+  if (o.mode == KF_INTEGRATION_BAND) {
+    // blocks the pixels' truncation bands cross
+    check(cudaMemsetAsync(p.band_bits.ptr, 0, p.band_bits.bytes(), s), "band bits clear");
+    band_mark_kernel<<<dim3(ceil_div(width, 16), ceil_div(height, 16)), dim3(16, 16), 0, s>>>(
+        table, width, height, k, T, p.view.truncation, o.truncation_distance_scale, o.distance_scaled_truncation,
+        p.view, state, p.band_bits.ptr);
+    check(cudaGetLastError(), "band_mark_kernel launch");
+    const uint32_t words = static_cast<uint32_t>(p.band_bits.count);
+    band_compact_kernel<<<ceil_div(words, 256), 256, 0, s>>>(p.band_bits.ptr, words, p.block_list.ptr,
+                                                             p.block_count.ptr, state);
+    check(cudaGetLastError(), "band_compact_kernel launch");
+  } else {
+    // depth-tile pyramid
+    const TileLevels lv = tile_levels_of(p);
+    tile_max_kernel<<<dim3(ceil_div(lv.w[0], 16), ceil_div(lv.h[0], 16)), dim3(16, 16), 0, s>>>(
+        table, width, height, lv.w[0], lv.h[0], p.depth_tiles.ptr);
+    check(cudaGetLastError(), "tile_max_kernel launch");
+    tile_pyramid_kernel<<<1, 1024, 0, s>>>(p.depth_tiles.ptr, lv);
+    check(cudaGetLastError(), "tile_pyramid_kernel launch");
+    // block culling
+    CullParams cp;
+    cp.trunc_base = p.view.truncation;
+    cp.trunc_scale = o.truncation_distance_scale;
+    cp.distance_scaled = o.distance_scaled_truncation;
+    cp.slack = 1.0f / (1.0f - 2.0f / fminf(k.fx, k.fy));
+    cp.width = width;
+    cp.height = height;
+    cull_blocks_kernel<<<ceil_div(blocks, 256), 256, 0, s>>>(p.view, T, k, p.depth_tiles.ptr, lv, cp, state,
+                                                             p.block_list.ptr, p.block_count.ptr);
+    check(cudaGetLastError(), "cull_blocks_kernel launch");
+  }
   // listed blocks
   IntegParams ip;
   ip.max_weight = o.max_weight;

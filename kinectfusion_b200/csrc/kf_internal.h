@@ -253,6 +253,7 @@ struct Pipeline {
   // Per brick: 1 = every stencil based in the brick is nullopt, 2 = every
   // one is exactly 1.0 (all eight corners observed with tsdf exactly 1).
   DeviceArray<uint8_t> brick_class;
+  DeviceArray<uint32_t> band_bits;       // band integration: blocks the bands cross
   // Block culling of the full sweep
   DeviceArray<float> depth_tiles;        // max depth per 8x8 pixel tile, then coarser levels
   DeviceArray<uint32_t> block_list;

@@ -626,15 +626,13 @@ static void set_bit(void* user, uint64_t block) {
   bitmap[block / 32] |= 1u << (block % 32);
 }
 
-void kfo_integrate_band(kfo_volume* v, const kf_frame_view* frame,
-                        const kf_integration_options* o, int32_t rule) {
-  /* BandIntegrationSweep<kHost>::run (tsdf_integration.hpp:439-471): the
-   * host walks at voxel-size steps. */
+static void integrate_band_with_step(kfo_volume* v, const kf_frame_view* frame,
+                                     const kf_integration_options* o, int32_t rule, float step) {
   const kf_volume_geometry* g = &v->geometry;
   const uint64_t blocks = blocks_along(g->res_x) * blocks_along(g->res_y) * blocks_along(g->res_z);
   const uint64_t words = (blocks + 31) / 32;
   uint32_t* bitmap = (uint32_t*)calloc(words, sizeof(uint32_t));
-  band_walk(frame, o, g, g->voxel_size, set_bit, bitmap);
+  band_walk(frame, o, g, step, set_bit, bitmap);
   const icontext ctx = {frame, o, rule};
   for (uint64_t w = 0; w < words; ++w) {
     uint32_t word = bitmap[w];
@@ -645,6 +643,21 @@ void kfo_integrate_band(kfo_volume* v, const kf_frame_view* frame,
     }
   }
   free(bitmap);
+}
+
+void kfo_integrate_band(kfo_volume* v, const kf_frame_view* frame,
+                        const kf_integration_options* o, int32_t rule) {
+  /* BandIntegrationSweep<kHost>::run (tsdf_integration.hpp:439-471): the
+   * host walks at voxel-size steps. */
+  integrate_band_with_step(v, frame, o, rule, v->geometry.voxel_size);
+}
+
+void kfo_integrate_band_device(kfo_volume* v, const kf_frame_view* frame,
+                               const kf_integration_options* o, int32_t rule) {
+  /* BandIntegrationSweep<kDevice>::run (tsdf_integration.cu:240-291): the
+   * device walks at half-block steps (band_walk.cuh:41-55,
+   * TruncationBandWalk::half_block_step, tsdf_integration.hpp:379-382). */
+  integrate_band_with_step(v, frame, o, rule, 0.5f * 8.0f * v->geometry.voxel_size);
 }
 
 static void sparse_allocate(void* user, uint64_t block) {

@@ -70,6 +70,9 @@ void kfo_integrate(kfo_volume* volume, const kf_frame_view* frame,
 void kfo_integrate_band(kfo_volume* volume, const kf_frame_view* frame,
                         const kf_integration_options* options, int32_t rule);
 /* Sparse allocation + listed-block integration (BlockRep<kHost>, block_rep.hpp:193-329). */
+/* The device band sweep: the same walk at half-block steps. */
+void kfo_integrate_band_device(kfo_volume* volume, const kf_frame_view* frame,
+                               const kf_integration_options* options, int32_t rule);
 void kfo_integrate_sparse(kfo_volume* volume, const kf_frame_view* frame,
                           const kf_integration_options* options, int32_t rule);
 

@@ -54,6 +54,8 @@ def load() -> C.CDLL:
                                  C.c_int32, C.c_int32]),
         "kfo_integrate_band": (None, [C.POINTER(Volume), C.POINTER(abi.FrameView),
                                       C.POINTER(abi.IntegrationOptions), C.c_int32]),
+        "kfo_integrate_band_device": (None, [C.POINTER(Volume), C.POINTER(abi.FrameView),
+                                             C.POINTER(abi.IntegrationOptions), C.c_int32]),
         "kfo_integrate_sparse": (None, [C.POINTER(Volume), C.POINTER(abi.FrameView),
                                         C.POINTER(abi.IntegrationOptions), C.c_int32]),
         "kfo_raycast": (None, [C.POINTER(Volume), C.POINTER(abi.RaycastCamera), C.POINTER(abi.RaycastOptions),
@@ -268,12 +270,15 @@ def frame_view(depth, k, world_to_camera, color=None, normals_map=None) -> tuple
 
 
 def integrate(vol: OracleVolume, depth, k, world_to_camera, o: abi.IntegrationOptions,
-              rule=abi.KF_RULE_ANGLE_WEIGHTED, color=None, normals_map=None, threads=1):
+              rule=abi.KF_RULE_ANGLE_WEIGHTED, color=None, normals_map=None, threads=1, band_walk="host"):
+    """band_walk: "host" walks the band at voxel steps (BandIntegrationSweep<kHost>),
+    "device" at half-block steps (BandIntegrationSweep<kDevice>)."""
     f, keep = frame_view(depth, k, world_to_camera, color, normals_map)
     if vol.sparse:
         load().kfo_integrate_sparse(C.byref(vol.struct), C.byref(f), C.byref(o), rule)
     elif o.mode == abi.KF_INTEGRATION_BAND:
-        load().kfo_integrate_band(C.byref(vol.struct), C.byref(f), C.byref(o), rule)
+        fn = load().kfo_integrate_band_device if band_walk == "device" else load().kfo_integrate_band
+        fn(C.byref(vol.struct), C.byref(f), C.byref(o), rule)
     else:
         load().kfo_integrate(C.byref(vol.struct), C.byref(f), C.byref(o), rule, threads)
     del keep
@@ -361,7 +366,7 @@ ICP_ITERATIONS = {0: 10, 1: 5, 2: 4}
 
 
 def track_frame(vol: OracleVolume, raw_depth, k, pose, depth_opts, integ_opts, ray_opts, icp_opts,
-                rule=abi.KF_RULE_ANGLE_WEIGHTED, color=None, threads=1, first=False):
+                rule=abi.KF_RULE_ANGLE_WEIGHTED, color=None, threads=1, first=False, band_walk="host"):
     """One frame of the reference loop on the oracle; returns (pose, tracked, per-level outcomes)."""
     levels = pyramid(raw_depth, k, depth_opts)
     outcomes = {}
@@ -382,5 +387,5 @@ def track_frame(vol: OracleVolume, raw_depth, k, pose, depth_opts, integ_opts, r
     if ok:
         w2c = rigid_inverse(abi.rigid_from_matrix(tracked_pose))
         integrate(vol, raw_depth, k, w2c, integ_opts, rule, color=color, normals_map=levels[0]["normals"],
-                  threads=threads)
+                  threads=threads, band_walk=band_walk)
     return tracked_pose, ok, outcomes

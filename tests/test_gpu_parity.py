@@ -357,3 +357,51 @@ def test_mesh_weight_threshold_and_closed_edges(seq):
     mesh = gpu.extract_mesh(0.0)
     assert len(mesh["triangles"]) > 0
     assert max(mesh_edge_uses(mesh["triangles"]).values()) <= 2
+
+
+# ---- band integration ----------------------------------------------------------------------
+@pytest.mark.parametrize("voxel,color", [(abi.KF_VOXEL_FLOAT, True), (abi.KF_VOXEL_BF16, False)])
+def test_band_integration_bit_exact(seq, voxel, color):
+    # BandIntegrationSweep<kDevice> (tsdf_integration.cu:240-291): the band
+    # walk at half-block steps, then the marked blocks fused like the sweep
+    res, vs, origin, trunc = cfg1_geometry()
+    cfg = kf.pipeline_config(res, vs, origin, trunc, voxel=voxel, integration_mode=abi.KF_INTEGRATION_BAND,
+                             color=abi.KF_COLOR_FLOAT if color else abi.KF_COLOR_NONE)
+    gpu = kf.Pipeline(cfg)
+    ref = ko.OracleVolume(res, vs, origin, trunc, voxel=voxel, color=color)
+    full = ko.OracleVolume(res, vs, origin, trunc, voxel=voxel, color=color)
+    o = ko.integration_options(mode=abi.KF_INTEGRATION_BAND)
+    for frame in range(3):
+        raw = seq.depth[frame]
+        normals = ko.pyramid(raw, K640, ko.depth_options())[0]["normals"]
+        w2c = ko.rigid_inverse(abi.rigid_from_matrix(seq.poses[frame]))
+        col = seq.color[frame] if color else None
+        gpu.integrate(raw, K640, w2c, color=col, normals=normals)
+        ko.integrate(ref, raw, K640, w2c, o, color=col, normals_map=normals, threads=8, band_walk="device")
+        ko.integrate(full, raw, K640, w2c, ko.integration_options(), color=col, normals_map=normals, threads=8)
+    got = gpu.download_raw()
+    assert np.array_equal(got.view(np.uint32), ref.voxels.view(np.uint32)), "raw voxels differ"
+    # tests.cpp:698-720: band == full on shared voxels, the full sweep carves more
+    d = compare_volumes(gpu.host_view()[:2], full.dense())
+    assert d["compared"] > 0 and d["max_distance_delta"] == 0.0 and d["only_primary"] == 0
+    assert d["only_reference"] > 0
+
+
+def test_band_frames_match_oracle(seq):
+    # the whole frame loop (kf_frame_process) with band integration
+    res, vs, origin, trunc = cfg1_geometry()
+    cfg = kf.pipeline_config(res, vs, origin, trunc, integration_mode=abi.KF_INTEGRATION_BAND,
+                             rule=abi.KF_RULE_CLASSIC)
+    loop = kf.Reconstruction(kf.Pipeline(cfg), K640)
+    ref = ko.OracleVolume(res, vs, origin, trunc, color=True)
+    pose = np.eye(4, dtype=np.float32)
+    opts = dict(depth_opts=ko.depth_options(), integ_opts=ko.integration_options(mode=abi.KF_INTEGRATION_BAND),
+                ray_opts=ko.raycast_options(), icp_opts=ko.icp_options(), rule=abi.KF_RULE_CLASSIC, threads=8,
+                band_walk="device")
+    for frame in range(3):
+        result = loop.process(seq.depth[frame], seq.color[frame])
+        pose, ok, _ = ko.track_frame(ref, seq.depth[frame], K640, pose, color=seq.color[frame], first=frame == 0,
+                                     **opts)
+        assert bool(result.tracked) == ok
+        dt, da = pose_error(loop.trajectory[-1], pose)
+        assert dt < 1e-4 and da < 1e-4, (frame, dt, da)
