@@ -278,6 +278,14 @@ kf_status kf_pipeline_download_volume(kf_pipeline* pipeline, float* tsdf, float*
 /* Raw storage bytes of the volume (dense: voxel_count*voxel_bytes). */
 kf_status kf_pipeline_download_raw(kf_pipeline* pipeline, void* voxels, size_t voxel_bytes,
                                    void* colors, size_t color_bytes);
+/* Sparse storage: allocation attempts so far (BlockRep's `allocated`
+ * counter, block_rep.cu:18-41, overflow included; allocated blocks =
+ * min(attempts, capacity)) and the pool capacity in blocks.  Dense: 0, 0. */
+kf_status kf_pipeline_block_stats(kf_pipeline* pipeline, uint64_t* attempts, uint64_t* capacity);
+/* Sparse storage: the block-slot grid (BlockRep::grid, block_rep.hpp:26-110),
+ * one uint32 per 8^3 block in x-major block order, 0xFFFFFFFF = unallocated. */
+kf_status kf_pipeline_download_block_grid(kf_pipeline* pipeline, uint32_t* grid, size_t count);
+
 /* Pipeline::extract_mesh (pipeline.hpp:95) on the device; free with kf_mesh_free. */
 kf_status kf_pipeline_extract_mesh(kf_pipeline* pipeline, float min_weight, kf_mesh* out);
 void kf_mesh_free(kf_mesh* mesh);

@@ -219,7 +219,6 @@ kf_status kf_pipeline_create(const kf_pipeline_config* config, kf_pipeline** out
     require(c.voxel >= KF_VOXEL_FLOAT && c.voxel <= KF_VOXEL_BF16, "Unknown voxel store");
     require(c.color == KF_COLOR_FLOAT || c.color == KF_COLOR_NONE, "Unknown color store");
     require(c.tsdf_rule == KF_RULE_CLASSIC || c.tsdf_rule == KF_RULE_ANGLE_WEIGHTED, "Unknown TSDF rule");
-    if (c.storage == KF_STORAGE_SPARSE) throw Unsupported("sparse storage is not built yet");
     if (c.raycast_backend == KF_RAYCAST_BAND_MARCH) throw Unsupported("band-march raycast is not built yet");
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
@@ -231,15 +230,28 @@ kf_status kf_pipeline_create(const kf_pipeline_config* config, kf_pipeline** out
       p.config = c;
       check(cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking), "cudaStreamCreate");
       const kf_volume_geometry& g = c.volume;
-      // bricked storage: whole 8^3 bricks (edge blocks padded)
-      p.voxel_count = static_cast<uint64_t>((g.res_x + 7) / 8) * ((g.res_y + 7) / 8) * ((g.res_z + 7) / 8) * 512;
+      const uint64_t blocks = static_cast<uint64_t>((g.res_x + 7) / 8) * ((g.res_y + 7) / 8) * ((g.res_z + 7) / 8);
+      require(blocks < 0xFFFFFFFFull, "Volume has too many blocks");
+      // bricked storage: whole 8^3 bricks (edge blocks padded); a sparse
+      // volume holds its pool of `capacity` bricks (BlockRep, block_rep.cu:76-96,
+      // default capacity = blocks / 4)
+      if (c.storage == KF_STORAGE_SPARSE) {
+        p.sparse_capacity = c.sparse_block_capacity != 0 ? c.sparse_block_capacity : blocks / 4;
+        require(p.sparse_capacity > 0 && p.sparse_capacity < 0xFFFFFFFFull, "Sparse block capacity out of range");
+        p.voxel_count = p.sparse_capacity * 512;
+        p.grid.resize(blocks);
+        p.slot_block.resize(p.sparse_capacity);
+        p.allocated.resize(2);
+      } else {
+        p.voxel_count = blocks * 512;
+      }
       p.voxel_bytes = voxel_bytes_of(c.voxel);
       p.voxels.resize(p.voxel_count * p.voxel_bytes);
       if (c.color == KF_COLOR_FLOAT) p.colors.resize(p.voxel_count);
       VolumeDev& v = p.view;
       v.voxels = p.voxels.ptr;
       v.colors = c.color == KF_COLOR_FLOAT ? p.colors.ptr : nullptr;
-      v.grid = nullptr;
+      v.grid = c.storage == KF_STORAGE_SPARSE ? p.grid.ptr : nullptr;
       v.rx = g.res_x;
       v.ry = g.res_y;
       v.rz = g.res_z;
@@ -251,6 +263,7 @@ kf_status kf_pipeline_create(const kf_pipeline_config* config, kf_pipeline** out
       v.origin = make(g.origin[0], g.origin[1], g.origin[2]);
       v.truncation = g.truncation_distance;
       launch_fill_volume(p, p.stream);
+      reset_sparse(p, p.stream);
       p.counters.resize(2);
       check(cudaMemsetAsync(p.counters.ptr, 0, p.counters.bytes(), p.stream), "counter init");
       check(cudaStreamSynchronize(p.stream), "volume fill");
@@ -278,6 +291,8 @@ kf_status kf_pipeline_reset(kf_pipeline* pipeline) {
     require(pipeline != nullptr, "kf_pipeline_reset: null pipeline");
     Pipeline& p = pipeline->impl;
     launch_fill_volume(p, p.stream);
+    reset_sparse(p, p.stream);
+    reset_blocks(p, p.stream);  // the raycast's skip structures describe the volume
     check(cudaMemsetAsync(p.counters.ptr, 0, p.counters.bytes(), p.stream), "counter reset");
     check(cudaStreamSynchronize(p.stream), "volume reset");
   });
@@ -342,24 +357,82 @@ kf_status kf_pipeline_observed_voxel_count(kf_pipeline* pipeline, uint64_t* coun
 
 namespace {
 // Copies the bricked device volume to the host in the reference's x-fastest
-// order (Size3::flatten, vector.hpp:61-67): elem_bytes per voxel.
-void download_dense(const void* device, size_t elem_bytes, const kf_volume_geometry& g, void* out) {
+// order (Size3::flatten, vector.hpp:61-67): elem_bytes per voxel.  Sparse
+// volumes resolve each block through the grid; unallocated blocks read as
+// `unallocated` (elem_bytes of an unobserved voxel).
+void download_dense(const Pipeline& p, const void* device, size_t elem_bytes, void* out, const void* unallocated) {
+  const kf_volume_geometry& g = p.config.volume;
   const uint64_t bx = (g.res_x + 7) / 8, by = (g.res_y + 7) / 8, bz = (g.res_z + 7) / 8;
-  std::vector<uint8_t> raw(bx * by * bz * 512 * elem_bytes);
+  const bool sparse = p.view.grid != nullptr;
+  std::vector<uint8_t> raw((sparse ? p.sparse_capacity : bx * by * bz) * 512 * elem_bytes);
   check(cudaMemcpy(raw.data(), device, raw.size(), cudaMemcpyDeviceToHost), "volume download");
+  std::vector<uint32_t> grid;
+  if (sparse) {
+    grid.resize(bx * by * bz);
+    check(cudaMemcpy(grid.data(), p.grid.ptr, grid.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost),
+          "grid download");
+  }
   uint8_t* dst = static_cast<uint8_t*>(out);
   for (uint64_t z = 0; z < g.res_z; ++z) {
     for (uint64_t y = 0; y < g.res_y; ++y) {
       for (uint64_t x0 = 0; x0 < g.res_x; x0 += 8) {
         const uint64_t block = ((z / 8) * by + (y / 8)) * bx + (x0 / 8);
-        const uint64_t src = (block * 512 + ((z % 8) * 8 + (y % 8)) * 8) * elem_bytes;
         const uint64_t n = std::min<uint64_t>(8, g.res_x - x0);
-        std::memcpy(dst + ((z * g.res_y + y) * g.res_x + x0) * elem_bytes, raw.data() + src, n * elem_bytes);
+        uint8_t* d = dst + ((z * g.res_y + y) * g.res_x + x0) * elem_bytes;
+        const uint64_t slot = sparse ? grid[block] : block;
+        if (sparse && grid[block] == kUnallocated) {
+          for (uint64_t i = 0; i < n; ++i) std::memcpy(d + i * elem_bytes, unallocated, elem_bytes);
+          continue;
+        }
+        const uint64_t src = (slot * 512 + ((z % 8) * 8 + (y % 8)) * 8) * elem_bytes;
+        std::memcpy(d, raw.data() + src, n * elem_bytes);
       }
     }
   }
 }
+
+// Raw bytes of an unobserved voxel (volume.hpp:115-117) and colour.
+struct Unobserved {
+  uint8_t voxel[8];
+  uint8_t color[16];
+};
+Unobserved unobserved_of(int kind) {
+  Unobserved u{};
+  if (kind == KF_VOXEL_FLOAT) {
+    const float f[2] = {1.0f, 0.0f};
+    std::memcpy(u.voxel, f, 8);
+  } else {
+    const uint32_t r = kind == KF_VOXEL_QUANTIZED ? 32767u : 0x3F80u;
+    std::memcpy(u.voxel, &r, 4);
+  }
+  return u;
+}
 }  // namespace
+
+kf_status kf_pipeline_block_stats(kf_pipeline* pipeline, uint64_t* attempts, uint64_t* capacity) {
+  return guarded([&] {
+    require(pipeline != nullptr && attempts != nullptr && capacity != nullptr,
+            "kf_pipeline_block_stats: null argument");
+    Pipeline& p = pipeline->impl;
+    check(cudaStreamSynchronize(p.stream), "block stats sync");
+    *attempts = 0;
+    *capacity = p.sparse_capacity;
+    if (p.allocated.count != 0) {
+      check(cudaMemcpy(attempts, p.allocated.ptr, sizeof(uint64_t), cudaMemcpyDeviceToHost), "block stats");
+    }
+  });
+}
+
+kf_status kf_pipeline_download_block_grid(kf_pipeline* pipeline, uint32_t* grid, size_t count) {
+  return guarded([&] {
+    require(pipeline != nullptr && grid != nullptr, "kf_pipeline_download_block_grid: null argument");
+    Pipeline& p = pipeline->impl;
+    require(p.grid.count != 0, "kf_pipeline_download_block_grid: the pipeline is not sparse");
+    require(count == p.grid.count, "kf_pipeline_download_block_grid: grid size mismatch");
+    check(cudaStreamSynchronize(p.stream), "grid download sync");
+    check(cudaMemcpy(grid, p.grid.ptr, count * sizeof(uint32_t), cudaMemcpyDeviceToHost), "grid download");
+  });
+}
 
 kf_status kf_pipeline_download_raw(kf_pipeline* pipeline, void* voxels, size_t voxel_bytes, void* colors,
                                    size_t color_bytes) {
@@ -371,12 +444,12 @@ kf_status kf_pipeline_download_raw(kf_pipeline* pipeline, void* voxels, size_t v
     const uint64_t dense = static_cast<uint64_t>(g.res_x) * g.res_y * g.res_z;
     if (voxels) {
       require(voxel_bytes == dense * p.voxel_bytes, "kf_pipeline_download_raw: voxel buffer size mismatch");
-      download_dense(p.voxels.ptr, p.voxel_bytes, g, voxels);
+      download_dense(p, p.voxels.ptr, p.voxel_bytes, voxels, unobserved_of(p.config.voxel).voxel);
     }
     if (colors) {
       require(p.colors.count != 0, "kf_pipeline_download_raw: the pipeline stores no colour");
       require(color_bytes == dense * sizeof(float4), "kf_pipeline_download_raw: colour buffer size mismatch");
-      download_dense(p.colors.ptr, sizeof(float4), g, colors);
+      download_dense(p, p.colors.ptr, sizeof(float4), colors, unobserved_of(p.config.voxel).color);
     }
   });
 }
@@ -389,7 +462,7 @@ kf_status kf_pipeline_download_volume(kf_pipeline* pipeline, float* tsdf, float*
     const kf_volume_geometry& g = p.config.volume;
     const uint64_t dense = static_cast<uint64_t>(g.res_x) * g.res_y * g.res_z;
     std::vector<uint8_t> raw(dense * p.voxel_bytes);
-    download_dense(p.voxels.ptr, p.voxel_bytes, g, raw.data());
+    download_dense(p, p.voxels.ptr, p.voxel_bytes, raw.data(), unobserved_of(p.config.voxel).voxel);
     // host_dense_view decode (volume.hpp:28-100)
     for (uint64_t i = 0; i < dense; ++i) {
       if (p.config.voxel == KF_VOXEL_FLOAT) {
@@ -410,7 +483,7 @@ kf_status kf_pipeline_download_volume(kf_pipeline* pipeline, float* tsdf, float*
     }
     if (color != nullptr) {
       require(p.colors.count != 0, "kf_pipeline_download_volume: the pipeline stores no colour");
-      download_dense(p.colors.ptr, sizeof(float4), g, color);
+      download_dense(p, p.colors.ptr, sizeof(float4), color, unobserved_of(p.config.voxel).color);
     }
   });
 }

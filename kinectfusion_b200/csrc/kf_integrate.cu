@@ -216,6 +216,8 @@ __global__ void __launch_bounds__(kBlockThreads)
   unsigned updates = 0, color_updates = 0;
   for (unsigned item = blockIdx.x; item < n; item += gridDim.x) {
     const uint32_t block = list[item];
+    // sparse volumes: listed blocks are allocated (SparseVolumeView::find_voxel)
+    const uint32_t slot = v.grid != nullptr ? __ldg(v.grid + block) : block;
     const uint32_t bxi = block % v.bx, byi = (block / v.bx) % v.by, bzi = block / (v.bx * v.by);
     const uint32_t x = bxi * 8 + lx, y = byi * 8 + ly;
     uint32_t fused_z = 0;  // bit i: voxel z = lz + i fused this frame
@@ -241,7 +243,7 @@ __global__ void __launch_bounds__(kBlockThreads)
               if (!(sdf < -truncation) && ow > 0.0f) {
                 const float tsdf = clampf(sdf / truncation, -1.0f, 1.0f);
                 // BasicVoxel::fused (volume.hpp:137-146)
-                const size_t index = static_cast<size_t>(block) * 512 + brick_offset(x, y, z);
+                const size_t index = static_cast<size_t>(slot) * 512 + brick_offset(x, y, z);
                 const Raw old = voxels[index];
                 const float t0 = VT::tsdf(old);
                 const float w0 = VT::weight(old);
@@ -276,6 +278,7 @@ __global__ void __launch_bounds__(kBlockThreads)
     // consecutive voxels of one layer half for each of its four z, i.e.
     // exactly one word: ballots give the new bits of the voxels fused this
     // frame, the other bits are kept.
+    if (voxel_bits == nullptr) continue;  // no skip structures (sparse storage)
     uint32_t* bits = voxel_bits + static_cast<size_t>(block) * 32u;
     const uint32_t half = (threadIdx.x >> 5) & 1u;
     uint32_t changed = 0u;
@@ -451,6 +454,147 @@ __global__ void band_compact_kernel(const uint32_t* __restrict__ bits, uint32_t 
   }
 }
 
+// ---- sparse allocation (BlockRep<kDevice>::integrate, block_rep.cu:100-152) ----
+// The reference allocates marked blocks first come, first served (atomicAdd
+// on the slot counter, block_rep.cu:18-41).  Here slots go to the newly
+// marked blocks in block-index order (a scan over the marked words), so the
+// allocation is deterministic; as in the reference every attempt counts, a
+// block past the capacity stays unallocated and its updates are dropped.
+constexpr int kAllocWords = 1024;  // words per CTA of the allocation scan
+
+// Marked blocks not allocated yet, and their count per word.
+__global__ void sparse_new_kernel(const uint32_t* __restrict__ marked, const uint32_t* __restrict__ grid,
+                                  uint32_t words, uint32_t* __restrict__ new_bits, uint32_t* __restrict__ counts,
+                                  const IcpState* __restrict__ state) {
+  if (state != nullptr && state->failed) return;
+  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= words) return;
+  uint32_t m = marked[w], fresh = 0u;
+  while (m != 0u) {
+    const uint32_t b = static_cast<uint32_t>(__ffs(m) - 1);
+    m &= m - 1u;
+    if (grid[w * 32u + b] == kUnallocated) fresh |= 1u << b;
+  }
+  new_bits[w] = fresh;
+  counts[w] = static_cast<uint32_t>(__popc(fresh));
+}
+
+// Exclusive scan of the counts within CTAs of kAllocWords words; CTA totals
+// to `totals`.
+__global__ void __launch_bounds__(kAllocWords)
+    sparse_scan_local_kernel(uint32_t* __restrict__ counts, uint32_t words, uint32_t* __restrict__ totals,
+                             const IcpState* __restrict__ state) {
+  if (state != nullptr && state->failed) return;
+  __shared__ uint32_t s_warp[kAllocWords / 32];
+  const uint32_t w = blockIdx.x * kAllocWords + threadIdx.x;
+  const uint32_t value = w < words ? counts[w] : 0u;
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t incl = value;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t up = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+    if (lane >= static_cast<unsigned>(off)) incl += up;
+  }
+  if (lane == 31u) s_warp[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t t = s_warp[lane];
+    uint32_t x = t;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t up = __shfl_up_sync(0xFFFFFFFFu, x, off);
+      if (lane >= static_cast<unsigned>(off)) x += up;
+    }
+    s_warp[lane] = x - t;  // exclusive warp offsets
+    if (lane == 31u) totals[blockIdx.x] = x;
+  }
+  __syncthreads();
+  if (w < words) counts[w] = s_warp[warp] + incl - value;  // exclusive prefix within the CTA
+}
+
+// One CTA: exclusive scan of the CTA totals, this frame's first slot, and
+// the attempt counter moved past this frame's new blocks.
+__global__ void __launch_bounds__(1024)
+    sparse_scan_top_kernel(uint32_t* __restrict__ totals, uint32_t ctas, unsigned long long* __restrict__ allocated,
+                           const IcpState* __restrict__ state) {
+  if (state != nullptr && state->failed) return;
+  __shared__ uint32_t s_warp[32];
+  __shared__ unsigned long long s_carry;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  for (uint32_t first = 0; first < ctas; first += 1024) {
+    const uint32_t i = first + threadIdx.x;
+    const uint32_t value = i < ctas ? totals[i] : 0u;
+    uint32_t incl = value;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t up = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+      if (lane >= static_cast<unsigned>(off)) incl += up;
+    }
+    if (lane == 31u) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t t = s_warp[lane];
+      uint32_t x = t;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t up = __shfl_up_sync(0xFFFFFFFFu, x, off);
+        if (lane >= static_cast<unsigned>(off)) x += up;
+      }
+      s_warp[lane] = x - t;
+    }
+    __syncthreads();
+    const unsigned long long carry = s_carry;
+    if (i < ctas) totals[i] = static_cast<uint32_t>(carry + s_warp[warp] + incl - value);
+    __syncthreads();
+    if (threadIdx.x == 1023) s_carry = carry + s_warp[31] + incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    allocated[1] = allocated[0];
+    allocated[0] += s_carry;
+  }
+}
+
+// Slots for the new blocks of each word, then the frame's work list: every
+// marked block that holds a slot.
+__global__ void sparse_assign_kernel(const uint32_t* __restrict__ marked, const uint32_t* __restrict__ new_bits,
+                                     const uint32_t* __restrict__ prefix, const uint32_t* __restrict__ cta_prefix,
+                                     uint32_t words, const unsigned long long* __restrict__ allocated,
+                                     unsigned long long capacity, uint32_t* __restrict__ grid,
+                                     uint32_t* __restrict__ slot_block, uint32_t* __restrict__ list,
+                                     unsigned* __restrict__ count, const IcpState* __restrict__ state) {
+  if (state != nullptr && state->failed) return;
+  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= words) return;
+  uint32_t fresh = new_bits[w];
+  unsigned long long slot = allocated[1] + cta_prefix[w / kAllocWords] + prefix[w];
+  while (fresh != 0u) {
+    const uint32_t b = static_cast<uint32_t>(__ffs(fresh) - 1);
+    fresh &= fresh - 1u;
+    if (slot < capacity) {
+      grid[w * 32u + b] = static_cast<uint32_t>(slot);
+      slot_block[slot] = w * 32u + b;
+    }
+    ++slot;
+  }
+  uint32_t m = marked[w], usable = 0u;
+  while (m != 0u) {
+    const uint32_t b = static_cast<uint32_t>(__ffs(m) - 1);
+    m &= m - 1u;
+    if (grid[w * 32u + b] != kUnallocated) usable |= 1u << b;
+  }
+  if (usable == 0u) return;
+  const unsigned base = atomicAdd(count, static_cast<unsigned>(__popc(usable)));
+  unsigned n = 0;
+  while (usable != 0u) {
+    const uint32_t b = static_cast<uint32_t>(__ffs(usable) - 1);
+    usable &= usable - 1u;
+    list[base + n++] = w * 32u + b;
+  }
+}
+
 template <int Kind>
 __global__ void fill_kernel(void* voxels, float4* colors, size_t count) {
   using VT = VoxelTraits<Kind>;
@@ -491,8 +635,8 @@ void launch_blocks_typed(Pipeline& p, const float4* table, uint32_t width, uint3
                          const IntegParams& ip, const IcpState* state, cudaStream_t s) {
   if (state == nullptr && p.kernel_start != nullptr) check(cudaEventRecord(p.kernel_start, s), "event record");
   integrate_blocks_kernel<Kind, Color><<<148 * 12, kBlockThreads, 0, s>>>(
-      p.view, table, width, height, k, T, ip, state, p.block_list.ptr, p.block_count.ptr, p.voxel_bits.ptr,
-      p.brick_dirty.ptr, p.counters.ptr);
+      p.view, table, width, height, k, T, ip, state, p.block_list.ptr, p.block_count.ptr,
+      p.voxel_bits.count ? p.voxel_bits.ptr : nullptr, p.brick_dirty.ptr, p.counters.ptr);
   check(cudaGetLastError(), "integrate_blocks_kernel launch");
   if (state == nullptr && p.kernel_stop != nullptr) check(cudaEventRecord(p.kernel_stop, s), "event record");
 }
@@ -505,11 +649,18 @@ void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t s
   if (p.brick_dirty.count != words) {
     p.block_list.resize(blocks);
     p.block_count.resize(1);
-    p.voxel_bits.resize(static_cast<size_t>(blocks) * 32u);
-    p.stencil_bits.resize(static_cast<size_t>(blocks) * 32u);
     p.brick_dirty.resize(words);
-    p.brick_class.resize(blocks);
     p.band_bits.resize(words);
+    if (p.view.grid == nullptr) {
+      // the raycast's skip structures (dense storage only)
+      p.voxel_bits.resize(static_cast<size_t>(blocks) * 32u);
+      p.stencil_bits.resize(static_cast<size_t>(blocks) * 32u);
+      p.brick_class.resize(blocks);
+    } else {
+      p.new_bits.resize(words);
+      p.word_prefix.resize(words);
+      p.cta_prefix.resize(ceil_div(static_cast<unsigned>(words), 1024u));
+    }
     reset_blocks(p, s);
   }
   // depth-tile pyramid geometry for this frame size
@@ -532,11 +683,18 @@ void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t s
 
 void reset_blocks(Pipeline& p, cudaStream_t s) {
   if (p.brick_dirty.count == 0) return;
+  check(cudaMemsetAsync(p.brick_dirty.ptr, 0, p.brick_dirty.bytes(), s), "skip bits reset");
+  if (p.voxel_bits.count == 0) return;
   // nothing observed: every stencil is decided nullopt
   check(cudaMemsetAsync(p.voxel_bits.ptr, 0, p.voxel_bits.bytes(), s), "skip bits reset");
   check(cudaMemsetAsync(p.stencil_bits.ptr, 0, p.stencil_bits.bytes(), s), "skip bits reset");
   check(cudaMemsetAsync(p.brick_class.ptr, 1, p.brick_class.bytes(), s), "skip bits reset");
-  check(cudaMemsetAsync(p.brick_dirty.ptr, 0, p.brick_dirty.bytes(), s), "skip bits reset");
+}
+
+void reset_sparse(Pipeline& p, cudaStream_t s) {
+  if (p.grid.count == 0) return;
+  check(cudaMemsetAsync(p.grid.ptr, 0xFF, p.grid.bytes(), s), "sparse grid reset");
+  check(cudaMemsetAsync(p.allocated.ptr, 0, p.allocated.bytes(), s), "sparse counter reset");
 }
 
 void launch_pixel_table(const uint16_t* depth, const uint32_t* color, const float* normals, uint32_t width,
@@ -565,9 +723,25 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
         p.view, state, p.band_bits.ptr);
     check(cudaGetLastError(), "band_mark_kernel launch");
     const uint32_t words = static_cast<uint32_t>(p.band_bits.count);
-    band_compact_kernel<<<ceil_div(words, 256), 256, 0, s>>>(p.band_bits.ptr, words, p.block_list.ptr,
-                                                             p.block_count.ptr, state);
-    check(cudaGetLastError(), "band_compact_kernel launch");
+    if (p.view.grid != nullptr) {
+      // sparse: allocate the newly marked blocks, list the allocated ones
+      const uint32_t ctas = ceil_div(words, static_cast<uint32_t>(kAllocWords));
+      sparse_new_kernel<<<ceil_div(words, 256), 256, 0, s>>>(p.band_bits.ptr, p.grid.ptr, words, p.new_bits.ptr,
+                                                             p.word_prefix.ptr, state);
+      check(cudaGetLastError(), "sparse_new_kernel launch");
+      sparse_scan_local_kernel<<<ctas, kAllocWords, 0, s>>>(p.word_prefix.ptr, words, p.cta_prefix.ptr, state);
+      check(cudaGetLastError(), "sparse_scan_local_kernel launch");
+      sparse_scan_top_kernel<<<1, 1024, 0, s>>>(p.cta_prefix.ptr, ctas, p.allocated.ptr, state);
+      check(cudaGetLastError(), "sparse_scan_top_kernel launch");
+      sparse_assign_kernel<<<ceil_div(words, 256), 256, 0, s>>>(
+          p.band_bits.ptr, p.new_bits.ptr, p.word_prefix.ptr, p.cta_prefix.ptr, words, p.allocated.ptr,
+          p.sparse_capacity, p.grid.ptr, p.slot_block.ptr, p.block_list.ptr, p.block_count.ptr, state);
+      check(cudaGetLastError(), "sparse_assign_kernel launch");
+    } else {
+      band_compact_kernel<<<ceil_div(words, 256), 256, 0, s>>>(p.band_bits.ptr, words, p.block_list.ptr,
+                                                               p.block_count.ptr, state);
+      check(cudaGetLastError(), "band_compact_kernel launch");
+    }
   } else {
     // depth-tile pyramid
     const TileLevels lv = tile_levels_of(p);
@@ -611,6 +785,7 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
       break;
   }
   // raycast skip bits
+  if (p.voxel_bits.count == 0) return;
   stencil_bits_kernel<<<ceil_div(blocks * 8u, 256), 256, 0, s>>>(
       reinterpret_cast<const uint4*>(p.voxel_bits.ptr), reinterpret_cast<uint4*>(p.stencil_bits.ptr),
       p.brick_class.ptr, p.brick_dirty.ptr, p.view.bx, p.view.by, p.view.bz, p.config.raycast.corner_policy == KF_CORNERS_REQUIRE_ALL,

@@ -254,6 +254,13 @@ struct Pipeline {
   // one is exactly 1.0 (all eight corners observed with tsdf exactly 1).
   DeviceArray<uint8_t> brick_class;
   DeviceArray<uint32_t> band_bits;       // band integration: blocks the bands cross
+  // Sparse storage (BlockRep, block_rep.hpp:26-110): a slot per 8^3 block in
+  // `grid` (kUnallocated when none), `sparse_capacity` slots in the pools.
+  DeviceArray<uint32_t> grid;
+  DeviceArray<uint32_t> slot_block;      // block of each allocated slot
+  DeviceArray<unsigned long long> allocated;  // [0] attempts so far (overflow included), [1] this frame's base
+  DeviceArray<uint32_t> new_bits, word_prefix, cta_prefix;
+  uint64_t sparse_capacity = 0;
   // Block culling of the full sweep
   DeviceArray<float> depth_tiles;        // max depth per 8x8 pixel tile, then coarser levels
   DeviceArray<uint32_t> block_list;
@@ -327,6 +334,8 @@ void launch_raycast(const Pipeline& p, const kf_raycast_camera& camera, float* p
                     cudaStream_t stream);
 void launch_fill_volume(Pipeline& p, cudaStream_t stream);
 uint64_t count_observed(Pipeline& p);
+// Sparse storage: every block unallocated again.
+void reset_sparse(Pipeline& p, cudaStream_t stream);
 
 }  // namespace kf
 

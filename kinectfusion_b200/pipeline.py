@@ -232,6 +232,19 @@ class Pipeline:
         _check(lib().kf_pipeline_download_raw(self.handle, _ptr(raw), raw.nbytes, None, 0))
         return raw
 
+    def block_stats(self) -> tuple[int, int]:
+        """Sparse storage: (allocation attempts, capacity) of the block pool."""
+        attempts, capacity = C.c_uint64(), C.c_uint64()
+        _check(lib().kf_pipeline_block_stats(self.handle, C.byref(attempts), C.byref(capacity)))
+        return attempts.value, capacity.value
+
+    def block_grid(self) -> np.ndarray:
+        """Sparse storage: the block-slot grid (0xFFFFFFFF = unallocated)."""
+        rx, ry, rz = self.resolution
+        grid = np.empty(((rx + 7) // 8) * ((ry + 7) // 8) * ((rz + 7) // 8), dtype=np.uint32)
+        _check(lib().kf_pipeline_download_block_grid(self.handle, _ptr(grid), grid.size))
+        return grid
+
     def extract_mesh(self, min_weight: float = 0.0) -> dict:
         """Pipeline::extract_mesh (pipeline.hpp:95) on the device."""
         mesh = abi.Mesh()

@@ -405,3 +405,93 @@ def test_band_frames_match_oracle(seq):
         assert bool(result.tracked) == ok
         dt, da = pose_error(loop.trajectory[-1], pose)
         assert dt < 1e-4 and da < 1e-4, (frame, dt, da)
+
+
+# ---- sparse storage ------------------------------------------------------------------------
+def _sparse_pair(seq, frames, capacity=0, voxel=abi.KF_VOXEL_BF16, color=False):
+    res, vs, origin, trunc = cfg1_geometry()
+    common = dict(voxel=voxel, integration_mode=abi.KF_INTEGRATION_BAND,
+                  color=abi.KF_COLOR_FLOAT if color else abi.KF_COLOR_NONE)
+    sparse = kf.Pipeline(kf.pipeline_config(res, vs, origin, trunc, storage=abi.KF_STORAGE_SPARSE,
+                                            sparse_block_capacity=capacity, **common))
+    dense = kf.Pipeline(kf.pipeline_config(res, vs, origin, trunc, **common))
+    ref = ko.OracleVolume(res, vs, origin, trunc, voxel=voxel, color=color, sparse=True, capacity=capacity)
+    o = ko.integration_options(mode=abi.KF_INTEGRATION_BAND)
+    for frame in range(frames):
+        raw = seq.depth[frame]
+        normals = ko.pyramid(raw, K640, ko.depth_options())[0]["normals"]
+        w2c = ko.rigid_inverse(abi.rigid_from_matrix(seq.poses[frame]))
+        col = seq.color[frame] if color else None
+        for p in (sparse, dense):
+            p.integrate(raw, K640, w2c, color=col, normals=normals)
+        ko.integrate(ref, raw, K640, w2c, o, color=col, normals_map=normals, threads=8)
+    return sparse, dense, ref
+
+
+@pytest.mark.parametrize("voxel,color", [(abi.KF_VOXEL_BF16, False), (abi.KF_VOXEL_FLOAT, True)])
+def test_sparse_matches_dense_band_and_oracle(seq, voxel, color):
+    # BlockRep<kDevice>::integrate (block_rep.cu:100-152) vs the oracle's
+    # BlockRep<kHost>: the same blocks allocated, the same voxels (slots differ:
+    # the device numbers new blocks in block order, the host first come)
+    sparse, dense, ref = _sparse_pair(seq, 3, voxel=voxel, color=color)
+    grid = sparse.block_grid()
+    assert np.array_equal(grid != 0xFFFFFFFF, ref.grid != 0xFFFFFFFF)
+    attempts, capacity = sparse.block_stats()
+    assert attempts == ref.struct.allocated == (grid != 0xFFFFFFFF).sum() and attempts <= capacity
+    assert np.array_equal(sparse.download_raw().view(np.uint32), dense.download_raw().view(np.uint32))
+    st, sw = sparse.host_view()
+    rt, rw = ref.dense()
+    assert same_float(st, rt) and same_float(sw, rw)
+    assert sparse.observed_voxel_count() == dense.observed_voxel_count() == ref.observed_voxel_count() > 0
+
+
+def test_sparse_overflow_drops_updates_only(seq):
+    # tests.cpp:747-770: past the capacity, blocks stay unallocated and their
+    # updates are dropped; everything that is stored matches the dense band
+    sparse, dense, _ = _sparse_pair(seq, 2, capacity=40)
+    attempts, capacity = sparse.block_stats()
+    assert capacity == 40 and attempts > capacity
+    assert (sparse.block_grid() != 0xFFFFFFFF).sum() == 40
+    d = compare_volumes(sparse.host_view()[:2], dense.host_view()[:2])
+    assert d["max_distance_delta"] == 0.0 and d["only_primary"] == 0 and d["only_reference"] > 0
+
+
+def test_sparse_raycast_bit_exact(seq):
+    sparse, _, ref = _sparse_pair(seq, 3, voxel=abi.KF_VOXEL_FLOAT, color=True)
+    for level in (1, 2):
+        k = ko.scaled(K640, level)
+        w, h = 640 >> level, 480 >> level
+        maps = sparse.raycast(k, w, h, seq.poses[3])
+        p, n, c = ko.raycast(ref, k, w, h, seq.poses[3], ko.raycast_options(), threads=8)
+        assert np.isfinite(p).all(-1).sum() > 0.3 * w * h
+        assert same_float(maps.points, p) and same_float(maps.normals, n) and np.array_equal(maps.colors, c)
+
+
+def test_sparse_frames_match_oracle(seq):
+    res, vs, origin, trunc = cfg1_geometry()
+    cfg = kf.pipeline_config(res, vs, origin, trunc, storage=abi.KF_STORAGE_SPARSE, voxel=abi.KF_VOXEL_BF16,
+                             integration_mode=abi.KF_INTEGRATION_BAND, color=abi.KF_COLOR_NONE)
+    loop = kf.Reconstruction(kf.Pipeline(cfg), K640)
+    ref = ko.OracleVolume(res, vs, origin, trunc, voxel=abi.KF_VOXEL_BF16, sparse=True)
+    pose = np.eye(4, dtype=np.float32)
+    opts = dict(depth_opts=ko.depth_options(), integ_opts=ko.integration_options(mode=abi.KF_INTEGRATION_BAND),
+                ray_opts=ko.raycast_options(), icp_opts=ko.icp_options(), threads=8)
+    for frame in range(3):
+        result = loop.process(seq.depth[frame])
+        pose, ok, _ = ko.track_frame(ref, seq.depth[frame], K640, pose, first=frame == 0, **opts)
+        assert bool(result.tracked) == ok
+        dt, da = pose_error(loop.trajectory[-1], pose)
+        assert dt < 1e-4 and da < 1e-4, (frame, dt, da)
+
+
+def test_reset_clears_skip_structures(seq):
+    # kf_pipeline_reset: a reset volume raycasts like a fresh one
+    gpu, _ = _integrated_pair(seq, 2)
+    gpu.reset()
+    fresh, _ = _integrated_pair(seq, 0)
+    for p in (gpu, fresh):
+        p.integrate(seq.depth[3], K640, ko.rigid_inverse(abi.rigid_from_matrix(seq.poses[3])),
+                    color=seq.color[3], normals=ko.pyramid(seq.depth[3], K640, ko.depth_options())[0]["normals"])
+    a = gpu.raycast(K640, 640, 480, seq.poses[3])
+    b = fresh.raycast(K640, 640, 480, seq.poses[3])
+    assert a.points.tobytes() == b.points.tobytes() and a.normals.tobytes() == b.normals.tobytes()
