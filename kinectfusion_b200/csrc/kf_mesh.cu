@@ -1,15 +1,16 @@
 // kf_mesh.cu - marching cubes on the device (MarchingCubes::extract and
-// MeshBuilder, marching_cubes.cpp:311-485) for dense volumes.
+// MeshBuilder, marching_cubes.cpp:311-485), dense and sparse volumes.
 //
 // The mesh is the one the host builder makes, element for element: the same
-// cells in the same order (x fastest over the (res-1)^3 cells), the same
+// cells in the same order (x fastest over the (res-1)^3 cells; sparse:
+// allocated blocks in block order, x fastest within each), the same
 // welded vertices numbered in order of first use, the same positions,
 // normals and colours.  The triangulation table is this library's generated
 // one (kf_mc_tables.h).  Passes:
-//  1. per row of cells (fixed y, z), classify the cells: a cell whose corners
-//     are all observed, finite and at least min_weight has a sign case; set a
-//     bit per crossed edge (key = near voxel's flat index * 3 + axis) and
-//     count the row's triangles.  Cells whose stencil the raycast's stencil
+//  1. per row of cells (fixed y, z; sparse: per allocated block), classify
+//     the cells: a cell whose corners are all observed, finite and at least
+//     min_weight has a sign case; set a bit per crossed edge (key = near
+//     voxel's storage index * 3 + axis) and count the unit's triangles.  Cells whose stencil the raycast's stencil
 //     bits decide (no observed corner, or all corners exactly 1) cannot cross
 //     the surface and are not read;
 //  2. exclusive scans give each row its first triangle and each crossed edge
@@ -69,11 +70,14 @@ __device__ __forceinline__ bool stencil_undecided(const uint4* __restrict__ sten
   return (((bit < 32u ? r.x >> bit : r.y >> (bit - 32u))) & 1u) != 0u;
 }
 
+// Weld key of cube edge `edge` of cell (x, y, z): the near voxel's storage
+// index * 3 + axis (unique per edge; the near voxel is stored whenever a
+// cell using the edge is meshed).
 __device__ __forceinline__ unsigned long long edge_key(const VolumeDev& v, uint32_t x, uint32_t y, uint32_t z,
                                                        int edge) {
   const int near = c_edge[edge][0];
-  const unsigned long long nx = x + c_corner[near][0], ny = y + c_corner[near][1], nz = z + c_corner[near][2];
-  return ((nz * v.ry + ny) * v.rx + nx) * 3ull + c_edge[edge][2];
+  const long long i = storage_index(v, x + c_corner[near][0], y + c_corner[near][1], z + c_corner[near][2]);
+  return static_cast<unsigned long long>(i) * 3ull + c_edge[edge][2];
 }
 
 __device__ __forceinline__ uint32_t triangle_count(int cube) {
@@ -103,8 +107,37 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t value, uint32_
   return total;
 }
 
-// Pass 1 (Write = false): crossed-edge bits and triangles per row.  Pass 3
-// (Write = true): every triangle corner's edge id, and each edge's first use.
+// Pass 1 (Write = false): the crossed-edge bits of an active cell.  Pass 3
+// (Write = true): its triangle corners' edge ids from `first` on, and each
+// edge's first use.
+template <bool Write>
+__device__ __forceinline__ void emit_cell(const VolumeDev& v, uint32_t x, uint32_t y, uint32_t z, int cube,
+                                          uint32_t tris, uint32_t first, uint32_t* __restrict__ edge_words,
+                                          const uint32_t* __restrict__ word_first, uint32_t* __restrict__ corner_edge,
+                                          uint32_t* __restrict__ first_use) {
+  if constexpr (!Write) {
+    const uint32_t mask = c_edge_mask[cube];
+    for (int e = 0; e < 12; ++e) {
+      if (!((mask >> e) & 1u)) continue;
+      const unsigned long long key = edge_key(v, x, y, z, e);
+      atomicOr(edge_words + (key >> 5), 1u << (key & 31u));
+    }
+  } else {
+    for (uint32_t t = 0; t < tris; ++t) {
+      for (int k = 0; k < 3; ++k) {
+        const unsigned long long key = edge_key(v, x, y, z, c_triangles[cube][3 * t + k]);
+        const uint32_t w = static_cast<uint32_t>(key >> 5), b = static_cast<uint32_t>(key & 31u);
+        const uint32_t id = word_first[w] + __popc(edge_words[w] & ((1u << b) - 1u));
+        const uint32_t position = 3u * (first + t) + static_cast<uint32_t>(k);
+        corner_edge[position] = id;
+        atomicMin(first_use + id, position);
+      }
+    }
+  }
+}
+
+// Dense volumes: one CTA per row of cells (fixed y, z), x fastest (the host
+// builder's GridIndices order).  Pass 1 counts the row's triangles.
 template <int Kind, bool Write>
 __global__ void __launch_bounds__(kRowThreads)
     mc_rows_kernel(VolumeDev v, const uint4* __restrict__ stencil_bits, float min_weight,
@@ -126,30 +159,53 @@ __global__ void __launch_bounds__(kRowThreads)
     }
     uint32_t prefix;
     const uint32_t total = block_exclusive_scan(tris, prefix, s_warp);
-    if (tris != 0u) {
-      if (!Write) {
-        const uint32_t mask = c_edge_mask[cube];
-        for (int e = 0; e < 12; ++e) {
-          if (!((mask >> e) & 1u)) continue;
-          const unsigned long long key = edge_key(v, x, y, z, e);
-          atomicOr(edge_words + (key >> 5), 1u << (key & 31u));
-        }
-      } else {
-        for (uint32_t t = 0; t < tris; ++t) {
-          for (int k = 0; k < 3; ++k) {
-            const unsigned long long key = edge_key(v, x, y, z, c_triangles[cube][3 * t + k]);
-            const uint32_t w = static_cast<uint32_t>(key >> 5), b = static_cast<uint32_t>(key & 31u);
-            const uint32_t id = word_first[w] + __popc(edge_words[w] & ((1u << b) - 1u));
-            const uint32_t position = 3u * (base + prefix + t) + static_cast<uint32_t>(k);
-            corner_edge[position] = id;
-            atomicMin(first_use + id, position);
-          }
-        }
-      }
-    }
+    if (tris != 0u) emit_cell<Write>(v, x, y, z, cube, tris, base + prefix, edge_words, word_first, corner_edge,
+                                     first_use);
     base += total;
   }
   if (!Write && threadIdx.x == 0) row_tris[row] = base;
+}
+
+// Sparse volumes: one CTA of 512 threads per allocated block, in block order,
+// its cells x fastest, then y, then z (BlockVoxels order, clipped to the
+// cells of the volume).  Pass 1 counts the block's triangles.
+template <int Kind, bool Write>
+__global__ void __launch_bounds__(512)
+    mc_blocks_kernel(VolumeDev v, const uint32_t* __restrict__ blocks, float min_weight,
+                     uint32_t* __restrict__ edge_words, uint32_t* __restrict__ unit_tris,
+                     const uint32_t* __restrict__ unit_first, const uint32_t* __restrict__ word_first,
+                     uint32_t* __restrict__ corner_edge, uint32_t* __restrict__ first_use) {
+  __shared__ uint32_t s_warp[512 / 32];
+  const uint32_t block = blocks[blockIdx.x];
+  const uint32_t x = (block % v.bx) * 8u + (threadIdx.x & 7u);
+  const uint32_t y = ((block / v.bx) % v.by) * 8u + ((threadIdx.x >> 3) & 7u);
+  const uint32_t z = (block / (v.bx * v.by)) * 8u + (threadIdx.x >> 6);
+  int cube = -1;
+  uint32_t tris = 0;
+  if (x < v.rx - 1 && y < v.ry - 1 && z < v.rz - 1) {
+    cube = cell_case<Kind>(v, x, y, z, min_weight);
+    if (cube >= 0 && c_edge_mask[cube] != 0) tris = triangle_count(cube);
+  }
+  uint32_t prefix;
+  const uint32_t total = block_exclusive_scan(tris, prefix, s_warp);
+  if (tris != 0u) {
+    emit_cell<Write>(v, x, y, z, cube, tris, (Write ? unit_first[blockIdx.x] : 0u) + prefix, edge_words, word_first,
+                     corner_edge, first_use);
+  }
+  if (!Write && threadIdx.x == 0) unit_tris[blockIdx.x] = total;
+}
+
+// Allocated blocks of a sparse grid, in block order.
+__global__ void allocated_flags_kernel(const uint32_t* __restrict__ grid, uint32_t blocks,
+                                       uint32_t* __restrict__ flags) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < blocks) flags[b] = grid[b] != kUnallocated ? 1u : 0u;
+}
+
+__global__ void allocated_list_kernel(const uint32_t* __restrict__ grid, const uint32_t* __restrict__ position,
+                                      uint32_t blocks, uint32_t* __restrict__ list) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < blocks && grid[b] != kUnallocated) list[position[b]] = b;
 }
 
 // Exclusive scan of n values (or of their popcounts) in blocks of
@@ -222,7 +278,8 @@ __global__ void mark_first_use_kernel(const uint32_t* __restrict__ first_use, ui
 // edge of one bitmap word; vertex number = rank of the edge's first use.
 template <int Kind>
 __global__ void __launch_bounds__(256)
-    mc_vertex_kernel(VolumeDev v, const uint32_t* __restrict__ edge_words, const uint32_t* __restrict__ word_first,
+    mc_vertex_kernel(VolumeDev v, const uint32_t* __restrict__ slot_block, const uint32_t* __restrict__ edge_words,
+                     const uint32_t* __restrict__ word_first,
                      const uint32_t* __restrict__ first_use, const uint32_t* __restrict__ use_words,
                      const uint32_t* __restrict__ use_first, uint32_t words, float* __restrict__ positions,
                      float* __restrict__ normals, float* __restrict__ colors, uint32_t* __restrict__ vertex_of) {
@@ -239,9 +296,11 @@ __global__ void __launch_bounds__(256)
     word &= word - 1u;
     const unsigned long long key = (static_cast<unsigned long long>(w) << 5) | b;
     const uint32_t axis = static_cast<uint32_t>(key % 3ull);
-    const unsigned long long flat = key / 3ull;
-    const uint32_t nx = static_cast<uint32_t>(flat % v.rx), ny = static_cast<uint32_t>((flat / v.rx) % v.ry),
-                   nz = static_cast<uint32_t>(flat / (static_cast<unsigned long long>(v.rx) * v.ry));
+    const unsigned long long stored = key / 3ull;
+    const uint32_t slot = static_cast<uint32_t>(stored >> 9), local = static_cast<uint32_t>(stored & 511ull);
+    const uint32_t block = slot_block != nullptr ? slot_block[slot] : slot;
+    const uint32_t nx = (block % v.bx) * 8u + (local & 7u), ny = ((block / v.bx) % v.by) * 8u + ((local >> 3) & 7u),
+                   nz = (block / (v.bx * v.by)) * 8u + (local >> 6);
     const uint32_t fx = nx + (axis == 0), fy = ny + (axis == 1), fz = nz + (axis == 2);
     const float near_value = VT::tsdf(__ldg(voxels + storage_index(v, nx, ny, nz)));
     const float far_value = VT::tsdf(__ldg(voxels + storage_index(v, fx, fy, fz)));
@@ -311,29 +370,55 @@ void fill_missing_normals(kf_mesh& m) {
 template <int Kind>
 void extract_typed(Pipeline& p, float min_weight, kf_mesh& out, cudaStream_t s) {
   const VolumeDev& v = p.view;
-  const uint32_t rows = (v.ry - 1) * (v.rz - 1);
-  const unsigned long long keys = static_cast<unsigned long long>(v.rx) * v.ry * v.rz * 3ull;
+  const bool sparse = v.grid != nullptr;
+  // edge keys: storage index of the near voxel * 3 + axis
+  const unsigned long long keys = static_cast<unsigned long long>(p.voxel_count) * 3ull;
   const unsigned long long words64 = (keys + 31ull) / 32ull;
   if (words64 > 0xFFFFFFFFull) throw Unsupported("volume too large for the device mesher");
   const uint32_t words = static_cast<uint32_t>(words64);
   const uint4* stencil = p.brick_class.count ? reinterpret_cast<const uint4*>(p.stencil_bits.ptr) : nullptr;
 
-  DeviceArray<uint32_t> edge_words(words), word_first(words), row_tris(rows), row_first(rows);
+  // units: rows of cells (dense) or allocated blocks in block order (sparse)
+  uint32_t units = (v.ry - 1) * (v.rz - 1);
+  DeviceArray<uint32_t> block_list;
+  if (sparse) {
+    const uint32_t blocks = v.bx * v.by * v.bz;
+    DeviceArray<uint32_t> flags(blocks), position(blocks);
+    allocated_flags_kernel<<<ceil_div(blocks, 256), 256, 0, s>>>(v.grid, blocks, flags.ptr);
+    check(cudaGetLastError(), "allocated_flags_kernel launch");
+    units = exclusive_scan(flags.ptr, position.ptr, blocks, false, s);
+    if (units == 0) return;
+    block_list.resize(units);
+    allocated_list_kernel<<<ceil_div(blocks, 256), 256, 0, s>>>(v.grid, position.ptr, blocks, block_list.ptr);
+    check(cudaGetLastError(), "allocated_list_kernel launch");
+  }
+  DeviceArray<uint32_t> edge_words(words), word_first(words), unit_tris(units), unit_first(units);
   check(cudaMemsetAsync(edge_words.ptr, 0, edge_words.bytes(), s), "mesh edge bits");
-  mc_rows_kernel<Kind, false><<<rows, kRowThreads, 0, s>>>(v, stencil, min_weight, edge_words.ptr, row_tris.ptr,
-                                                          nullptr, nullptr, nullptr, nullptr);
-  check(cudaGetLastError(), "mc_rows_kernel launch");
-  const uint32_t triangles = exclusive_scan(row_tris.ptr, row_first.ptr, rows, false, s);
+  if (sparse) {
+    mc_blocks_kernel<Kind, false><<<units, 512, 0, s>>>(v, block_list.ptr, min_weight, edge_words.ptr,
+                                                         unit_tris.ptr, nullptr, nullptr, nullptr, nullptr);
+  } else {
+    mc_rows_kernel<Kind, false><<<units, kRowThreads, 0, s>>>(v, stencil, min_weight, edge_words.ptr, unit_tris.ptr,
+                                                              nullptr, nullptr, nullptr, nullptr);
+  }
+  check(cudaGetLastError(), "mesh cell pass launch");
+  const uint32_t triangles = exclusive_scan(unit_tris.ptr, unit_first.ptr, units, false, s);
   const uint32_t vertices = exclusive_scan(edge_words.ptr, word_first.ptr, words, true, s);
   if (triangles == 0 || vertices == 0) return;
   if (static_cast<unsigned long long>(triangles) * 3ull > 0xFFFFFFFFull) throw Unsupported("mesh too large");
   const uint32_t corners = triangles * 3u;
   DeviceArray<uint32_t> corner_edge(corners), first_use(vertices), vertex_of(vertices), tris(corners);
   check(cudaMemsetAsync(first_use.ptr, 0xFF, first_use.bytes(), s), "mesh first use");
-  mc_rows_kernel<Kind, true><<<rows, kRowThreads, 0, s>>>(v, stencil, min_weight, edge_words.ptr, nullptr,
-                                                         row_first.ptr, word_first.ptr, corner_edge.ptr,
-                                                         first_use.ptr);
-  check(cudaGetLastError(), "mc_rows_kernel launch");
+  if (sparse) {
+    mc_blocks_kernel<Kind, true><<<units, 512, 0, s>>>(v, block_list.ptr, min_weight, edge_words.ptr, nullptr,
+                                                        unit_first.ptr, word_first.ptr, corner_edge.ptr,
+                                                        first_use.ptr);
+  } else {
+    mc_rows_kernel<Kind, true><<<units, kRowThreads, 0, s>>>(v, stencil, min_weight, edge_words.ptr, nullptr,
+                                                             unit_first.ptr, word_first.ptr, corner_edge.ptr,
+                                                             first_use.ptr);
+  }
+  check(cudaGetLastError(), "mesh corner pass launch");
   const uint32_t use_words_n = ceil_div(corners, 32u);
   DeviceArray<uint32_t> use_words(use_words_n), use_first(use_words_n);
   check(cudaMemsetAsync(use_words.ptr, 0, use_words.bytes(), s), "mesh use bits");
@@ -342,9 +427,9 @@ void extract_typed(Pipeline& p, float min_weight, kf_mesh& out, cudaStream_t s) 
   exclusive_scan(use_words.ptr, use_first.ptr, use_words_n, true, s);
   DeviceArray<float> positions(static_cast<size_t>(vertices) * 3), normals(static_cast<size_t>(vertices) * 3),
       colors(static_cast<size_t>(vertices) * 3);
-  mc_vertex_kernel<Kind><<<ceil_div(words, 256), 256, 0, s>>>(v, edge_words.ptr, word_first.ptr, first_use.ptr,
-                                                              use_words.ptr, use_first.ptr, words, positions.ptr,
-                                                              normals.ptr, colors.ptr, vertex_of.ptr);
+  mc_vertex_kernel<Kind><<<ceil_div(words, 256), 256, 0, s>>>(
+      v, sparse ? p.slot_block.ptr : nullptr, edge_words.ptr, word_first.ptr, first_use.ptr, use_words.ptr,
+      use_first.ptr, words, positions.ptr, normals.ptr, colors.ptr, vertex_of.ptr);
   check(cudaGetLastError(), "mc_vertex_kernel launch");
   mc_triangle_kernel<<<ceil_div(corners, 256), 256, 0, s>>>(corner_edge.ptr, vertex_of.ptr, tris.ptr, corners);
   check(cudaGetLastError(), "mc_triangle_kernel launch");
@@ -375,7 +460,6 @@ void upload_tables() {
 
 void extract_mesh(Pipeline& p, float min_weight, kf_mesh& out) {
   std::memset(&out, 0, sizeof(out));
-  if (p.view.grid != nullptr) throw Unsupported("device marching cubes of sparse volumes is not built yet");
   if (p.view.rx < 2 || p.view.ry < 2 || p.view.rz < 2) return;
   upload_tables();
   const cudaStream_t s = p.stream;

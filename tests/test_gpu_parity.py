@@ -495,3 +495,18 @@ def test_reset_clears_skip_structures(seq):
     a = gpu.raycast(K640, 640, 480, seq.poses[3])
     b = fresh.raycast(K640, 640, 480, seq.poses[3])
     assert a.points.tobytes() == b.points.tobytes() and a.normals.tobytes() == b.normals.tobytes()
+
+
+def test_sparse_mesh_identical_to_oracle(seq):
+    # MarchingCubes::extract over a sparse view (marching_cubes.cpp:475-485):
+    # allocated blocks in order; and tests.cpp:409-437: the sparse mesh has
+    # the dense band mesh's vertices
+    sparse, dense, ref = _sparse_pair(seq, 3, voxel=abi.KF_VOXEL_FLOAT, color=True)
+    got = sparse.extract_mesh()
+    want = ko.marching_cubes(ref)
+    assert len(want["triangles"]) > 1000
+    _same_mesh(got, want)
+    band = dense.extract_mesh()
+    key = lambda p: p[np.lexsort((p[:, 2], p[:, 1], p[:, 0]))]
+    assert len(band["triangles"]) == len(got["triangles"])
+    assert np.array_equal(key(band["positions"]), key(got["positions"]))
