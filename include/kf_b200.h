@@ -367,6 +367,28 @@ kf_status kf_frame_result_fetch(kf_pipeline* pipeline, kf_frame_result* result);
  * reference, which launches frame by frame from the host. */
 kf_status kf_frame_kernel_count(kf_pipeline* pipeline, uint32_t* kernels);
 
+/* ---- batches of independent sequences (no counterpart in the reference) ----
+ * Members are (pipeline, pyramid, tracker) triples of different volumes
+ * (resolutions and storages may differ).  kf_batch_step runs one frame of
+ * every member whose depth pointer is non-null as ONE graph launch: each
+ * member's frame graph (the one kf_frame_enqueue would launch) is a branch
+ * of the step's graph, so the members run concurrently.  Colour is not
+ * batched.  first_frame (may be NULL) has one flag per member.  The step is
+ * ordered after each active member's earlier work and before its later
+ * work; kf_frame_result_fetch reads a member's result as usual. */
+typedef struct kf_batch kf_batch;
+kf_status kf_batch_create(kf_pipeline* const* pipelines, kf_pyramid* const* pyramids,
+                          kf_tracker* const* trackers, uint32_t count, kf_batch** out);
+kf_status kf_batch_destroy(kf_batch* batch);
+kf_status kf_batch_step(kf_batch* batch, const uint16_t* const* depths, uint32_t width,
+                        uint32_t height, const kf_intrinsics* intrinsics,
+                        const uint32_t* iterations_per_level, const uint8_t* first_frame,
+                        int32_t memory);
+/* The stream the steps run on (a cudaStream_t). */
+kf_status kf_batch_stream(kf_batch* batch, void** stream);
+/* Kernel nodes of the last step's graph. */
+kf_status kf_batch_kernel_count(kf_batch* batch, uint32_t* kernels);
+
 /* Sets the device-resident camera_to_world that the next enqueued frame
  * starts from (ordered on the pipeline's stream). */
 kf_status kf_frame_set_pose(kf_pipeline* pipeline, kf_tracker* tracker, const kf_rigid* pose);

@@ -164,6 +164,11 @@ _PROTOTYPES = {
     "kf_pipeline_download_raw": (C.c_int, [P, P, C.c_size_t, P, C.c_size_t]),
     "kf_pipeline_extract_mesh": (C.c_int, [P, C.c_float, C.POINTER(Mesh)]),
     "kf_frame_kernel_count": (C.c_int, [P, C.POINTER(C.c_uint32)]),
+    "kf_batch_create": (C.c_int, [P, P, P, C.c_uint32, C.POINTER(P)]),
+    "kf_batch_destroy": (C.c_int, [P]),
+    "kf_batch_step": (C.c_int, [P, P, C.c_uint32, C.c_uint32, P, P, P, C.c_int32]),
+    "kf_batch_stream": (C.c_int, [P, C.POINTER(P)]),
+    "kf_batch_kernel_count": (C.c_int, [P, C.POINTER(C.c_uint32)]),
     "kf_pipeline_block_stats": (C.c_int, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "kf_pipeline_download_block_grid": (C.c_int, [P, P, C.c_size_t]),
     "kf_mesh_free": (None, [C.POINTER(Mesh)]),

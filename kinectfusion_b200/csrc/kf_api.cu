@@ -122,7 +122,11 @@ Pipeline::Maps& Pipeline::maps_for(uint32_t w, uint32_t h) {
 }
 
 void Pipeline::clear_graphs() {
-  for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
+  for (auto& kv : graphs) {
+    cudaGraphExecDestroy(kv.second.exec);
+    cudaGraphDestroy(kv.second.graph);
+  }
+  ++graph_epoch;
   graphs.clear();
 }
 

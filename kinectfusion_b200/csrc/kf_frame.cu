@@ -7,6 +7,7 @@
 // One graph launch and at most one host synchronisation per frame.  The
 // reference syncs once per ICP iteration (icp_correspondence.cu:589-596).
 #include <cstring>
+#include <map>
 
 #include <vector>
 
@@ -17,6 +18,9 @@ namespace {
 
 __global__ void frame_begin_kernel(IcpState* st) {
   if (threadIdx.x != 0) return;
+  // The reference keeps the camera pose as a float matrix between frames
+  // (reconstruction.cpp:237-275): each frame starts from the float pose.
+  for (int i = 0; i < 12; ++i) st->pose[i] = static_cast<double>(static_cast<float>(st->pose[i]));
   st->failed = 0;
   for (int l = 0; l < 4; ++l) {
     st->level_status[l] = KF_ICP_NOT_RUN;
@@ -71,10 +75,12 @@ void record_frame(Pipeline& p, Pyramid& pyr, Tracker& t, const Pipeline::GraphKe
   check(cudaMemcpyAsync(p.result_staging.ptr, st, sizeof(IcpState), cudaMemcpyDeviceToHost, s), "result download");
 }
 
-void enqueue(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker, const uint16_t* depth,
-             const uint32_t* color, uint32_t width, uint32_t height, kf_intrinsics intrinsics, int32_t memory,
-             const uint32_t* iterations, int32_t first_frame) {
-  require(pipeline && pyramid && tracker && depth, "kf_frame_enqueue: null argument");
+// The frame graph of (pipeline, pyramid, tracker) for this frame's size,
+// schedule, first-frame flag and colour, captured on first use.
+Pipeline::FrameGraph& frame_graph_for(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker,
+                                      uint32_t width, uint32_t height, kf_intrinsics intrinsics,
+                                      const uint32_t* iterations, int32_t first_frame, bool has_color) {
+  require(pipeline && pyramid && tracker, "kf_frame_enqueue: null argument");
   require(intrinsics.fx > 0.0f && intrinsics.fy > 0.0f, "Depth frame intrinsics must have positive focal lengths");
   Pipeline& p = pipeline->impl;
   Pyramid& pyr = pyramid->impl;
@@ -93,7 +99,7 @@ void enqueue(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker, co
   if (p.pixel_table.count != n) p.pixel_table.resize(n);
   if (p.frame_color.count != n) p.frame_color.resize(n);
   p.result_staging.resize(1);
-  Pipeline::GraphKey key{width, height, 0, 0, 0, 0, first_frame ? 1u : 0u, color != nullptr ? 1u : 0u};
+  Pipeline::GraphKey key{width, height, 0, 0, 0, 0, first_frame ? 1u : 0u, has_color ? 1u : 0u};
   uint32_t* its[4] = {&key.it0, &key.it1, &key.it2, &key.it3};
   for (uint32_t l = 0; l < 4; ++l) *its[l] = (iterations != nullptr && l < pyr.level_count) ? iterations[l] : 0u;
   if (iterations == nullptr) {
@@ -102,59 +108,75 @@ void enqueue(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker, co
     key.it1 = 5;
     key.it2 = key.it3 = 4;
   }
-  // Inputs into the graph's fixed buffers.
+  auto it = p.graphs.find(key);
+  if (it != p.graphs.end()) return it->second;
+  // Size every buffer the graph touches before capture.
+  for (uint32_t level = 0; level < pyr.level_count; ++level) p.maps_for(width >> level, height >> level);
+  prepare_blocks(p, width, height, s);
+  check(cudaStreamSynchronize(s), "pre-capture sync");
+  cudaGraph_t graph = nullptr;
+  check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+  try {
+    record_frame(p, pyr, t, key, has_color, s);
+  } catch (...) {
+    cudaStreamEndCapture(s, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  check(cudaStreamEndCapture(s, &graph), "end capture");
+  Pipeline::FrameGraph fg;
+  fg.graph = graph;
+  size_t nodes = 0;
+  cudaError_t e = cudaGraphGetNodes(graph, nullptr, &nodes);
+  if (e == cudaSuccess && nodes > 0) {
+    std::vector<cudaGraphNode_t> list(nodes);
+    e = cudaGraphGetNodes(graph, list.data(), &nodes);
+    for (size_t i = 0; e == cudaSuccess && i < nodes; ++i) {
+      cudaGraphNodeType type;
+      e = cudaGraphNodeGetType(list[i], &type);
+      if (e == cudaSuccess && type == cudaGraphNodeTypeKernel) ++fg.kernels;
+    }
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&fg.exec, graph, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    check(e, "graph instantiate");
+  }
+  return p.graphs.emplace(key, fg).first->second;
+}
+
+// The frame's inputs into the graph's fixed buffers, on stream `s`.
+void stage_inputs(Pipeline& p, Pyramid& pyr, const uint16_t* depth, const uint32_t* color, size_t n,
+                  int32_t memory, cudaStream_t s) {
   if (memory == KF_MEMORY_DEVICE) {
     check(cudaMemcpyAsync(pyr.raw.ptr, depth, n * sizeof(uint16_t), cudaMemcpyDeviceToDevice, s), "depth copy");
     if (color) check(cudaMemcpyAsync(p.frame_color.ptr, color, n * 4, cudaMemcpyDeviceToDevice, s), "color copy");
-  } else {
-    // Host buffers go through pinned staging so the copy is a true async DMA;
-    // wait for the previous frame's copy before overwriting the staging.
-    check(cudaStreamSynchronize(s), "staging reuse");
-    p.depth_staging.resize(n);
-    std::memcpy(p.depth_staging.ptr, depth, n * sizeof(uint16_t));
-    check(cudaMemcpyAsync(pyr.raw.ptr, p.depth_staging.ptr, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s),
-          "depth upload");
-    if (color) {
-      p.color_staging.resize(n);
-      std::memcpy(p.color_staging.ptr, color, n * 4);
-      check(cudaMemcpyAsync(p.frame_color.ptr, p.color_staging.ptr, n * 4, cudaMemcpyHostToDevice, s), "color upload");
-    }
+    return;
   }
-  auto it = p.graphs.find(key);
-  if (it == p.graphs.end()) {
-    // Size every buffer the graph touches before capture.
-    for (uint32_t level = 0; level < pyr.level_count; ++level) p.maps_for(width >> level, height >> level);
-    prepare_blocks(p, width, height, s);
-    check(cudaStreamSynchronize(s), "pre-capture sync");
-    cudaGraph_t graph = nullptr;
-    check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
-    try {
-      record_frame(p, pyr, t, key, color != nullptr, s);
-    } catch (...) {
-      cudaStreamEndCapture(s, &graph);
-      if (graph) cudaGraphDestroy(graph);
-      throw;
-    }
-    check(cudaStreamEndCapture(s, &graph), "end capture");
-    Pipeline::FrameGraph fg;
-    size_t nodes = 0;
-    cudaError_t e = cudaGraphGetNodes(graph, nullptr, &nodes);
-    if (e == cudaSuccess && nodes > 0) {
-      std::vector<cudaGraphNode_t> list(nodes);
-      e = cudaGraphGetNodes(graph, list.data(), &nodes);
-      for (size_t i = 0; e == cudaSuccess && i < nodes; ++i) {
-        cudaGraphNodeType type;
-        e = cudaGraphNodeGetType(list[i], &type);
-        if (e == cudaSuccess && type == cudaGraphNodeTypeKernel) ++fg.kernels;
-      }
-    }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&fg.exec, graph, 0);
-    cudaGraphDestroy(graph);
-    check(e, "graph instantiate");
-    it = p.graphs.emplace(key, fg).first;
+  // Host buffers go through pinned staging so the copy is a true async DMA;
+  // wait for the previous frame's copy before overwriting the staging.
+  check(cudaStreamSynchronize(s), "staging reuse");
+  p.depth_staging.resize(n);
+  std::memcpy(p.depth_staging.ptr, depth, n * sizeof(uint16_t));
+  check(cudaMemcpyAsync(pyr.raw.ptr, p.depth_staging.ptr, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s),
+        "depth upload");
+  if (color) {
+    p.color_staging.resize(n);
+    std::memcpy(p.color_staging.ptr, color, n * 4);
+    check(cudaMemcpyAsync(p.frame_color.ptr, p.color_staging.ptr, n * 4, cudaMemcpyHostToDevice, s), "color upload");
   }
-  check(cudaGraphLaunch(it->second.exec, s), "frame graph launch");
-  p.last_frame_kernels = it->second.kernels;
+}
+
+void enqueue(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker, const uint16_t* depth,
+             const uint32_t* color, uint32_t width, uint32_t height, kf_intrinsics intrinsics, int32_t memory,
+             const uint32_t* iterations, int32_t first_frame) {
+  require(depth != nullptr, "kf_frame_enqueue: null argument");
+  Pipeline::FrameGraph& fg = frame_graph_for(pipeline, pyramid, tracker, width, height, intrinsics, iterations,
+                                             first_frame, color != nullptr);
+  Pipeline& p = pipeline->impl;
+  stage_inputs(p, pyramid->impl, depth, color, static_cast<size_t>(width) * height, memory, p.stream);
+  check(cudaGraphLaunch(fg.exec, p.stream), "frame graph launch");
+  p.last_frame_kernels = fg.kernels;
 }
 
 void fill_result(const IcpState& st, int first, kf_frame_result* r) {
@@ -170,12 +192,151 @@ void fill_result(const IcpState& st, int first, kf_frame_result* r) {
   }
 }
 
+// A set of independent sequences stepped together: every member's frame
+// graph becomes a child node of one parent graph, so one launch runs all of
+// them concurrently (no dependencies between the branches).
+struct BatchGraph {
+  cudaGraphExec_t exec = nullptr;
+  uint32_t kernels = 0;
+};
+
+}  // namespace
+}  // namespace kf
+
+struct kf_batch {
+  std::vector<kf_pipeline*> pipelines;
+  std::vector<kf_pyramid*> pyramids;
+  std::vector<kf_tracker*> trackers;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;
+  std::vector<cudaEvent_t> member_ready;
+  std::map<std::vector<uint64_t>, kf::BatchGraph> graphs;
+  uint32_t last_kernels = 0;
+  ~kf_batch() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
+    for (cudaEvent_t e : member_ready) cudaEventDestroy(e);
+    if (done) cudaEventDestroy(done);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace kf {
+namespace {
+
+void batch_step(kf_batch* b, const uint16_t* const* depths, uint32_t width, uint32_t height,
+                const kf_intrinsics* intrinsics, const uint32_t* iterations, const uint8_t* first, int32_t memory) {
+  require(b != nullptr && depths != nullptr && intrinsics != nullptr, "kf_batch_step: null argument");
+  const size_t count = b->pipelines.size();
+  std::vector<Pipeline::FrameGraph*> graphs(count, nullptr);
+  std::vector<uint64_t> key(2 * count, 0);
+  for (size_t i = 0; i < count; ++i) {
+    if (depths[i] == nullptr) continue;  // this member sits out the step
+    graphs[i] = &frame_graph_for(b->pipelines[i], b->pyramids[i], b->trackers[i], width, height, intrinsics[i],
+                                 iterations, first != nullptr && first[i] != 0, false);
+    key[2 * i] = reinterpret_cast<uint64_t>(graphs[i]->graph);
+    key[2 * i + 1] = b->pipelines[i]->impl.graph_epoch;
+  }
+  // the batch stream runs after each member's earlier work
+  for (size_t i = 0; i < count; ++i) {
+    if (!graphs[i]) continue;
+    check(cudaEventRecord(b->member_ready[i], b->pipelines[i]->impl.stream), "batch order");
+    check(cudaStreamWaitEvent(b->stream, b->member_ready[i], 0), "batch order");
+  }
+  for (size_t i = 0; i < count; ++i) {
+    if (!graphs[i]) continue;
+    stage_inputs(b->pipelines[i]->impl, b->pyramids[i]->impl, depths[i], nullptr,
+                 static_cast<size_t>(width) * height, memory, b->stream);
+  }
+  auto it = b->graphs.find(key);
+  if (it == b->graphs.end()) {
+    cudaGraph_t parent = nullptr;
+    check(cudaGraphCreate(&parent, 0), "batch graph");
+    BatchGraph bg;
+    cudaError_t e = cudaSuccess;
+    for (size_t i = 0; i < count && e == cudaSuccess; ++i) {
+      if (!graphs[i]) continue;
+      cudaGraphNode_t node;
+      e = cudaGraphAddChildGraphNode(&node, parent, nullptr, 0, graphs[i]->graph);
+      bg.kernels += graphs[i]->kernels;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&bg.exec, parent, 0);
+    cudaGraphDestroy(parent);
+    check(e, "batch graph instantiate");
+    it = b->graphs.emplace(key, bg).first;
+  }
+  check(cudaGraphLaunch(it->second.exec, b->stream), "batch graph launch");
+  b->last_kernels = it->second.kernels;
+  // later work of each member runs after the step
+  check(cudaEventRecord(b->done, b->stream), "batch order");
+  for (size_t i = 0; i < count; ++i) {
+    if (!graphs[i]) continue;
+    check(cudaStreamWaitEvent(b->pipelines[i]->impl.stream, b->done, 0), "batch order");
+    b->pipelines[i]->impl.last_frame_kernels = graphs[i]->kernels;
+  }
+}
+
 }  // namespace
 }  // namespace kf
 
 using namespace kf;
 
 extern "C" {
+
+kf_status kf_batch_create(kf_pipeline* const* pipelines, kf_pyramid* const* pyramids, kf_tracker* const* trackers,
+                          uint32_t count, kf_batch** out) {
+  return guarded([&] {
+    require(pipelines != nullptr && pyramids != nullptr && trackers != nullptr && out != nullptr && count > 0,
+            "kf_batch_create: null argument");
+    auto* b = new kf_batch();
+    try {
+      for (uint32_t i = 0; i < count; ++i) {
+        require(pipelines[i] && pyramids[i] && trackers[i], "kf_batch_create: null member");
+        for (uint32_t j = 0; j < i; ++j) {
+          require(pipelines[j] != pipelines[i] && pyramids[j] != pyramids[i] && trackers[j] != trackers[i],
+                  "kf_batch_create: members must not share a pipeline, pyramid or tracker");
+        }
+        b->pipelines.push_back(pipelines[i]);
+        b->pyramids.push_back(pyramids[i]);
+        b->trackers.push_back(trackers[i]);
+        cudaEvent_t e;
+        check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "batch event");
+        b->member_ready.push_back(e);
+      }
+      check(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "batch stream");
+      check(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming), "batch event");
+    } catch (...) {
+      delete b;
+      throw;
+    }
+    *out = b;
+  });
+}
+
+kf_status kf_batch_destroy(kf_batch* batch) {
+  return guarded([&] { delete batch; });
+}
+
+kf_status kf_batch_step(kf_batch* batch, const uint16_t* const* depths, uint32_t width, uint32_t height,
+                        const kf_intrinsics* intrinsics, const uint32_t* iterations_per_level,
+                        const uint8_t* first_frame, int32_t memory) {
+  return guarded(
+      [&] { batch_step(batch, depths, width, height, intrinsics, iterations_per_level, first_frame, memory); });
+}
+
+kf_status kf_batch_stream(kf_batch* batch, void** stream) {
+  return guarded([&] {
+    require(batch != nullptr && stream != nullptr, "kf_batch_stream: null argument");
+    *stream = batch->stream;
+  });
+}
+
+kf_status kf_batch_kernel_count(kf_batch* batch, uint32_t* kernels) {
+  return guarded([&] {
+    require(batch != nullptr && kernels != nullptr, "kf_batch_kernel_count: null argument");
+    *kernels = batch->last_kernels;
+  });
+}
 
 kf_status kf_frame_kernel_count(kf_pipeline* pipeline, uint32_t* kernels) {
   return guarded([&] {

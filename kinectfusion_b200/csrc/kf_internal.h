@@ -294,10 +294,12 @@ struct Pipeline {
     }
   };
   struct FrameGraph {
+    cudaGraph_t graph = nullptr;     // kept for batches (child graph nodes)
     cudaGraphExec_t exec = nullptr;
     uint32_t kernels = 0;  // kernel nodes of the captured frame
   };
   std::map<GraphKey, FrameGraph> graphs;
+  uint64_t graph_epoch = 0;  // bumped whenever the frame graphs are dropped
   uint32_t last_frame_kernels = 0;
   kf_pyramid* graph_pyramid = nullptr;
   kf_tracker* graph_tracker = nullptr;

@@ -294,3 +294,57 @@ class Reconstruction:
         self.trajectory.append(abi.matrix_from_rigid(self.pose))
         self.results.append(result)
         return result
+
+
+class Batch:
+    """Independent sequences stepped together (kf_batch_*): one graph launch
+    runs one frame of every member.  Each member is a Reconstruction-like
+    triple (pipeline, pyramid, tracker) over its own volume."""
+
+    def __init__(self, pipelines: list[Pipeline], intrinsics: abi.Intrinsics, depth_options=None, icp_options=None,
+                 iterations=ICP_ITERATIONS):
+        self.pipelines = list(pipelines)
+        self.pyramids = [PyramidSource(depth_options) for _ in self.pipelines]
+        self.trackers = [ProjectiveIcpTracker(icp_options) for _ in self.pipelines]
+        n = len(self.pipelines)
+        arr = C.c_void_p * n
+        self.handle = C.c_void_p()
+        _check(lib().kf_batch_create(arr(*[p.handle for p in self.pipelines]),
+                                     arr(*[p.handle for p in self.pyramids]),
+                                     arr(*[t.handle for t in self.trackers]), n, C.byref(self.handle)))
+        self.intrinsics = (abi.Intrinsics * n)(*([intrinsics] * n))
+        self.iterations = (C.c_uint32 * 4)(*iterations)
+        self.frames = [0] * n
+
+    def __del__(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            lib().kf_batch_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def step(self, device_depths: list, width: int = 640, height: int = 480):
+        """device_depths[i]: device address of member i's u16 depth frame, or
+        None when member i sits this step out."""
+        n = len(self.pipelines)
+        depths = (C.c_void_p * n)(*[d if d is not None else None for d in device_depths])
+        first = (C.c_uint8 * n)(*[1 if (d is not None and self.frames[i] == 0) else 0
+                                  for i, d in enumerate(device_depths)])
+        _check(lib().kf_batch_step(self.handle, depths, width, height, self.intrinsics, self.iterations, first,
+                                   abi.KF_MEMORY_DEVICE))
+        for i, d in enumerate(device_depths):
+            if d is not None:
+                self.frames[i] += 1
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(lib().kf_batch_stream(self.handle, C.byref(s)))
+        return s.value
+
+    def kernel_count(self) -> int:
+        k = C.c_uint32()
+        _check(lib().kf_batch_kernel_count(self.handle, C.byref(k)))
+        return k.value
+
+    def result(self, i: int) -> abi.FrameResult:
+        r = abi.FrameResult()
+        _check(lib().kf_frame_result_fetch(self.pipelines[i].handle, C.byref(r)))
+        return r

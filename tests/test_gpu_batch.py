@@ -1,0 +1,49 @@
+"""Batches of independent sequences (kf_batch_*): one graph launch per step
+runs every member's frame; the results are those of the members run alone."""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import kinectfusion_b200 as kf
+from kinectfusion_b200 import abi, synthetic
+
+pytestmark = pytest.mark.gpu
+
+K640 = abi.Intrinsics(synthetic.FX, synthetic.FY, synthetic.CX, synthetic.CY)
+MEMBERS = [(64, 0.04, abi.KF_VOXEL_QUANTIZED), (96, 0.03, abi.KF_VOXEL_BF16), (128, 0.02, abi.KF_VOXEL_QUANTIZED)]
+
+
+def _config(res, vs, voxel):
+    half = 0.5 * res * vs
+    return kf.pipeline_config(res, vs, (-half, -half, -0.5), 0.05, voxel=voxel, color=abi.KF_COLOR_NONE)
+
+
+def test_batch_matches_members_run_alone():
+    import torch  # device memory plumbing only
+    seqs = [synthetic.make_sequence(seed=40 + i, frames=4) for i in range(len(MEMBERS))]
+    frames = [torch.from_numpy(s.depth.view(np.int16)).cuda() for s in seqs]
+    torch.cuda.synchronize()
+    batch = kf.Batch([kf.Pipeline(_config(*m)) for m in MEMBERS], K640)
+    poses = [[] for _ in MEMBERS]
+    for f in range(4):
+        # member 1 sits out step 2 and catches up at the end
+        ptrs = [frames[i][f].data_ptr() if not (i == 1 and f == 2) else None for i in range(len(MEMBERS))]
+        batch.step(ptrs)
+        for i, p in enumerate(ptrs):
+            if p is not None:
+                poses[i].append(abi.matrix_from_rigid(batch.result(i).camera_to_world))
+    batch.step([None, frames[1][2].data_ptr(), None])
+    poses[1].insert(2, abi.matrix_from_rigid(batch.result(1).camera_to_world))
+    assert batch.kernel_count() > 0
+    for i, m in enumerate(MEMBERS):
+        alone = kf.Reconstruction(kf.Pipeline(_config(*m)), K640)
+        order = [0, 1, 2, 3] if i != 1 else [0, 1, 3, 2]
+        got = {}
+        for f in order:
+            alone.process(seqs[i].depth[f])
+            got[f] = alone.trajectory[-1]
+        for f in range(4):
+            assert np.array_equal(np.asarray(got[f], dtype=np.float32), np.asarray(poses[i][f], dtype=np.float32)), (i, f)
+        assert np.array_equal(alone.pipeline.download_raw(), batch.pipelines[i].download_raw()), i
