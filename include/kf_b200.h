@@ -302,6 +302,23 @@ kf_status kf_pipeline_set_kernel_events(kf_pipeline* pipeline, void* start, void
 kf_status kf_pipeline_update_counts(kf_pipeline* pipeline, uint64_t* voxel_updates,
                                     uint64_t* color_updates);
 
+/* ---- launch shapes and the autotuner (no counterpart in the reference) ----
+ * Shapes that leave every output bit unchanged: the march kernel's CTA
+ * (raycast_block_x * raycast_block_y <= 64 threads) and the fusion grid. */
+typedef struct {
+  uint32_t raycast_block_x, raycast_block_y;
+  uint32_t integrate_ctas;
+} kf_launch_shapes;
+kf_status kf_pipeline_get_launch_shapes(kf_pipeline* pipeline, kf_launch_shapes* shapes);
+kf_status kf_pipeline_set_launch_shapes(kf_pipeline* pipeline, const kf_launch_shapes* shapes);
+/* Times the candidate shapes on a scratch pipeline of the same configuration
+ * over `count` consecutive device-resident width x height depth frames (the
+ * first fused, the rest tracked), applies the fastest to `pipeline` and
+ * returns it (and its time for frames 1..count-1 in best_ms, may be NULL). */
+kf_status kf_pipeline_autotune(kf_pipeline* pipeline, const uint16_t* frames, uint32_t count,
+                               uint32_t width, uint32_t height, kf_intrinsics intrinsics,
+                               kf_launch_shapes* chosen, float* best_ms);
+
 /* ---- tracker: ProjectiveIcpTracker::estimate_pose(DeviceTrackingRequest)
  * (icp_optimizer.hpp:115-116, icp_optimizer.cpp:58-76) with the device solve. */
 kf_status kf_tracker_create(const kf_icp_options* options, kf_tracker** out);

@@ -83,6 +83,10 @@ class VolumeGeometry(C.Structure):
                 ("origin", C.c_float * 3), ("truncation_distance", C.c_float)]
 
 
+class LaunchShapes(C.Structure):
+    _fields_ = [("raycast_block_x", C.c_uint32), ("raycast_block_y", C.c_uint32), ("integrate_ctas", C.c_uint32)]
+
+
 class PipelineConfig(C.Structure):
     _fields_ = [("volume", VolumeGeometry), ("voxel", C.c_int32), ("color", C.c_int32), ("storage", C.c_int32),
                 ("sparse_block_capacity", C.c_uint64), ("tsdf_rule", C.c_int32),
@@ -165,6 +169,10 @@ _PROTOTYPES = {
     "kf_pipeline_extract_mesh": (C.c_int, [P, C.c_float, C.POINTER(Mesh)]),
     "kf_frame_kernel_count": (C.c_int, [P, C.POINTER(C.c_uint32)]),
     "kf_batch_create": (C.c_int, [P, P, P, C.c_uint32, C.POINTER(P)]),
+    "kf_pipeline_get_launch_shapes": (C.c_int, [P, C.POINTER(LaunchShapes)]),
+    "kf_pipeline_set_launch_shapes": (C.c_int, [P, C.POINTER(LaunchShapes)]),
+    "kf_pipeline_autotune": (C.c_int, [P, P, C.c_uint32, C.c_uint32, C.c_uint32, Intrinsics, C.POINTER(LaunchShapes),
+                                       C.POINTER(C.c_float)]),
     "kf_batch_destroy": (C.c_int, [P]),
     "kf_batch_step": (C.c_int, [P, P, C.c_uint32, C.c_uint32, P, P, P, C.c_int32]),
     "kf_batch_stream": (C.c_int, [P, C.POINTER(P)]),

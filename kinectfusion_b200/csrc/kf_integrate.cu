@@ -634,7 +634,7 @@ template <int Kind, bool Color>
 void launch_blocks_typed(Pipeline& p, const float4* table, uint32_t width, uint32_t height, Intr k, Rigid T,
                          const IntegParams& ip, const IcpState* state, cudaStream_t s) {
   if (state == nullptr && p.kernel_start != nullptr) check(cudaEventRecord(p.kernel_start, s), "event record");
-  integrate_blocks_kernel<Kind, Color><<<148 * 12, kBlockThreads, 0, s>>>(
+  integrate_blocks_kernel<Kind, Color><<<p.integrate_ctas, kBlockThreads, 0, s>>>(
       p.view, table, width, height, k, T, ip, state, p.block_list.ptr, p.block_count.ptr,
       p.voxel_bits.count ? p.voxel_bits.ptr : nullptr, p.brick_dirty.ptr, p.counters.ptr);
   check(cudaGetLastError(), "integrate_blocks_kernel launch");

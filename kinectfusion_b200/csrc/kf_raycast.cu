@@ -504,8 +504,8 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
   rp.policy = p.config.raycast.corner_policy;
   rp.cell_normals = p.config.raycast.cell_gradient_normals;
   rp.seed_previous = p.config.raycast.seed_from_previous;
-  const dim3 block(8, 8);
-  const dim3 grid(ceil_div(cam.width, 8), ceil_div(cam.height, 8));
+  const dim3 block(p.raycast_block_x, p.raycast_block_y);
+  const dim3 grid(ceil_div(cam.width, block.x), ceil_div(cam.height, block.y));
   // the skip structures exist once a full-sweep integration prepared them
   const uint32_t* voxel_bits = p.brick_class.count && p.view.grid == nullptr ? p.voxel_bits.ptr : nullptr;
   const uint4* stencil_bits = reinterpret_cast<const uint4*>(p.stencil_bits.ptr);

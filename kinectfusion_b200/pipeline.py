@@ -232,6 +232,23 @@ class Pipeline:
         _check(lib().kf_pipeline_download_raw(self.handle, _ptr(raw), raw.nbytes, None, 0))
         return raw
 
+    def launch_shapes(self) -> abi.LaunchShapes:
+        shapes = abi.LaunchShapes()
+        _check(lib().kf_pipeline_get_launch_shapes(self.handle, C.byref(shapes)))
+        return shapes
+
+    def set_launch_shapes(self, raycast_block=(8, 8), integrate_ctas=148 * 12):
+        shapes = abi.LaunchShapes(raycast_block[0], raycast_block[1], integrate_ctas)
+        _check(lib().kf_pipeline_set_launch_shapes(self.handle, C.byref(shapes)))
+
+    def autotune(self, device_frames: int, count: int, intrinsics: abi.Intrinsics, width: int = 640,
+                 height: int = 480) -> tuple[abi.LaunchShapes, float]:
+        """kf_pipeline_autotune over `count` consecutive device-resident frames."""
+        shapes, ms = abi.LaunchShapes(), C.c_float()
+        _check(lib().kf_pipeline_autotune(self.handle, C.c_void_p(device_frames), count, width, height, intrinsics,
+                                          C.byref(shapes), C.byref(ms)))
+        return shapes, ms.value
+
     def block_stats(self) -> tuple[int, int]:
         """Sparse storage: (allocation attempts, capacity) of the block pool."""
         attempts, capacity = C.c_uint64(), C.c_uint64()

@@ -47,3 +47,25 @@ def test_batch_matches_members_run_alone():
         for f in range(4):
             assert np.array_equal(np.asarray(got[f], dtype=np.float32), np.asarray(poses[i][f], dtype=np.float32)), (i, f)
         assert np.array_equal(alone.pipeline.download_raw(), batch.pipelines[i].download_raw()), i
+
+
+def test_autotuned_shapes_change_no_bit():
+    # kf_pipeline_autotune: the tuned launch shapes give the same poses and
+    # volume as the defaults
+    import torch
+    seq = synthetic.make_sequence(seed=50, frames=5)
+    frames = torch.from_numpy(seq.depth.view(np.int16)).cuda()
+    torch.cuda.synchronize()
+    tuned = kf.Pipeline(_config(128, 0.02, abi.KF_VOXEL_BF16))
+    shapes, ms = tuned.autotune(frames.data_ptr(), 4, K640)
+    assert shapes.raycast_block_x * shapes.raycast_block_y <= 64 and shapes.integrate_ctas > 0 and ms > 0
+    odd = kf.Pipeline(_config(128, 0.02, abi.KF_VOXEL_BF16))
+    odd.set_launch_shapes((32, 2), 148 * 4)
+    plain = kf.Pipeline(_config(128, 0.02, abi.KF_VOXEL_BF16))
+    loops = [kf.Reconstruction(p, K640) for p in (tuned, odd, plain)]
+    for f in range(5):
+        for loop in loops:
+            loop.process(seq.depth[f])
+    for loop in loops[:2]:
+        assert all(np.array_equal(a, b) for a, b in zip(loop.trajectory, loops[2].trajectory))
+        assert np.array_equal(loop.pipeline.download_raw(), plain.download_raw())
