@@ -1584,3 +1584,65 @@ kf_status kfo_marching_cubes(const kfo_volume* volume, float min_weight, kf_mesh
   out->triangle_count = b.nt;
   return KF_OK;
 }
+
+/* ------------------------------------------------------------------------ */
+/* FP64 integration: IntegrationContext::observe + BasicVoxel::fused        */
+/* (tsdf_integration.hpp:183-263, volume.hpp:137-146) in double, into a      */
+/* (tsdf, weight) double pair per voxel, x fastest.  The reference point     */
+/* for the FP32/int16/bf16 volumes' error statements.                        */
+/* ------------------------------------------------------------------------ */
+void kfo_integrate_f64(double* voxels, const kf_volume_geometry* g, const kf_frame_view* f,
+                       const kf_integration_options* o, int32_t rule, int32_t threads) {
+  const double R[9] = {f->world_to_camera.r[0], f->world_to_camera.r[1], f->world_to_camera.r[2],
+                       f->world_to_camera.r[3], f->world_to_camera.r[4], f->world_to_camera.r[5],
+                       f->world_to_camera.r[6], f->world_to_camera.r[7], f->world_to_camera.r[8]};
+  const double T[3] = {f->world_to_camera.t[0], f->world_to_camera.t[1], f->world_to_camera.t[2]};
+  const double fx = f->intrinsics.fx, fy = f->intrinsics.fy, cx = f->intrinsics.cx, cy = f->intrinsics.cy;
+  (void)threads;
+#ifdef _OPENMP
+  const int nt = threads > 0 ? threads : 1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+#endif
+  for (int64_t z = 0; z < (int64_t)g->res_z; ++z) {
+    for (uint64_t y = 0; y < g->res_y; ++y) {
+      for (uint64_t x = 0; x < g->res_x; ++x) {
+        const double c[3] = {g->origin[0] + ((double)x + 0.5) * g->voxel_size,
+                             g->origin[1] + ((double)y + 0.5) * g->voxel_size,
+                             g->origin[2] + ((double)z + 0.5) * g->voxel_size};
+        double cp[3];
+        for (int i = 0; i < 3; ++i) cp[i] = R[i * 3] * c[0] + R[i * 3 + 1] * c[1] + R[i * 3 + 2] * c[2] + T[i];
+        if (cp[2] <= 0.0) continue;
+        const long rx = lround(fx * cp[0] / cp[2] + cx), ry = lround(fy * cp[1] / cp[2] + cy);
+        if (rx < 0 || ry < 0 || (unsigned long)rx >= f->width || (unsigned long)ry >= f->height) continue;
+        const size_t pix = (size_t)ry * f->width + (size_t)rx;
+        const uint16_t raw = f->depth[pix];
+        if (raw == 0) continue;
+        const double measured = (double)raw / o->depth_scale;
+        if (measured < o->min_depth || measured > o->max_depth) continue;
+        const double ray[3] = {((double)rx - cx) / fx, ((double)ry - cy) / fy, 1.0};
+        const double lambda = sqrt(ray[0] * ray[0] + ray[1] * ray[1] + 1.0);
+        const double trunc = o->distance_scaled_truncation
+                                 ? (double)g->truncation_distance + o->truncation_distance_scale * measured
+                                 : (double)g->truncation_distance;
+        const double dist = sqrt(cp[0] * cp[0] + cp[1] * cp[1] + cp[2] * cp[2]);
+        const double sdf = o->projective_distance ? measured - dist / lambda : measured - cp[2];
+        if (sdf < -trunc) continue;
+        const double tsdf = sdf / trunc > 1.0 ? 1.0 : (sdf / trunc < -1.0 ? -1.0 : sdf / trunc);
+        double weight = o->observation_weight;
+        if (rule == KF_RULE_ANGLE_WEIGHTED && f->normals != NULL) {
+          const float* n = f->normals + pix * 3;
+          if (isfinite(n[0]) && isfinite(n[1]) && isfinite(n[2])) {
+            const double nn = sqrt((double)n[0] * n[0] + (double)n[1] * n[1] + (double)n[2] * n[2]);
+            const double d = -((double)n[0] * ray[0] + (double)n[1] * ray[1] + (double)n[2] * ray[2]) / (nn * lambda);
+            weight *= (d > 0.0 ? d : 0.0) / measured;
+          }
+        }
+        if (weight <= 0.0) continue;
+        double* vx = voxels + ((z * g->res_y + y) * g->res_x + x) * 2;
+        const double w0 = vx[1];
+        vx[0] = (vx[0] * w0 + tsdf * weight) / (w0 + weight);
+        vx[1] = o->max_weight < w0 + weight ? o->max_weight : w0 + weight;
+      }
+    }
+  }
+}

@@ -73,6 +73,9 @@ void kfo_integrate_band(kfo_volume* volume, const kf_frame_view* frame,
 /* The device band sweep: the same walk at half-block steps. */
 void kfo_integrate_band_device(kfo_volume* volume, const kf_frame_view* frame,
                                const kf_integration_options* options, int32_t rule);
+/* The same integration in FP64 into (tsdf, weight) double pairs, x fastest. */
+void kfo_integrate_f64(double* voxels, const kf_volume_geometry* geometry, const kf_frame_view* frame,
+                       const kf_integration_options* options, int32_t rule, int32_t threads);
 void kfo_integrate_sparse(kfo_volume* volume, const kf_frame_view* frame,
                           const kf_integration_options* options, int32_t rule);
 

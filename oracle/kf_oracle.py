@@ -56,6 +56,8 @@ def load() -> C.CDLL:
                                       C.POINTER(abi.IntegrationOptions), C.c_int32]),
         "kfo_integrate_band_device": (None, [C.POINTER(Volume), C.POINTER(abi.FrameView),
                                              C.POINTER(abi.IntegrationOptions), C.c_int32]),
+        "kfo_integrate_f64": (None, [P, C.POINTER(abi.VolumeGeometry), C.POINTER(abi.FrameView),
+                                     C.POINTER(abi.IntegrationOptions), C.c_int32, C.c_int32]),
         "kfo_integrate_sparse": (None, [C.POINTER(Volume), C.POINTER(abi.FrameView),
                                         C.POINTER(abi.IntegrationOptions), C.c_int32]),
         "kfo_raycast": (None, [C.POINTER(Volume), C.POINTER(abi.RaycastCamera), C.POINTER(abi.RaycastOptions),
@@ -281,6 +283,28 @@ def integrate(vol: OracleVolume, depth, k, world_to_camera, o: abi.IntegrationOp
         fn(C.byref(vol.struct), C.byref(f), C.byref(o), rule)
     else:
         load().kfo_integrate(C.byref(vol.struct), C.byref(f), C.byref(o), rule, threads)
+    del keep
+
+
+class OracleVolumeF64:
+    """FP64 (tsdf, weight) volume for the error statements of the stored volumes."""
+
+    def __init__(self, res, voxel_size, origin, truncation):
+        rx, ry, rz = (res, res, res) if np.isscalar(res) else res
+        self.geometry = abi.VolumeGeometry(rx, ry, rz, voxel_size, (C.c_float * 3)(*origin), truncation)
+        self.voxels = np.zeros((rx * ry * rz, 2), dtype=np.float64)
+        self.voxels[:, 0] = 1.0
+
+    def dense(self):
+        g = self.geometry
+        shape = (g.res_z, g.res_y, g.res_x)
+        return self.voxels[:, 0].reshape(shape), self.voxels[:, 1].reshape(shape)
+
+
+def integrate_f64(vol: OracleVolumeF64, depth, k, world_to_camera, o: abi.IntegrationOptions,
+                  rule=abi.KF_RULE_ANGLE_WEIGHTED, normals_map=None, threads=1):
+    f, keep = frame_view(depth, k, world_to_camera, None, normals_map)
+    load().kfo_integrate_f64(ptr(vol.voxels), C.byref(vol.geometry), C.byref(f), C.byref(o), rule, threads)
     del keep
 
 
