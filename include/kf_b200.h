@@ -302,6 +302,14 @@ kf_status kf_pipeline_set_kernel_events(kf_pipeline* pipeline, void* start, void
 kf_status kf_pipeline_update_counts(kf_pipeline* pipeline, uint64_t* voxel_updates,
                                     uint64_t* color_updates);
 
+/* ---- tensor-core GEMM of the learned warm-start (no counterpart in the
+ * reference): c[m x n] (fp32) = a[m x k] * b[n x k]^T (+ bias[n]) (ReLU when
+ * relu != 0), a and b bf16 row-major on the device, k a multiple of 8, all
+ * three 16-byte aligned; stream is a cudaStream_t (NULL: the default
+ * stream).  Runs on tcgen05 (sm_100a). */
+kf_status kf_gemm_bf16(const void* a, const void* b, float* c, int32_t m, int32_t n, int32_t k,
+                       const float* bias, int32_t relu, void* stream);
+
 /* ---- launch shapes and the autotuner (no counterpart in the reference) ----
  * Shapes that leave every output bit unchanged: the march kernel's CTA
  * (raycast_block_x * raycast_block_y <= 64 threads) and the fusion grid. */

@@ -169,6 +169,7 @@ _PROTOTYPES = {
     "kf_pipeline_extract_mesh": (C.c_int, [P, C.c_float, C.POINTER(Mesh)]),
     "kf_frame_kernel_count": (C.c_int, [P, C.POINTER(C.c_uint32)]),
     "kf_batch_create": (C.c_int, [P, P, P, C.c_uint32, C.POINTER(P)]),
+    "kf_gemm_bf16": (C.c_int, [P, P, P, C.c_int32, C.c_int32, C.c_int32, P, C.c_int32, P]),
     "kf_pipeline_get_launch_shapes": (C.c_int, [P, C.POINTER(LaunchShapes)]),
     "kf_pipeline_set_launch_shapes": (C.c_int, [P, C.POINTER(LaunchShapes)]),
     "kf_pipeline_autotune": (C.c_int, [P, P, C.c_uint32, C.c_uint32, C.c_uint32, Intrinsics, C.POINTER(LaunchShapes),

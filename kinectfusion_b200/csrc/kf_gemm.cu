@@ -1,0 +1,221 @@
+// kf_gemm.cu - bf16 GEMM on the 5th-generation tensor cores (tcgen05), the
+// matrix engine of the learned ICP warm-start (no counterpart in the
+// reference).
+//
+//   C[M x N] (fp32) = A[M x K] (bf16, row-major) * B[N x K]^T (bf16, row-major)
+//                     (+ bias[N]) (ReLU)
+//
+// One CTA of 128 threads computes a 128 x BN tile of C.  Per 64-wide K slab:
+// the threads copy the A and B slabs into shared memory in the canonical
+// K-major layout without swizzle (8-row x 16-byte core matrices; the two
+// 8-element halves of a 16-element K step LBO = 128 B apart, consecutive
+// 8-row groups SBO = 256 B apart), then one thread issues four
+// tcgen05.mma.kind::f16 (M = 128, N = BN, K = 16) that accumulate in FP32 in
+// tensor memory, and tcgen05.commit signals an mbarrier when they are done.
+// The epilogue reads the accumulator with tcgen05.ld (each warp its 32 TMEM
+// lanes = 32 rows of the tile).  Every wait is bounded: past the limit the
+// kernel records an error, waits (bounded) for its own MMAs, frees its tensor
+// memory and returns.
+#include <cuda_bf16.h>
+
+#include "kf_internal.h"
+
+namespace kf {
+namespace {
+
+constexpr int kGemmThreads = 128;
+constexpr int kGemmBM = 128;
+constexpr int kGemmBK = 64;
+constexpr unsigned long long kWaitCycles = 2000000000ull;  // ~1 s at 2 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor: K-major, no swizzle (layout type 0),
+// version 1 (sm_100), start address / LBO / SBO in 16-byte units.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((addr >> 4) & 0x3FFFu);
+  d |= static_cast<uint64_t>((lbo_bytes >> 4) & 0x3FFFu) << 16;
+  d |= static_cast<uint64_t>((sbo_bytes >> 4) & 0x3FFFu) << 32;
+  d |= 1ull << 46;  // version
+  return d;
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t instr_desc(uint32_t m, uint32_t n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
+  const unsigned long long start = clock64();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    if (done) return true;
+    if (clock64() - start > kWaitCycles) return false;
+  }
+}
+
+// Byte offset of element (row, k) of a ROWS x 64 slab in the canonical layout.
+__device__ __forceinline__ uint32_t slab_offset(uint32_t row, uint32_t k, uint32_t rows) {
+  return (k >> 4) * (rows / 8u) * 256u + (row >> 3) * 256u + ((k >> 3) & 1u) * 128u + (row & 7u) * 16u;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kGemmThreads)
+    gemm_bf16_kernel(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict__ B, float* __restrict__ C,
+                     int M, int N, int K, int lda, int ldb, int ldc, const float* __restrict__ bias, int relu,
+                     int* __restrict__ error) {
+  constexpr uint32_t kCols = BN < 32 ? 32 : BN;  // tensor-memory columns (a power of two >= 32)
+  __shared__ __align__(1024) uint8_t s_a[kGemmBM * kGemmBK * 2];
+  __shared__ __align__(1024) uint8_t s_b[BN * kGemmBK * 2];
+  __shared__ __align__(8) unsigned long long s_mbar;
+  __shared__ uint32_t s_tmem;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tile_m = blockIdx.x * kGemmBM, tile_n = blockIdx.y * BN;
+  const uint32_t mbar = smem_u32(&s_mbar);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(kCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = s_tmem;
+  const uint32_t idesc = instr_desc(kGemmBM, BN);
+  uint32_t phase = 0;
+  bool ok = true;
+
+  for (int k0 = 0; k0 < K && ok; k0 += kGemmBK) {
+    // A slab: thread t copies row t (8 chunks of 8 bf16)
+    {
+      const int row = tile_m + tid;
+#pragma unroll
+      for (int c = 0; c < kGemmBK / 8; ++c) {
+        const int k = k0 + c * 8;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (row < M && k < K) v = *reinterpret_cast<const uint4*>(A + static_cast<size_t>(row) * lda + k);
+        *reinterpret_cast<uint4*>(s_a + slab_offset(tid, c * 8, kGemmBM)) = v;
+      }
+    }
+    for (int r = tid; r < BN; r += kGemmThreads) {
+      const int row = tile_n + r;
+#pragma unroll
+      for (int c = 0; c < kGemmBK / 8; ++c) {
+        const int k = k0 + c * 8;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (row < N && k < K) v = *reinterpret_cast<const uint4*>(B + static_cast<size_t>(row) * ldb + k);
+        *reinterpret_cast<uint4*>(s_b + slab_offset(r, c * 8, BN)) = v;
+      }
+    }
+    // generic-proxy stores -> visible to the tensor core's async proxy
+    asm volatile("fence.proxy.async.shared::cta;");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+      for (int s = 0; s < kGemmBK / 16; ++s) {
+        const uint64_t da = smem_desc(smem_u32(s_a) + s * (kGemmBM / 8) * 256, 128, 256);
+        const uint64_t db = smem_desc(smem_u32(s_b) + s * (BN / 8) * 256, 128, 256);
+        const uint32_t accumulate = (k0 > 0 || s > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                   : "memory");
+    }
+    ok = mbar_wait(mbar, phase);
+    phase ^= 1u;
+    ok = __syncthreads_and(ok);
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(error, 1);
+  } else {
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const int row = tile_m + warp * 32 + lane;
+#pragma unroll
+    for (int c = 0; c < BN; c += 16) {
+      uint32_t r[16];
+      const uint32_t addr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(addr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < M) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = tile_n + c + j;
+          if (col >= N) continue;
+          float v = __uint_as_float(r[j]);
+          if (bias != nullptr) v += bias[col];
+          if (relu && v < 0.0f) v = 0.0f;
+          C[static_cast<size_t>(row) * ldc + col] = v;
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
+}
+
+}  // namespace
+
+void launch_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int K, int lda, int ldb, int ldc,
+                      const float* bias, int relu, int* error, cudaStream_t s) {
+  require(M > 0 && N > 0 && K > 0, "gemm: empty shape");
+  require(lda % 8 == 0 && ldb % 8 == 0 && K % 8 == 0, "gemm: K and the leading dimensions must be multiples of 8");
+  require(reinterpret_cast<uintptr_t>(A) % 16 == 0 && reinterpret_cast<uintptr_t>(B) % 16 == 0,
+          "gemm: operands must be 16-byte aligned");
+  const auto* a = static_cast<const __nv_bfloat16*>(A);
+  const auto* b = static_cast<const __nv_bfloat16*>(B);
+  const unsigned gm = ceil_div(static_cast<unsigned>(M), static_cast<unsigned>(kGemmBM));
+  if (N <= 16) {
+    gemm_bf16_kernel<16><<<dim3(gm, 1), kGemmThreads, 0, s>>>(a, b, C, M, N, K, lda, ldb, ldc, bias, relu, error);
+  } else if (N <= 32) {
+    gemm_bf16_kernel<32><<<dim3(gm, 1), kGemmThreads, 0, s>>>(a, b, C, M, N, K, lda, ldb, ldc, bias, relu, error);
+  } else if (N <= 64) {
+    gemm_bf16_kernel<64><<<dim3(gm, 1), kGemmThreads, 0, s>>>(a, b, C, M, N, K, lda, ldb, ldc, bias, relu, error);
+  } else {
+    const unsigned gn = ceil_div(static_cast<unsigned>(N), 128u);
+    gemm_bf16_kernel<128><<<dim3(gm, gn), kGemmThreads, 0, s>>>(a, b, C, M, N, K, lda, ldb, ldc, bias, relu, error);
+  }
+  check(cudaGetLastError(), "gemm_bf16_kernel launch");
+}
+
+}  // namespace kf
+
+extern "C" kf_status kf_gemm_bf16(const void* a, const void* b, float* c, int32_t m, int32_t n, int32_t k,
+                                  const float* bias, int32_t relu, void* stream) {
+  return kf::guarded([&] {
+    kf::require(a != nullptr && b != nullptr && c != nullptr, "kf_gemm_bf16: null argument");
+    kf::DeviceArray<int> error(1);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    kf::check(cudaMemsetAsync(error.ptr, 0, sizeof(int), s), "gemm error flag");
+    kf::launch_gemm_bf16(a, b, c, m, n, k, k, k, n, bias, relu, error.ptr, s);
+    int flag = 0;
+    kf::check(cudaMemcpyAsync(&flag, error.ptr, sizeof(int), cudaMemcpyDeviceToHost, s), "gemm error flag");
+    kf::check(cudaStreamSynchronize(s), "gemm");
+    if (flag) throw kf::CudaError("kf_gemm_bf16: tensor-core wait timed out");
+  });
+}

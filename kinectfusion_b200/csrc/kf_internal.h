@@ -327,6 +327,11 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
                       Intr intrinsics, Rigid world_to_camera, int has_color,
                       const IcpState* pose_state, cudaStream_t stream);
 // Allocates and clears the per-block skip and culling buffers.
+// C = A * B^T (+bias)(ReLU) on the tensor cores: A M x K, B N x K bf16
+// row-major (leading dimensions lda, ldb), C M x N fp32 (ldc).  `error`
+// (device int) is set when a tensor-core wait times out.
+void launch_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int K, int lda, int ldb, int ldc,
+                      const float* bias, int relu, int* error, cudaStream_t stream);
 // MarchingCubes::extract on the device (dense volumes); fills a host mesh.
 void extract_mesh(Pipeline& p, float min_weight, kf_mesh& out);
 void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t stream);
