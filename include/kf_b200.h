@@ -414,6 +414,66 @@ kf_status kf_batch_stream(kf_batch* batch, void** stream);
 /* Kernel nodes of the last step's graph. */
 kf_status kf_batch_kernel_count(kf_batch* batch, uint32_t* kernels);
 
+/* ---- learned ICP warm start (no counterpart in the reference) ------------
+ * A bf16 CNN on the tcgen05 tensor cores reads two 80x60 maps - the current
+ * depth (8x8 block means) and the model rendered at the constant-velocity
+ * pose - and proposes the twist from that pose to the tracked one.
+ * Layers: four 3x3 stride-2 pad-1 convolutions (2-32-32-64-64, ReLU), then
+ * 1280-256 (ReLU) and 256-6.  The parameters are one flat fp32 vector: per
+ * layer the weights [out][in] then the bias, every tensor starting at a
+ * multiple of 8 floats; convolution weights are [out][c*9 + ky*3 + kx], conv1
+ * padded to 24 columns whose last 6 stay zero.  Inputs are NHWC bf16
+ * [batch][60][80][2] (channel 0: current depth minus the mean predicted
+ * depth; channel 1: 10 x (current - predicted) clamped to [-1, 1]; metres, 0
+ * where invalid); outputs [batch][6] = (tx, ty, tz, wx, wy, wz) times
+ * KF_WARM_START_TWIST_SCALE, applied as pose * exp: translation added in the
+ * pose's frame, rotation by Rodrigues' formula.  Batches are multiples of 8. */
+#define KF_WARM_START_TWIST_SCALE 50.0
+typedef struct kf_learner kf_learner;
+kf_status kf_learner_create(uint32_t batch_capacity, uint32_t seed, kf_learner** out);
+kf_status kf_learner_destroy(kf_learner* learner);
+kf_status kf_learner_param_count(kf_learner* learner, uint64_t* count);
+kf_status kf_learner_get_params(kf_learner* learner, float* host);
+kf_status kf_learner_set_params(kf_learner* learner, const float* host);
+/* Forward pass of device inputs into device outputs [batch][6] (async). */
+kf_status kf_learner_forward(kf_learner* learner, const void* inputs, uint32_t batch, float* out, void* stream);
+/* Gradient of the batch mean of the squared error against device targets
+ * [batch][6] into host_grads (param_count floats) and the loss into *loss
+ * (both host, either may be NULL).  Synchronous. */
+kf_status kf_learner_gradients(kf_learner* learner, const void* inputs, const float* targets, uint32_t batch,
+                               float* host_grads, float* loss, void* stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on that loss; `loss` (a device
+ * float, may be NULL) receives the loss before the step.  Async. */
+kf_status kf_learner_train_step(kf_learner* learner, const void* inputs, const float* targets, uint32_t batch,
+                                float learning_rate, float* loss, void* stream);
+/* 1 when a tensor-core wait of an earlier async call timed out (synchronises). */
+kf_status kf_learner_error(kf_learner* learner, int32_t* timed_out);
+
+typedef struct kf_warm_start kf_warm_start;
+typedef struct {
+  kf_rigid start;          /* the pose ICP should start from */
+  kf_rigid proposal;       /* predicted * exp(twist) */
+  float twist[6];          /* unscaled */
+  float cost_predicted, matches_predicted;
+  float cost_proposal, matches_proposal;
+  int32_t used_proposal;   /* 0: the constant-velocity pose was kept */
+} kf_warm_start_result;
+kf_status kf_warm_start_create(float depth_scale, kf_warm_start** out);
+kf_status kf_warm_start_destroy(kf_warm_start* warm);
+/* The net input of one 640x480 depth frame against the model rendered at
+ * render_pose, into `input` (device, 9600 bf16, 16-byte aligned).  Ordered on
+ * the pipeline's stream. */
+kf_status kf_warm_start_input(kf_warm_start* warm, kf_pipeline* pipeline, const uint16_t* depth, uint32_t width,
+                              uint32_t height, kf_intrinsics intrinsics, int32_t memory, const kf_rigid* render_pose,
+                              void* input);
+/* The start pose for the next frame: the net's proposal when its truncated
+ * point-to-plane cost (80x60, against the model rendered at `predicted`, 5 cm
+ * cap, unmatched pixels at the cap) is not above that of `predicted`, else
+ * `predicted`.  Call before kf_frame_process of the same depth frame. */
+kf_status kf_warm_start_propose(kf_warm_start* warm, kf_learner* learner, kf_pipeline* pipeline,
+                                const uint16_t* depth, uint32_t width, uint32_t height, kf_intrinsics intrinsics,
+                                int32_t memory, const kf_rigid* predicted, kf_warm_start_result* result);
+
 /* Sets the device-resident camera_to_world that the next enqueued frame
  * starts from (ordered on the pipeline's stream). */
 kf_status kf_frame_set_pose(kf_pipeline* pipeline, kf_tracker* tracker, const kf_rigid* pose);

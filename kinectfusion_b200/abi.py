@@ -143,6 +143,14 @@ class Mesh(C.Structure):
                 ("vertex_count", C.c_uint64), ("triangle_count", C.c_uint64)]
 
 
+class WarmStartResult(C.Structure):
+    _fields_ = [("start", Rigid), ("proposal", Rigid), ("twist", C.c_float * 6),
+                ("cost_predicted", C.c_float), ("matches_predicted", C.c_float),
+                ("cost_proposal", C.c_float), ("matches_proposal", C.c_float), ("used_proposal", C.c_int32)]
+
+
+WARM_START_TWIST_SCALE = 50.0  # KF_WARM_START_TWIST_SCALE
+
 P = C.c_void_p
 _PROTOTYPES = {
     "kf_last_error": (C.c_char_p, []),
@@ -199,6 +207,20 @@ _PROTOTYPES = {
     "kf_frame_enqueue": (C.c_int, [P, P, P, P, P, C.c_uint32, C.c_uint32, Intrinsics, C.c_int32, P, C.c_int32]),
     "kf_frame_result_fetch": (C.c_int, [P, C.POINTER(FrameResult)]),
     "kf_frame_set_pose": (C.c_int, [P, P, C.POINTER(Rigid)]),
+    "kf_learner_create": (C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(P)]),
+    "kf_learner_destroy": (C.c_int, [P]),
+    "kf_learner_param_count": (C.c_int, [P, C.POINTER(C.c_uint64)]),
+    "kf_learner_get_params": (C.c_int, [P, P]),
+    "kf_learner_set_params": (C.c_int, [P, P]),
+    "kf_learner_forward": (C.c_int, [P, P, C.c_uint32, P, P]),
+    "kf_learner_gradients": (C.c_int, [P, P, P, C.c_uint32, P, P, P]),
+    "kf_learner_train_step": (C.c_int, [P, P, P, C.c_uint32, C.c_float, P, P]),
+    "kf_learner_error": (C.c_int, [P, C.POINTER(C.c_int32)]),
+    "kf_warm_start_create": (C.c_int, [C.c_float, C.POINTER(P)]),
+    "kf_warm_start_destroy": (C.c_int, [P]),
+    "kf_warm_start_input": (C.c_int, [P, P, P, C.c_uint32, C.c_uint32, Intrinsics, C.c_int32, C.POINTER(Rigid), P]),
+    "kf_warm_start_propose": (C.c_int, [P, P, P, P, C.c_uint32, C.c_uint32, Intrinsics, C.c_int32,
+                                        C.POINTER(Rigid), C.POINTER(WarmStartResult)]),
 }
 
 _lib = None

@@ -179,6 +179,88 @@ def make_sequence(seed: int, frames: int, max_step_m: float = 0.01,
     return Sequence(scene, poses, depth, color, (FX, FY, CX, CY), seed)
 
 
+def make_sequence_device(seed: int, frames: int, max_step_m: float = 0.01, max_step_deg: float = 0.5,
+                         device: str = "cuda") -> Sequence:
+    """make_sequence with the ray casting done by torch on `device` (float64):
+    the same scene, trajectory and noise draws (the random stream is consumed
+    in the same order), for the long training runs where the numpy renderer
+    would dominate.  A depth may differ from make_sequence's by one unit where
+    the device rounds a float64 operation differently; colour is not rendered
+    (zeros)."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    scene = make_scene(rng)
+    poses = make_trajectory(rng, frames, max_step_m, max_step_deg)
+    depth = np.zeros((frames, HEIGHT, WIDTH), dtype=np.uint16)
+    dev = torch.device(device)
+    u, v = torch.meshgrid(torch.arange(WIDTH, dtype=torch.float64, device=dev),
+                          torch.arange(HEIGHT, dtype=torch.float64, device=dev), indexing="xy")
+    d_cam = torch.stack([(u - CX) / FX, (v - CY) / FY, torch.ones_like(u)], dim=-1)
+    spheres = torch.tensor(scene.spheres, dtype=torch.float64, device=dev)
+    boxes = torch.tensor(scene.boxes, dtype=torch.float64, device=dev)
+    for k in range(frames):
+        z, pid = _render_torch(d_cam, spheres, boxes, torch.tensor(poses[k], dtype=torch.float64, device=dev))
+        sigma = 0.0012 + 0.0019 * (z - 0.4) ** 2
+        noise = torch.from_numpy(rng.standard_normal((HEIGHT, WIDTH))).to(dev)
+        noisy = z + noise * sigma
+        disc = torch.zeros_like(z, dtype=torch.bool)
+        for dy, dx in ((0, 1), (0, -1), (1, 0), (-1, 0)):
+            zn = torch.roll(z, (dy, dx), dims=(0, 1))
+            pn = torch.roll(pid, (dy, dx), dims=(0, 1))
+            disc |= (pn != pid) & ((zn - z).abs() > 0.05)
+        drop = torch.from_numpy(rng.random((HEIGHT, WIDTH)) < 0.02).to(dev)
+        valid = torch.isfinite(noisy) & (noisy >= 0.4) & (noisy <= 4.0) & ~disc & ~drop
+        raw = torch.where(valid, torch.round(noisy * DEPTH_SCALE), torch.zeros_like(noisy))
+        depth[k] = raw.to(torch.int32).cpu().numpy().astype(np.uint16)
+    color = np.zeros((frames, HEIGHT, WIDTH), dtype=np.uint32)
+    return Sequence(scene, poses, depth, color, (FX, FY, CX, CY), seed)
+
+
+def _render_torch(d_cam, spheres, boxes, pose):
+    """_render in torch: the nearest hit per pixel (camera z, primitive id)."""
+    import torch
+
+    rot = pose[:3, :3]
+    origin = pose[:3, 3]
+    d = d_cam @ rot.T
+    inf = torch.full(d.shape[:2], math.inf, dtype=torch.float64, device=d.device)
+    best_t = inf.clone()
+    best_id = torch.full(d.shape[:2], -1, dtype=torch.int64, device=d.device)
+
+    def take(t, pid):
+        nonlocal best_t, best_id
+        hit = (t > 1e-9) & (t < best_t)
+        best_t = torch.where(hit, t, best_t)
+        best_id = torch.where(hit, torch.full_like(best_id, pid), best_id)
+
+    for axis in range(3):
+        da = d[..., axis]
+        t_hi = (float(ROOM_MAX[axis]) - origin[axis]) / da
+        t_lo = (float(ROOM_MIN[axis]) - origin[axis]) / da
+        take(torch.where(da > 0, t_hi, inf), 2 * axis + 1)
+        take(torch.where(da < 0, t_lo, inf), 2 * axis)
+    a = (d * d).sum(-1)
+    for i in range(spheres.shape[0]):
+        oc = origin - spheres[i, :3]
+        r = spheres[i, 3]
+        b = 2.0 * (d @ oc)
+        c = (oc @ oc) - r * r
+        disc = b * b - 4 * a * c
+        sq = torch.sqrt(torch.clamp(disc, min=0.0))
+        t0 = (-b - sq) / (2 * a)
+        take(torch.where(disc >= 0, t0, inf), 6 + i)
+    for j in range(boxes.shape[0]):
+        lo, hi = boxes[j, :3], boxes[j, 3:]
+        t1 = (lo - origin) / d
+        t2 = (hi - origin) / d
+        tmin = torch.minimum(t1, t2).max(-1).values
+        tmax = torch.maximum(t1, t2).min(-1).values
+        ok = (tmax >= tmin) & (tmax > 0)
+        take(torch.where(ok, tmin, inf), 6 + spheres.shape[0] + j)
+    return best_t, best_id
+
+
 def tum_trajectory(poses: np.ndarray, fps: float = 30.0) -> str:
     """TUM format lines 'timestamp tx ty tz qx qy qz qw' (reconstruction.cpp:362-391)."""
     lines = []
