@@ -495,6 +495,77 @@ def run_reference(args, rank: int) -> dict | None:
             "e2e": {"value": round(fps, 4), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_learned(args) -> dict:
+    """cfg5: ICP iterations per frame with the learned warm start against the
+    plain constant-velocity start, on held-out seeds at 512^3 dense float,
+    with ATE; plus the frame rate of the learned loop through the public API
+    (host depth frames) and the net's device latency."""
+    import torch
+
+    import kinectfusion_b200 as kf
+    from kinectfusion_b200 import learned, synthetic
+
+    seeds = list(range(5000, 5000 + args.learned_seeds))
+    net = learned.Learner(8, seed=0)
+    net.load(learned.PARAMS)
+    gpu = kf.Pipeline(learned.volume_config(RES, VOXEL))
+    report = learned.evaluate(net, seeds, args.learned_frames, pipeline=gpu)
+    mean = report["mean"]
+    tracked = [r for r in report["per_seed"] if r["ate_velocity_m"] < 0.01]
+
+    # frame rate of each loop over one held-out sequence (host frames in,
+    # pose out, every call synchronous as a caller sees it)
+    seq = synthetic.make_sequence_device(seeds[0], args.learned_frames, 0.05, 3.0)
+    rates = {}
+    for mode in ("velocity", "learned"):
+        gpu.reset()
+        loop = learned.WarmStartedReconstruction(gpu, learned.intrinsics640(), start=mode, learner=net)
+        for f in range(3):
+            loop.process(seq.depth[f])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for f in range(3, args.learned_frames):
+            loop.process(seq.depth[f])
+        rates[mode] = (args.learned_frames - 3) / (time.perf_counter() - t0)
+    # the net's forward pass alone (batch 8, device-resident input)
+    x = torch.zeros((8, 60, 80, 2), dtype=torch.bfloat16, device="cuda")
+    for _ in range(10):
+        net.forward(x)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(200):
+        net.forward(x)
+    stop.record()
+    stop.synchronize()
+    forward_ms = start.elapsed_time(stop) / 200
+    return {
+        "metric": "ICP iterations per frame (learned warm start vs constant velocity, equal ATE)",
+        "value": round(mean["iters_learned"], 4), "unit": "iterations/frame", "n_gpus": 1,
+        "steps": len(seeds) * (args.learned_frames - 2), "warmup": 2, "higher_is_better": False,
+        "scaling": "none", "vs_baseline": None, "dtype": "bf16 net, f32 pipeline",
+        "data": "synthetic (seeded held-out sequences, 5 cm / 3 deg per frame)",
+        "config": {"workload": f"cfg5: {len(seeds)} held-out seeds x {args.learned_frames} frames, "
+                               f"dense {RES}^3 float, voxel {VOXEL} m",
+                   "params": learned.PARAMS.name},
+        "plain_iterations_per_frame": round(mean["iters_velocity"], 4),
+        "iteration_reduction": round(mean["iteration_reduction"], 4),
+        "ate_m": {"velocity": mean["ate_velocity_m"], "learned": mean["ate_learned_m"],
+                  "learned_vs_plain_rms": mean["learned_vs_plain_rms_m"],
+                  "seeds_tracked_by_plain": len(tracked),
+                  "velocity_tracked_seeds": float(np.mean([r["ate_velocity_m"] for r in tracked])) if tracked
+                  else None,
+                  "learned_tracked_seeds": float(np.mean([r["ate_learned_m"] for r in tracked])) if tracked
+                  else None},
+        "proposal_used": mean["proposal_used"],
+        "start_error_m": {"velocity": mean["start_error_velocity_m"], "proposal": mean["start_error_proposal_m"]},
+        "frames_per_s": {k: round(v, 2) for k, v in rates.items()},
+        "net_forward_ms": round(forward_ms, 4),
+        "e2e": {"value": round(rates["learned"], 2), "unit": "frames/s", "h2d_bytes_per_step": 2 * 640 * 480 * 2,
+                "d2h_bytes_per_step": 0},
+        "per_seed": report["per_seed"],
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -502,8 +573,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--config", choices=["cfg2", "batch16"], default="cfg2",
-                    help="cfg2: the headline 512^3 workload (default); batch16: 16 sequences batched")
+    ap.add_argument("--config", choices=["cfg2", "batch16", "learned"], default="cfg2",
+                    help="cfg2: the headline 512^3 workload (default); batch16: 16 sequences batched; "
+                         "learned: the learned ICP warm start against constant velocity")
+    ap.add_argument("--learned-seeds", type=int, default=20)
+    ap.add_argument("--learned-frames", type=int, default=60)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -512,6 +586,8 @@ def main():
         line = run_reference(args, rank)
     elif args.config == "batch16":
         line = run_batch(args) if rank == 0 else None
+    elif args.config == "learned":
+        line = run_learned(args) if rank == 0 else None
     else:
         if world > 1:
             import datetime

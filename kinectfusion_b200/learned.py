@@ -22,6 +22,7 @@ from __future__ import annotations
 import ctypes as C
 import dataclasses
 import math
+import pathlib
 
 import numpy as np
 
@@ -30,6 +31,10 @@ from .pipeline import Pipeline, Reconstruction, _check, lib, pipeline_config
 
 TWIST_SCALE = abi.WARM_START_TWIST_SCALE
 NET_H, NET_W = 60, 80
+# The trained parameters shipped with the package: `python -m
+# kinectfusion_b200.learned train` over seeds 0-399 (25 frames each, 5 cm / 3
+# degree steps, 512^3 dense float), 8000 Adam steps of 64.
+PARAMS = pathlib.Path(__file__).resolve().parent / "warm_start_params.npy"
 
 
 def _torch():
@@ -303,11 +308,19 @@ def _ball_twist(rng, max_t, max_r):
 
 
 # ---- training -----------------------------------------------------------------------
+# Mirroring the camera's x (y) axis flips the 80x60 maps left-right (up-down;
+# the principal point sits at the image centre) and negates these twist
+# components: translation x (y) and the rotation about the other two axes.
+_FLIP_SIGNS = {2: (-1.0, 1.0, 1.0, 1.0, -1.0, -1.0), 1: (1.0, -1.0, 1.0, -1.0, 1.0, -1.0)}
+
+
 def train(learner: Learner, data: Dataset, steps: int, *, batch: int = 64, lr: float = 1e-3,
-          final_lr: float = 1e-5, seed: int = 0, log_every: int = 0, validation: Dataset | None = None) -> list:
-    """Adam over shuffled minibatches with a cosine learning-rate decay;
-    returns [(step, mean training loss over the last log_every steps,
-    validation loss or None)]."""
+          final_lr: float = 1e-5, seed: int = 0, log_every: int = 0, validation: Dataset | None = None,
+          mirror: bool = True) -> list:
+    """Adam over shuffled minibatches with a cosine learning-rate decay; with
+    `mirror`, each batch is flipped left-right and/or up-down at random (the
+    twists follow).  Returns [(step, mean training loss over the last
+    log_every steps, validation loss or None)]."""
     torch = _torch()
     if batch % 8 or batch > learner.capacity:
         raise ValueError("batch must be a multiple of 8 within the learner's capacity")
@@ -322,6 +335,8 @@ def train(learner: Learner, data: Dataset, steps: int, *, batch: int = 64, lr: f
     perm = torch.randperm(n, generator=gen, device="cuda")
     pos = 0
     val_losses = {}
+    rng = np.random.default_rng(seed)
+    signs = {d: torch.tensor(v, dtype=torch.float32, device="cuda") for d, v in _FLIP_SIGNS.items()}
     for s in range(steps):
         if pos + batch > n:
             perm = torch.randperm(n, generator=gen, device="cuda")
@@ -330,6 +345,11 @@ def train(learner: Learner, data: Dataset, steps: int, *, batch: int = 64, lr: f
         pos += batch
         torch.index_select(data.inputs, 0, sel, out=bx)
         torch.index_select(data.targets, 0, sel, out=by)
+        if mirror:
+            for dim, flip in zip((2, 1), rng.random(2) < 0.5):
+                if flip:
+                    bx.copy_(torch.flip(bx, dims=(dim,)))
+                    by.mul_(signs[dim])
         rate = final_lr + 0.5 * (lr - final_lr) * (1.0 + math.cos(math.pi * s / max(1, steps)))
         learner.train_step(bx, by, rate, losses[s])
         if log_every and validation is not None and (s + 1) % log_every == 0:
@@ -459,13 +479,13 @@ def main(argv=None) -> None:
     ap = argparse.ArgumentParser(prog="python -m kinectfusion_b200.learned")
     sub = ap.add_subparsers(dest="cmd", required=True)
     t = sub.add_parser("train", help="generate data with the plain pipeline, train, save the parameters")
-    t.add_argument("--seeds", default="0-95")
-    t.add_argument("--val-seeds", default="900-903")
-    t.add_argument("--frames", type=int, default=100)
+    t.add_argument("--seeds", default="0-399")
+    t.add_argument("--val-seeds", default="900-915")
+    t.add_argument("--frames", type=int, default=25)
     t.add_argument("--perturbations", type=int, default=3)
-    t.add_argument("--perturb-m", type=float, default=0.015)
-    t.add_argument("--perturb-deg", type=float, default=1.5)
-    t.add_argument("--steps", type=int, default=30000)
+    t.add_argument("--perturb-m", type=float, default=0.008)
+    t.add_argument("--perturb-deg", type=float, default=0.6)
+    t.add_argument("--steps", type=int, default=8000)
     t.add_argument("--batch", type=int, default=64)
     t.add_argument("--lr", type=float, default=1e-3)
     t.add_argument("--resolution", type=int, default=512)

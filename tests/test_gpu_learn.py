@@ -152,3 +152,19 @@ def test_proposal_fallback_rule():
     net.set_params(p)
     res = warm.propose(net, gpu, seq.depth[-1], k, pred)
     assert res.used_proposal == 0 and res.cost_proposal > res.cost_predicted
+
+
+def test_trained_net_gains_over_constant_velocity():
+    """The shipped network (trained on seeds 0-399 by `python -m
+    kinectfusion_b200.learned train`) on held-out seeds at 512^3: its
+    proposals start ICP closer to the pose plain ICP reaches than the
+    constant-velocity prediction does, and the learned loop's trajectory
+    stays within 1 mm RMS of the plain loop's."""
+    net = learned.Learner(8)
+    net.load(learned.PARAMS)
+    report = learned.evaluate(net, [5000, 5002], 25)
+    m = report["mean"]
+    assert m["start_error_proposal_m"] < 0.8 * m["start_error_velocity_m"]
+    assert m["learned_vs_plain_rms_m"] < 1e-3
+    assert abs(m["ate_learned_m"] - m["ate_velocity_m"]) < 1e-3
+    assert m["proposal_used"] > 0.5
