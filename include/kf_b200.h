@@ -285,6 +285,11 @@ kf_status kf_pipeline_block_stats(kf_pipeline* pipeline, uint64_t* attempts, uin
 /* Sparse storage: the block-slot grid (BlockRep::grid, block_rep.hpp:26-110),
  * one uint32 per 8^3 block in x-major block order, 0xFFFFFFFF = unallocated. */
 kf_status kf_pipeline_download_block_grid(kf_pipeline* pipeline, uint32_t* grid, size_t count);
+/* band-march backend: the dilated band bitmap the raycast reads
+ * (BasicBandBitmap::view, occupancy.hpp:262-267), one bit per 8^3 block in
+ * z-major order (((x * blocks_y) + y) * blocks_z + z), count =
+ * ceil(blocks / 32) words. */
+kf_status kf_pipeline_download_band_bitmap(kf_pipeline* pipeline, uint32_t* words, size_t count);
 
 /* Pipeline::extract_mesh (pipeline.hpp:95) on the device; free with kf_mesh_free. */
 kf_status kf_pipeline_extract_mesh(kf_pipeline* pipeline, float min_weight, kf_mesh* out);

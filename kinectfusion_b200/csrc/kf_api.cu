@@ -223,7 +223,8 @@ kf_status kf_pipeline_create(const kf_pipeline_config* config, kf_pipeline** out
     require(c.voxel >= KF_VOXEL_FLOAT && c.voxel <= KF_VOXEL_BF16, "Unknown voxel store");
     require(c.color == KF_COLOR_FLOAT || c.color == KF_COLOR_NONE, "Unknown color store");
     require(c.tsdf_rule == KF_RULE_CLASSIC || c.tsdf_rule == KF_RULE_ANGLE_WEIGHTED, "Unknown TSDF rule");
-    if (c.raycast_backend == KF_RAYCAST_BAND_MARCH) throw Unsupported("band-march raycast is not built yet");
+    require(c.raycast_backend >= KF_RAYCAST_MARCH && c.raycast_backend <= KF_RAYCAST_BAND_MARCH,
+            "Unknown raycast backend");
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
       throw CudaError("no CUDA device available");
@@ -268,6 +269,15 @@ kf_status kf_pipeline_create(const kf_pipeline_config* config, kf_pipeline** out
       v.truncation = g.truncation_distance;
       launch_fill_volume(p, p.stream);
       reset_sparse(p, p.stream);
+      if (c.raycast_backend == KF_RAYCAST_BAND_MARCH) {
+        // EmptySpaceIndex (raycasting.hpp:31-38): the band bitmap, empty for
+        // a fresh (unobserved) volume
+        const size_t words = static_cast<size_t>((blocks + 31) / 32);
+        p.band_raw.resize(words);
+        p.band_map.resize(words);
+        check(cudaMemsetAsync(p.band_raw.ptr, 0, p.band_raw.bytes(), p.stream), "band bitmap init");
+        check(cudaMemsetAsync(p.band_map.ptr, 0, p.band_map.bytes(), p.stream), "band bitmap init");
+      }
       p.counters.resize(2);
       check(cudaMemsetAsync(p.counters.ptr, 0, p.counters.bytes(), p.stream), "counter init");
       check(cudaStreamSynchronize(p.stream), "volume fill");
@@ -297,6 +307,10 @@ kf_status kf_pipeline_reset(kf_pipeline* pipeline) {
     launch_fill_volume(p, p.stream);
     reset_sparse(p, p.stream);
     reset_blocks(p, p.stream);  // the raycast's skip structures describe the volume
+    if (p.band_map.count) {
+      check(cudaMemsetAsync(p.band_raw.ptr, 0, p.band_raw.bytes(), p.stream), "band bitmap reset");
+      check(cudaMemsetAsync(p.band_map.ptr, 0, p.band_map.bytes(), p.stream), "band bitmap reset");
+    }
     check(cudaMemsetAsync(p.counters.ptr, 0, p.counters.bytes(), p.stream), "counter reset");
     check(cudaStreamSynchronize(p.stream), "volume reset");
   });
@@ -435,6 +449,17 @@ kf_status kf_pipeline_download_block_grid(kf_pipeline* pipeline, uint32_t* grid,
     require(count == p.grid.count, "kf_pipeline_download_block_grid: grid size mismatch");
     check(cudaStreamSynchronize(p.stream), "grid download sync");
     check(cudaMemcpy(grid, p.grid.ptr, count * sizeof(uint32_t), cudaMemcpyDeviceToHost), "grid download");
+  });
+}
+
+kf_status kf_pipeline_download_band_bitmap(kf_pipeline* pipeline, uint32_t* words, size_t count) {
+  return guarded([&] {
+    require(pipeline != nullptr && words != nullptr, "kf_pipeline_download_band_bitmap: null argument");
+    Pipeline& p = pipeline->impl;
+    require(p.band_map.count != 0, "kf_pipeline_download_band_bitmap: the raycast backend is not band-march");
+    require(count == p.band_map.count, "kf_pipeline_download_band_bitmap: word count mismatch");
+    check(cudaStreamSynchronize(p.stream), "band bitmap download sync");
+    check(cudaMemcpy(words, p.band_map.ptr, count * sizeof(uint32_t), cudaMemcpyDeviceToHost), "band download");
   });
 }
 

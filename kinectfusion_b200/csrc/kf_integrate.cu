@@ -784,6 +784,8 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
             : launch_blocks_typed<KF_VOXEL_FLOAT, false>(p, table, width, height, k, T, ip, state, s);
       break;
   }
+  // the band-march bitmap (EmptySpaceIndex::rebuild after integration)
+  launch_band_rebuild(p, s);
   // raycast skip bits
   if (p.voxel_bits.count == 0) return;
   stencil_bits_kernel<<<ceil_div(blocks * 8u, 256), 256, 0, s>>>(

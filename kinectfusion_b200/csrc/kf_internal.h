@@ -254,6 +254,10 @@ struct Pipeline {
   // one is exactly 1.0 (all eight corners observed with tsdf exactly 1).
   DeviceArray<uint8_t> brick_class;
   DeviceArray<uint32_t> band_bits;       // band integration: blocks the bands cross
+  // band-march raycast (BasicBandBitmap, occupancy.hpp:240-278): block bits
+  // in z-major order (32 z-blocks per word), raw and 3^3-dilated; rebuilt
+  // after every integration.
+  DeviceArray<uint32_t> band_raw, band_map;
   // Sparse storage (BlockRep, block_rep.hpp:26-110): a slot per 8^3 block in
   // `grid` (kUnallocated when none), `sparse_capacity` slots in the pools.
   DeviceArray<uint32_t> grid;
@@ -339,6 +343,8 @@ void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t s
 void reset_blocks(Pipeline& p, cudaStream_t stream);
 // Raycast into device maps.  `pose_state` (optional) supplies the
 // camera_to_world from the tracker and skips the render after a failure.
+// Rebuilds the band-march bitmap from the volume (BandRebuild, occupancy.hpp:229-238).
+void launch_band_rebuild(Pipeline& p, cudaStream_t stream);
 void launch_raycast(const Pipeline& p, const kf_raycast_camera& camera, float* points,
                     float* normals, uint32_t* colors, const IcpState* pose_state,
                     cudaStream_t stream);

@@ -494,6 +494,262 @@ __global__ void __launch_bounds__(128)
   colors[pix] = out_color;
 }
 
+// ---- band march (BandSkip, empty_space_skip.hpp:19-153, 196-287) ----------
+// The reference's approximate skip: the ray jumps to the entry of the next
+// block of the dilated band bitmap (blocks holding an observed voxel with
+// tsdf < 1 - 1/64, grown by one block).  Its output differs from the plain
+// march by design; these kernels reproduce the reference's band march
+// operation for operation, so they match the oracle's band march bit for bit.
+struct BandDev {
+  const uint32_t* words;  // dilated bits, z-major: ((x * by) + y) * bz + z
+  uint32_t bx, by, bz;
+};
+
+constexpr float kBandEpsilon = 1.0f / 64.0f;  // occupancy.hpp:148
+constexpr float kMarchInfinity = 1.0e30f;     // BlockMarch::kInfinity
+
+// compat::min / compat::max (cuda_compat.hpp:75-86)
+__device__ __forceinline__ float cmin(float lhs, float rhs) { return rhs < lhs ? rhs : lhs; }
+__device__ __forceinline__ float cmax(float lhs, float rhs) { return lhs < rhs ? rhs : lhs; }
+
+__device__ __forceinline__ bool band_test(const BandDev& b, uint32_t x, uint32_t y, uint32_t z) {
+  const uint64_t i = (static_cast<uint64_t>(x) * b.by + y) * b.bz + z;
+  return ((__ldg(b.words + (i >> 5)) >> (i & 31u)) & 1u) != 0u;
+}
+
+__device__ __forceinline__ float axis_exit(float origin, float direction, float low, float high) {
+  return ((direction >= 0.0f ? high : low) - origin) / direction;
+}
+
+// BlockMarch over one ray (empty_space_skip.hpp:19-153)
+struct BlockMarchDev {
+  const VolumeDev& v;
+  float block_size;
+  f3 o, d;
+
+  __device__ float block_exit(uint32_t x, uint32_t y, uint32_t z) const {
+    const float lx = v.origin.x + (static_cast<float>(x) * block_size);
+    const float ly = v.origin.y + (static_cast<float>(y) * block_size);
+    const float lz = v.origin.z + (static_cast<float>(z) * block_size);
+    const float hx = lx + (1.0f * block_size), hy = ly + (1.0f * block_size), hz = lz + (1.0f * block_size);
+    return cmin(axis_exit(o.x, d.x, lx, hx), cmin(axis_exit(o.y, d.y, ly, hy), axis_exit(o.z, d.z, lz, hz)));
+  }
+  __device__ float column_exit(uint32_t x, uint32_t y) const {
+    const float lx = v.origin.x + (static_cast<float>(x) * block_size);
+    const float ly = v.origin.y + (static_cast<float>(y) * block_size);
+    float exit = kMarchInfinity;
+    if (d.x != 0.0f) exit = cmin(exit, axis_exit(o.x, d.x, lx, lx + block_size));
+    if (d.y != 0.0f) exit = cmin(exit, axis_exit(o.y, d.y, ly, ly + block_size));
+    return exit;
+  }
+  __device__ float z_entry(uint64_t z) const {
+    const float side = d.z >= 0.0f ? 0.0f : 1.0f;
+    const float plane = v.origin.z + ((static_cast<float>(z) + side) * block_size);
+    return (plane - o.z) / d.z;
+  }
+  __device__ static void slab(float origin, float direction, float low, float high, float& entry, float& exit) {
+    if (direction == 0.0f) {
+      if (origin < low || origin > high) entry = kMarchInfinity;
+      return;
+    }
+    const float t_low = (low - origin) / direction;
+    const float t_high = (high - origin) / direction;
+    entry = cmax(entry, cmin(t_low, t_high));
+    exit = cmin(exit, cmax(t_low, t_high));
+  }
+  __device__ float volume_entry() const {
+    float entry = 0.0f, exit = kMarchInfinity;
+    slab(o.x, d.x, v.origin.x, v.origin.x + (static_cast<float>(v.rx) * v.voxel_size), entry, exit);
+    slab(o.y, d.y, v.origin.y, v.origin.y + (static_cast<float>(v.ry) * v.voxel_size), entry, exit);
+    slab(o.z, d.z, v.origin.z, v.origin.z + (static_cast<float>(v.rz) * v.voxel_size), entry, exit);
+    return entry <= exit ? entry : kMarchInfinity;
+  }
+};
+
+// BandSkip::word_scan_z (empty_space_skip.hpp:266-284)
+__device__ float band_word_scan_z(const BandDev& b, const BlockMarchDev& m, uint32_t x, uint32_t y, uint32_t z) {
+  const uint64_t index = (static_cast<uint64_t>(x) * b.by + y) * b.bz + z;
+  const uint32_t word = __ldg(b.words + (index >> 5));
+  const uint32_t offset = static_cast<uint32_t>(index & 31u);
+  const bool forward = m.d.z >= 0.0f;
+  int found;
+  if (forward) {
+    const uint32_t masked = word & ~((1u << offset) - 1u);  // find_set_at_or_after
+    found = masked == 0u ? -1 : __ffs(static_cast<int>(masked)) - 1;
+  } else {
+    const uint32_t masked = word & (offset >= 31u ? ~0u : ((1u << (offset + 1u)) - 1u));  // at_or_before
+    found = masked == 0u ? -1 : 31 - __clz(static_cast<int>(masked));
+  }
+  uint64_t target_z;
+  if (found >= 0) {
+    target_z = z + static_cast<uint64_t>(found) - offset;
+  } else {
+    target_z = forward ? z + (32u - offset) : z - (offset < z ? offset : z);
+  }
+  return cmin(m.z_entry(target_z), m.column_exit(x, y));
+}
+
+// BandSkip::advance (empty_space_skip.hpp:225-262)
+__device__ float band_advance(const BandDev& b, const VolumeDev& v, f3 o, f3 d, float ray_length, float base_step,
+                              float max_depth) {
+  const BlockMarchDev m{v, 8.0f * v.voxel_size, o, d};
+  const float nudge = 0.25f * v.voxel_size;
+  const bool z_major = fabsf(d.z) >= fabsf(d.x) && fabsf(d.z) >= fabsf(d.y) && (b.bz % 32u) == 0u;
+  while (ray_length <= max_depth) {
+    const f3 point = o + (d * ray_length);
+    const float gx = (point.x - v.origin.x) / v.voxel_size;
+    const float gy = (point.y - v.origin.y) / v.voxel_size;
+    const float gz = (point.z - v.origin.z) / v.voxel_size;
+    if (!(gx >= 0.0f && gy >= 0.0f && gz >= 0.0f && gx < static_cast<float>(v.rx) &&
+          gy < static_cast<float>(v.ry) && gz < static_cast<float>(v.rz))) {
+      const float entry = m.volume_entry();
+      if (entry >= kMarchInfinity || entry > max_depth) return max_depth + base_step;
+      ray_length = cmax(ray_length + base_step, entry + nudge);
+      continue;
+    }
+    const uint32_t x = static_cast<uint32_t>(gx) / 8u, y = static_cast<uint32_t>(gy) / 8u,
+                   z = static_cast<uint32_t>(gz) / 8u;
+    if (band_test(b, x, y, z)) return ray_length;
+    float target = kMarchInfinity;
+    if (z_major) target = band_word_scan_z(b, m, x, y, z);
+    if (target >= kMarchInfinity) target = m.block_exit(x, y, z);
+    ray_length = cmax(ray_length + base_step, target + nudge);
+  }
+  return ray_length;
+}
+
+// find_zero_crossing with BandSkip (raycasting.hpp:165-211): one thread per
+// pixel; writes the crossing (NaN for none) for surface_kernel.
+template <int Kind>
+__global__ void __launch_bounds__(64)
+    band_march_kernel(VolumeDev v, BandDev band, RaycastParams rp, Intr k, uint32_t width, uint32_t height,
+                      Rigid pose, const IcpState* __restrict__ state, float* __restrict__ points) {
+  if (state != nullptr) {
+    if (state->failed) return;
+    const float* c = state->camera;
+    pose = Rigid{{c[0], c[1], c[2]}, {c[3], c[4], c[5]}, {c[6], c[7], c[8]}, {c[9], c[10], c[11]}};
+  }
+  const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t row = blockIdx.y * blockDim.y + threadIdx.y;
+  if (col >= width || row >= height) return;
+  const size_t pix = static_cast<size_t>(row) * width + col;
+  const Sampler<Kind> s{v};
+  float seed = rp.min_depth;
+  if (rp.seed_previous) {
+    const f3 previous = load3(points + pix * 3);
+    if (finite3(previous) && dot(previous, previous) > 0.0f) {
+      const float previous_depth = norm(previous - pose.t);
+      const float truncated = previous_depth - (2.0f * v.truncation);
+      seed = rp.min_depth < truncated ? truncated : rp.min_depth;
+    }
+  }
+  const f3 translated = back_project(k, static_cast<float>(col), static_cast<float>(row), 1.0f);
+  const f3 direction = rotate(pose, translated);
+  const float dn = norm(direction);
+  bool found = false;
+  f3 surface = make(0.0f, 0.0f, 0.0f);
+  if (dn > 0.0f) {
+    const f3 dir = direction / dn;
+    const float base_step = v.voxel_size * rp.step_scale;
+    bool have_prev = false;
+    float prev_tsdf = 0.0f;
+    f3 prev_point = make(0.0f, 0.0f, 0.0f);
+    float ray_length = seed;
+    while (ray_length <= rp.max_depth) {
+      const float advanced = band_advance(band, v, pose.t, dir, ray_length, base_step, rp.max_depth);
+      if (advanced != ray_length) {
+        have_prev = false;  // the skipped samples were all nullopt
+        ray_length = advanced;
+        if (ray_length > rp.max_depth) break;
+      }
+      const f3 point = pose.t + (dir * ray_length);
+      float tsdf;
+      if (!s.tsdf(point, rp.policy, tsdf)) {
+        have_prev = false;
+        ray_length += base_step;
+        continue;
+      }
+      if (have_prev && prev_tsdf > 0.0f && tsdf <= 0.0f) {
+        const float gap = prev_tsdf - tsdf;
+        const float alpha = gap != 0.0f ? prev_tsdf / gap : 0.0f;
+        surface = prev_point + ((point - prev_point) * alpha);
+        found = true;
+        break;
+      }
+      if (have_prev && prev_tsdf < 0.0f && tsdf > 0.0f) break;
+      have_prev = true;
+      prev_tsdf = tsdf;
+      prev_point = point;
+      const float precomp = tsdf * v.truncation * rp.step_scale;
+      const float step = base_step < precomp ? precomp : base_step;
+      ray_length += tsdf > 0.0f ? step : base_step;
+    }
+  }
+  store3(points + pix * 3, found ? surface : nan3());
+}
+
+// BlockBitmapOps::rebuild with BandFilter (occupancy.hpp:105-121, 150-171):
+// warp w computes raw word w (32 blocks in z-major order), reading each
+// block's 512 contiguous voxels; blocks past the extent read as clear.
+template <int Kind>
+__global__ void __launch_bounds__(256) band_raw_kernel(VolumeDev v, uint32_t* __restrict__ raw, uint32_t words) {
+  using VT = VoxelTraits<Kind>;
+  using Raw = typename VT::Raw;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t first = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t stride = (gridDim.x * blockDim.x) >> 5;
+  const uint64_t total = static_cast<uint64_t>(v.bx) * v.by * v.bz;
+  const Raw* vox = static_cast<const Raw*>(v.voxels);
+  for (uint32_t w = first; w < words; w += stride) {
+    uint32_t word = 0;
+    for (uint32_t j = 0; j < 32u; ++j) {
+      const uint64_t i = static_cast<uint64_t>(w) * 32u + j;
+      if (i >= total) break;  // warp-uniform
+      const uint32_t z = static_cast<uint32_t>(i % v.bz);
+      const uint32_t y = static_cast<uint32_t>((i / v.bz) % v.by);
+      const uint32_t x = static_cast<uint32_t>(i / (static_cast<uint64_t>(v.bz) * v.by));
+      const Raw* brick = vox + ((static_cast<size_t>(z) * v.by + y) * v.bx + x) * 512u;
+      bool any = false;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const Raw r = brick[lane + 32u * q];
+        any |= VT::observed(r) && VT::tsdf(r) < (1.0f - kBandEpsilon);
+      }
+      if (__any_sync(0xFFFFFFFFu, any)) word |= 1u << j;
+    }
+    if (lane == 0) raw[w] = word;
+  }
+}
+
+// BlockBitmapOps::dilate (occupancy.hpp:69-103): bit i is set when a block
+// of its clipped 3^3 neighbourhood is in the raw band.  One thread per bit,
+// one warp per word.
+__global__ void __launch_bounds__(256) band_dilate_kernel(const uint32_t* __restrict__ raw, uint32_t* __restrict__ map,
+                                                          uint32_t bx, uint32_t by, uint32_t bz, uint32_t words) {
+  const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const uint64_t total = static_cast<uint64_t>(bx) * by * bz;
+  bool hit = false;
+  if (i < total) {
+    const int z = static_cast<int>(i % bz), y = static_cast<int>((i / bz) % by);
+    const int x = static_cast<int>(i / (static_cast<uint64_t>(bz) * by));
+    for (int oz = -1; oz <= 1 && !hit; ++oz) {
+      for (int oy = -1; oy <= 1 && !hit; ++oy) {
+        for (int ox = -1; ox <= 1 && !hit; ++ox) {
+          const int nx = x + ox, ny = y + oy, nz = z + oz;
+          if (nx < 0 || ny < 0 || nz < 0 || nx >= static_cast<int>(bx) || ny >= static_cast<int>(by) ||
+              nz >= static_cast<int>(bz)) {
+            continue;
+          }
+          const uint64_t n = (static_cast<uint64_t>(nx) * by + ny) * bz + nz;
+          hit = ((__ldg(raw + (n >> 5)) >> (n & 31u)) & 1u) != 0u;
+        }
+      }
+    }
+  }
+  const uint32_t word = __ballot_sync(0xFFFFFFFFu, hit);
+  if ((threadIdx.x & 31u) == 0 && (i >> 5) < words) map[i >> 5] = word;
+}
+
 template <int Kind, bool Color>
 void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points, float* normals,
                   uint32_t* colors, const IcpState* state, cudaStream_t s) {
@@ -510,9 +766,17 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
   const uint32_t* voxel_bits = p.brick_class.count && p.view.grid == nullptr ? p.voxel_bits.ptr : nullptr;
   const uint4* stencil_bits = reinterpret_cast<const uint4*>(p.stencil_bits.ptr);
   const Rigid pose = rigid_from(cam.camera_to_world);
-  raycast_kernel<Kind><<<grid, block, 0, s>>>(p.view, voxel_bits, stencil_bits, p.brick_class.ptr, rp,
-                                              intr_from(cam.intrinsics), cam.width, cam.height, pose, state, points);
-  check(cudaGetLastError(), "raycast_kernel launch");
+  if (p.config.raycast_backend == KF_RAYCAST_BAND_MARCH) {
+    const BandDev band{p.band_map.ptr, p.view.bx, p.view.by, p.view.bz};
+    band_march_kernel<Kind><<<grid, block, 0, s>>>(p.view, band, rp, intr_from(cam.intrinsics), cam.width,
+                                                   cam.height, pose, state, points);
+    check(cudaGetLastError(), "band_march_kernel launch");
+  } else {
+    raycast_kernel<Kind><<<grid, block, 0, s>>>(p.view, voxel_bits, stencil_bits, p.brick_class.ptr, rp,
+                                                intr_from(cam.intrinsics), cam.width, cam.height, pose, state,
+                                                points);
+    check(cudaGetLastError(), "raycast_kernel launch");
+  }
   const dim3 sblock(32, 4);
   const dim3 sgrid(ceil_div(cam.width, 32), ceil_div(cam.height, 4));
   surface_kernel<Kind, Color><<<sgrid, sblock, 0, s>>>(p.view, rp, cam.width, cam.height, pose, state, points,
@@ -521,6 +785,27 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
 }
 
 }  // namespace
+
+void launch_band_rebuild(Pipeline& p, cudaStream_t s) {
+  if (p.band_map.count == 0) return;
+  const uint32_t words = static_cast<uint32_t>(p.band_map.count);
+  const unsigned grid = std::min<unsigned>(148u * 8u, ceil_div(words * 32u, 256u));
+  switch (p.config.voxel) {
+    case KF_VOXEL_QUANTIZED:
+      band_raw_kernel<KF_VOXEL_QUANTIZED><<<grid, 256, 0, s>>>(p.view, p.band_raw.ptr, words);
+      break;
+    case KF_VOXEL_BF16:
+      band_raw_kernel<KF_VOXEL_BF16><<<grid, 256, 0, s>>>(p.view, p.band_raw.ptr, words);
+      break;
+    default:
+      band_raw_kernel<KF_VOXEL_FLOAT><<<grid, 256, 0, s>>>(p.view, p.band_raw.ptr, words);
+      break;
+  }
+  check(cudaGetLastError(), "band_raw_kernel launch");
+  band_dilate_kernel<<<ceil_div(words * 32u, 256u), 256, 0, s>>>(p.band_raw.ptr, p.band_map.ptr, p.view.bx,
+                                                                  p.view.by, p.view.bz, words);
+  check(cudaGetLastError(), "band_dilate_kernel launch");
+}
 
 void launch_raycast(const Pipeline& p, const kf_raycast_camera& cam, float* points, float* normals,
                     uint32_t* colors, const IcpState* state, cudaStream_t s) {

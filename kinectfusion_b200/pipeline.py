@@ -262,6 +262,14 @@ class Pipeline:
         _check(lib().kf_pipeline_download_block_grid(self.handle, _ptr(grid), grid.size))
         return grid
 
+    def band_bitmap(self) -> np.ndarray:
+        """band-march backend: the dilated band bitmap (z-major block bits)."""
+        rx, ry, rz = self.resolution
+        blocks = ((rx + 7) // 8) * ((ry + 7) // 8) * ((rz + 7) // 8)
+        words = np.empty((blocks + 31) // 32, dtype=np.uint32)
+        _check(lib().kf_pipeline_download_band_bitmap(self.handle, _ptr(words), words.size))
+        return words
+
     def extract_mesh(self, min_weight: float = 0.0) -> dict:
         """Pipeline::extract_mesh (pipeline.hpp:95) on the device."""
         mesh = abi.Mesh()

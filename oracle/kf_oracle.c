@@ -859,9 +859,210 @@ static int cell_normal(const sampler* s, v3 p, v3* out) {
 }
 
 /* ------------------------------------------------------------------------ */
+/* Band bitmap (occupancy.hpp:105-121, 150-278) and BandSkip                  */
+/* (empty_space_skip.hpp:19-153, 196-287)                                      */
+/* ------------------------------------------------------------------------ */
+#define KFO_BAND_EPSILON (1.0f / 64.0f) /* kBandEpsilon, occupancy.hpp:148 */
+#define KFO_INF 1.0e30f                 /* BlockMarch::kInfinity */
+
+typedef struct {
+  const uint32_t* words;
+  uint64_t bx, by, bz;
+} band_view;
+
+static inline void band_extent(const kfo_volume* v, uint64_t* bx, uint64_t* by, uint64_t* bz) {
+  /* BlockGrid::for_resolution (grid.hpp:27-33) */
+  *bx = (v->geometry.res_x + 7u) / 8u;
+  *by = (v->geometry.res_y + 7u) / 8u;
+  *bz = (v->geometry.res_z + 7u) / 8u;
+}
+
+/* BandView::block_index (occupancy.hpp:179-182): z-major, 32 z-blocks per word. */
+static inline uint64_t band_index(uint64_t by, uint64_t bz, uint64_t x, uint64_t y, uint64_t z) {
+  return ((x * by) + y) * bz + z;
+}
+
+static inline int band_test(const band_view* b, uint64_t x, uint64_t y, uint64_t z) {
+  const uint64_t i = band_index(b->by, b->bz, x, y, z);
+  return (int)((b->words[i / 32u] >> (i % 32u)) & 1u);
+}
+
+uint64_t kfo_band_word_count(const kfo_volume* v) {
+  uint64_t bx, by, bz;
+  band_extent(v, &bx, &by, &bz);
+  return (bx * by * bz + 31u) / 32u;
+}
+
+void kfo_band_bitmap(const kfo_volume* v, uint32_t* raw, uint32_t* dilated) {
+  /* BlockBitmapOps::rebuild (occupancy.hpp:105-121) with BandFilter
+   * (occupancy.hpp:150-153, 166-171): a block is in the band when any voxel
+   * is observed with tsdf < 1 - kBandEpsilon; the view is the 3^3 dilation
+   * (neighborhood_occupied, occupancy.hpp:69-94). */
+  uint64_t bx, by, bz;
+  band_extent(v, &bx, &by, &bz);
+  const uint64_t words = (bx * by * bz + 31u) / 32u;
+  memset(raw, 0, words * sizeof(uint32_t));
+  memset(dilated, 0, words * sizeof(uint32_t));
+  const kf_volume_geometry* g = &v->geometry;
+  for (uint32_t z = 0; z < g->res_z; ++z) {
+    for (uint32_t y = 0; y < g->res_y; ++y) {
+      for (uint32_t x = 0; x < g->res_x; ++x) {
+        const int64_t i = storage_index(v, x, y, z);
+        if (i < 0) continue;
+        const decoded_voxel d = decode_voxel(v->voxel, v->voxels, (size_t)i);
+        if (d.observed && d.tsdf < (1.0f - KFO_BAND_EPSILON)) {
+          const uint64_t b = band_index(by, bz, x / 8u, y / 8u, z / 8u);
+          raw[b / 32u] |= 1u << (b % 32u);
+        }
+      }
+    }
+  }
+  const band_view rv = {raw, bx, by, bz};
+  for (uint64_t x = 0; x < bx; ++x) {
+    for (uint64_t y = 0; y < by; ++y) {
+      for (uint64_t z = 0; z < bz; ++z) {
+        int hit = 0;
+        for (int oz = -1; oz <= 1 && !hit; ++oz) {
+          for (int oy = -1; oy <= 1 && !hit; ++oy) {
+            for (int ox = -1; ox <= 1 && !hit; ++ox) {
+              const int64_t nx = (int64_t)x + ox, ny = (int64_t)y + oy, nz = (int64_t)z + oz;
+              if (nx < 0 || ny < 0 || nz < 0 || (uint64_t)nx >= bx || (uint64_t)ny >= by || (uint64_t)nz >= bz) {
+                continue;
+              }
+              hit = band_test(&rv, (uint64_t)nx, (uint64_t)ny, (uint64_t)nz);
+            }
+          }
+        }
+        if (hit) {
+          const uint64_t b = band_index(by, bz, x, y, z);
+          dilated[b / 32u] |= 1u << (b % 32u);
+        }
+      }
+    }
+  }
+}
+
+/* compat::min / compat::max (cuda_compat.hpp:75-86) */
+static inline float cmin(float lhs, float rhs) { return rhs < lhs ? rhs : lhs; }
+static inline float cmax(float lhs, float rhs) { return lhs < rhs ? rhs : lhs; }
+
+/* BlockMarch (empty_space_skip.hpp:19-153): one ray in one volume. */
+typedef struct {
+  const kf_volume_geometry* g;
+  float block_size;
+  v3 origin, dir;
+} block_march;
+
+static inline float axis_exit(float origin, float direction, float low, float high) {
+  return ((direction >= 0.0f ? high : low) - origin) / direction;
+}
+
+static float bm_block_exit(const block_march* m, uint64_t bx, uint64_t by, uint64_t bz) {
+  const float lx = m->g->origin[0] + ((float)bx * m->block_size);
+  const float ly = m->g->origin[1] + ((float)by * m->block_size);
+  const float lz = m->g->origin[2] + ((float)bz * m->block_size);
+  const float hx = lx + (1.0f * m->block_size), hy = ly + (1.0f * m->block_size), hz = lz + (1.0f * m->block_size);
+  return cmin(axis_exit(m->origin.x, m->dir.x, lx, hx),
+              cmin(axis_exit(m->origin.y, m->dir.y, ly, hy), axis_exit(m->origin.z, m->dir.z, lz, hz)));
+}
+
+static float bm_column_exit(const block_march* m, uint64_t bx, uint64_t by) {
+  const float lx = m->g->origin[0] + ((float)bx * m->block_size);
+  const float ly = m->g->origin[1] + ((float)by * m->block_size);
+  float exit = KFO_INF;
+  if (m->dir.x != 0.0f) exit = cmin(exit, axis_exit(m->origin.x, m->dir.x, lx, lx + m->block_size));
+  if (m->dir.y != 0.0f) exit = cmin(exit, axis_exit(m->origin.y, m->dir.y, ly, ly + m->block_size));
+  return exit;
+}
+
+static float bm_z_entry(const block_march* m, uint64_t bz) {
+  const float side = m->dir.z >= 0.0f ? 0.0f : 1.0f;
+  const float plane = m->g->origin[2] + (((float)bz + side) * m->block_size);
+  return (plane - m->origin.z) / m->dir.z;
+}
+
+static void bm_slab(float origin, float direction, float low, float high, float* entry, float* exit) {
+  if (direction == 0.0f) {
+    if (origin < low || origin > high) *entry = KFO_INF;
+    return;
+  }
+  const float t_low = (low - origin) / direction;
+  const float t_high = (high - origin) / direction;
+  *entry = cmax(*entry, cmin(t_low, t_high));
+  *exit = cmin(*exit, cmax(t_low, t_high));
+}
+
+static float bm_volume_entry(const block_march* m) {
+  const kf_volume_geometry* g = m->g;
+  float entry = 0.0f, exit = KFO_INF;
+  bm_slab(m->origin.x, m->dir.x, g->origin[0], g->origin[0] + ((float)g->res_x * g->voxel_size), &entry, &exit);
+  bm_slab(m->origin.y, m->dir.y, g->origin[1], g->origin[1] + ((float)g->res_y * g->voxel_size), &entry, &exit);
+  bm_slab(m->origin.z, m->dir.z, g->origin[2], g->origin[2] + ((float)g->res_z * g->voxel_size), &entry, &exit);
+  return entry <= exit ? entry : KFO_INF;
+}
+
+/* find_set_at_or_after / find_set_at_or_before (empty_space_skip.hpp:196-217) */
+static inline int set_at_or_after(uint32_t word, unsigned offset) {
+  const uint32_t masked = word & ~((1u << offset) - 1u);
+  return masked == 0u ? -1 : __builtin_ctz(masked);
+}
+static inline int set_at_or_before(uint32_t word, unsigned offset) {
+  const uint32_t masked = word & (offset >= 31u ? ~0u : ((1u << (offset + 1u)) - 1u));
+  return masked == 0u ? -1 : 31 - __builtin_clz(masked);
+}
+
+/* BandSkip::word_scan_z (empty_space_skip.hpp:266-284) */
+static float band_word_scan_z(const band_view* b, const block_march* m, uint64_t x, uint64_t y, uint64_t z) {
+  const uint64_t index = band_index(b->by, b->bz, x, y, z);
+  const uint32_t word = b->words[index / 32u];
+  const unsigned offset = (unsigned)(index % 32u);
+  const int forward = m->dir.z >= 0.0f;
+  const int found = forward ? set_at_or_after(word, offset) : set_at_or_before(word, offset);
+  uint64_t target_z;
+  if (found >= 0) {
+    target_z = z + (uint64_t)found - offset;
+  } else {
+    target_z = forward ? z + (32u - offset) : z - (offset < z ? offset : z);
+  }
+  return cmin(bm_z_entry(m, target_z), bm_column_exit(m, x, y));
+}
+
+/* BandSkip::advance (empty_space_skip.hpp:225-262) */
+static float band_advance(const band_view* b, const kf_volume_geometry* g, v3 origin, v3 dir, float ray_length,
+                          float base_step, float max_depth) {
+  const block_march m = {g, 8.0f * g->voxel_size, origin, dir};
+  const float nudge = 0.25f * g->voxel_size;
+  const int z_major = fabsf(dir.z) >= fabsf(dir.x) && fabsf(dir.z) >= fabsf(dir.y) && (b->bz % 32u) == 0u;
+  while (ray_length <= max_depth) {
+    const v3 point = v3add(origin, v3mul(dir, ray_length));
+    const v3 grid = v3m((point.x - g->origin[0]) / g->voxel_size, (point.y - g->origin[1]) / g->voxel_size,
+                        (point.z - g->origin[2]) / g->voxel_size);
+    if (!grid_contains(g, grid)) {
+      const float entry = bm_volume_entry(&m);
+      if (entry >= KFO_INF || entry > max_depth) {
+        return max_depth + base_step;
+      }
+      ray_length = cmax(ray_length + base_step, entry + nudge);
+      continue;
+    }
+    const uint64_t x = (uint64_t)grid.x / 8u, y = (uint64_t)grid.y / 8u, z = (uint64_t)grid.z / 8u;
+    if (band_test(b, x, y, z)) {
+      return ray_length;
+    }
+    float target = KFO_INF;
+    if (z_major) target = band_word_scan_z(b, &m, x, y, z);
+    if (target >= KFO_INF) target = bm_block_exit(&m, x, y, z);
+    ray_length = cmax(ray_length + base_step, target + nudge);
+  }
+  return ray_length;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Raycasting (raycasting.hpp:116-245)                                       */
 /* ------------------------------------------------------------------------ */
-static void render_pixel(const sampler* s, const kf_raycast_camera* cam,
+/* `band` selects BandSkip (the band-march backend); NULL is the plain march
+ * (NoSkip), whose output the bitmap-march backend reproduces bit for bit. */
+static void render_pixel(const sampler* s, const band_view* band, const kf_raycast_camera* cam,
                          const kf_raycast_options* o, uint32_t col, uint32_t row, float* points,
                          float* normals, uint32_t* colors) {
   const size_t pix = (size_t)row * cam->width + col;
@@ -898,6 +1099,17 @@ static void render_pixel(const sampler* s, const kf_raycast_camera* cam,
   int found = 0;
   v3 surface = v3m(0, 0, 0);
   while (ray_length <= o->max_depth) {
+    if (band != NULL) {
+      const float advanced =
+          band_advance(band, &s->v->geometry, translation, dir, ray_length, base_step, o->max_depth);
+      if (advanced != ray_length) {
+        have_prev = 0; /* the skipped samples were all nullopt */
+        ray_length = advanced;
+        if (ray_length > o->max_depth) {
+          break;
+        }
+      }
+    }
     const v3 point = v3add(translation, v3mul(dir, ray_length));
     float tsdf;
     if (!sample_tsdf(s, point, o->corner_policy, &tsdf)) {
@@ -958,7 +1170,28 @@ void kfo_raycast(const kfo_volume* v, const kf_raycast_camera* cam, const kf_ray
 #endif
   for (int64_t row = 0; row < (int64_t)cam->height; ++row) {
     for (uint32_t col = 0; col < cam->width; ++col) {
-      render_pixel(&s, cam, o, col, (uint32_t)row, points, normals, colors);
+      render_pixel(&s, NULL, cam, o, col, (uint32_t)row, points, normals, colors);
+    }
+  }
+}
+
+void kfo_raycast_band(const kfo_volume* v, const uint32_t* band_words, const kf_raycast_camera* cam,
+                      const kf_raycast_options* o, float* points, float* normals, uint32_t* colors,
+                      int32_t threads) {
+  /* Raycaster::render with EmptySpaceIndex::visit -> BandSkip
+   * (raycasting.hpp:22-60, 165-211) over the dilated band bitmap. */
+  const sampler s = {v, 1.0f / v->geometry.voxel_size};
+  band_view b;
+  b.words = band_words;
+  band_extent(v, &b.bx, &b.by, &b.bz);
+  (void)threads;
+#ifdef _OPENMP
+  const int nt = threads > 0 ? threads : 1;
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt)
+#endif
+  for (int64_t row = 0; row < (int64_t)cam->height; ++row) {
+    for (uint32_t col = 0; col < cam->width; ++col) {
+      render_pixel(&s, &b, cam, o, col, (uint32_t)row, points, normals, colors);
     }
   }
 }

@@ -80,6 +80,14 @@ void kfo_integrate_sparse(kfo_volume* volume, const kf_frame_view* frame,
                           const kf_integration_options* options, int32_t rule);
 
 /* ---- raycasting (include/kinectfusion/raycasting.hpp) ---- */
+/* The band bitmap of a dense volume (BandRebuild<kHost>, occupancy.hpp:229-238):
+ * raw and dilated words, kfo_band_word_count of each, z-major block bits. */
+uint64_t kfo_band_word_count(const kfo_volume* volume);
+void kfo_band_bitmap(const kfo_volume* volume, uint32_t* raw, uint32_t* dilated);
+/* The band-march raycast (BandSkip over the dilated band words). */
+void kfo_raycast_band(const kfo_volume* volume, const uint32_t* band_words, const kf_raycast_camera* camera,
+                      const kf_raycast_options* options, float* points, float* normals, uint32_t* colors,
+                      int32_t threads);
 void kfo_raycast(const kfo_volume* volume, const kf_raycast_camera* camera,
                  const kf_raycast_options* options, float* points, float* normals,
                  uint32_t* colors, int32_t threads);

@@ -62,6 +62,10 @@ def load() -> C.CDLL:
                                         C.POINTER(abi.IntegrationOptions), C.c_int32]),
         "kfo_raycast": (None, [C.POINTER(Volume), C.POINTER(abi.RaycastCamera), C.POINTER(abi.RaycastOptions),
                                P, P, P, C.c_int32]),
+        "kfo_band_word_count": (C.c_uint64, [C.POINTER(Volume)]),
+        "kfo_band_bitmap": (None, [C.POINTER(Volume), P, P]),
+        "kfo_raycast_band": (None, [C.POINTER(Volume), P, C.POINTER(abi.RaycastCamera),
+                                    C.POINTER(abi.RaycastOptions), P, P, P, C.c_int32]),
         "kfo_icp_equations": (None, [P, P, C.c_uint32, C.c_uint32, P, P, C.c_uint32, C.c_uint32, abi.Intrinsics,
                                      C.POINTER(abi.Rigid), C.POINTER(abi.Rigid), C.c_float, C.c_float, P,
                                      C.POINTER(C.c_uint64)]),
@@ -318,6 +322,31 @@ def raycast(vol: OracleVolume, k, width, height, camera_to_world, o: abi.Raycast
     nrm = np.empty((height, width, 3), dtype=np.float32)
     colors = np.empty((height, width), dtype=np.uint32)
     load().kfo_raycast(C.byref(vol.struct), C.byref(cam), C.byref(o), ptr(points), ptr(nrm), ptr(colors), threads)
+    return points, nrm, colors
+
+
+def band_bitmap(vol: OracleVolume):
+    """(raw, dilated) band words of a dense volume (BandRebuild<kHost>)."""
+    n = int(load().kfo_band_word_count(C.byref(vol.struct)))
+    raw = np.zeros(n, dtype=np.uint32)
+    dilated = np.zeros(n, dtype=np.uint32)
+    load().kfo_band_bitmap(C.byref(vol.struct), ptr(raw), ptr(dilated))
+    return raw, dilated
+
+
+def raycast_band(vol: OracleVolume, band_words, k, width, height, camera_to_world, o: abi.RaycastOptions,
+                 threads=1, seed_points=None):
+    """The band-march raycast (BandSkip over the dilated band words)."""
+    cam = abi.RaycastCamera(k, width, height,
+                            camera_to_world if isinstance(camera_to_world, abi.Rigid)
+                            else abi.rigid_from_matrix(camera_to_world))
+    points = np.full((height, width, 3), np.nan, dtype=np.float32) if seed_points is None else \
+        np.ascontiguousarray(seed_points, dtype=np.float32).copy()
+    nrm = np.empty((height, width, 3), dtype=np.float32)
+    colors = np.empty((height, width), dtype=np.uint32)
+    words = np.ascontiguousarray(band_words, dtype=np.uint32)
+    load().kfo_raycast_band(C.byref(vol.struct), ptr(words), C.byref(cam), C.byref(o), ptr(points), ptr(nrm),
+                            ptr(colors), threads)
     return points, nrm, colors
 
 

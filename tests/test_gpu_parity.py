@@ -510,3 +510,57 @@ def test_sparse_mesh_identical_to_oracle(seq):
     key = lambda p: p[np.lexsort((p[:, 2], p[:, 1], p[:, 0]))]
     assert len(band["triangles"]) == len(got["triangles"])
     assert np.array_equal(key(band["positions"]), key(got["positions"]))
+
+
+# ---- band march ----------------------------------------------------------------------------
+def _band_pair(seq, frames, res, voxel):
+    vs = 5.12 / res
+    origin = (-2.56, -2.56, -0.5)
+    cfg = kf.pipeline_config(res, vs, origin, 0.05, voxel=voxel, color=abi.KF_COLOR_NONE,
+                             raycast_backend=abi.KF_RAYCAST_BAND_MARCH)
+    gpu = kf.Pipeline(cfg)
+    ref = ko.OracleVolume(res, vs, origin, 0.05, voxel=voxel, color=False)
+    for frame in range(frames):
+        raw = seq.depth[frame]
+        normals = ko.pyramid(raw, K640, ko.depth_options())[0]["normals"]
+        w2c = ko.rigid_inverse(abi.rigid_from_matrix(seq.poses[frame]))
+        gpu.integrate(raw, K640, w2c, normals=normals)
+        ko.integrate(ref, raw, K640, w2c, ko.integration_options(), abi.KF_RULE_ANGLE_WEIGHTED,
+                     normals_map=normals, threads=8)
+    return gpu, ref
+
+
+@pytest.mark.parametrize("res,voxel", [(128, abi.KF_VOXEL_FLOAT), (256, abi.KF_VOXEL_FLOAT),
+                                       (256, abi.KF_VOXEL_QUANTIZED), (256, abi.KF_VOXEL_BF16)])
+def test_band_march_bit_exact(seq, res, voxel):
+    # 256^3 has 32 z-blocks: the one-word z scan of BandSkip runs; 128^3 has 16
+    gpu, ref = _band_pair(seq, 3, res, voxel)
+    _, dilated = ko.band_bitmap(ref)
+    assert dilated.any() and np.array_equal(gpu.band_bitmap(), dilated)
+    for level in (0, 1):
+        k = ko.scaled(K640, level)
+        w, h = 640 >> level, 480 >> level
+        maps = gpu.raycast(k, w, h, seq.poses[3])
+        p, n, c = ko.raycast_band(ref, dilated, k, w, h, seq.poses[3], ko.raycast_options(), threads=8)
+        assert np.isfinite(p).all(-1).sum() > 0.3 * w * h
+        assert same_float(maps.points, p) and same_float(maps.normals, n)
+        assert np.array_equal(maps.colors, c)
+
+
+def test_band_march_frames_track_like_march(seq):
+    # the approximate skip moves interpolation endpoints by sub-voxel amounts
+    # (empty_space_skip.hpp:219-222): the tracked poses stay within 1 mm
+    def run(backend):
+        cfg = kf.pipeline_config(256, 0.02, (-2.56, -2.56, -0.5), 0.05, color=abi.KF_COLOR_NONE,
+                                 raycast_backend=backend)
+        gpu = kf.Pipeline(cfg)
+        loop = kf.Reconstruction(gpu, K640)
+        for f in range(5):
+            loop.process(seq.depth[f])
+            assert loop.results[-1].tracked
+        return gpu, np.array(loop.trajectory)
+    band, tb = run(abi.KF_RAYCAST_BAND_MARCH)
+    _, tm = run(abi.KF_RAYCAST_MARCH)
+    assert np.abs(tb[:, :3, 3] - tm[:, :3, 3]).max() < 1e-3
+    band.reset()
+    assert not band.band_bitmap().any()
