@@ -317,10 +317,15 @@ kf_status kf_gemm_bf16(const void* a, const void* b, float* c, int32_t m, int32_
 
 /* ---- launch shapes and the autotuner (no counterpart in the reference) ----
  * Shapes that leave every output bit unchanged: the march kernel's CTA
- * (raycast_block_x * raycast_block_y <= 64 threads) and the fusion grid. */
+ * (raycast_block_x * raycast_block_y <= 64 threads), the fusion grid, and
+ * the lanes that march each ray together (1, 2 or 4; a warp then holds 32,
+ * 16 or 8 rays) for renders of at most 20,000 rays, at most 80,000 rays,
+ * and more.  Small renders have too few rays to fill the GPU one lane per
+ * ray; with several lanes a ray takes up to that many samples per round. */
 typedef struct {
   uint32_t raycast_block_x, raycast_block_y;
   uint32_t integrate_ctas;
+  uint32_t raycast_lanes[3];
 } kf_launch_shapes;
 kf_status kf_pipeline_get_launch_shapes(kf_pipeline* pipeline, kf_launch_shapes* shapes);
 kf_status kf_pipeline_set_launch_shapes(kf_pipeline* pipeline, const kf_launch_shapes* shapes);

@@ -84,7 +84,8 @@ class VolumeGeometry(C.Structure):
 
 
 class LaunchShapes(C.Structure):
-    _fields_ = [("raycast_block_x", C.c_uint32), ("raycast_block_y", C.c_uint32), ("integrate_ctas", C.c_uint32)]
+    _fields_ = [("raycast_block_x", C.c_uint32), ("raycast_block_y", C.c_uint32), ("integrate_ctas", C.c_uint32),
+                ("raycast_lanes", C.c_uint32 * 3)]
 
 
 class PipelineConfig(C.Structure):

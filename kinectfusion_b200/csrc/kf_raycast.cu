@@ -39,7 +39,21 @@ struct RaycastParams {
   int policy;
   int cell_normals;
   int seed_previous;
+  uint32_t rays_per_warp;  // 32: one lane per ray, 2D CTA tile; 16 or 8: warp tiles below
 };
+
+// Pixel tile of one warp that holds `rays` rays (lanes 0..rays-1; the other
+// lanes start done and lend themselves to the live rays' cooperative rounds):
+// 16 rays -> 4 x 4 pixels, 8 rays -> 4 x 2.  A CTA stacks its warps in y.
+__device__ __forceinline__ void warp_tile_pixel(uint32_t rays, uint32_t& col, uint32_t& row, bool& has_ray) {
+  const uint32_t tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const uint32_t warp = tid >> 5, lane = tid & 31u;
+  const uint32_t warps = (blockDim.x * blockDim.y) >> 5;
+  const uint32_t tw = 4u, th = rays / 4u;
+  col = blockIdx.x * tw + (lane % tw);
+  row = (blockIdx.y * warps + warp) * th + (lane / tw) % th;
+  has_ray = lane < rays;
+}
 
 // Corner masks of the trilinear stencil with base voxel (sx, sy, sz), read
 // from the per-voxel bits (per brick layer z, 16 bytes: 64 bits "tsdf
@@ -271,9 +285,11 @@ __global__ void __launch_bounds__(64)
   // ray are done from the start), so that the warp reconverges at each
   // sample instead of running its lanes' divergent marches one after
   // another.
-  const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t row = blockIdx.y * blockDim.y + threadIdx.y;
-  const bool in_image = col < width && row < height;
+  uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t row = blockIdx.y * blockDim.y + threadIdx.y;
+  bool has_ray = true;
+  if (rp.rays_per_warp < 32u) warp_tile_pixel(rp.rays_per_warp, col, row, has_ray);
+  const bool in_image = has_ray && col < width && row < height;
   const size_t pix = in_image ? static_cast<size_t>(row) * width + col : 0;
   const Sampler<Kind> s{v};
 
@@ -760,8 +776,16 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
   rp.policy = p.config.raycast.corner_policy;
   rp.cell_normals = p.config.raycast.cell_gradient_normals;
   rp.seed_previous = p.config.raycast.seed_from_previous;
-  const dim3 block(p.raycast_block_x, p.raycast_block_y);
-  const dim3 grid(ceil_div(cam.width, block.x), ceil_div(cam.height, block.y));
+  const uint64_t rays = static_cast<uint64_t>(cam.width) * cam.height;
+  const uint32_t lanes = p.raycast_lanes[rays <= 20000u ? 0 : (rays <= 80000u ? 1 : 2)];
+  rp.rays_per_warp = p.config.raycast_backend == KF_RAYCAST_BAND_MARCH ? 32u : 32u / lanes;
+  dim3 block(p.raycast_block_x, p.raycast_block_y);
+  dim3 grid(ceil_div(cam.width, block.x), ceil_div(cam.height, block.y));
+  if (rp.rays_per_warp < 32u) {
+    // two warps per CTA, each a 4 x (rays / 4) pixel tile
+    block = dim3(64, 1);
+    grid = dim3(ceil_div(cam.width, 4u), ceil_div(cam.height, 2u * (rp.rays_per_warp / 4u)));
+  }
   // the skip structures exist once a full-sweep integration prepared them
   const uint32_t* voxel_bits = p.brick_class.count && p.view.grid == nullptr ? p.voxel_bits.ptr : nullptr;
   const uint4* stencil_bits = reinterpret_cast<const uint4*>(p.stencil_bits.ptr);

@@ -64,13 +64,15 @@ float time_frames(Scratch& s, const uint16_t* frames, uint32_t count, uint32_t w
 
 void apply(Pipeline& p, const kf_launch_shapes& shapes) {
   if (p.raycast_block_x == shapes.raycast_block_x && p.raycast_block_y == shapes.raycast_block_y &&
-      p.integrate_ctas == shapes.integrate_ctas) {
+      p.integrate_ctas == shapes.integrate_ctas && p.raycast_lanes[0] == shapes.raycast_lanes[0] &&
+      p.raycast_lanes[1] == shapes.raycast_lanes[1] && p.raycast_lanes[2] == shapes.raycast_lanes[2]) {
     return;
   }
   check(cudaStreamSynchronize(p.stream), "launch shapes");
   p.raycast_block_x = shapes.raycast_block_x;
   p.raycast_block_y = shapes.raycast_block_y;
   p.integrate_ctas = shapes.integrate_ctas;
+  for (int i = 0; i < 3; ++i) p.raycast_lanes[i] = shapes.raycast_lanes[i];
   p.clear_graphs();  // the graphs hold the old shapes
 }
 
@@ -78,6 +80,10 @@ void validate(const kf_launch_shapes& s) {
   require(s.raycast_block_x > 0 && s.raycast_block_y > 0 && s.raycast_block_x * s.raycast_block_y <= 64,
           "Raycast CTA shape must have 1..64 threads");
   require(s.integrate_ctas > 0 && s.integrate_ctas <= 65535u, "Fusion grid must have 1..65535 CTAs");
+  for (int i = 0; i < 3; ++i) {
+    require(s.raycast_lanes[i] == 1 || s.raycast_lanes[i] == 2 || s.raycast_lanes[i] == 4,
+            "Lanes per ray must be 1, 2 or 4");
+  }
 }
 
 }  // namespace
@@ -91,6 +97,7 @@ kf_status kf_pipeline_get_launch_shapes(kf_pipeline* pipeline, kf_launch_shapes*
     shapes->raycast_block_x = p.raycast_block_x;
     shapes->raycast_block_y = p.raycast_block_y;
     shapes->integrate_ctas = p.integrate_ctas;
+    for (int i = 0; i < 3; ++i) shapes->raycast_lanes[i] = p.raycast_lanes[i];
   });
 }
 
@@ -119,9 +126,10 @@ kf_status kf_pipeline_autotune(kf_pipeline* pipeline, const uint16_t* frames, ui
     check(cudaEventCreate(&s.start), "autotune event");
     check(cudaEventCreate(&s.stop), "autotune event");
     Pipeline& sp = s.pipeline->impl;
-    kf_launch_shapes best{sp.raycast_block_x, sp.raycast_block_y, sp.integrate_ctas};
+    kf_launch_shapes best{sp.raycast_block_x, sp.raycast_block_y, sp.integrate_ctas,
+                          {sp.raycast_lanes[0], sp.raycast_lanes[1], sp.raycast_lanes[2]}};
     float best_time = time_frames(s, frames, count, width, height, intrinsics);
-    // the march CTA first, then the fusion grid with the chosen CTA
+    // the march CTA first, then the lanes per ray, then the fusion grid
     const uint32_t shapes[][2] = {{8, 8}, {16, 4}, {32, 2}, {4, 16}, {8, 4}, {16, 2}};
     for (const auto& sh : shapes) {
       kf_launch_shapes c = best;
@@ -132,6 +140,20 @@ kf_status kf_pipeline_autotune(kf_pipeline* pipeline, const uint16_t* frames, ui
       if (t < best_time) {
         best_time = t;
         best = c;
+      }
+    }
+    // lanes per ray of each render-size class (one class at a time)
+    for (int cls = 0; cls < 3; ++cls) {
+      for (uint32_t lanes : {1u, 2u, 4u}) {
+        if (lanes == best.raycast_lanes[cls]) continue;
+        kf_launch_shapes c = best;
+        c.raycast_lanes[cls] = lanes;
+        apply(sp, c);
+        const float t = time_frames(s, frames, count, width, height, intrinsics);
+        if (t < best_time) {
+          best_time = t;
+          best = c;
+        }
       }
     }
     const uint32_t grids[] = {148 * 4, 148 * 8, 148 * 12, 148 * 16, 148 * 24};

@@ -237,8 +237,11 @@ class Pipeline:
         _check(lib().kf_pipeline_get_launch_shapes(self.handle, C.byref(shapes)))
         return shapes
 
-    def set_launch_shapes(self, raycast_block=(8, 8), integrate_ctas=148 * 12):
-        shapes = abi.LaunchShapes(raycast_block[0], raycast_block[1], integrate_ctas)
+    def set_launch_shapes(self, raycast_block=(8, 8), integrate_ctas=148 * 12, raycast_lanes=None):
+        """raycast_lanes: lanes per ray for renders of <= 20,000 rays, <=
+        80,000 rays and more (each 1, 2 or 4); None keeps the current ones."""
+        lanes = tuple(self.launch_shapes().raycast_lanes) if raycast_lanes is None else tuple(raycast_lanes)
+        shapes = abi.LaunchShapes(raycast_block[0], raycast_block[1], integrate_ctas, (C.c_uint32 * 3)(*lanes))
         _check(lib().kf_pipeline_set_launch_shapes(self.handle, C.byref(shapes)))
 
     def autotune(self, device_frames: int, count: int, intrinsics: abi.Intrinsics, width: int = 640,

@@ -60,12 +60,23 @@ def test_autotuned_shapes_change_no_bit():
     shapes, ms = tuned.autotune(frames.data_ptr(), 4, K640)
     assert shapes.raycast_block_x * shapes.raycast_block_y <= 64 and shapes.integrate_ctas > 0 and ms > 0
     odd = kf.Pipeline(_config(128, 0.02, abi.KF_VOXEL_BF16))
-    odd.set_launch_shapes((32, 2), 148 * 4)
+    odd.set_launch_shapes((32, 2), 148 * 4, raycast_lanes=(4, 2, 1))
+    odd2 = kf.Pipeline(_config(128, 0.02, abi.KF_VOXEL_BF16))
+    odd2.set_launch_shapes((8, 8), 148 * 12, raycast_lanes=(2, 4, 4))
     plain = kf.Pipeline(_config(128, 0.02, abi.KF_VOXEL_BF16))
-    loops = [kf.Reconstruction(p, K640) for p in (tuned, odd, plain)]
+    plain.set_launch_shapes((8, 8), 148 * 12, raycast_lanes=(1, 1, 1))
+    loops = [kf.Reconstruction(p, K640) for p in (tuned, odd, odd2, plain)]
     for f in range(5):
         for loop in loops:
             loop.process(seq.depth[f])
-    for loop in loops[:2]:
-        assert all(np.array_equal(a, b) for a, b in zip(loop.trajectory, loops[2].trajectory))
+    # the renders themselves, at every size class
+    for size in ((160, 120), (320, 240), (640, 480)):
+        k = abi.Intrinsics(K640.fx * size[0] / 640, K640.fy * size[0] / 640,
+                           (K640.cx + 0.5) * size[0] / 640 - 0.5, (K640.cy + 0.5) * size[0] / 640 - 0.5)
+        ref = plain.raycast(k, size[0], size[1], seq.poses[4])
+        for p in (odd, odd2):
+            got = p.raycast(k, size[0], size[1], seq.poses[4])
+            assert got.points.tobytes() == ref.points.tobytes() and got.normals.tobytes() == ref.normals.tobytes()
+    for loop in loops[:3]:
+        assert all(np.array_equal(a, b) for a, b in zip(loop.trajectory, loops[3].trajectory))
         assert np.array_equal(loop.pipeline.download_raw(), plain.download_raw())
