@@ -282,6 +282,10 @@ kf_status kf_pipeline_download_raw(kf_pipeline* pipeline, void* voxels, size_t v
  * counter, block_rep.cu:18-41, overflow included; allocated blocks =
  * min(attempts, capacity)) and the pool capacity in blocks.  Dense: 0, 0. */
 kf_status kf_pipeline_block_stats(kf_pipeline* pipeline, uint64_t* attempts, uint64_t* capacity);
+/* The 8^3 blocks the last integration visited (the culled or band-listed
+ * blocks every voxel of which ran the projective test; no counterpart in the
+ * reference, which visits every voxel). */
+kf_status kf_pipeline_listed_blocks(kf_pipeline* pipeline, uint64_t* blocks);
 /* Sparse storage: the block-slot grid (BlockRep::grid, block_rep.hpp:26-110),
  * one uint32 per 8^3 block in x-major block order, 0xFFFFFFFF = unallocated. */
 kf_status kf_pipeline_download_block_grid(kf_pipeline* pipeline, uint32_t* grid, size_t count);

@@ -190,6 +190,7 @@ _PROTOTYPES = {
     "kf_pipeline_block_stats": (C.c_int, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "kf_pipeline_download_block_grid": (C.c_int, [P, P, C.c_size_t]),
     "kf_pipeline_download_band_bitmap": (C.c_int, [P, P, C.c_size_t]),
+    "kf_pipeline_listed_blocks": (C.c_int, [P, C.POINTER(C.c_uint64)]),
     "kf_mesh_free": (None, [C.POINTER(Mesh)]),
     "kf_pipeline_synchronize": (C.c_int, [P]),
     "kf_pipeline_stream": (C.c_int, [P, C.POINTER(P)]),

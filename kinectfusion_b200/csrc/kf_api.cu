@@ -441,6 +441,19 @@ kf_status kf_pipeline_block_stats(kf_pipeline* pipeline, uint64_t* attempts, uin
   });
 }
 
+kf_status kf_pipeline_listed_blocks(kf_pipeline* pipeline, uint64_t* blocks) {
+  return guarded([&] {
+    require(pipeline != nullptr && blocks != nullptr, "kf_pipeline_listed_blocks: null argument");
+    Pipeline& p = pipeline->impl;
+    check(cudaStreamSynchronize(p.stream), "listed blocks sync");
+    unsigned n = 0;
+    if (p.block_count.count != 0) {
+      check(cudaMemcpy(&n, p.block_count.ptr, sizeof(unsigned), cudaMemcpyDeviceToHost), "listed blocks");
+    }
+    *blocks = n;
+  });
+}
+
 kf_status kf_pipeline_download_block_grid(kf_pipeline* pipeline, uint32_t* grid, size_t count) {
   return guarded([&] {
     require(pipeline != nullptr && grid != nullptr, "kf_pipeline_download_block_grid: null argument");

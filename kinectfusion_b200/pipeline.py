@@ -265,6 +265,12 @@ class Pipeline:
         _check(lib().kf_pipeline_download_block_grid(self.handle, _ptr(grid), grid.size))
         return grid
 
+    def listed_blocks(self) -> int:
+        """8^3 blocks the last integration visited."""
+        n = C.c_uint64()
+        _check(lib().kf_pipeline_listed_blocks(self.handle, C.byref(n)))
+        return n.value
+
     def band_bitmap(self) -> np.ndarray:
         """band-march backend: the dilated band bitmap (z-major block bits)."""
         rx, ry, rz = self.resolution
