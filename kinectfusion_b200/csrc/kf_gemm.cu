@@ -5,7 +5,9 @@
 //   C[M x N] (fp32) = A[M x K] (bf16, row-major) * B[N x K]^T (bf16, row-major)
 //                     (+ bias[N]) (ReLU)
 //
-// One CTA of 128 threads computes a 128 x BN tile of C.  Per 64-wide K slab:
+// One CTA of 128 threads computes a 128 x BN tile of C.  Per 64-wide K slab
+// (two shared-memory stages, so that copying the next slab overlaps the
+// tensor core's work on the current one):
 // the threads copy the A and B slabs into shared memory in the canonical
 // K-major layout without swizzle (8-row x 16-byte core matrices; the two
 // 8-element halves of a 16-element K step LBO = 128 B apart, consecutive
@@ -17,6 +19,8 @@
 // kernel records an error, waits (bounded) for its own MMAs, frees its tensor
 // memory and returns.
 #include <cuda_bf16.h>
+
+#include <algorithm>
 
 #include "kf_internal.h"
 
@@ -71,18 +75,37 @@ __device__ __forceinline__ uint32_t slab_offset(uint32_t row, uint32_t k, uint32
 }
 
 template <int BN>
+constexpr size_t gemm_smem_bytes() {
+  return 2u * (static_cast<size_t>(kGemmBM) + BN) * kGemmBK * 2u + 1024u;  // two stages + alignment slack
+}
+
+// One CTA computes a 128 x BN tile of C over the K slabs [blockIdx.z * slabs,
+// (blockIdx.z + 1) * slabs).  Two shared-memory stages: the threads fill the
+// next stage while the tensor core works on the current one; each stage's
+// tcgen05.commit arrives on that stage's mbarrier, which the threads wait on
+// before refilling the stage.  With gridDim.z == 1 the epilogue adds the bias
+// and applies the ReLU into C; otherwise it stores the raw partial tile into
+// C + blockIdx.z * M * ldc (split K, summed by gemm_splitk_reduce_kernel).
+template <int BN>
 __global__ void __launch_bounds__(kGemmThreads)
     gemm_bf16_kernel(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict__ B, float* __restrict__ C,
                      int M, int N, int K, int lda, int ldb, int ldc, const float* __restrict__ bias, int relu,
-                     int* __restrict__ error) {
+                     int slabs, int* __restrict__ error) {
   constexpr uint32_t kCols = BN < 32 ? 32 : BN;  // tensor-memory columns (a power of two >= 32)
-  __shared__ __align__(1024) uint8_t s_a[kGemmBM * kGemmBK * 2];
-  __shared__ __align__(1024) uint8_t s_b[BN * kGemmBK * 2];
-  __shared__ __align__(8) unsigned long long s_mbar;
+  constexpr uint32_t kStageA = kGemmBM * kGemmBK * 2, kStageB = BN * kGemmBK * 2;
+  extern __shared__ uint8_t s_dyn[];
+  // 1024-byte aligned stage buffers
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(s_dyn) + 1023u) & ~uintptr_t(1023u));
+  uint8_t* s_a[2] = {base, base + kStageA};
+  uint8_t* s_b[2] = {base + 2 * kStageA, base + 2 * kStageA + kStageB};
+  __shared__ __align__(8) unsigned long long s_mbar[2];
   __shared__ uint32_t s_tmem;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int tile_m = blockIdx.x * kGemmBM, tile_n = blockIdx.y * BN;
-  const uint32_t mbar = smem_u32(&s_mbar);
+  const int total_slabs = (K + kGemmBK - 1) / kGemmBK;
+  const int slab0 = blockIdx.z * slabs;
+  const int nslabs = min(slabs, total_slabs - slab0);
+  const uint32_t mbar[2] = {smem_u32(&s_mbar[0]), smem_u32(&s_mbar[1])};
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
@@ -90,7 +113,8 @@ __global__ void __launch_bounds__(kGemmThreads)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar[0]), "r"(1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar[1]), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -98,11 +122,15 @@ __global__ void __launch_bounds__(kGemmThreads)
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = s_tmem;
   const uint32_t idesc = instr_desc(kGemmBM, BN);
-  uint32_t phase = 0;
   bool ok = true;
+  int issued = 0;  // slabs whose MMAs were issued
 
-  for (int k0 = 0; k0 < K && ok; k0 += kGemmBK) {
-    // A slab: thread t copies row t (8 chunks of 8 bf16)
+  for (int i = 0; i < nslabs && ok; ++i) {
+    const int st = i & 1;
+    // the stage's previous MMAs (slab i - 2) must be done before it is refilled
+    if (i >= 2) ok = __syncthreads_and(mbar_wait(mbar[st], static_cast<uint32_t>(((i - 2) >> 1) & 1)));
+    if (!ok) break;
+    const int k0 = (slab0 + i) * kGemmBK;
     {
       const int row = tile_m + tid;
 #pragma unroll
@@ -110,7 +138,7 @@ __global__ void __launch_bounds__(kGemmThreads)
         const int k = k0 + c * 8;
         uint4 v = make_uint4(0u, 0u, 0u, 0u);
         if (row < M && k < K) v = *reinterpret_cast<const uint4*>(A + static_cast<size_t>(row) * lda + k);
-        *reinterpret_cast<uint4*>(s_a + slab_offset(tid, c * 8, kGemmBM)) = v;
+        *reinterpret_cast<uint4*>(s_a[st] + slab_offset(tid, c * 8, kGemmBM)) = v;
       }
     }
     for (int r = tid; r < BN; r += kGemmThreads) {
@@ -120,7 +148,7 @@ __global__ void __launch_bounds__(kGemmThreads)
         const int k = k0 + c * 8;
         uint4 v = make_uint4(0u, 0u, 0u, 0u);
         if (row < N && k < K) v = *reinterpret_cast<const uint4*>(B + static_cast<size_t>(row) * ldb + k);
-        *reinterpret_cast<uint4*>(s_b + slab_offset(r, c * 8, BN)) = v;
+        *reinterpret_cast<uint4*>(s_b[st] + slab_offset(r, c * 8, BN)) = v;
       }
     }
     // generic-proxy stores -> visible to the tensor core's async proxy
@@ -130,26 +158,32 @@ __global__ void __launch_bounds__(kGemmThreads)
       asm volatile("tcgen05.fence::after_thread_sync;");
 #pragma unroll
       for (int s = 0; s < kGemmBK / 16; ++s) {
-        const uint64_t da = smem_desc(smem_u32(s_a) + s * (kGemmBM / 8) * 256, 128, 256);
-        const uint64_t db = smem_desc(smem_u32(s_b) + s * (BN / 8) * 256, 128, 256);
-        const uint32_t accumulate = (k0 > 0 || s > 0) ? 1u : 0u;
+        const uint64_t da = smem_desc(smem_u32(s_a[st]) + s * (kGemmBM / 8) * 256, 128, 256);
+        const uint64_t db = smem_desc(smem_u32(s_b[st]) + s * (BN / 8) * 256, 128, 256);
+        const uint32_t accumulate = (i > 0 || s > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "setp.ne.b32 p, %4, 0;\n\t"
             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
             ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar[st])
                    : "memory");
     }
-    ok = mbar_wait(mbar, phase);
-    phase ^= 1u;
-    ok = __syncthreads_and(ok);
+    issued = i + 1;
+  }
+  // the last commit arrives once every MMA issued before it is complete
+  if (issued > 0) {
+    const int last = issued - 1;
+    const bool done = __syncthreads_and(mbar_wait(mbar[last & 1], static_cast<uint32_t>((last >> 1) & 1)));
+    ok = ok && done;
   }
   if (!ok) {
     if (tid == 0) atomicExch(error, 1);
   } else {
     asm volatile("tcgen05.fence::after_thread_sync;");
+    const bool split = gridDim.z > 1;
+    float* out = C + (split ? static_cast<size_t>(blockIdx.z) * M * ldc : 0u);
     const int row = tile_m + warp * 32 + lane;
 #pragma unroll
     for (int c = 0; c < BN; c += 16) {
@@ -166,10 +200,12 @@ __global__ void __launch_bounds__(kGemmThreads)
         for (int j = 0; j < 16; ++j) {
           const int col = tile_n + c + j;
           if (col >= N) continue;
-          float v = __uint_as_float(r[j]);
-          if (bias != nullptr) v += bias[col];
-          if (relu && v < 0.0f) v = 0.0f;
-          C[static_cast<size_t>(row) * ldc + col] = v;
+          float v = issued > 0 ? __uint_as_float(r[j]) : 0.0f;
+          if (!split) {
+            if (bias != nullptr) v += bias[col];
+            if (relu && v < 0.0f) v = 0.0f;
+          }
+          out[static_cast<size_t>(row) * ldc + col] = v;
         }
       }
     }
@@ -179,28 +215,74 @@ __global__ void __launch_bounds__(kGemmThreads)
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
 }
 
+// C = sum over the split partials (in split order) (+ bias) (ReLU).
+__global__ void gemm_splitk_reduce_kernel(const float* __restrict__ partial, int splits, int M, int N, int ldp,
+                                          float* __restrict__ C, int ldc, const float* __restrict__ bias, int relu) {
+  const size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= static_cast<size_t>(M) * N) return;
+  const int row = static_cast<int>(i / N), col = static_cast<int>(i % N);
+  float v = 0.0f;
+  for (int z = 0; z < splits; ++z) v += partial[(static_cast<size_t>(z) * M + row) * ldp + col];
+  if (bias != nullptr) v += bias[col];
+  if (relu && v < 0.0f) v = 0.0f;
+  C[static_cast<size_t>(row) * ldc + col] = v;
+}
+
+template <int BN>
+void launch_tiles(const __nv_bfloat16* a, const __nv_bfloat16* b, float* c, int M, int N, int K, int lda, int ldb,
+                  int ldc, const float* bias, int relu, int slabs, unsigned splits, int* error, cudaStream_t s) {
+  static bool configured = false;  // per process: every device gets the same attribute
+  if (!configured) {
+    check(cudaFuncSetAttribute(gemm_bf16_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(gemm_smem_bytes<BN>())),
+          "gemm attribute");
+    configured = true;
+  }
+  const unsigned gm = ceil_div(static_cast<unsigned>(M), static_cast<unsigned>(kGemmBM));
+  const unsigned gn = ceil_div(static_cast<unsigned>(N), static_cast<unsigned>(BN));
+  gemm_bf16_kernel<BN><<<dim3(gm, gn, splits), kGemmThreads, gemm_smem_bytes<BN>(), s>>>(
+      a, b, c, M, N, K, lda, ldb, ldc, bias, relu, slabs, error);
+}
+
 }  // namespace
 
 void launch_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int K, int lda, int ldb, int ldc,
-                      const float* bias, int relu, int* error, cudaStream_t s) {
+                      const float* bias, int relu, int* error, cudaStream_t s, float* workspace,
+                      size_t workspace_floats) {
   require(M > 0 && N > 0 && K > 0, "gemm: empty shape");
   require(lda % 8 == 0 && ldb % 8 == 0 && K % 8 == 0, "gemm: K and the leading dimensions must be multiples of 8");
   require(reinterpret_cast<uintptr_t>(A) % 16 == 0 && reinterpret_cast<uintptr_t>(B) % 16 == 0,
           "gemm: operands must be 16-byte aligned");
   const auto* a = static_cast<const __nv_bfloat16*>(A);
   const auto* b = static_cast<const __nv_bfloat16*>(B);
-  const unsigned gm = ceil_div(static_cast<unsigned>(M), static_cast<unsigned>(kGemmBM));
-  if (N <= 16) {
-    gemm_bf16_kernel<16><<<dim3(gm, 1), kGemmThreads, 0, s>>>(a, b, C, M, N, K, lda, ldb, ldc, bias, relu, error);
-  } else if (N <= 32) {
-    gemm_bf16_kernel<32><<<dim3(gm, 1), kGemmThreads, 0, s>>>(a, b, C, M, N, K, lda, ldb, ldc, bias, relu, error);
-  } else if (N <= 64) {
-    gemm_bf16_kernel<64><<<dim3(gm, 1), kGemmThreads, 0, s>>>(a, b, C, M, N, K, lda, ldb, ldc, bias, relu, error);
-  } else {
-    const unsigned gn = ceil_div(static_cast<unsigned>(N), 128u);
-    gemm_bf16_kernel<128><<<dim3(gm, gn), kGemmThreads, 0, s>>>(a, b, C, M, N, K, lda, ldb, ldc, bias, relu, error);
+  const int bn = N <= 16 ? 16 : (N <= 32 ? 32 : (N <= 64 ? 64 : 128));
+  const unsigned tiles = ceil_div(static_cast<unsigned>(M), static_cast<unsigned>(kGemmBM)) *
+                         ceil_div(static_cast<unsigned>(N), static_cast<unsigned>(bn));
+  const int total_slabs = (K + kGemmBK - 1) / kGemmBK;
+  // split K when the tiles leave most SMs idle and each split keeps >= 8 slabs
+  unsigned splits = 1;
+  if (workspace != nullptr && tiles < 148u && total_slabs >= 16) {
+    splits = std::min<unsigned>(ceil_div(296u, tiles), static_cast<unsigned>(total_slabs / 8));
+    splits = std::min<unsigned>(splits, static_cast<unsigned>(workspace_floats / (static_cast<size_t>(M) * N)));
+    if (splits < 2) splits = 1;
+  }
+  const int slabs = (total_slabs + static_cast<int>(splits) - 1) / static_cast<int>(splits);
+  splits = static_cast<unsigned>((total_slabs + slabs - 1) / slabs);  // no empty split
+  float* out = splits > 1 ? workspace : C;
+  const int ldo = splits > 1 ? N : ldc;
+  switch (bn) {
+    case 16: launch_tiles<16>(a, b, out, M, N, K, lda, ldb, ldo, bias, relu, slabs, splits, error, s); break;
+    case 32: launch_tiles<32>(a, b, out, M, N, K, lda, ldb, ldo, bias, relu, slabs, splits, error, s); break;
+    case 64: launch_tiles<64>(a, b, out, M, N, K, lda, ldb, ldo, bias, relu, slabs, splits, error, s); break;
+    default: launch_tiles<128>(a, b, out, M, N, K, lda, ldb, ldo, bias, relu, slabs, splits, error, s); break;
   }
   check(cudaGetLastError(), "gemm_bf16_kernel launch");
+  if (splits > 1) {
+    const size_t n = static_cast<size_t>(M) * N;
+    gemm_splitk_reduce_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(workspace, static_cast<int>(splits),
+                                                                                  M, N, N, C, ldc, bias, relu);
+    check(cudaGetLastError(), "gemm_splitk_reduce_kernel launch");
+  }
 }
 
 }  // namespace kf
@@ -212,7 +294,9 @@ extern "C" kf_status kf_gemm_bf16(const void* a, const void* b, float* c, int32_
     kf::DeviceArray<int> error(1);
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
     kf::check(cudaMemsetAsync(error.ptr, 0, sizeof(int), s), "gemm error flag");
-    kf::launch_gemm_bf16(a, b, c, m, n, k, k, k, n, bias, relu, error.ptr, s);
+    // split-K partials for GEMMs of few output tiles (at most 16 MB)
+    kf::DeviceArray<float> workspace(std::min<size_t>(static_cast<size_t>(m) * n * 64, size_t{1} << 22));
+    kf::launch_gemm_bf16(a, b, c, m, n, k, k, k, n, bias, relu, error.ptr, s, workspace.ptr, workspace.count);
     int flag = 0;
     kf::check(cudaMemcpyAsync(&flag, error.ptr, sizeof(int), cudaMemcpyDeviceToHost, s), "gemm error flag");
     kf::check(cudaStreamSynchronize(s), "gemm");

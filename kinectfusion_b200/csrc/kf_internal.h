@@ -334,9 +334,12 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
 // Allocates and clears the per-block skip and culling buffers.
 // C = A * B^T (+bias)(ReLU) on the tensor cores: A M x K, B N x K bf16
 // row-major (leading dimensions lda, ldb), C M x N fp32 (ldc).  `error`
-// (device int) is set when a tensor-core wait times out.
+// (device int) is set when a tensor-core wait times out.  With a workspace
+// (device floats) a GEMM of few output tiles and long K is split along K
+// across CTAs (partials in the workspace, summed in split order).
 void launch_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int K, int lda, int ldb, int ldc,
-                      const float* bias, int relu, int* error, cudaStream_t stream);
+                      const float* bias, int relu, int* error, cudaStream_t stream, float* workspace = nullptr,
+                      size_t workspace_floats = 0);
 // MarchingCubes::extract on the device (dense volumes); fills a host mesh.
 void extract_mesh(Pipeline& p, float min_weight, kf_mesh& out);
 void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t stream);

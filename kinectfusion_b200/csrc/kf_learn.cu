@@ -223,6 +223,7 @@ struct Learner {
   int rows_pad[6] = {};
   DeviceArray<__nv_bfloat16> col[4], xbf[6], t_a, t_b;
   DeviceArray<float> act[5], dact[5], dcol, dout8, loss, out, partial;
+  DeviceArray<float> workspace;  // split-K partials of the weight-gradient GEMMs
   DeviceArray<int> error;
   int steps = 0;
 
@@ -280,6 +281,7 @@ struct Learner {
     partial.resize(static_cast<size_t>((batch * kConv[0].hout * kConv[0].wout + kColsumRows - 1) / kColsumRows) *
                    kHidden);
     loss.resize(1);
+    workspace.resize(size_t{1} << 22);  // 16 MB
     out.resize(static_cast<size_t>(batch) * kOut);
     error.resize(1);
     check(cudaMemset(error.ptr, 0, sizeof(int)), "learner init");
@@ -299,7 +301,7 @@ struct Learner {
 
   void gemm(const __nv_bfloat16* a, const __nv_bfloat16* b, float* c, int m, int n, int k, int lda, int ldb,
             int ldc, const float* bias, int relu, cudaStream_t s) {
-    launch_gemm_bf16(a, b, c, m, n, k, lda, ldb, ldc, bias, relu, error.ptr, s);
+    launch_gemm_bf16(a, b, c, m, n, k, lda, ldb, ldc, bias, relu, error.ptr, s, workspace.ptr, workspace.count);
   }
 
   void colsum(const float* m, int rows, int cols, float* sums, cudaStream_t s) {

@@ -109,7 +109,7 @@ class Learner:
         if getattr(self, "handle", None) and self.handle.value:
             try:
                 lib().kf_learner_destroy(self.handle)
-            except TypeError:  # interpreter shutdown: the module is gone
+            except Exception:  # interpreter shutdown: the modules are gone
                 pass
             self.handle = C.c_void_p()
 
@@ -171,7 +171,7 @@ class WarmStart:
         if getattr(self, "handle", None) and self.handle.value:
             try:
                 lib().kf_warm_start_destroy(self.handle)
-            except TypeError:  # interpreter shutdown: the module is gone
+            except Exception:  # interpreter shutdown: the modules are gone
                 pass
             self.handle = C.c_void_p()
 
