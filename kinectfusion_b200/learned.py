@@ -106,12 +106,12 @@ class Learner:
         self.param_count = n.value
 
     def __del__(self):
-        if getattr(self, "handle", None) and self.handle.value:
-            try:
+        try:
+            if getattr(self, "handle", None) and self.handle.value:
                 lib().kf_learner_destroy(self.handle)
-            except Exception:  # interpreter shutdown: the modules are gone
-                pass
-            self.handle = C.c_void_p()
+                self.handle = C.c_void_p()
+        except Exception:  # interpreter shutdown: the modules are gone
+            pass
 
     def params(self) -> np.ndarray:
         p = np.empty(self.param_count, dtype=np.float32)
@@ -168,12 +168,12 @@ class WarmStart:
         _check(lib().kf_warm_start_create(depth_scale, C.byref(self.handle)))
 
     def __del__(self):
-        if getattr(self, "handle", None) and self.handle.value:
-            try:
+        try:
+            if getattr(self, "handle", None) and self.handle.value:
                 lib().kf_warm_start_destroy(self.handle)
-            except Exception:  # interpreter shutdown: the modules are gone
-                pass
-            self.handle = C.c_void_p()
+                self.handle = C.c_void_p()
+        except Exception:  # interpreter shutdown: the modules are gone
+            pass
 
     def input(self, pipeline: Pipeline, depth: np.ndarray, intrinsics: abi.Intrinsics, render_pose, out) -> None:
         """The net input for `depth` against the model rendered at
