@@ -256,6 +256,60 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         kernel_updates.append(u1.value - u0.value)
     abi.check(lib.kf_pipeline_set_kernel_events(pipe2.handle, None, None))
 
+    # ---- secondary figures: the march alone, and the colour-on volume ---------------
+    # one 640x480 render of the model at the last tracked pose into device maps,
+    # timed with events on the pipeline's stream (the call syncs after them)
+    rays = 640 * 480
+    d_points = torch.empty(rays * 3, device="cuda")
+    d_normals = torch.empty(rays * 3, device="cuda")
+    d_colors = torch.empty(rays, dtype=torch.int32, device="cuda")
+    maps = abi.SurfaceMapsView(d_points.data_ptr(), d_normals.data_ptr(), d_colors.data_ptr(), 640, 480,
+                               abi.KF_MEMORY_DEVICE)
+    cam = abi.RaycastCamera(k, 640, 480, abi.rigid_from_matrix(loop.trajectory[-1]))
+    torch.cuda.synchronize()
+    rc_ms = []
+    for i in range(13):
+        r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        r0.record(stream2)
+        abi.check(lib.kf_pipeline_raycast(pipe2.handle, C.byref(cam), C.byref(maps)))
+        r1.record(stream2)
+        r1.synchronize()
+        if i >= 3:
+            rc_ms.append(r0.elapsed_time(r1))
+    raycast_ms = float(np.median(rc_ms))
+    hits = int(torch.isfinite(d_points.view(-1, 3)).all(1).sum())
+    colour = None
+    if rank == 0:
+        cfg_c = kf.pipeline_config(RES, VOXEL, ORIGIN, TRUNC, color=abi.KF_COLOR_FLOAT,
+                                   rule=abi.KF_RULE_ANGLE_WEIGHTED)
+        pipe_c = kf.Pipeline(cfg_c)
+        pyr_c, tracker_c = kf.PyramidSource(), kf.ProjectiveIcpTracker()
+        sc_ptr = C.c_void_p()
+        abi.check(lib.kf_pipeline_stream(pipe_c.handle, C.byref(sc_ptr)))
+        stream_c = torch.cuda.ExternalStream(sc_ptr.value)
+        color_dev = torch.from_numpy(seq.color.view(np.int32)).cuda()
+        csteps = min(args.steps, 200)
+
+        def enqueue_c(step: int):
+            idx = frame_schedule(step)
+            abi.check(lib.kf_frame_enqueue(pipe_c.handle, pyr_c.handle, tracker_c.handle,
+                                           C.c_void_p(base + idx * frame_bytes),
+                                           C.c_void_p(color_dev.data_ptr() + idx * 640 * 480 * 4), 640, 480, k,
+                                           abi.KF_MEMORY_DEVICE, iters, 1 if step == 0 else 0))
+
+        for s in range(3):
+            enqueue_c(s)
+        torch.cuda.synchronize()
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(stream_c)
+        for s in range(csteps):
+            enqueue_c(3 + s)
+        c1.record(stream_c)
+        c1.synchronize()
+        colour = {"value": round(csteps / (c0.elapsed_time(c1) / 1e3), 2), "unit": "frames/s", "steps": csteps,
+                  "voxel_bytes": 24, "volume_gib": 3.0}
+        del pipe_c
+
     times = torch.tensor([elapsed_ms, e2e_ms], dtype=torch.float64, device="cuda")
     if dist is not None:
         dist.all_reduce(times, op=dist.ReduceOp.MAX)
@@ -291,7 +345,12 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
                      "frac": round(achieved / peaks.get("hbm_gbs", 6650.0), 4),
                      "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
                      "launch_ms": round(kernel_s * 1e3, 4),
-                     "peak_source": "measured" if not peaks.get("fallback") else "fallback"},
+                     "peak_source": "measured" if not peaks.get("fallback") else "fallback",
+                     # the reference's full sweep visits every voxel: 512^3 x 16 B per launch
+                     "full_grid_equivalent_gbs": round(RES ** 3 * 16 / kernel_s / 1e9, 1)},
+        "raycast_640x480": {"ms": round(raycast_ms, 4), "rays_per_s": round(rays / (raycast_ms / 1e3), 1),
+                            "surface_pixels": hits, "note": "march + surface kernels, one render, device maps"},
+        "colour_on": colour,
         "clocks": clocks.summary(),
     }
     if args.cpu_baseline:
@@ -495,6 +554,169 @@ def run_reference(args, rank: int) -> dict | None:
             "e2e": {"value": round(fps, 4), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+# The reference's published ablation rows (README.md:199-214, RTX 5080, TUM
+# freiburg1_desk, 512^3 at 0.01 m, colour on): flag -> (config keywords, fps).
+ABLATIONS = [
+    ("baseline", {}, 545),
+    ("--cell-normals", {"raycast_cell_gradient_normals": 1}, 840),
+    ("--integration band", {"integration_mode": 1}, 680),
+    ("--icp-device-solve", {}, 570),
+    ("--tsdf-variant classic", {"rule": 0}, 565),
+    ("--color none", {"color": 0}, 560),
+    ("--distance-scaled-truncation", {"integration_distance_scaled_truncation": 1}, 550),
+    ("--no-projective-tsdf-distance", {"integration_projective_distance": 0}, 550),
+    ("--voxel bf16", {"voxel": 2}, 550),
+    ("--voxel quantized", {"voxel": 1}, 545),
+    ("--icp-capture-graph", {}, 540),
+    ("--raycast-seed-previous", {"raycast_seed_from_previous": 1}, 540),
+    ("--raycast-tsdf-from-valid-corners", {"raycast_corner_policy": 1}, 515),
+    ("--storage sparse --integration band", {"storage": 1, "integration_mode": 1}, 505),
+    ("--raycast bitmap-march", {"raycast_backend": 1}, 140),
+    ("--raycast band-march", {"raycast_backend": 2}, 135),
+]
+
+
+def run_ablations(args) -> dict:
+    """The reference's ablation table on this pipeline: the cfg2 sequence
+    (512^3 at 0.01 m, angle-weighted, colour on unless the row turns it off)
+    under each of the reference's flags, frames/s over device-resident frames.
+    Rows whose flag selects what this pipeline always does (the device solve,
+    the captured graph) run the baseline configuration."""
+    import torch
+
+    import kinectfusion_b200 as kf
+    from kinectfusion_b200 import abi, synthetic
+
+    lib = abi.load()
+    seq = synthetic.make_sequence(seed=1000, frames=SEQ_FRAMES)
+    k = abi.Intrinsics(synthetic.FX, synthetic.FY, synthetic.CX, synthetic.CY)
+    depth_dev = torch.from_numpy(seq.depth.view(np.int16)).cuda()
+    color_dev = torch.from_numpy(seq.color.view(np.int32)).cuda()
+    iters = (C.c_uint32 * 4)(10, 5, 4, 4)
+    steps = min(args.steps, 300)
+    rows = []
+    for flag, kw, ref_fps in ABLATIONS:
+        kw = dict(kw)
+        color = kw.pop("color", abi.KF_COLOR_FLOAT)
+        rule = kw.pop("rule", abi.KF_RULE_ANGLE_WEIGHTED)
+        cfg = kf.pipeline_config(RES, VOXEL, ORIGIN, TRUNC, color=color, rule=rule, **kw)
+        pipe = kf.Pipeline(cfg)
+        pyr, tracker = kf.PyramidSource(), kf.ProjectiveIcpTracker()
+        sp = C.c_void_p()
+        abi.check(lib.kf_pipeline_stream(pipe.handle, C.byref(sp)))
+        stream = torch.cuda.ExternalStream(sp.value)
+
+        def enqueue(step: int):
+            idx = frame_schedule(step)
+            col = C.c_void_p(color_dev.data_ptr() + idx * 640 * 480 * 4) if color == abi.KF_COLOR_FLOAT else None
+            abi.check(lib.kf_frame_enqueue(pipe.handle, pyr.handle, tracker.handle,
+                                           C.c_void_p(depth_dev.data_ptr() + idx * 640 * 480 * 2), col, 640, 480,
+                                           k, abi.KF_MEMORY_DEVICE, iters, 1 if step == 0 else 0))
+
+        for st in range(3):
+            enqueue(st)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for st in range(steps):
+            enqueue(3 + st)
+        b.record(stream)
+        b.synchronize()
+        fps = steps / (a.elapsed_time(b) / 1e3)
+        last = abi.FrameResult()
+        abi.check(lib.kf_frame_result_fetch(pipe.handle, C.byref(last)))
+        rows.append({"flag": flag, "fps": round(fps, 1), "reference_rtx5080_fps": ref_fps,
+                     "tracked_last_frame": bool(last.tracked)})
+        del pipe, pyr, tracker
+        torch.cuda.synchronize()
+    base = rows[0]["fps"]
+    return {
+        "metric": "frames/s per reference ablation flag (640x480, 512^3)", "value": base, "unit": "frames/s",
+        "n_gpus": 1, "steps": steps, "warmup": 3, "higher_is_better": True, "scaling": "none", "vs_baseline": None,
+        "dtype": "per row", "data": "synthetic (seeded analytic RGB-D scene)",
+        "config": {"workload": "cfg2 sequence, 512^3 at 0.01 m, colour on unless the row turns it off, "
+                               "ICP [10,5,4]; the reference's figures are from README.md on an RTX 5080 with "
+                               "TUM freiburg1_desk (another scene and GPU)"},
+        "rows": rows,
+    }
+
+
+def run_sparse(args) -> dict:
+    """cfg3: one sequence of 300 frames (steps up to 2 cm / 1 deg) tracked and
+    fused into a sparse 8^3-block hash over a 2048^3 domain of 5 mm voxels
+    (bf16 voxels, band integration, angle-weighted TSDF, plain march), then
+    the block-wise mesh with min weight 2."""
+    import torch
+
+    import kinectfusion_b200 as kf
+    from kinectfusion_b200 import abi, synthetic
+
+    lib = abi.load()
+    frames = args.sparse_frames
+    seq = synthetic.make_sequence_device(seed=3000, frames=frames, max_step_m=0.02, max_step_deg=1.0)
+    k = abi.Intrinsics(synthetic.FX, synthetic.FY, synthetic.CX, synthetic.CY)
+    res, vs = 2048, 0.005
+    cfg = kf.pipeline_config(res, vs, (-0.5 * res * vs, -0.5 * res * vs, -0.5), 0.05, voxel=abi.KF_VOXEL_BF16,
+                             color=abi.KF_COLOR_NONE, rule=abi.KF_RULE_ANGLE_WEIGHTED,
+                             storage=abi.KF_STORAGE_SPARSE, integration_mode=abi.KF_INTEGRATION_BAND)
+    pipe = kf.Pipeline(cfg)
+    pyr, tracker = kf.PyramidSource(), kf.ProjectiveIcpTracker()
+    iters = (C.c_uint32 * 4)(10, 5, 4, 4)
+    sp = C.c_void_p()
+    abi.check(lib.kf_pipeline_stream(pipe.handle, C.byref(sp)))
+    stream = torch.cuda.ExternalStream(sp.value)
+    depth_dev = torch.from_numpy(seq.depth.view(np.int16)).cuda()
+    frame_bytes = 640 * 480 * 2
+
+    def enqueue(f: int):
+        abi.check(lib.kf_frame_enqueue(pipe.handle, pyr.handle, tracker.handle,
+                                       C.c_void_p(depth_dev.data_ptr() + f * frame_bytes), None, 640, 480, k,
+                                       abi.KF_MEMORY_DEVICE, iters, 1 if f == 0 else 0))
+
+    warm = max(args.warmup, 3)
+    for f in range(warm):
+        enqueue(f)
+    torch.cuda.synchronize()
+    u0 = C.c_uint64()
+    abi.check(lib.kf_pipeline_update_counts(pipe.handle, C.byref(u0), None))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        clocks.wait_started()
+        e0.record(stream)
+        for f in range(warm, frames):
+            enqueue(f)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    u1 = C.c_uint64()
+    abi.check(lib.kf_pipeline_update_counts(pipe.handle, C.byref(u1), None))
+    attempts, capacity = pipe.block_stats()
+    last = abi.FrameResult()
+    abi.check(lib.kf_frame_result_fetch(pipe.handle, C.byref(last)))
+    t0 = time.perf_counter()
+    mesh = pipe.extract_mesh(2.0)
+    mesh_s = time.perf_counter() - t0
+    timed = frames - warm
+    fps = timed / (ms / 1e3)
+    return {
+        "metric": "frames/s (640x480, sparse 2048^3 domain, bf16)", "value": round(fps, 2), "unit": "frames/s",
+        "n_gpus": 1, "steps": timed, "warmup": warm, "ms_per_step": round(ms / timed, 4),
+        "higher_is_better": True, "scaling": "none", "vs_baseline": None, "dtype": "bf16 voxels, f32 math",
+        "data": "synthetic (seeded analytic RGB-D scene, steps up to 2 cm / 1 deg, frames rendered on the device)",
+        "config": {"workload": f"cfg3: {frames} frames into a sparse 8^3-block hash over a 2048^3 domain of 5 mm "
+                               "voxels (bf16, band integration, angle-weighted TSDF, march raycast), then the "
+                               "block-wise mesh (min weight 2)",
+                   "blocks_capacity": capacity, "pool_gib": round(capacity * 512 * 4 / 2 ** 30, 2)},
+        "voxel_updates_per_s": round((u1.value - u0.value) / (ms / 1e3), 1),
+        "allocated_blocks": min(attempts, capacity), "allocation_attempts": attempts,
+        "tracked_last_frame": bool(last.tracked),
+        "mesh": {"seconds": round(mesh_s, 3), "vertices": int(len(mesh["positions"])),
+                 "triangles": int(len(mesh["triangles"]))},
+        "gpu_launches": None,
+        "clocks": clocks.summary(),
+    }
+
+
 def run_learned(args) -> dict:
     """cfg5: ICP iterations per frame with the learned warm start against the
     plain constant-velocity start, on held-out seeds at 512^3 dense float,
@@ -573,9 +795,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--config", choices=["cfg2", "batch16", "learned"], default="cfg2",
+    ap.add_argument("--config", choices=["cfg2", "batch16", "learned", "sparse", "ablations"], default="cfg2",
                     help="cfg2: the headline 512^3 workload (default); batch16: 16 sequences batched; "
-                         "learned: the learned ICP warm start against constant velocity")
+                         "learned: the learned ICP warm start against constant velocity; sparse: cfg3, "
+                         "a 2048^3 sparse domain; ablations: the reference's ablation flags")
+    ap.add_argument("--sparse-frames", type=int, default=300)
     ap.add_argument("--learned-seeds", type=int, default=20)
     ap.add_argument("--learned-frames", type=int, default=60)
     args = ap.parse_args()
@@ -588,6 +812,10 @@ def main():
         line = run_batch(args) if rank == 0 else None
     elif args.config == "learned":
         line = run_learned(args) if rank == 0 else None
+    elif args.config == "sparse":
+        line = run_sparse(args) if rank == 0 else None
+    elif args.config == "ablations":
+        line = run_ablations(args) if rank == 0 else None
     else:
         if world > 1:
             import datetime

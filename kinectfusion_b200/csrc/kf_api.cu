@@ -245,6 +245,7 @@ kf_status kf_pipeline_create(const kf_pipeline_config* config, kf_pipeline** out
         require(p.sparse_capacity > 0 && p.sparse_capacity < 0xFFFFFFFFull, "Sparse block capacity out of range");
         p.voxel_count = p.sparse_capacity * 512;
         p.grid.resize(blocks);
+        p.null_bricks.resize(blocks);
         p.slot_block.resize(p.sparse_capacity);
         p.allocated.resize(2);
       } else {

@@ -564,7 +564,8 @@ __global__ void sparse_assign_kernel(const uint32_t* __restrict__ marked, const 
                                      uint32_t words, const unsigned long long* __restrict__ allocated,
                                      unsigned long long capacity, uint32_t* __restrict__ grid,
                                      uint32_t* __restrict__ slot_block, uint32_t* __restrict__ list,
-                                     unsigned* __restrict__ count, const IcpState* __restrict__ state) {
+                                     unsigned* __restrict__ count, uint8_t* __restrict__ null_bricks, uint32_t bx,
+                                     uint32_t by, uint32_t bz, const IcpState* __restrict__ state) {
   if (state != nullptr && state->failed) return;
   const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= words) return;
@@ -574,8 +575,18 @@ __global__ void sparse_assign_kernel(const uint32_t* __restrict__ marked, const 
     const uint32_t b = static_cast<uint32_t>(__ffs(fresh) - 1);
     fresh &= fresh - 1u;
     if (slot < capacity) {
-      grid[w * 32u + b] = static_cast<uint32_t>(slot);
-      slot_block[slot] = w * 32u + b;
+      const uint32_t block = w * 32u + b;
+      grid[block] = static_cast<uint32_t>(slot);
+      slot_block[slot] = block;
+      // the stencils that can reach this block are no longer all nullopt
+      const int x = static_cast<int>(block % bx), y = static_cast<int>((block / bx) % by),
+                z = static_cast<int>(block / (bx * by));
+      for (int d = 0; d < 8; ++d) {
+        const int nx = x - (d & 1), ny = y - ((d >> 1) & 1), nz = z - (d >> 2);
+        if (nx >= 0 && ny >= 0 && nz >= 0) {
+          null_bricks[(static_cast<size_t>(nz) * by + static_cast<uint32_t>(ny)) * bx + static_cast<uint32_t>(nx)] = 0;
+        }
+      }
     }
     ++slot;
   }
@@ -694,6 +705,7 @@ void reset_blocks(Pipeline& p, cudaStream_t s) {
 void reset_sparse(Pipeline& p, cudaStream_t s) {
   if (p.grid.count == 0) return;
   check(cudaMemsetAsync(p.grid.ptr, 0xFF, p.grid.bytes(), s), "sparse grid reset");
+  check(cudaMemsetAsync(p.null_bricks.ptr, 1, p.null_bricks.bytes(), s), "sparse grid reset");
   check(cudaMemsetAsync(p.allocated.ptr, 0, p.allocated.bytes(), s), "sparse counter reset");
 }
 
@@ -735,7 +747,8 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
       check(cudaGetLastError(), "sparse_scan_top_kernel launch");
       sparse_assign_kernel<<<ceil_div(words, 256), 256, 0, s>>>(
           p.band_bits.ptr, p.new_bits.ptr, p.word_prefix.ptr, p.cta_prefix.ptr, words, p.allocated.ptr,
-          p.sparse_capacity, p.grid.ptr, p.slot_block.ptr, p.block_list.ptr, p.block_count.ptr, state);
+          p.sparse_capacity, p.grid.ptr, p.slot_block.ptr, p.block_list.ptr, p.block_count.ptr, p.null_bricks.ptr,
+          p.view.bx, p.view.by, p.view.bz, state);
       check(cudaGetLastError(), "sparse_assign_kernel launch");
     } else {
       band_compact_kernel<<<ceil_div(words, 256), 256, 0, s>>>(p.band_bits.ptr, words, p.block_list.ptr,

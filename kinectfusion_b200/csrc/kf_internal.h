@@ -258,6 +258,9 @@ struct Pipeline {
   // in z-major order (32 z-blocks per word), raw and 3^3-dilated; rebuilt
   // after every integration.
   DeviceArray<uint32_t> band_raw, band_map;
+  // sparse storage: per block b (x-major), 1 while the blocks b + {0,1}^3 are
+  // all unallocated (every trilinear stencil based in b is then nullopt)
+  DeviceArray<uint8_t> null_bricks;
   // Sparse storage (BlockRep, block_rep.hpp:26-110): a slot per 8^3 block in
   // `grid` (kUnallocated when none), `sparse_capacity` slots in the pools.
   DeviceArray<uint32_t> grid;

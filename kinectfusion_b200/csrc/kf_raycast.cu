@@ -191,9 +191,27 @@ template <int Kind>
 __device__ __forceinline__ int march_sample(const Sampler<Kind>& s, const VolumeDev& v,
                                             const uint32_t* __restrict__ voxel_bits,
                                             const uint4* __restrict__ stencil_bits,
-                                            const uint8_t* __restrict__ brick_class, int policy, f3 point,
+                                            const uint8_t* __restrict__ brick_class,
+                                            const uint8_t* __restrict__ null_bricks, int policy, f3 point,
                                             float& tsdf, uint32_t& jump) {
   jump = 0u;
+  if (null_bricks != nullptr) {
+    // sparse storage: a stencil based in a block whose 2x2x2 block
+    // neighbourhood is unallocated has no observed corner
+    const f3 g = (point - v.origin) * v.inv_voxel_size;
+    if (!in_grid(v, g)) return kNull;
+    const int sx = static_cast<int>(floorf(g.x - 0.5f)), sy = static_cast<int>(floorf(g.y - 0.5f)),
+              sz = static_cast<int>(floorf(g.z - 0.5f));
+    if (sx >= 0 && sy >= 0 && sz >= 0) {
+      const uint32_t bx = static_cast<uint32_t>(sx) >> 3, by = static_cast<uint32_t>(sy) >> 3,
+                     bz = static_cast<uint32_t>(sz) >> 3;
+      if (__ldg(null_bricks + (static_cast<size_t>(bz) * v.by + by) * v.bx + bx)) {
+        if (bx < 1024u && by < 1024u && bz < 1024u) jump = 0x80000000u | bx | (by << 10) | (bz << 20);
+        return kNull;
+      }
+    }
+    return s.tsdf(point, policy, tsdf) ? kValue : kNull;
+  }
   if (voxel_bits != nullptr) {
     const f3 g = (point - v.origin) * v.inv_voxel_size;
     if (!in_grid(v, g)) return kNull;
@@ -273,7 +291,7 @@ __device__ __forceinline__ void box_range(const VolumeDev& v, f3 o, f3 d, float&
 template <int Kind>
 __global__ void __launch_bounds__(64)
     raycast_kernel(VolumeDev v, const uint32_t* __restrict__ voxel_bits, const uint4* __restrict__ stencil_bits,
-                   const uint8_t* __restrict__ brick_class,
+                   const uint8_t* __restrict__ brick_class, const uint8_t* __restrict__ null_bricks,
                    RaycastParams rp, Intr k, uint32_t width,
                    uint32_t height, Rigid pose, const IcpState* __restrict__ state, float* __restrict__ points) {
   if (state != nullptr) {
@@ -391,7 +409,7 @@ __global__ void __launch_bounds__(64)
         f3 point = make(0.0f, 0.0f, 0.0f);
         if (r <= rp.max_depth && !(r > t_out)) {
           point = pose.t + (dir * r);
-          kind = march_sample(s, v, voxel_bits, stencil_bits, brick_class, rp.policy, point, tsdf, jump);
+          kind = march_sample(s, v, voxel_bits, stencil_bits, brick_class, null_bricks, rp.policy, point, tsdf, jump);
         }
         f3 surf = make(0.0f, 0.0f, 0.0f);
         const int event = sample_event(kind, tsdf, point, have_prev, prev_tsdf, prev_point, surf);
@@ -432,7 +450,7 @@ __global__ void __launch_bounds__(64)
     f3 point = make(0.0f, 0.0f, 0.0f);
     if (active && r <= rp.max_depth && !(r > o_tout)) {
       point = pose.t + (o_dir * r);
-      kind = march_sample(s, v, voxel_bits, stencil_bits, brick_class, rp.policy, point, tsdf, jump);
+      kind = march_sample(s, v, voxel_bits, stencil_bits, brick_class, null_bricks, rp.policy, point, tsdf, jump);
     }
     // the state before this sample: the previous lane's sample, or the ray's
     const int up_kind = __shfl_up_sync(0xFFFFFFFFu, kind, 1);
@@ -796,7 +814,8 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
                                                    cam.height, pose, state, points);
     check(cudaGetLastError(), "band_march_kernel launch");
   } else {
-    raycast_kernel<Kind><<<grid, block, 0, s>>>(p.view, voxel_bits, stencil_bits, p.brick_class.ptr, rp,
+    const uint8_t* null_bricks = p.view.grid != nullptr ? p.null_bricks.ptr : nullptr;
+    raycast_kernel<Kind><<<grid, block, 0, s>>>(p.view, voxel_bits, stencil_bits, p.brick_class.ptr, null_bricks, rp,
                                                 intr_from(cam.intrinsics), cam.width, cam.height, pose, state,
                                                 points);
     check(cudaGetLastError(), "raycast_kernel launch");
