@@ -725,13 +725,14 @@ def run_learned(args) -> dict:
     import torch
 
     import kinectfusion_b200 as kf
-    from kinectfusion_b200 import learned, synthetic
+    from kinectfusion_b200 import abi, learned, synthetic
 
     seeds = list(range(5000, 5000 + args.learned_seeds))
     net = learned.Learner(8, seed=0)
     net.load(learned.PARAMS)
     gpu = kf.Pipeline(learned.volume_config(RES, VOXEL))
     report = learned.evaluate(net, seeds, args.learned_frames, pipeline=gpu)
+    one_step = learned.one_step_errors(net, seeds, args.learned_frames, pipeline=gpu)
     mean = report["mean"]
     tracked = [r for r in report["per_seed"] if r["ate_velocity_m"] < 0.01]
 
@@ -749,6 +750,26 @@ def run_learned(args) -> dict:
         for f in range(3, args.learned_frames):
             loop.process(seq.depth[f])
         rates[mode] = (args.learned_frames - 3) / (time.perf_counter() - t0)
+    # the same two loops with every step on the device and device-resident
+    # frames (kf_warm_start_enqueue + kf_frame_enqueue, one sync at the end)
+    dev_depth = torch.from_numpy(seq.depth.view(np.int16)).cuda()
+    device_rates = {}
+    for mode in ("velocity", "learned"):
+        gpu.reset()
+        aloop = learned.AsyncLearnedLoop(gpu, learned.intrinsics640(), net, use_net=(mode == "learned"))
+        stream_ptr = C.c_void_p()
+        abi.check(abi.load().kf_pipeline_stream(gpu.handle, C.byref(stream_ptr)))
+        astream = torch.cuda.ExternalStream(stream_ptr.value)
+        for f in range(3):
+            aloop.enqueue(dev_depth.data_ptr() + f * 640 * 480 * 2)
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(astream)
+        for f in range(3, args.learned_frames):
+            aloop.enqueue(dev_depth.data_ptr() + f * 640 * 480 * 2)
+        a1.record(astream)
+        a1.synchronize()
+        device_rates[mode] = (args.learned_frames - 3) / (a0.elapsed_time(a1) / 1e3)
     # the net's forward pass alone (batch 8, device-resident input)
     x = torch.zeros((8, 60, 80, 2), dtype=torch.bfloat16, device="cuda")
     for _ in range(10):
@@ -780,7 +801,9 @@ def run_learned(args) -> dict:
                   else None},
         "proposal_used": mean["proposal_used"],
         "start_error_m": {"velocity": mean["start_error_velocity_m"], "proposal": mean["start_error_proposal_m"]},
+        "one_step_start_error_m": one_step,
         "frames_per_s": {k: round(v, 2) for k, v in rates.items()},
+        "frames_per_s_device": {k: round(v, 2) for k, v in device_rates.items()},
         "net_forward_ms": round(forward_ms, 4),
         "e2e": {"value": round(rates["learned"], 2), "unit": "frames/s", "h2d_bytes_per_step": 2 * 640 * 480 * 2,
                 "d2h_bytes_per_step": 0},

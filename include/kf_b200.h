@@ -489,6 +489,20 @@ kf_status kf_warm_start_input(kf_warm_start* warm, kf_pipeline* pipeline, const 
 kf_status kf_warm_start_propose(kf_warm_start* warm, kf_learner* learner, kf_pipeline* pipeline,
                                 const uint16_t* depth, uint32_t width, uint32_t height, kf_intrinsics intrinsics,
                                 int32_t memory, const kf_rigid* predicted, kf_warm_start_result* result);
+/* The same step kept on the device, for loops that enqueue frames without a
+ * host round trip (kf_frame_enqueue): ordered on the pipeline's stream, it
+ * reads the tracker's pose (the previous frame's result), predicts the
+ * constant-velocity pose from it and the pose the previous call read (the
+ * pose itself on the first call after kf_warm_start_reset), and, with
+ * use_net, runs the net and the fallback test; the chosen start is written
+ * into the tracker as kf_frame_set_pose does.  Call it once before each
+ * tracked frame; kf_warm_start_fetch (synchronises) reads the last step's
+ * candidates, costs and choice. */
+kf_status kf_warm_start_reset(kf_warm_start* warm);
+kf_status kf_warm_start_enqueue(kf_warm_start* warm, kf_learner* learner, kf_pipeline* pipeline, kf_tracker* tracker,
+                                const uint16_t* depth, uint32_t width, uint32_t height, kf_intrinsics intrinsics,
+                                int32_t memory, int32_t use_net);
+kf_status kf_warm_start_fetch(kf_warm_start* warm, kf_pipeline* pipeline, kf_warm_start_result* result);
 
 /* Sets the device-resident camera_to_world that the next enqueued frame
  * starts from (ordered on the pipeline's stream). */

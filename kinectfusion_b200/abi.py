@@ -224,6 +224,9 @@ _PROTOTYPES = {
     "kf_warm_start_input": (C.c_int, [P, P, P, C.c_uint32, C.c_uint32, Intrinsics, C.c_int32, C.POINTER(Rigid), P]),
     "kf_warm_start_propose": (C.c_int, [P, P, P, P, C.c_uint32, C.c_uint32, Intrinsics, C.c_int32,
                                         C.POINTER(Rigid), C.POINTER(WarmStartResult)]),
+    "kf_warm_start_reset": (C.c_int, [P]),
+    "kf_warm_start_enqueue": (C.c_int, [P, P, P, P, P, C.c_uint32, C.c_uint32, Intrinsics, C.c_int32, C.c_int32]),
+    "kf_warm_start_fetch": (C.c_int, [P, P, C.POINTER(WarmStartResult)]),
 }
 
 _lib = None

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <random>
 #include <vector>
@@ -449,8 +450,11 @@ __global__ void net_depth_kernel(const uint16_t* __restrict__ depth, uint32_t wi
 // The predicted depth is the camera-frame z of the model surface rendered at
 // `pose`.  One CTA of 1024 threads.
 constexpr float kDiffGain = 10.0f;
-__global__ void net_input_kernel(const float* __restrict__ current, const float* __restrict__ points, Pose34 pose,
-                                 __nv_bfloat16* __restrict__ out, float* __restrict__ predicted) {
+__global__ void net_input_kernel(const float* __restrict__ current, const float* __restrict__ points, Pose34 pose_arg,
+                                 const Pose34* __restrict__ pose_dev, __nv_bfloat16* __restrict__ out,
+                                 float* __restrict__ predicted) {
+  // the render pose: a kernel argument, or device memory when pose_dev is set
+  const Pose34 pose = pose_dev != nullptr ? *pose_dev : pose_arg;
   __shared__ float s_sum[1024];
   __shared__ int s_n[1024];
   float sum = 0.0f;
@@ -585,6 +589,214 @@ kf_rigid apply_twist(const kf_rigid& pose, const double tw[6]) {
   return out;
 }
 
+// ---- the asynchronous warm start: every step on the device ---------------
+// Row-major 3x4 rigid transforms in double.
+__device__ void rigid_mul(const double* a, const double* b, double* out) {
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 4; ++j) {
+      double v = a[i * 4 + 0] * b[0 * 4 + j] + a[i * 4 + 1] * b[1 * 4 + j] + a[i * 4 + 2] * b[2 * 4 + j];
+      if (j == 3) v += a[i * 4 + 3];
+      out[i * 4 + j] = v;
+    }
+  }
+}
+// Inverse of [A | t] as [A^-1 | -A^-1 t], A^-1 by cofactors: the inverse of
+// the float pose as stored, whose rotation is orthonormal only to float
+// precision (the transpose would compound that error through the
+// prediction).
+__device__ void rigid_inv(const double* a, double* out) {
+  const double a00 = a[0], a01 = a[1], a02 = a[2], a10 = a[4], a11 = a[5], a12 = a[6];
+  const double a20 = a[8], a21 = a[9], a22 = a[10];
+  const double c00 = a11 * a22 - a12 * a21, c01 = a12 * a20 - a10 * a22, c02 = a10 * a21 - a11 * a20;
+  const double det = a00 * c00 + a01 * c01 + a02 * c02;
+  const double inv_det = 1.0 / det;
+  double m[9];
+  m[0] = c00 * inv_det;
+  m[1] = (a02 * a21 - a01 * a22) * inv_det;
+  m[2] = (a01 * a12 - a02 * a11) * inv_det;
+  m[3] = c01 * inv_det;
+  m[4] = (a00 * a22 - a02 * a20) * inv_det;
+  m[5] = (a02 * a10 - a00 * a12) * inv_det;
+  m[6] = c02 * inv_det;
+  m[7] = (a01 * a20 - a00 * a21) * inv_det;
+  m[8] = (a00 * a11 - a01 * a10) * inv_det;
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) out[i * 4 + j] = m[i * 3 + j];
+    out[i * 4 + 3] = -(m[i * 3 + 0] * a[3] + m[i * 3 + 1] * a[7] + m[i * 3 + 2] * a[11]);
+  }
+}
+
+// Device state of the asynchronous warm start.
+struct WarmDevice {
+  double history[12];  // the pose the previous call saw (camera_to_world)
+  int known;           // calls so far (the history holds a pose once >= 1)
+  Pose34 predicted;    // this call's constant-velocity pose (floats)
+  Pose34 poses[2];     // predicted, proposal: the two candidate starts
+  float twist[6];
+  float costs[4];
+  int used_proposal;
+  int lost;            // the previous frame lost track: no velocity, no net
+};
+
+// Pushes the tracker's pose (the previous frame's result, rounded to float
+// as each frame starts from the float pose), predicts the constant-velocity
+// pose T1 (T0^-1 T1) from it and the previous push (T1 itself after a frame
+// that lost track), and points the render state at the prediction.
+__global__ void warm_predict_kernel(const IcpState* __restrict__ st, WarmDevice* w, IcpState* render) {
+  if (threadIdx.x != 0) return;
+  double t1[12], pred[12];
+  for (int i = 0; i < 12; ++i) t1[i] = static_cast<double>(static_cast<float>(st->pose[i]));
+  // after a frame that lost track the last motion says nothing: no velocity
+  w->lost = st->failed ? 1 : 0;
+  if (w->known >= 1 && !st->failed) {
+    double inv0[12], delta[12];
+    rigid_inv(w->history, inv0);
+    rigid_mul(inv0, t1, delta);
+    rigid_mul(t1, delta, pred);
+  } else {
+    for (int i = 0; i < 12; ++i) pred[i] = t1[i];
+  }
+  for (int i = 0; i < 12; ++i) w->history[i] = t1[i];
+  w->known += 1;
+  for (int i = 0; i < 12; ++i) w->predicted.m[i] = static_cast<float>(pred[i]);
+  // render state: camera = kf_rigid layout (rotation rows, then translation)
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) render->camera[i * 3 + j] = w->predicted.m[i * 4 + j];
+    render->camera[9 + i] = w->predicted.m[i * 4 + 3];
+  }
+  render->failed = 0;
+}
+
+// pose * exp(twist) as apply_twist, on the device.
+__device__ void apply_twist_dev(const Pose34& pose, const double* tw, Pose34& out) {
+  const double wx = tw[3], wy = tw[4], wz = tw[5];
+  const double th = sqrt(wx * wx + wy * wy + wz * wz);
+  double d[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  if (th > 1e-15) {
+    const double kx = wx / th, ky = wy / th, kz = wz / th, sn = sin(th), cs = 1.0 - cos(th);
+    const double K[9] = {0, -kz, ky, kz, 0, -kx, -ky, kx, 0};
+    for (int i = 0; i < 3; ++i) {
+      for (int j = 0; j < 3; ++j) {
+        double k2 = 0;
+        for (int q = 0; q < 3; ++q) k2 += K[3 * i + q] * K[3 * q + j];
+        d[3 * i + j] += sn * K[3 * i + j] + cs * k2;
+      }
+    }
+  }
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) {
+      double a = 0;
+      for (int q = 0; q < 3; ++q) a += static_cast<double>(pose.m[4 * i + q]) * d[3 * q + j];
+      out.m[4 * i + j] = static_cast<float>(a);
+    }
+    double t = pose.m[4 * i + 3];
+    for (int q = 0; q < 3; ++q) t += static_cast<double>(pose.m[4 * i + q]) * tw[q];
+    out.m[4 * i + 3] = static_cast<float>(t);
+  }
+}
+
+// The proposal from the net's output (or none), both candidates' truncated
+// costs (the warm_cost_kernel arithmetic, one CTA), the choice, and the
+// chosen start written into the tracker as kf_frame_set_pose would.
+__global__ void __launch_bounds__(256)
+    warm_choose_kernel(const float* __restrict__ current, const float* __restrict__ points,
+                       const float* __restrict__ normals, const float* __restrict__ net_out, float scale, Intr k,
+                       float cap, int use_net, WarmDevice* w, IcpState* st) {
+  __shared__ float s_cost[256];
+  __shared__ float s_match[256];
+  use_net = use_net && !w->lost;
+  if (threadIdx.x == 0) {
+    w->poses[0] = w->predicted;
+    if (use_net) {
+      double tw[6];
+      for (int i = 0; i < 6; ++i) {
+        tw[i] = static_cast<double>(net_out[i]) / static_cast<double>(scale);
+        w->twist[i] = static_cast<float>(tw[i]);
+      }
+      apply_twist_dev(w->predicted, tw, w->poses[1]);
+    } else {
+      w->poses[1] = w->predicted;
+      for (int i = 0; i < 6; ++i) w->twist[i] = 0.0f;
+    }
+  }
+  __syncthreads();
+  const Pose34 render = w->predicted;
+  for (int cand = 0; cand < 2; ++cand) {
+    const Pose34 p = w->poses[cand];
+    float cost = 0.0f, matched = 0.0f;
+    for (int i = threadIdx.x; i < kNetPixels; i += blockDim.x) {
+      const float d = current[i];
+      if (!(d > 0.0f)) continue;
+      const int u = i % kNetW, v = i / kNetW;
+      const float cx = (static_cast<float>(u) - k.cx) / k.fx * d, cy = (static_cast<float>(v) - k.cy) / k.fy * d;
+      const float wx = p.m[0] * cx + p.m[1] * cy + p.m[2] * d + p.m[3];
+      const float wy = p.m[4] * cx + p.m[5] * cy + p.m[6] * d + p.m[7];
+      const float wz = p.m[8] * cx + p.m[9] * cy + p.m[10] * d + p.m[11];
+      const float ex = wx - render.m[3], ey = wy - render.m[7], ez = wz - render.m[11];
+      const float rx = render.m[0] * ex + render.m[4] * ey + render.m[8] * ez;
+      const float ry = render.m[1] * ex + render.m[5] * ey + render.m[9] * ez;
+      const float rz = render.m[2] * ex + render.m[6] * ey + render.m[10] * ez;
+      float c = cap * cap;
+      if (rz > 0.0f) {
+        const float fu = k.fx * rx / rz + k.cx, fv = k.fy * ry / rz + k.cy;
+        if (fu > -0.5f && fu < kNetW - 0.5f && fv > -0.5f && fv < kNetH - 0.5f) {
+          const int mu = min(kNetW - 1, max(0, __float2int_rn(fu)));
+          const int mv = min(kNetH - 1, max(0, __float2int_rn(fv)));
+          const int j = mv * kNetW + mu;
+          const float mx = points[3 * j], my = points[3 * j + 1], mz = points[3 * j + 2];
+          const float nx = normals[3 * j], ny = normals[3 * j + 1], nz = normals[3 * j + 2];
+          if (isfinite(mx) && isfinite(nx)) {
+            const float qx = wx - mx, qy = wy - my, qz = wz - mz;
+            if (qx * qx + qy * qy + qz * qz < cap * cap) {
+              const float r = qx * nx + qy * ny + qz * nz;
+              c = fminf(r * r, cap * cap);
+              matched += 1.0f;
+            }
+          }
+        }
+      }
+      cost += c;
+    }
+    s_cost[threadIdx.x] = cost;
+    s_match[threadIdx.x] = matched;
+    __syncthreads();
+    for (int sh = blockDim.x / 2; sh > 0; sh >>= 1) {
+      if (threadIdx.x < sh) {
+        s_cost[threadIdx.x] += s_cost[threadIdx.x + sh];
+        s_match[threadIdx.x] += s_match[threadIdx.x + sh];
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      w->costs[2 * cand] = s_cost[0];
+      w->costs[2 * cand + 1] = s_match[0];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x != 0) return;
+  w->used_proposal = use_net && w->costs[2] <= w->costs[0] ? 1 : 0;
+  const Pose34& start = w->poses[w->used_proposal];
+  // icp_set_pose_kernel with reset_frame = 1
+  for (int i = 0; i < 12; ++i) st->pose[i] = static_cast<double>(start.m[i]);
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) st->camera[i * 3 + j] = start.m[i * 4 + j];
+    st->camera[9 + i] = start.m[i * 4 + 3];
+  }
+  // world_to_camera = {R^T, -R^T t} as icp_set_pose_kernel writes it
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) st->world_to_camera[i * 3 + j] = static_cast<float>(st->pose[j * 4 + i]);
+    st->world_to_camera[9 + i] = static_cast<float>(
+        -(st->pose[0 * 4 + i] * st->pose[3] + st->pose[1 * 4 + i] * st->pose[7] + st->pose[2 * 4 + i] * st->pose[11]));
+  }
+  st->failed = 0;
+  st->status = KF_ICP_NOT_RUN;
+  for (int l = 0; l < 4; ++l) {
+    st->level_status[l] = KF_ICP_NOT_RUN;
+    st->level_iterations[l] = 0;
+    st->level_correspondences[l] = 0;
+  }
+}
+
 }  // namespace
 
 struct WarmStart {
@@ -595,8 +807,16 @@ struct WarmStart {
   DeviceArray<uint32_t> colors;
   DeviceArray<Pose34> poses;
   DeviceArray<__nv_bfloat16> input;  // 8 samples (the smallest batch); only the first is filled
+  DeviceArray<WarmDevice> dev;       // the asynchronous warm start's state
+  DeviceArray<IcpState> render;      // the render pose of the asynchronous warm start
+  PinnedArray<WarmDevice> staging;
 
   void init() {
+    dev.resize(1);
+    render.resize(1);
+    staging.resize(1);
+    check(cudaMemset(dev.ptr, 0, dev.bytes()), "warm start init");
+    check(cudaMemset(render.ptr, 0, render.bytes()), "warm start init");
     current.resize(kNetPixels);
     predicted.resize(kNetPixels);
     points.resize(kNetPixels * 3);
@@ -633,8 +853,41 @@ struct WarmStart {
     cam.height = kNetH;
     cam.camera_to_world = render_pose;
     launch_raycast(p, cam, points.ptr, normals.ptr, colors.ptr, nullptr, s);
-    net_input_kernel<<<1, 1024, 0, s>>>(current.ptr, points.ptr, pose34(render_pose), out, predicted.ptr);
+    net_input_kernel<<<1, 1024, 0, s>>>(current.ptr, points.ptr, pose34(render_pose), nullptr, out, predicted.ptr);
     check(cudaGetLastError(), "warm start input");
+  }
+
+  // The asynchronous step: prediction from the tracker's pose, render, net,
+  // choice, and the start written into the tracker; no host round trip.
+  void enqueue(Pipeline& p, Learner* l, IcpState* st, const uint16_t* depth, uint32_t width, uint32_t height,
+               int memory, const kf_intrinsics& k, bool use_net) {
+    require(width == kNetW * kNetDown && height == kNetH * kNetDown, "warm start: depth frames must be 640 x 480");
+    require(k.fx > 0.0f && k.fy > 0.0f, "warm start: intrinsics must have positive focal lengths");
+    const cudaStream_t s = p.stream;
+    warm_predict_kernel<<<1, 32, 0, s>>>(st, dev.ptr, render.ptr);
+    check(cudaGetLastError(), "warm start predict");
+    const uint16_t* d = depth;
+    if (memory != KF_MEMORY_DEVICE) {
+      staged.resize(static_cast<size_t>(width) * height);
+      check(cudaMemcpyAsync(staged.ptr, depth, staged.bytes(), cudaMemcpyHostToDevice, s), "warm start depth");
+      d = staged.ptr;
+    }
+    net_depth_kernel<<<(kNetPixels + 255) / 256, 256, 0, s>>>(d, width, height, 1.0f / depth_scale, current.ptr);
+    kf_raycast_camera cam{};
+    cam.intrinsics = net_intrinsics(k);
+    cam.width = kNetW;
+    cam.height = kNetH;
+    std::memset(&cam.camera_to_world, 0, sizeof(cam.camera_to_world));  // the render state holds the pose
+    launch_raycast(p, cam, points.ptr, normals.ptr, colors.ptr, render.ptr, s);
+    const Pose34* pred = reinterpret_cast<const Pose34*>(reinterpret_cast<const char*>(dev.ptr) +
+                                                         offsetof(WarmDevice, predicted));
+    net_input_kernel<<<1, 1024, 0, s>>>(current.ptr, points.ptr, Pose34{}, pred, input.ptr, predicted.ptr);
+    check(cudaGetLastError(), "warm start input");
+    if (use_net) l->forward(input.ptr, 8, s);
+    warm_choose_kernel<<<1, 256, 0, s>>>(current.ptr, points.ptr, normals.ptr, use_net ? l->out.ptr : nullptr,
+                                         static_cast<float>(KF_WARM_START_TWIST_SCALE),
+                                         intr_from(net_intrinsics(k)), cost_cap, use_net ? 1 : 0, dev.ptr, st);
+    check(cudaGetLastError(), "warm start choose");
   }
 };
 
@@ -779,6 +1032,52 @@ kf_status kf_warm_start_input(kf_warm_start* warm, kf_pipeline* pipeline, const 
     require(reinterpret_cast<uintptr_t>(input) % 16 == 0, "kf_warm_start_input: input must be 16-byte aligned");
     warm->impl.build(pipeline->impl, depth, width, height, memory, intrinsics, *render_pose,
                      static_cast<__nv_bfloat16*>(input));
+  });
+}
+
+kf_status kf_warm_start_reset(kf_warm_start* warm) {
+  return guarded([&] {
+    require(warm != nullptr, "kf_warm_start_reset: null argument");
+    check(cudaMemset(warm->impl.dev.ptr, 0, warm->impl.dev.bytes()), "warm start reset");
+  });
+}
+
+kf_status kf_warm_start_enqueue(kf_warm_start* warm, kf_learner* learner, kf_pipeline* pipeline, kf_tracker* tracker,
+                                const uint16_t* depth, uint32_t width, uint32_t height, kf_intrinsics intrinsics,
+                                int32_t memory, int32_t use_net) {
+  return guarded([&] {
+    require(warm && pipeline && tracker && depth, "kf_warm_start_enqueue: null argument");
+    require(!use_net || learner != nullptr, "kf_warm_start_enqueue: the net's proposal needs a learner");
+    if (use_net) learner->impl.check_batch(8, "kf_warm_start_enqueue: the learner's capacity is below 8");
+    warm->impl.enqueue(pipeline->impl, use_net ? &learner->impl : nullptr, tracker->impl.state.ptr, depth, width,
+                       height, memory, intrinsics, use_net != 0);
+  });
+}
+
+kf_status kf_warm_start_fetch(kf_warm_start* warm, kf_pipeline* pipeline, kf_warm_start_result* result) {
+  return guarded([&] {
+    require(warm && pipeline && result, "kf_warm_start_fetch: null argument");
+    WarmStart& w = warm->impl;
+    const cudaStream_t s = pipeline->impl.stream;
+    check(cudaMemcpyAsync(w.staging.ptr, w.dev.ptr, sizeof(WarmDevice), cudaMemcpyDeviceToHost, s), "warm fetch");
+    check(cudaStreamSynchronize(s), "warm fetch");
+    const WarmDevice& d = *w.staging.ptr;
+    auto rigid = [](const Pose34& p) {
+      kf_rigid r;
+      for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) r.r[i * 3 + j] = p.m[i * 4 + j];
+        r.t[i] = p.m[i * 4 + 3];
+      }
+      return r;
+    };
+    result->proposal = rigid(d.poses[1]);
+    result->start = rigid(d.poses[d.used_proposal]);
+    for (int i = 0; i < 6; ++i) result->twist[i] = d.twist[i];
+    result->cost_predicted = d.costs[0];
+    result->matches_predicted = d.costs[1];
+    result->cost_proposal = d.costs[2];
+    result->matches_proposal = d.costs[3];
+    result->used_proposal = d.used_proposal;
   });
 }
 

@@ -85,7 +85,8 @@ def twist_between(a, b) -> np.ndarray:
 
 def constant_velocity(trajectory) -> np.ndarray:
     """T[-1] * (T[-2]^-1 T[-1]): the last motion repeated (the last pose when
-    fewer than two are known)."""
+    fewer than two are known), in double with the inverse of the float pose
+    as stored (kf_warm_start_enqueue computes the same on the device)."""
     last = np.asarray(trajectory[-1], dtype=np.float64)
     if len(trajectory) < 2:
         return last
@@ -214,17 +215,75 @@ class WarmStartedReconstruction(Reconstruction):
         self.proposals = []  # per frame: WarmStartResult or None
         self.starts = []
 
+    def prediction(self) -> np.ndarray:
+        """The constant-velocity pose for the next frame; the last pose when
+        the last frame lost track (its motion says nothing then)."""
+        if self.results and not self.results[-1].tracked:
+            return np.asarray(self.trajectory[-1], dtype=np.float64)
+        return constant_velocity(self.trajectory)
+
     def process(self, depth, color=None) -> abi.FrameResult:
         proposal = None
         if self.frames >= 1 and self.start != "previous":
-            start = constant_velocity(self.trajectory)
-            if self.start == "learned" and self.frames >= 2:
+            start = self.prediction()
+            if self.start == "learned" and self.frames >= 2 and self.results[-1].tracked:
                 proposal = self.warm.propose(self.learner, self.pipeline, depth, self.intrinsics, start)
                 start = abi.matrix_from_rigid(proposal.start).astype(np.float64)
             self.pose = abi.rigid_from_matrix(start)
         self.starts.append(abi.matrix_from_rigid(self.pose))
         self.proposals.append(proposal)
         return super().process(depth, color)
+
+
+class AsyncLearnedLoop:
+    """The learned loop with no host round trip per frame: each tracked frame
+    is kf_warm_start_enqueue (prediction, net, fallback test, start pose into
+    the tracker, all on the device) then kf_frame_enqueue.  Frame 1 starts
+    at frame 0's pose (no velocity yet, no net); later frames use the net
+    (with use_net=False: the constant-velocity start alone, on the device).
+    Depth frames may be host arrays or device addresses (ints).  Frames that
+    reach the device in HBM need no synchronisation until a result is read.""" 
+
+    def __init__(self, pipeline: Pipeline, intrinsics: abi.Intrinsics, learner: Learner | None,
+                 warm: WarmStart | None = None, iterations=(10, 5, 4, 4), use_net: bool = True):
+        from .pipeline import ProjectiveIcpTracker, PyramidSource
+        self.pipeline = pipeline
+        self.intrinsics = intrinsics
+        self.learner = learner
+        self.warm = warm if warm is not None else WarmStart()
+        self.pyramid = PyramidSource()
+        self.tracker = ProjectiveIcpTracker()
+        self.iterations = (C.c_uint32 * 4)(*iterations)
+        self.use_net = use_net and learner is not None
+        self.frames = 0
+        _check(lib().kf_warm_start_reset(self.warm.handle))
+
+    def enqueue(self, depth) -> None:
+        if isinstance(depth, int):
+            ptr, memory = C.c_void_p(depth), abi.KF_MEMORY_DEVICE
+            self._keep = None
+        else:
+            self._keep = np.ascontiguousarray(depth, dtype=np.uint16)
+            ptr, memory = self._keep.ctypes.data_as(C.c_void_p), abi.KF_MEMORY_HOST
+        if self.frames >= 1:
+            use_net = 1 if (self.use_net and self.frames >= 2) else 0
+            _check(lib().kf_warm_start_enqueue(self.warm.handle, self.learner.handle if use_net else None,
+                                               self.pipeline.handle, self.tracker.handle, ptr, 640, 480,
+                                               self.intrinsics, memory, use_net))
+        _check(lib().kf_frame_enqueue(self.pipeline.handle, self.pyramid.handle, self.tracker.handle, ptr, None,
+                                      640, 480, self.intrinsics, memory, self.iterations,
+                                      1 if self.frames == 0 else 0))
+        self.frames += 1
+
+    def result(self) -> abi.FrameResult:
+        r = abi.FrameResult()
+        _check(lib().kf_frame_result_fetch(self.pipeline.handle, C.byref(r)))
+        return r
+
+    def proposal(self) -> abi.WarmStartResult:
+        r = abi.WarmStartResult()
+        _check(lib().kf_warm_start_fetch(self.warm.handle, self.pipeline.handle, C.byref(r)))
+        return r
 
 
 def volume_config(resolution: int = 512, voxel: float = 0.01):
@@ -407,6 +466,8 @@ def evaluate(learner: Learner, seeds, frames: int, *, max_step_m: float = 0.05, 
         start_err_cv, start_err_learned, used = [], [], 0
         for f in range(2, frames):
             prop = learned_loop.proposals[f]
+            if prop is None:  # the learned loop had lost track: no proposal
+                continue
             cv = constant_velocity(list(runs["learned"][0][:f]))
             start_err_cv.append(np.linalg.norm(twist_between(cv, plain_traj[f])[:3]))
             learned_start = apply_twist(cv, np.array(prop.twist, dtype=np.float64))
@@ -420,13 +481,48 @@ def evaluate(learner: Learner, seeds, frames: int, *, max_step_m: float = 0.05, 
             "ate_learned_m": synthetic.ate_rmse(runs["learned"][0], seq.poses)["rmse"],
             "learned_vs_plain_rms_m": float(np.sqrt(np.mean(np.sum(
                 (runs["learned"][0][:, :3, 3] - plain_traj[:, :3, 3]) ** 2, axis=1)))),
-            "proposal_used": used / max(1, frames - 2),
+            "proposal_used": used / max(1, sum(p is not None for p in learned_loop.proposals[2:])),
             "start_error_velocity_m": float(np.mean(start_err_cv)),
             "start_error_proposal_m": float(np.mean(start_err_learned)),
         })
     summary = {key: float(np.mean([r[key] for r in rows])) for key in rows[0] if key != "seed"}
     summary["iteration_reduction"] = 1.0 - summary["iters_learned"] / max(1e-9, summary["iters_velocity"])
     return {"per_seed": rows, "mean": summary}
+
+
+def one_step_errors(learner: Learner, seeds, frames: int, *, max_step_m: float = 0.05, max_step_deg: float = 3.0,
+                    resolution: int = 512, voxel: float = 0.01, pipeline: Pipeline | None = None) -> dict:
+    """The net's gain on one trajectory, free of the loops' divergence: the
+    plain constant-velocity loop runs each sequence, and before each frame
+    from the third on the net proposes a start from that loop's own state;
+    both starts are compared with the pose plain ICP then reaches (mean and
+    median translation error, metres), over the frames plain ICP tracks."""
+    k = intrinsics640()
+    gpu = Pipeline(volume_config(resolution, voxel)) if pipeline is None else pipeline
+    warm = WarmStart()
+    cv_err, net_err, used = [], [], 0
+    for seed in seeds:
+        seq = synthetic.make_sequence_device(seed, frames, max_step_m, max_step_deg)
+        gpu.reset()
+        loop = WarmStartedReconstruction(gpu, k, start="velocity")
+        for f in range(frames):
+            prop = None
+            if f >= 2 and loop.results[-1].tracked:
+                cv = loop.prediction()
+                prop = warm.propose(learner, gpu, seq.depth[f], k, cv)
+            r = loop.process(seq.depth[f])
+            if prop is None or not r.tracked:
+                continue
+            tracked = np.asarray(loop.trajectory[-1], dtype=np.float64)
+            cv_err.append(np.linalg.norm(twist_between(cv, tracked)[:3]))
+            start = abi.matrix_from_rigid(prop.start).astype(np.float64)
+            net_err.append(np.linalg.norm(twist_between(start, tracked)[:3]))
+            used += int(prop.used_proposal)
+    n = max(1, len(cv_err))
+    return {"frames": len(cv_err), "start_error_velocity_m": float(np.mean(cv_err)),
+            "start_error_learned_m": float(np.mean(net_err)),
+            "median_start_error_velocity_m": float(np.median(cv_err)),
+            "median_start_error_learned_m": float(np.median(net_err)), "proposal_used": used / n}
 
 
 def start_bound(seeds, frames: int, noise_m=(0.0,), *, max_step_m: float = 0.05, max_step_deg: float = 3.0,
