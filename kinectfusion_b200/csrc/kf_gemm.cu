@@ -5,19 +5,19 @@
 //   C[M x N] (fp32) = A[M x K] (bf16, row-major) * B[N x K]^T (bf16, row-major)
 //                     (+ bias[N]) (ReLU)
 //
-// One CTA of 128 threads computes a 128 x BN tile of C.  Per 64-wide K slab
-// (two shared-memory stages, so that copying the next slab overlaps the
-// tensor core's work on the current one):
-// the threads copy the A and B slabs into shared memory in the canonical
-// K-major layout without swizzle (8-row x 16-byte core matrices; the two
-// 8-element halves of a 16-element K step LBO = 128 B apart, consecutive
-// 8-row groups SBO = 256 B apart), then one thread issues four
-// tcgen05.mma.kind::f16 (M = 128, N = BN, K = 16) that accumulate in FP32 in
-// tensor memory, and tcgen05.commit signals an mbarrier when they are done.
-// The epilogue reads the accumulator with tcgen05.ld (each warp its 32 TMEM
-// lanes = 32 rows of the tile).  Every wait is bounded: past the limit the
-// kernel records an error, waits (bounded) for its own MMAs, frees its tensor
-// memory and returns.
+// One CTA of 128 threads computes a 128 x BN tile of C.  The A and B tiles
+// move by TMA (cp.async.bulk.tensor, 128-byte swizzle: one 64-element K slab
+// of a row is one 128-byte line) into a ring of kStages shared-memory stages;
+// one thread issues the copies and the tcgen05.mma.kind::f16 (M = 128, N = BN,
+// K = 16, FP32 accumulator in tensor memory): a stage's "full" mbarrier
+// completes when its bytes have landed, its "empty" mbarrier when the MMAs
+// reading it are done (tcgen05.commit), and the copy of slab j + kStages - 1
+// waits only for the MMAs of slab j - 1, so the copies run kStages - 1 slabs
+// ahead of the tensor core.  The epilogue reads the accumulator with
+// tcgen05.ld (each warp its 32 TMEM lanes = 32 rows of the tile).  Every wait
+// is bounded: past the limit the kernel records an error, waits (bounded) for
+// its own MMAs, frees its tensor memory and returns.
+#include <cuda.h>  // CUtensorMap and its enums (the encoder comes through the runtime)
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -36,14 +36,20 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// Shared-memory matrix descriptor: K-major, no swizzle (layout type 0),
-// version 1 (sm_100), start address / LBO / SBO in 16-byte units.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+constexpr int kStages = 4;
+
+// Shared-memory matrix descriptor of a K-major operand in the 128-byte
+// swizzle layout TMA writes: rows of 128 bytes (one 64-element K slab),
+// 8-row groups 1024 bytes apart (SBO), version 1 (sm_100) at bit 46, layout
+// type SWIZZLE_128B (2) at bits 61-63.  The K step of 16 elements (32 bytes)
+// inside the swizzle atom moves the start address.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
   uint64_t d = 0;
   d |= static_cast<uint64_t>((addr >> 4) & 0x3FFFu);
-  d |= static_cast<uint64_t>((lbo_bytes >> 4) & 0x3FFFu) << 16;
-  d |= static_cast<uint64_t>((sbo_bytes >> 4) & 0x3FFFu) << 32;
-  d |= 1ull << 46;  // version
+  d |= static_cast<uint64_t>(1u) << 16;              // leading byte offset: unused by swizzled K-major
+  d |= static_cast<uint64_t>((1024u >> 4) & 0x3FFFu) << 32;
+  d |= 1ull << 46;
+  d |= 2ull << 61;
   return d;
 }
 
@@ -69,43 +75,42 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
   }
 }
 
-// Byte offset of element (row, k) of a ROWS x 64 slab in the canonical layout.
-__device__ __forceinline__ uint32_t slab_offset(uint32_t row, uint32_t k, uint32_t rows) {
-  return (k >> 4) * (rows / 8u) * 256u + (row >> 3) * 256u + ((k >> 3) & 1u) * 128u + (row & 7u) * 16u;
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(mbar)
+      : "memory");
 }
 
 template <int BN>
 constexpr size_t gemm_smem_bytes() {
-  return 2u * (static_cast<size_t>(kGemmBM) + BN) * kGemmBK * 2u + 1024u;  // two stages + alignment slack
+  return static_cast<size_t>(kStages) * (kGemmBM + BN) * kGemmBK * 2u + 1024u;  // stages + alignment slack
 }
 
 // One CTA computes a 128 x BN tile of C over the K slabs [blockIdx.z * slabs,
-// (blockIdx.z + 1) * slabs).  Two shared-memory stages: the threads fill the
-// next stage while the tensor core works on the current one; each stage's
-// tcgen05.commit arrives on that stage's mbarrier, which the threads wait on
-// before refilling the stage.  With gridDim.z == 1 the epilogue adds the bias
+// (blockIdx.z + 1) * slabs).  With gridDim.z == 1 the epilogue adds the bias
 // and applies the ReLU into C; otherwise it stores the raw partial tile into
 // C + blockIdx.z * M * ldc (split K, summed by gemm_splitk_reduce_kernel).
+// TMA coordinates: x = the K element (a multiple of 64, so 128-byte aligned),
+// y = the row; rows and K past the matrix read as zeros.
 template <int BN>
 __global__ void __launch_bounds__(kGemmThreads)
-    gemm_bf16_kernel(const __nv_bfloat16* __restrict__ A, const __nv_bfloat16* __restrict__ B, float* __restrict__ C,
-                     int M, int N, int K, int lda, int ldb, int ldc, const float* __restrict__ bias, int relu,
+    gemm_bf16_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+                     float* __restrict__ C, int M, int N, int K, int ldc, const float* __restrict__ bias, int relu,
                      int slabs, int* __restrict__ error) {
   constexpr uint32_t kCols = BN < 32 ? 32 : BN;  // tensor-memory columns (a power of two >= 32)
   constexpr uint32_t kStageA = kGemmBM * kGemmBK * 2, kStageB = BN * kGemmBK * 2;
+  constexpr uint32_t kStageBytes = kStageA + kStageB;  // a multiple of 1024 for every BN
   extern __shared__ uint8_t s_dyn[];
-  // 1024-byte aligned stage buffers
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(s_dyn) + 1023u) & ~uintptr_t(1023u));
-  uint8_t* s_a[2] = {base, base + kStageA};
-  uint8_t* s_b[2] = {base + 2 * kStageA, base + 2 * kStageA + kStageB};
-  __shared__ __align__(8) unsigned long long s_mbar[2];
+  __shared__ __align__(8) unsigned long long s_full[kStages], s_empty[kStages], s_done;
   __shared__ uint32_t s_tmem;
+  __shared__ int s_fail;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int tile_m = blockIdx.x * kGemmBM, tile_n = blockIdx.y * BN;
   const int total_slabs = (K + kGemmBK - 1) / kGemmBK;
   const int slab0 = blockIdx.z * slabs;
   const int nslabs = min(slabs, total_slabs - slab0);
-  const uint32_t mbar[2] = {smem_u32(&s_mbar[0]), smem_u32(&s_mbar[1])};
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
@@ -113,71 +118,73 @@ __global__ void __launch_bounds__(kGemmThreads)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar[0]), "r"(1));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar[1]), "r"(1));
+    for (int st = 0; st < kStages; ++st) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_full[st])), "r"(1));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_empty[st])), "r"(1));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_done)), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_a)) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_b)) : "memory");
+    s_fail = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = s_tmem;
   const uint32_t idesc = instr_desc(kGemmBM, BN);
-  bool ok = true;
-  int issued = 0;  // slabs whose MMAs were issued
 
-  for (int i = 0; i < nslabs && ok; ++i) {
-    const int st = i & 1;
-    // the stage's previous MMAs (slab i - 2) must be done before it is refilled
-    if (i >= 2) ok = __syncthreads_and(mbar_wait(mbar[st], static_cast<uint32_t>(((i - 2) >> 1) & 1)));
-    if (!ok) break;
-    const int k0 = (slab0 + i) * kGemmBK;
-    {
-      const int row = tile_m + tid;
-#pragma unroll
-      for (int c = 0; c < kGemmBK / 8; ++c) {
-        const int k = k0 + c * 8;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if (row < M && k < K) v = *reinterpret_cast<const uint4*>(A + static_cast<size_t>(row) * lda + k);
-        *reinterpret_cast<uint4*>(s_a[st] + slab_offset(tid, c * 8, kGemmBM)) = v;
-      }
-    }
-    for (int r = tid; r < BN; r += kGemmThreads) {
-      const int row = tile_n + r;
-#pragma unroll
-      for (int c = 0; c < kGemmBK / 8; ++c) {
-        const int k = k0 + c * 8;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if (row < N && k < K) v = *reinterpret_cast<const uint4*>(B + static_cast<size_t>(row) * ldb + k);
-        *reinterpret_cast<uint4*>(s_b[st] + slab_offset(r, c * 8, BN)) = v;
-      }
-    }
-    // generic-proxy stores -> visible to the tensor core's async proxy
-    asm volatile("fence.proxy.async.shared::cta;");
-    __syncthreads();
-    if (tid == 0) {
+  if (tid == 0 && nslabs > 0) {
+    bool ok = true;
+    auto produce = [&](int i) {
+      const int st = i % kStages;
+      const uint32_t full = smem_u32(&s_full[st]);
+      const uint32_t dst = smem_u32(base + st * kStageBytes);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full), "r"(kStageBytes)
+                   : "memory");
+      const int k0 = (slab0 + i) * kGemmBK;
+      tma_load_2d(dst, &map_a, k0, tile_m, full);
+      tma_load_2d(dst + kStageA, &map_b, k0, tile_n, full);
+    };
+    for (int i = 0; i < min(kStages, nslabs); ++i) produce(i);
+    for (int j = 0; j < nslabs && ok; ++j) {
+      const int st = j % kStages;
+      ok = mbar_wait(smem_u32(&s_full[st]), static_cast<uint32_t>((j / kStages) & 1));
+      if (!ok) break;
       asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t a0 = smem_u32(base + st * kStageBytes), b0 = a0 + kStageA;
 #pragma unroll
-      for (int s = 0; s < kGemmBK / 16; ++s) {
-        const uint64_t da = smem_desc(smem_u32(s_a[st]) + s * (kGemmBM / 8) * 256, 128, 256);
-        const uint64_t db = smem_desc(smem_u32(s_b[st]) + s * (BN / 8) * 256, 128, 256);
-        const uint32_t accumulate = (i > 0 || s > 0) ? 1u : 0u;
+      for (int kk = 0; kk < kGemmBK / 16; ++kk) {
+        const uint64_t da = smem_desc_sw128(a0 + kk * 32);
+        const uint64_t db = smem_desc_sw128(b0 + kk * 32);
+        const uint32_t accumulate = (j > 0 || kk > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "setp.ne.b32 p, %4, 0;\n\t"
             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
             ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar[st])
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   ::"r"(smem_u32(&s_empty[st]))
                    : "memory");
+      // refill the stage the previous slab's MMAs read (done by now or soon:
+      // the tensor core runs this slab's MMAs behind them)
+      if (j >= 1 && j - 1 + kStages < nslabs) {
+        const int ps = (j - 1) % kStages;
+        ok = mbar_wait(smem_u32(&s_empty[ps]), static_cast<uint32_t>(((j - 1) / kStages) & 1));
+        if (!ok) break;
+        produce(j - 1 + kStages);
+      }
     }
-    issued = i + 1;
+    // arrives once every MMA issued before it is complete
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(smem_u32(&s_done))
+                 : "memory");
+    if (!ok) s_fail = 1;
   }
-  // the last commit arrives once every MMA issued before it is complete
-  if (issued > 0) {
-    const int last = issued - 1;
-    const bool done = __syncthreads_and(mbar_wait(mbar[last & 1], static_cast<uint32_t>((last >> 1) & 1)));
-    ok = ok && done;
-  }
+  __syncthreads();
+  bool ok = s_fail == 0;
+  if (nslabs > 0) ok = __syncthreads_and(mbar_wait(smem_u32(&s_done), 0u)) && ok;
   if (!ok) {
     if (tid == 0) atomicExch(error, 1);
   } else {
@@ -200,7 +207,7 @@ __global__ void __launch_bounds__(kGemmThreads)
         for (int j = 0; j < 16; ++j) {
           const int col = tile_n + c + j;
           if (col >= N) continue;
-          float v = issued > 0 ? __uint_as_float(r[j]) : 0.0f;
+          float v = nslabs > 0 ? __uint_as_float(r[j]) : 0.0f;
           if (!split) {
             if (bias != nullptr) v += bias[col];
             if (relu && v < 0.0f) v = 0.0f;
@@ -228,6 +235,36 @@ __global__ void gemm_splitk_reduce_kernel(const float* __restrict__ partial, int
   C[static_cast<size_t>(row) * ldc + col] = v;
 }
 
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encoder() {
+  static EncodeTiled fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    check(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q), "tensor map encoder");
+    require(q == cudaDriverEntryPointSuccess && p != nullptr, "gemm: the driver has no cuTensorMapEncodeTiled");
+    return reinterpret_cast<EncodeTiled>(p);
+  }();
+  return fn;
+}
+
+// A rows x K bf16 row-major matrix (leading dimension ld) read in boxes of
+// 64 K elements x box_rows rows, 128-byte swizzle, zeros outside.
+CUtensorMap tensor_map(const void* base, int rows, int K, int ld, int box_rows) {
+  CUtensorMap map;
+  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(K), static_cast<cuuint64_t>(rows)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * 2u};
+  const cuuint32_t box[2] = {static_cast<cuuint32_t>(kGemmBK), static_cast<cuuint32_t>(box_rows)};
+  const cuuint32_t elem[2] = {1u, 1u};
+  const CUresult r = encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box,
+                               elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  require(r == CUDA_SUCCESS, "gemm: tensor map encoding failed");
+  return map;
+}
+
 template <int BN>
 void launch_tiles(const __nv_bfloat16* a, const __nv_bfloat16* b, float* c, int M, int N, int K, int lda, int ldb,
                   int ldc, const float* bias, int relu, int slabs, unsigned splits, int* error, cudaStream_t s) {
@@ -238,10 +275,12 @@ void launch_tiles(const __nv_bfloat16* a, const __nv_bfloat16* b, float* c, int 
           "gemm attribute");
     configured = true;
   }
+  const CUtensorMap ma = tensor_map(a, M, K, lda, kGemmBM);
+  const CUtensorMap mb = tensor_map(b, N, K, ldb, BN);
   const unsigned gm = ceil_div(static_cast<unsigned>(M), static_cast<unsigned>(kGemmBM));
   const unsigned gn = ceil_div(static_cast<unsigned>(N), static_cast<unsigned>(BN));
   gemm_bf16_kernel<BN><<<dim3(gm, gn, splits), kGemmThreads, gemm_smem_bytes<BN>(), s>>>(
-      a, b, c, M, N, K, lda, ldb, ldc, bias, relu, slabs, error);
+      ma, mb, c, M, N, K, ldc, bias, relu, slabs, error);
 }
 
 }  // namespace
