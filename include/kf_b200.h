@@ -316,8 +316,9 @@ kf_status kf_pipeline_update_counts(kf_pipeline* pipeline, uint64_t* voxel_updat
  * relu != 0), a and b bf16 row-major on the device, k a multiple of 8, all
  * three 16-byte aligned; stream is a cudaStream_t (NULL: the default
  * stream).  Runs on tcgen05 (sm_100a); a product of few 128-row output tiles
- * and long k is split along k over more CTAs (partials in a temporary
- * device workspace this call allocates, summed in a fixed order). */
+ * and long k is split along k over more CTAs (partials in a device workspace
+ * the library allocates on first need and keeps, summed in a fixed order).
+ * Waits for the product; concurrent calls from several threads take turns. */
 kf_status kf_gemm_bf16(const void* a, const void* b, float* c, int32_t m, int32_t n, int32_t k,
                        const float* bias, int32_t relu, void* stream);
 

@@ -21,6 +21,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "kf_internal.h"
 
@@ -326,18 +327,45 @@ void launch_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int 
 
 }  // namespace kf
 
+namespace {
+// Per-process scratch of kf_gemm_bf16, allocated on the first call that
+// needs it and kept: the error flag and the split-K partials.  Calls are
+// serialised by the lock (each call waits for its GEMM anyway).
+struct GemmScratch {
+  std::mutex lock;
+  int device = -1;
+  kf::DeviceArray<int> error;
+  kf::DeviceArray<float> workspace;
+};
+GemmScratch& gemm_scratch() {
+  static GemmScratch* s = new GemmScratch();  // never destroyed: lives past static teardown
+  return *s;
+}
+}  // namespace
+
 extern "C" kf_status kf_gemm_bf16(const void* a, const void* b, float* c, int32_t m, int32_t n, int32_t k,
                                   const float* bias, int32_t relu, void* stream) {
   return kf::guarded([&] {
     kf::require(a != nullptr && b != nullptr && c != nullptr, "kf_gemm_bf16: null argument");
-    kf::DeviceArray<int> error(1);
-    const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    kf::check(cudaMemsetAsync(error.ptr, 0, sizeof(int), s), "gemm error flag");
+    GemmScratch& g = gemm_scratch();
+    std::lock_guard<std::mutex> hold(g.lock);
+    int device = 0;
+    kf::check(cudaGetDevice(&device), "gemm device");
+    if (g.device != device) {  // another device: start over (the arrays belong to the old one)
+      g.error = kf::DeviceArray<int>();
+      g.workspace = kf::DeviceArray<float>();
+      g.device = device;
+    }
+    if (g.error.count == 0) g.error.resize(1);
     // split-K partials for GEMMs of few output tiles (at most 16 MB)
-    kf::DeviceArray<float> workspace(std::min<size_t>(static_cast<size_t>(m) * n * 64, size_t{1} << 22));
-    kf::launch_gemm_bf16(a, b, c, m, n, k, k, k, n, bias, relu, error.ptr, s, workspace.ptr, workspace.count);
+    const size_t want = std::min<size_t>(static_cast<size_t>(m) * n * 64, size_t{1} << 22);
+    const unsigned tiles = kf::ceil_div(static_cast<unsigned>(m), 128u) * kf::ceil_div(static_cast<unsigned>(n), 16u);
+    if (tiles < 148u * 8u && g.workspace.count < want) g.workspace.resize(want);
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    kf::check(cudaMemsetAsync(g.error.ptr, 0, sizeof(int), s), "gemm error flag");
+    kf::launch_gemm_bf16(a, b, c, m, n, k, k, k, n, bias, relu, g.error.ptr, s, g.workspace.ptr, g.workspace.count);
     int flag = 0;
-    kf::check(cudaMemcpyAsync(&flag, error.ptr, sizeof(int), cudaMemcpyDeviceToHost, s), "gemm error flag");
+    kf::check(cudaMemcpyAsync(&flag, g.error.ptr, sizeof(int), cudaMemcpyDeviceToHost, s), "gemm error flag");
     kf::check(cudaStreamSynchronize(s), "gemm");
     if (flag) throw kf::CudaError("kf_gemm_bf16: tensor-core wait timed out");
   });
