@@ -7,13 +7,12 @@
 //
 // One CTA of 128 threads computes a 128 x BN tile of C.  The A and B tiles
 // move by TMA (cp.async.bulk.tensor, 128-byte swizzle: one 64-element K slab
-// of a row is one 128-byte line) into a ring of kStages shared-memory stages;
-// one thread issues the copies and the tcgen05.mma.kind::f16 (M = 128, N = BN,
-// K = 16, FP32 accumulator in tensor memory): a stage's "full" mbarrier
-// completes when its bytes have landed, its "empty" mbarrier when the MMAs
-// reading it are done (tcgen05.commit), and the copy of slab j + kStages - 1
-// waits only for the MMAs of slab j - 1, so the copies run kStages - 1 slabs
-// ahead of the tensor core.  The epilogue reads the accumulator with
+// of a row is one 128-byte line) into a ring of kStages shared-memory stages.
+// Warp 1 issues the copies, warp 0 the tcgen05.mma.kind::f16 (M = 128,
+// N = BN, K = 16, FP32 accumulator in tensor memory): a stage's "full"
+// mbarrier completes when its bytes have landed, its "empty" mbarrier when
+// the MMAs reading it are done (tcgen05.commit), so the copies run up to
+// kStages slabs ahead of the tensor core.  The epilogue reads the accumulator with
 // tcgen05.ld (each warp its 32 TMEM lanes = 32 rows of the tile).  Every wait
 // is bounded: past the limit the kernel records an error, waits (bounded) for
 // its own MMAs, frees its tensor memory and returns.
@@ -37,7 +36,8 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-constexpr int kStages = 4;
+constexpr int kStages = 3;  // 97 KB of stages: two CTAs per SM
+constexpr int kGroupM = 16;  // row tiles per group of the CTA order
 
 // Shared-memory matrix descriptor of a K-major operand in the 128-byte
 // swizzle layout TMA writes: rows of 128 bytes (one 64-element K slab),
@@ -98,7 +98,7 @@ template <int BN>
 __global__ void __launch_bounds__(kGemmThreads)
     gemm_bf16_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
                      float* __restrict__ C, int M, int N, int K, int ldc, const float* __restrict__ bias, int relu,
-                     int slabs, int* __restrict__ error) {
+                     int slabs, int gm, int gn, int* __restrict__ error) {
   constexpr uint32_t kCols = BN < 32 ? 32 : BN;  // tensor-memory columns (a power of two >= 32)
   constexpr uint32_t kStageA = kGemmBM * kGemmBK * 2, kStageB = BN * kGemmBK * 2;
   constexpr uint32_t kStageBytes = kStageA + kStageB;  // a multiple of 1024 for every BN
@@ -108,7 +108,15 @@ __global__ void __launch_bounds__(kGemmThreads)
   __shared__ uint32_t s_tmem;
   __shared__ int s_fail;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int tile_m = blockIdx.x * kGemmBM, tile_n = blockIdx.y * BN;
+  // Grouped tile order: consecutive CTAs walk kGroupM row tiles down one
+  // column tile before moving right, so a wave of CTAs shares its A rows and
+  // B columns in L2 instead of streaming all of A once per column of tiles.
+  const int id = static_cast<int>(blockIdx.x);
+  const int per_group = kGroupM * gn;
+  const int first_m = (id / per_group) * kGroupM;
+  const int group_rows = min(gm - first_m, kGroupM);
+  const int tile_m = (first_m + (id % per_group) % group_rows) * kGemmBM;
+  const int tile_n = ((id % per_group) / group_rows) * BN;
   const int total_slabs = (K + kGemmBK - 1) / kGemmBK;
   const int slab0 = blockIdx.z * slabs;
   const int nslabs = min(slabs, total_slabs - slab0);
@@ -135,10 +143,15 @@ __global__ void __launch_bounds__(kGemmThreads)
   const uint32_t tmem = s_tmem;
   const uint32_t idesc = instr_desc(kGemmBM, BN);
 
-  if (tid == 0 && nslabs > 0) {
-    bool ok = true;
-    auto produce = [&](int i) {
+  if (nslabs > 0 && tid == 32) {
+    // producer (warp 1): refill a stage once the MMAs that read it are done
+    for (int i = 0; i < nslabs; ++i) {
       const int st = i % kStages;
+      if (i >= kStages &&
+          !mbar_wait(smem_u32(&s_empty[st]), static_cast<uint32_t>(((i - kStages) / kStages) & 1))) {
+        s_fail = 1;
+        break;
+      }
       const uint32_t full = smem_u32(&s_full[st]);
       const uint32_t dst = smem_u32(base + st * kStageBytes);
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full), "r"(kStageBytes)
@@ -146,12 +159,15 @@ __global__ void __launch_bounds__(kGemmThreads)
       const int k0 = (slab0 + i) * kGemmBK;
       tma_load_2d(dst, &map_a, k0, tile_m, full);
       tma_load_2d(dst + kStageA, &map_b, k0, tile_n, full);
-    };
-    for (int i = 0; i < min(kStages, nslabs); ++i) produce(i);
-    for (int j = 0; j < nslabs && ok; ++j) {
+    }
+  } else if (nslabs > 0 && tid == 0) {
+    // MMA issuer (warp 0): one slab's four MMAs per full stage
+    for (int j = 0; j < nslabs; ++j) {
       const int st = j % kStages;
-      ok = mbar_wait(smem_u32(&s_full[st]), static_cast<uint32_t>((j / kStages) & 1));
-      if (!ok) break;
+      if (!mbar_wait(smem_u32(&s_full[st]), static_cast<uint32_t>((j / kStages) & 1))) {
+        s_fail = 1;
+        break;
+      }
       asm volatile("tcgen05.fence::after_thread_sync;");
       const uint32_t a0 = smem_u32(base + st * kStageBytes), b0 = a0 + kStageA;
 #pragma unroll
@@ -168,20 +184,11 @@ __global__ void __launch_bounds__(kGemmThreads)
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                    ::"r"(smem_u32(&s_empty[st]))
                    : "memory");
-      // refill the stage the previous slab's MMAs read (done by now or soon:
-      // the tensor core runs this slab's MMAs behind them)
-      if (j >= 1 && j - 1 + kStages < nslabs) {
-        const int ps = (j - 1) % kStages;
-        ok = mbar_wait(smem_u32(&s_empty[ps]), static_cast<uint32_t>(((j - 1) / kStages) & 1));
-        if (!ok) break;
-        produce(j - 1 + kStages);
-      }
     }
     // arrives once every MMA issued before it is complete
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                  ::"r"(smem_u32(&s_done))
                  : "memory");
-    if (!ok) s_fail = 1;
   }
   __syncthreads();
   bool ok = s_fail == 0;
@@ -280,8 +287,8 @@ void launch_tiles(const __nv_bfloat16* a, const __nv_bfloat16* b, float* c, int 
   const CUtensorMap mb = tensor_map(b, N, K, ldb, BN);
   const unsigned gm = ceil_div(static_cast<unsigned>(M), static_cast<unsigned>(kGemmBM));
   const unsigned gn = ceil_div(static_cast<unsigned>(N), static_cast<unsigned>(BN));
-  gemm_bf16_kernel<BN><<<dim3(gm, gn, splits), kGemmThreads, gemm_smem_bytes<BN>(), s>>>(
-      ma, mb, c, M, N, K, ldc, bias, relu, slabs, error);
+  gemm_bf16_kernel<BN><<<dim3(gm * gn, 1, splits), kGemmThreads, gemm_smem_bytes<BN>(), s>>>(
+      ma, mb, c, M, N, K, ldc, bias, relu, slabs, static_cast<int>(gm), static_cast<int>(gn), error);
 }
 
 }  // namespace
