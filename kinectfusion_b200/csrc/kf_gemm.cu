@@ -36,7 +36,11 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-constexpr int kStages = 3;  // 97 KB of stages: two CTAs per SM
+// Stages per tile width: at most about 97 KB of stages, two CTAs per SM.
+template <int BN>
+constexpr int stages_for() {
+  return BN >= 256 ? 2 : 3;
+}
 constexpr int kGroupM = 16;  // row tiles per group of the CTA order
 
 // Shared-memory matrix descriptor of a K-major operand in the 128-byte
@@ -85,7 +89,7 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
 
 template <int BN>
 constexpr size_t gemm_smem_bytes() {
-  return static_cast<size_t>(kStages) * (kGemmBM + BN) * kGemmBK * 2u + 1024u;  // stages + alignment slack
+  return static_cast<size_t>(stages_for<BN>()) * (kGemmBM + BN) * kGemmBK * 2u + 1024u;  // + alignment slack
 }
 
 // One CTA computes a 128 x BN tile of C over the K slabs [blockIdx.z * slabs,
@@ -102,9 +106,10 @@ __global__ void __launch_bounds__(kGemmThreads)
   constexpr uint32_t kCols = BN < 32 ? 32 : BN;  // tensor-memory columns (a power of two >= 32)
   constexpr uint32_t kStageA = kGemmBM * kGemmBK * 2, kStageB = BN * kGemmBK * 2;
   constexpr uint32_t kStageBytes = kStageA + kStageB;  // a multiple of 1024 for every BN
+  constexpr int kStages = stages_for<BN>();
   extern __shared__ uint8_t s_dyn[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(s_dyn) + 1023u) & ~uintptr_t(1023u));
-  __shared__ __align__(8) unsigned long long s_full[kStages], s_empty[kStages], s_done;
+  __shared__ __align__(8) unsigned long long s_full[3], s_empty[3], s_done;
   __shared__ uint32_t s_tmem;
   __shared__ int s_fail;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -302,7 +307,11 @@ void launch_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int 
           "gemm: operands must be 16-byte aligned");
   const auto* a = static_cast<const __nv_bfloat16*>(A);
   const auto* b = static_cast<const __nv_bfloat16*>(B);
-  const int bn = N <= 16 ? 16 : (N <= 32 ? 32 : (N <= 64 ? 64 : 128));
+  // 256-wide tiles halve the A traffic per flop, but only pay when there are
+  // enough of them to fill the GPU twice over; small products keep 128
+  const unsigned wide_tiles = ceil_div(static_cast<unsigned>(M), static_cast<unsigned>(kGemmBM)) *
+                              ceil_div(static_cast<unsigned>(N), 256u);
+  const int bn = N <= 16 ? 16 : (N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 || wide_tiles < 296u ? 128 : 256)));
   const unsigned tiles = ceil_div(static_cast<unsigned>(M), static_cast<unsigned>(kGemmBM)) *
                          ceil_div(static_cast<unsigned>(N), static_cast<unsigned>(bn));
   const int total_slabs = (K + kGemmBK - 1) / kGemmBK;
@@ -321,7 +330,8 @@ void launch_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int 
     case 16: launch_tiles<16>(a, b, out, M, N, K, lda, ldb, ldo, bias, relu, slabs, splits, error, s); break;
     case 32: launch_tiles<32>(a, b, out, M, N, K, lda, ldb, ldo, bias, relu, slabs, splits, error, s); break;
     case 64: launch_tiles<64>(a, b, out, M, N, K, lda, ldb, ldo, bias, relu, slabs, splits, error, s); break;
-    default: launch_tiles<128>(a, b, out, M, N, K, lda, ldb, ldo, bias, relu, slabs, splits, error, s); break;
+    case 128: launch_tiles<128>(a, b, out, M, N, K, lda, ldb, ldo, bias, relu, slabs, splits, error, s); break;
+    default: launch_tiles<256>(a, b, out, M, N, K, lda, ldb, ldo, bias, relu, slabs, splits, error, s); break;
   }
   check(cudaGetLastError(), "gemm_bf16_kernel launch");
   if (splits > 1) {

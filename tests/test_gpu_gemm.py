@@ -12,7 +12,8 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("m,n,k", [(128, 16, 64), (256, 32, 128), (300, 64, 96), (128, 200, 64), (1200, 32, 32),
-                                   (64, 256, 1280), (32, 24, 8192), (256, 288, 4800)])
+                                   (64, 256, 1280), (32, 24, 8192), (256, 288, 4800),
+                                   (38016, 300, 192)])
 @pytest.mark.parametrize("epilogue", [False, True])
 def test_gemm_matches_fp32_reference(m, n, k, epilogue):
     import torch
