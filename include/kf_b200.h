@@ -38,7 +38,8 @@ enum {
   KF_ERR_NO_DEVICE = 3,        /* create_device without a CUDA device */
   KF_ERR_OUT_OF_MEMORY = 4,
   KF_ERR_DEVICE_TIMEOUT = 5,   /* a bounded device-side wait gave up */
-  KF_ERR_UNSUPPORTED = 6       /* storage combination not offered (pipeline.cpp:104-118) */
+  KF_ERR_UNSUPPORTED = 6,      /* storage combination not offered (pipeline.cpp:104-118) */
+  KF_ERR_IO = 7                /* file read, write or decode failure (std::runtime_error in read_png.cpp) */
 };
 
 /* Memory space of a caller buffer passed through the ABI. */
@@ -504,6 +505,27 @@ kf_status kf_warm_start_enqueue(kf_warm_start* warm, kf_learner* learner, kf_pip
                                 const uint16_t* depth, uint32_t width, uint32_t height, kf_intrinsics intrinsics,
                                 int32_t memory, int32_t use_net);
 kf_status kf_warm_start_fetch(kf_warm_start* warm, kf_pipeline* pipeline, kf_warm_start_result* result);
+
+/* ---- files around the loop (host code) ---------------------------------
+ * PNG frames as a TUM RGB-D sequence stores them (read_png.cpp / write_png.cpp,
+ * VirtualSensor, virtual_sensor.cpp:41-147) and binary PLY output
+ * (FrameOutput, frame_output.cpp:76-181).  Failures return KF_ERR_IO. */
+/* Size and pixel format of a PNG file (color_type, bit_depth may be NULL). */
+kf_status kf_png_info(const char* path, uint32_t* width, uint32_t* height, int32_t* color_type, int32_t* bit_depth);
+/* read_png<DepthImage>: the file must be 16-bit grayscale; raw values copied. */
+kf_status kf_png_read_depth(const char* path, uint16_t* out, uint32_t width, uint32_t height);
+/* read_png<ColorImage>: any 8/16-bit grey, grey+alpha, RGB, RGBA or 8-bit
+ * palette image as RGBA8 packed R | G << 8 | B << 16 | A << 24. */
+kf_status kf_png_read_color(const char* path, uint32_t* out, uint32_t width, uint32_t height);
+kf_status kf_png_write_depth(const char* path, const uint16_t* depth, uint32_t width, uint32_t height);
+kf_status kf_png_write_color(const char* path, const uint32_t* rgba, uint32_t width, uint32_t height);
+/* FrameOutput::write_mesh: binary little-endian PLY, vertices (position,
+ * normal, uchar colour clamped to [0, 255]) and triangles (host mesh). */
+kf_status kf_mesh_write_ply(const char* path, const kf_mesh* mesh);
+/* FrameOutput::write_raycast_point_cloud: every pixel whose point and
+ * normal are finite (host maps, width*height*3 floats each, RGBA8 colours). */
+kf_status kf_maps_write_ply(const char* path, const float* points, const float* normals, const uint32_t* colors,
+                            uint32_t width, uint32_t height);
 
 /* Sets the device-resident camera_to_world that the next enqueued frame
  * starts from (ordered on the pipeline's stream). */

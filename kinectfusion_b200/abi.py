@@ -21,6 +21,7 @@ KF_ERR_NO_DEVICE = 3
 KF_ERR_OUT_OF_MEMORY = 4
 KF_ERR_DEVICE_TIMEOUT = 5
 KF_ERR_UNSUPPORTED = 6
+KF_ERR_IO = 7
 
 KF_MEMORY_HOST = 0
 KF_MEMORY_DEVICE = 1
@@ -210,6 +211,14 @@ _PROTOTYPES = {
     "kf_frame_enqueue": (C.c_int, [P, P, P, P, P, C.c_uint32, C.c_uint32, Intrinsics, C.c_int32, P, C.c_int32]),
     "kf_frame_result_fetch": (C.c_int, [P, C.POINTER(FrameResult)]),
     "kf_frame_set_pose": (C.c_int, [P, P, C.POINTER(Rigid)]),
+    "kf_png_info": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_int32),
+                              C.POINTER(C.c_int32)]),
+    "kf_png_read_depth": (C.c_int, [C.c_char_p, P, C.c_uint32, C.c_uint32]),
+    "kf_png_read_color": (C.c_int, [C.c_char_p, P, C.c_uint32, C.c_uint32]),
+    "kf_png_write_depth": (C.c_int, [C.c_char_p, P, C.c_uint32, C.c_uint32]),
+    "kf_png_write_color": (C.c_int, [C.c_char_p, P, C.c_uint32, C.c_uint32]),
+    "kf_mesh_write_ply": (C.c_int, [C.c_char_p, C.POINTER(Mesh)]),
+    "kf_maps_write_ply": (C.c_int, [C.c_char_p, P, P, P, C.c_uint32, C.c_uint32]),
     "kf_learner_create": (C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(P)]),
     "kf_learner_destroy": (C.c_int, [P]),
     "kf_learner_param_count": (C.c_int, [P, C.POINTER(C.c_uint64)]),

@@ -59,7 +59,7 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> pathlib.Path:
     with concurrent.futures.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as pool:
         objs = list(pool.map(lambda s: _compile(s, extra), _sources()))
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [NVCC, *ARCH, "-shared", "-ccbin", HOST_CXX, "-o", str(tmp), *map(str, objs)]
+    cmd = [NVCC, *ARCH, "-shared", "-ccbin", HOST_CXX, "-o", str(tmp), *map(str, objs), "-lz"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")

@@ -26,6 +26,11 @@ struct CudaError : std::runtime_error {
 struct Unsupported : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
+// File read, write or decode failure (std::runtime_error in the reference,
+// image_proc/read_png.cpp, src/app/frame_output.cpp).
+struct IoError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
 
 void set_last_error(const std::string& message);
 void check(cudaError_t status, const char* what);
@@ -46,6 +51,9 @@ kf_status guarded(Body&& body) {
   } catch (const CudaError& e) {
     set_last_error(e.what());
     return KF_ERR_CUDA;
+  } catch (const IoError& e) {
+    set_last_error(e.what());
+    return KF_ERR_IO;
   } catch (const std::bad_alloc&) {
     set_last_error("host allocation failed");
     return KF_ERR_OUT_OF_MEMORY;
