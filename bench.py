@@ -641,6 +641,141 @@ def run_ablations(args) -> dict:
     }
 
 
+def _live_bricks(a, b) -> int:
+    """8^3 bricks where either volume holds a voxel of weight > 0 (from the
+    dense host views): the bricks the volume comparator must read."""
+    counts = []
+    for p in (a, b):
+        _, w = p.host_view()
+        rz, ry, rx = w.shape
+        counts.append((w > 0).reshape(rz // 8, 8, ry // 8, 8, rx // 8, 8).any(axis=(1, 3, 5)))
+    return int((counts[0] | counts[1]).sum())
+
+
+def run_compare(args) -> dict:
+    """The pipeline-set ablation run with a comparison every frame
+    (--pipelines ... with compare_every_n_frames 1): three 512^3 members
+    (baseline float + colour, classic float, bf16) each track and integrate
+    the cfg2 frames, then all are raycast at 640x480 from the baseline's pose
+    and compared with it on the device.  `value` is set frames/s; the
+    roofline is the volume comparator's kernel (one read of both volumes)."""
+    import torch
+
+    import kinectfusion_b200 as kf
+    from kinectfusion_b200 import abi, synthetic
+    from kinectfusion_b200.pipeline_set import PipelineSet, compare_volumes
+
+    lib = abi.load()
+    seq = synthetic.make_sequence(seed=1000, frames=SEQ_FRAMES)
+    k = abi.Intrinsics(synthetic.FX, synthetic.FY, synthetic.CX, synthetic.CY)
+    depth_dev = torch.from_numpy(seq.depth.view(np.int16)).cuda()
+    color_dev = torch.from_numpy(seq.color.view(np.int32)).cuda()
+    iters = (C.c_uint32 * 4)(10, 5, 4, 4)
+    res = args.compare_res
+    origin = (-0.5 * res * VOXEL, -0.5 * res * VOXEL, -0.5)
+    members = [kf.Pipeline(kf.pipeline_config(res, VOXEL, origin, TRUNC), "baseline"),
+               kf.Pipeline(kf.pipeline_config(res, VOXEL, origin, TRUNC, rule=abi.KF_RULE_CLASSIC,
+                                              color=abi.KF_COLOR_NONE), "classic"),
+               kf.Pipeline(kf.pipeline_config(res, VOXEL, origin, TRUNC, voxel=abi.KF_VOXEL_BF16,
+                                              color=abi.KF_COLOR_NONE), "bf16")]
+    pset = PipelineSet(members, reference="baseline")
+    pyramids = [kf.PyramidSource() for _ in members]
+    trackers = [kf.ProjectiveIcpTracker() for _ in members]
+    sp = C.c_void_p()
+    abi.check(lib.kf_pipeline_stream(members[1].handle, C.byref(sp)))
+    classic_stream = torch.cuda.ExternalStream(sp.value)
+
+    def step(s: int, compare: bool = True):
+        idx = frame_schedule(s)
+        d = C.c_void_p(depth_dev.data_ptr() + idx * 640 * 480 * 2)
+        for i, m in enumerate(members):
+            col = C.c_void_p(color_dev.data_ptr() + idx * 640 * 480 * 4) if i == 0 else None
+            abi.check(lib.kf_frame_enqueue(m.handle, pyramids[i].handle, trackers[i].handle, d, col, 640, 480, k,
+                                           abi.KF_MEMORY_DEVICE, iters, 1 if s == 0 else 0))
+        r = abi.FrameResult()
+        for m in members:
+            abi.check(lib.kf_frame_result_fetch(m.handle, C.byref(r)))
+        if compare:
+            abi.check(lib.kf_frame_result_fetch(members[0].handle, C.byref(r)))
+            outputs = pset.raycast_all(k, 640, 480, r.camera_to_world)
+            return pset.compare(outputs)
+        return None
+
+    warm = max(args.warmup, 3)
+    for s in range(warm):
+        step(s)
+    torch.cuda.synchronize()
+    steps = min(args.steps, 100)
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        clocks.wait_started()
+        t0 = time.perf_counter()
+        for s in range(steps):
+            last = step(warm + s)
+        torch.cuda.synchronize()
+        set_s = time.perf_counter() - t0
+        # the same frames without the comparisons, for the comparison's share
+        t0 = time.perf_counter()
+        for s in range(steps):
+            step(warm + steps + s, compare=False)
+        torch.cuda.synchronize()
+        plain_s = time.perf_counter() - t0
+        # the volume comparator alone (classic vs baseline: two float volumes),
+        # CUDA events on the primary's stream around the whole call
+        times = []
+        for _ in range(20):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(classic_stream)
+            compare_volumes(members[1], members[0])
+            e1.record(classic_stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+    compare_ms = float(np.median(times))
+    # algorithmic bytes: the observed bits of both volumes (128 B per brick
+    # each) and both float bricks wherever either volume observed a voxel
+    blocks = (res // 8) ** 3
+    live = _live_bricks(members[1], members[0])
+    traffic_bytes = blocks * 2 * 128 + live * 2 * 4096
+    gbs = traffic_bytes / (compare_ms / 1e3) / 1e9
+    peaks = measured_peaks()
+    peak = peaks.get("hbm_gbs", 6650.0)
+    # CPU baseline: the oracle's Comparator on the two downloaded host views
+    # (the reference's path: host_view of both volumes, then a host loop)
+    cpu = None
+    if args.cpu_baseline:
+        sys.path.insert(0, str(pathlib.Path(__file__).resolve().parent / "oracle"))
+        import kf_compare_oracle as kco
+        t0 = time.perf_counter()
+        views = (members[1].host_view(), members[0].host_view())
+        download_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        kco.compare_volumes(*views)
+        cpu_s = time.perf_counter() - t0
+        cpu = {"value": round(1000.0 * (cpu_s + download_s), 1), "unit": "ms per volume comparison", "cores": 1,
+               "kind": "port", "sample": "one 512^3 float-vs-float comparison: host_view download of both volumes "
+                                         f"({round(1000 * download_s, 1)} ms) + numpy Comparator"}
+    return {
+        "metric": f"pipeline-set frames/s, 3 members at {res}^3, compared every frame", "value": round(steps / set_s, 1),
+        "unit": "frames/s", "n_gpus": 1, "steps": steps, "warmup": warm, "ms_per_step": round(1000 * set_s / steps, 3),
+        "higher_is_better": True, "scaling": "none", "vs_baseline": None, "dtype": "f32 / bf16 voxels, f64 sums",
+        "data": "synthetic (seeded analytic RGB-D scene)",
+        "config": {"workload": "members baseline (float + colour), classic (float), bf16; 640x480 cfg2 frames from "
+                               "HBM; per frame: every member tracks and integrates, all raycast at 640x480 from the "
+                               "baseline's pose, kf_compare_volumes + kf_compare_surface_maps per member; inputs "
+                               "larger than L2"},
+        "frames_per_s_without_comparison": round(steps / plain_s, 1),
+        "compare_volumes_ms": round(compare_ms, 4),
+        "compare_live_bricks": {"live": int(live), "of": int(blocks), "algorithmic_bytes": int(traffic_bytes),
+                                "full_read_bytes": int(res ** 3 * 16)},
+        "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(gbs / peak, 4), "traffic": None,
+                     "peak_source": "measured" if not peaks.get("fallback") else "fallback",
+                     "kernel": "compare_volumes_kernel<float, float> (+ finish kernel and result copy)"},
+        "last_comparisons": [c.csv() for c in last],
+        "cpu_baseline": cpu,
+        "clocks": clocks.summary(),
+    }
+
+
 def run_gemm(args) -> dict:
     """The tensor-core kernel alone (kf_gemm_bf16, the learned warm start's
     matrix engine): a square 8192^3 bf16 product with FP32 accumulation,
@@ -875,13 +1010,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--config", choices=["cfg2", "batch16", "learned", "sparse", "ablations", "gemm"],
+    ap.add_argument("--config", choices=["cfg2", "batch16", "learned", "sparse", "ablations", "gemm", "compare"],
                     default="cfg2",
                     help="cfg2: the headline 512^3 workload (default); batch16: 16 sequences batched; "
                          "learned: the learned ICP warm start against constant velocity; sparse: cfg3, "
-                         "a 2048^3 sparse domain; ablations: the reference's ablation flags")
+                         "a 2048^3 sparse domain; ablations: the reference's ablation flags; compare: a "
+                         "pipeline set compared every frame")
     ap.add_argument("--sparse-frames", type=int, default=300)
     ap.add_argument("--gemm-size", type=int, default=8192)
+    ap.add_argument("--compare-res", type=int, default=RES)
     ap.add_argument("--learned-seeds", type=int, default=20)
     ap.add_argument("--learned-frames", type=int, default=60)
     args = ap.parse_args()
@@ -900,6 +1037,8 @@ def main():
         line = run_ablations(args) if rank == 0 else None
     elif args.config == "gemm":
         line = run_gemm(args) if rank == 0 else None
+    elif args.config == "compare":
+        line = run_compare(args) if rank == 0 else None
     else:
         if world > 1:
             import datetime

@@ -312,6 +312,39 @@ kf_status kf_pipeline_set_kernel_events(kf_pipeline* pipeline, void* start, void
 kf_status kf_pipeline_update_counts(kf_pipeline* pipeline, uint64_t* voxel_updates,
                                     uint64_t* color_updates);
 
+/* ---- comparator: Comparator::compare (comparison.hpp:30-38, comparison.cpp:12-81)
+ * Deviations of a pipeline-set member against the set's reference member,
+ * computed on the device (the reference downloads both volumes first).
+ * Counts and maxima are exact; a mean is a double sum of the float
+ * deviations over the compared count, cast to float (Deviation). */
+typedef struct {
+  uint64_t compared_voxels; /* observed (weight > 0) in both volumes */
+  uint64_t only_primary;
+  uint64_t only_reference;
+  float max_distance_delta; /* |tsdf delta| */
+  float mean_distance_delta;
+  float max_weight_delta;
+} kf_volume_comparison;   /* VolumeComparison (comparison.hpp:21-28) */
+
+typedef struct {
+  uint64_t compared_pixels; /* point and normal finite in both maps */
+  uint64_t only_primary;
+  uint64_t only_reference;
+  float max_point_distance;
+  float mean_point_distance;
+  float max_normal_angle;   /* radians, atan2(|n x n'|, n . n') of the normalised normals */
+  float mean_normal_angle;
+} kf_surface_maps_comparison; /* SurfaceMapsComparison (comparison.hpp:11-19) */
+
+/* Comparator::compare(ConstHostVolumeView, ConstHostVolumeView) over two
+ * pipelines' volumes in place; voxel formats and storages may differ, the
+ * geometries must match (KF_ERR_INVALID_ARGUMENT otherwise). */
+kf_status kf_compare_volumes(kf_pipeline* primary, kf_pipeline* reference, kf_volume_comparison* out);
+/* Comparator::compare(SurfaceMaps, SurfaceMaps); each side in host or device
+ * memory (colors are not read and may be NULL); extents must match. */
+kf_status kf_compare_surface_maps(const kf_surface_maps* primary, const kf_surface_maps* reference,
+                                  kf_surface_maps_comparison* out);
+
 /* ---- tensor-core GEMM of the learned warm-start (no counterpart in the
  * reference): c[m x n] (fp32) = a[m x k] * b[n x k]^T (+ bias[n]) (ReLU when
  * relu != 0), a and b bf16 row-major on the device, k a multiple of 8, all

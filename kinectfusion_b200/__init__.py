@@ -5,11 +5,14 @@ include/kf_b200.h); this package is the Python host mirror of the reference's
 Pipeline / PyramidSource / ProjectiveIcpTracker interfaces over that ABI.
 """
 
-from . import abi, learned, synthetic, tum  # noqa: F401
+from . import abi, learned, pipeline_set, synthetic, tum  # noqa: F401
 from .pipeline import (ICP_ITERATIONS, Batch, Pipeline, ProjectiveIcpTracker, PyramidSource,  # noqa: F401
                        Reconstruction, SurfaceMaps, default_depth_options, default_icp_options,
                        device_available, pipeline_config)
 
-__all__ = ["abi", "learned", "synthetic", "tum", "Batch", "Pipeline", "PyramidSource", "ProjectiveIcpTracker", "Reconstruction",
+from .pipeline_set import AblationStats, PipelineComparison, PipelineSet, SetReconstruction  # noqa: F401
+
+__all__ = ["abi", "learned", "pipeline_set", "synthetic", "tum", "Batch", "PipelineSet", "SetReconstruction",
+           "PipelineComparison", "AblationStats", "Pipeline", "PyramidSource", "ProjectiveIcpTracker", "Reconstruction",
            "SurfaceMaps", "pipeline_config", "default_depth_options", "default_icp_options",
            "device_available", "ICP_ITERATIONS"]

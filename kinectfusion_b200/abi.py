@@ -151,6 +151,18 @@ class WarmStartResult(C.Structure):
                 ("cost_proposal", C.c_float), ("matches_proposal", C.c_float), ("used_proposal", C.c_int32)]
 
 
+class VolumeComparison(C.Structure):
+    _fields_ = [("compared_voxels", C.c_uint64), ("only_primary", C.c_uint64), ("only_reference", C.c_uint64),
+                ("max_distance_delta", C.c_float), ("mean_distance_delta", C.c_float),
+                ("max_weight_delta", C.c_float)]
+
+
+class SurfaceMapsComparison(C.Structure):
+    _fields_ = [("compared_pixels", C.c_uint64), ("only_primary", C.c_uint64), ("only_reference", C.c_uint64),
+                ("max_point_distance", C.c_float), ("mean_point_distance", C.c_float),
+                ("max_normal_angle", C.c_float), ("mean_normal_angle", C.c_float)]
+
+
 WARM_START_TWIST_SCALE = 50.0  # KF_WARM_START_TWIST_SCALE
 
 P = C.c_void_p
@@ -197,6 +209,9 @@ _PROTOTYPES = {
     "kf_pipeline_stream": (C.c_int, [P, C.POINTER(P)]),
     "kf_pipeline_set_kernel_events": (C.c_int, [P, P, P]),
     "kf_pipeline_update_counts": (C.c_int, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "kf_compare_volumes": (C.c_int, [P, P, C.POINTER(VolumeComparison)]),
+    "kf_compare_surface_maps": (C.c_int, [C.POINTER(SurfaceMapsView), C.POINTER(SurfaceMapsView),
+                                          C.POINTER(SurfaceMapsComparison)]),
     "kf_tracker_create": (C.c_int, [C.POINTER(IcpOptions), C.POINTER(P)]),
     "kf_tracker_destroy": (C.c_int, [P]),
     "kf_pipeline_track": (C.c_int, [P, P, C.POINTER(RaycastCamera), C.POINTER(LevelView), C.c_uint32,
