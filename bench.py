@@ -730,11 +730,11 @@ def run_compare(args) -> dict:
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
     compare_ms = float(np.median(times))
-    # algorithmic bytes: the observed bits of both volumes (128 B per brick
+    # algorithmic bytes: the observed bits of both volumes (64 B per brick
     # each) and both float bricks wherever either volume observed a voxel
     blocks = (res // 8) ** 3
     live = _live_bricks(members[1], members[0])
-    traffic_bytes = blocks * 2 * 128 + live * 2 * 4096
+    traffic_bytes = blocks * 2 * 64 + live * 2 * 4096
     gbs = traffic_bytes / (compare_ms / 1e3) / 1e9
     peaks = measured_peaks()
     peak = peaks.get("hbm_gbs", 6650.0)
@@ -769,7 +769,8 @@ def run_compare(args) -> dict:
         "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(gbs / peak, 4), "traffic": None,
                      "peak_source": "measured" if not peaks.get("fallback") else "fallback",
-                     "kernel": "compare_volumes_kernel<float, float> (+ finish kernel and result copy)"},
+                     "kernel": "kf_compare_volumes, float vs float: live-block passes (mask, scan, list), "
+                               "compare_volumes_kernel, finish kernel and result copy, event to event"},
         "last_comparisons": [c.csv() for c in last],
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),

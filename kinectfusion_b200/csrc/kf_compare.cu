@@ -19,7 +19,7 @@ namespace kf {
 namespace {
 
 constexpr unsigned kCompareThreads = 256;
-constexpr unsigned kCompareCtas = 148 * 8;
+constexpr unsigned kCompareCtas = 148 * 4;
 
 // One CTA's share of a comparison.  Volumes: sum[0] / max[0] = |tsdf delta|,
 // max[1] = |weight delta|.  Maps: sum[0] / max[0] = point distance, sum[1] /
@@ -148,57 +148,127 @@ __device__ __forceinline__ uint32_t slot_of(const CompareSide& s, uint32_t blk) 
 __device__ __forceinline__ bool may_hold_observed(const CompareSide& s, uint32_t blk) {
   if (s.fresh) return false;
   if (s.grid != nullptr) return __ldg(s.grid + blk) != kUnallocated;
-  const uint4* layers = s.observed + static_cast<size_t>(blk) * 8u;
+  // the upper 8 bytes of each layer's 16: its two observed words
+  const uint2* layers = reinterpret_cast<const uint2*>(s.observed + static_cast<size_t>(blk) * 8u);
   uint32_t any = 0u;
 #pragma unroll
   for (int z = 0; z < 8; ++z) {
-    const uint4 q = __ldg(layers + z);
-    any |= q.z | q.w;
+    const uint2 q = __ldg(layers + 2 * z + 1);
+    any |= q.x | q.y;
   }
   return any != 0u;
 }
 
-constexpr uint32_t kChunkBricks = 32;
+constexpr uint32_t kChunkBricks = 32;                      // blocks per live-mask word
+constexpr uint32_t kChunksPerCta = kCompareThreads / 32;  // one chunk per warp
 
-// Grid-strided over chunks of 32 consecutive 8^3 blocks (x-major block
-// index).  Warp 0 finds the chunk's blocks where either volume may hold an
-// observed voxel; the CTA then reads those bricks of both volumes, 16 bytes
-// (float voxels) or 8 bytes per thread each, and skips the rest: a voxel
-// unobserved on both sides counts nowhere.  Voxels of the padding of edge
-// bricks (outside the resolution) are left out.
+// The live blocks (where either volume may hold an observed voxel) as a list
+// in block order, built in three passes: masks, a scan of the per-CTA counts,
+// a scatter.  The comparison then spreads the list evenly over all warps.
+//
+// Pass 1: one warp per chunk of 32 consecutive blocks (x-major block index).
+__global__ void __launch_bounds__(kCompareThreads)
+    live_mask_kernel(CompareSide side_a, CompareSide side_b, uint32_t blocks, uint32_t* __restrict__ masks,
+                     uint32_t* __restrict__ cta_counts) {
+  __shared__ uint32_t warp_counts[kChunksPerCta];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t chunk = blockIdx.x * kChunksPerCta + warp;
+  const uint32_t blk = chunk * kChunkBricks + lane;
+  const bool live = blk < blocks && (may_hold_observed(side_a, blk) || may_hold_observed(side_b, blk));
+  const uint32_t mask = __ballot_sync(0xFFFFFFFFu, live);
+  if (lane == 0) {
+    if (chunk * kChunkBricks < blocks) masks[chunk] = mask;
+    warp_counts[warp] = static_cast<uint32_t>(__popc(mask));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t n = 0;
+    for (uint32_t w = 0; w < kChunksPerCta; ++w) n += warp_counts[w];
+    cta_counts[blockIdx.x] = n;
+  }
+}
+
+// Pass 2 (one CTA): exclusive prefix sums of the CTA counts; offsets[ctas]
+// receives the number of live blocks.
+__global__ void __launch_bounds__(1024)
+    live_scan_kernel(const uint32_t* __restrict__ counts, uint32_t ctas, uint32_t* __restrict__ offsets) {
+  __shared__ uint32_t partial[1024];
+  const uint32_t per = (ctas + 1023u) / 1024u;
+  const uint32_t begin = min(threadIdx.x * per, ctas), end = min(begin + per, ctas);
+  uint32_t sum = 0;
+  for (uint32_t i = begin; i < end; ++i) sum += counts[i];
+  partial[threadIdx.x] = sum;
+  __syncthreads();
+  for (uint32_t off = 1; off < 1024u; off <<= 1) {
+    const uint32_t v = threadIdx.x >= off ? partial[threadIdx.x - off] : 0u;
+    __syncthreads();
+    partial[threadIdx.x] += v;
+    __syncthreads();
+  }
+  uint32_t run = partial[threadIdx.x] - sum;
+  for (uint32_t i = begin; i < end; ++i) {
+    offsets[i] = run;
+    run += counts[i];
+  }
+  if (threadIdx.x == 1023u) offsets[ctas] = partial[1023];
+}
+
+// Pass 3: every live block's index at its rank.
+__global__ void __launch_bounds__(kCompareThreads)
+    live_list_kernel(const uint32_t* __restrict__ masks, uint32_t chunks, const uint32_t* __restrict__ offsets,
+                     uint32_t* __restrict__ list) {
+  __shared__ uint32_t warp_counts[kChunksPerCta];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t chunk = blockIdx.x * kChunksPerCta + warp;
+  const uint32_t mask = chunk < chunks ? masks[chunk] : 0u;
+  if (lane == 0) warp_counts[warp] = static_cast<uint32_t>(__popc(mask));
+  __syncthreads();
+  uint32_t base = offsets[blockIdx.x];
+  for (uint32_t w = 0; w < warp; ++w) base += warp_counts[w];
+  if ((mask >> lane) & 1u) {
+    list[base + static_cast<uint32_t>(__popc(mask & ((1u << lane) - 1u)))] = chunk * kChunkBricks + lane;
+  }
+}
+
+// Pass 4: a warp per live block, grid-strided over the list; each lane reads
+// pairs j * 32 + lane (j = 0..7) of the brick in two batches of four, one
+// 16-byte (float) or 8-byte load per pair and volume, so every lane keeps
+// eight loads in flight.  Voxels of the padding of edge bricks (outside the
+// resolution) are left out.
 template <int KindA, int KindB>
 __global__ void __launch_bounds__(kCompareThreads)
     compare_volumes_kernel(VolumeDev a, VolumeDev b, CompareSide side_a, CompareSide side_b,
+                           const uint32_t* __restrict__ list, const uint32_t* __restrict__ list_count,
                            ComparePartial* __restrict__ partials) {
-  __shared__ uint32_t live_mask;
+  using RawA = typename VoxelTraits<KindA>::Raw;
+  using RawB = typename VoxelTraits<KindB>::Raw;
   ComparePartial t;
   clear(t);
-  const uint32_t blocks = a.bx * a.by * a.bz;
-  const uint32_t chunks = (blocks + kChunkBricks - 1u) / kChunkBricks;
-  const uint32_t o0 = 2u * threadIdx.x;  // storage offset of the first voxel of the pair
-  const uint32_t x0 = o0 & 7u, y0 = (o0 >> 3) & 7u, z0 = o0 >> 6;  // x0 + 1 for the second
-  for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
-    if (threadIdx.x < 32u) {
-      const uint32_t blk = c * kChunkBricks + threadIdx.x;
-      const bool live = blk < blocks && (may_hold_observed(side_a, blk) || may_hold_observed(side_b, blk));
-      const uint32_t mask = __ballot_sync(0xFFFFFFFFu, live);
-      if (threadIdx.x == 0) live_mask = mask;
-    }
-    __syncthreads();
-    uint32_t mask = live_mask;
-    __syncthreads();  // warp 0 may write the next chunk's mask
-    while (mask != 0u) {
-      const uint32_t blk = c * kChunkBricks + static_cast<uint32_t>(__ffs(mask) - 1);
-      mask &= mask - 1u;
-      const uint32_t bxi = blk % a.bx, byi = (blk / a.bx) % a.by, bzi = blk / (a.bx * a.by);
-      const uint32_t x = bxi * 8u + x0, y = byi * 8u + y0, z = bzi * 8u + z0;
-      typename VoxelTraits<KindA>::Raw a0, a1;
-      typename VoxelTraits<KindB>::Raw b0, b1;
-      load_pair<KindA>(a.voxels, slot_of(side_a, blk), threadIdx.x, a0, a1);
-      load_pair<KindB>(b.voxels, slot_of(side_b, blk), threadIdx.x, b0, b1);
-      if (y < a.ry && z < a.rz) {
-        if (x < a.rx) compare_voxel<KindA, KindB>(a0, b0, t);
-        if (x + 1u < a.rx) compare_voxel<KindA, KindB>(a1, b1, t);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warps = gridDim.x * kChunksPerCta;
+  const uint32_t live = __ldg(list_count);
+  for (uint32_t i = blockIdx.x * kChunksPerCta + (threadIdx.x >> 5); i < live; i += warps) {
+    const uint32_t blk = __ldg(list + i);
+    const uint32_t sa = slot_of(side_a, blk), sb = slot_of(side_b, blk);
+    const uint32_t bxi = blk % a.bx, byi = (blk / a.bx) % a.by, bzi = blk / (a.bx * a.by);
+#pragma unroll
+    for (uint32_t half = 0; half < 2; ++half) {
+      RawA a0[4], a1[4];
+      RawB b0[4], b1[4];
+#pragma unroll
+      for (uint32_t j = 0; j < 4; ++j) {
+        const uint32_t pair = (half * 4u + j) * 32u + lane;
+        load_pair<KindA>(a.voxels, sa, pair, a0[j], a1[j]);
+        load_pair<KindB>(b.voxels, sb, pair, b0[j], b1[j]);
+      }
+#pragma unroll
+      for (uint32_t j = 0; j < 4; ++j) {
+        const uint32_t o0 = 2u * ((half * 4u + j) * 32u + lane);
+        const uint32_t x = bxi * 8u + (o0 & 7u), y = byi * 8u + ((o0 >> 3) & 7u), z = bzi * 8u + (o0 >> 6);
+        if (y < a.ry && z < a.rz) {
+          if (x < a.rx) compare_voxel<KindA, KindB>(a0[j], b0[j], t);
+          if (x + 1u < a.rx) compare_voxel<KindA, KindB>(a1[j], b1[j], t);
+        }
       }
     }
   }
@@ -245,7 +315,8 @@ struct CompareScratch {
   std::mutex lock;
   int device = -1;
   DeviceArray<ComparePartial> partials;
-  DeviceArray<float> maps;  // staging of host surface maps
+  DeviceArray<float> maps;     // staging of host surface maps
+  DeviceArray<uint32_t> live;  // live-block masks, CTA counts, offsets, list
   PinnedArray<ComparePartial> result;
 };
 CompareScratch& compare_scratch() {
@@ -259,6 +330,7 @@ void prepare(CompareScratch& s) {
   if (s.device != device) {  // another device: start over (the arrays belong to the old one)
     s.partials = DeviceArray<ComparePartial>();
     s.maps = DeviceArray<float>();
+    s.live = DeviceArray<uint32_t>();
     s.device = device;
   }
   if (s.partials.count == 0) s.partials.resize(kCompareCtas + 1);
@@ -293,33 +365,51 @@ CompareSide side_of(const Pipeline& p) {
 }
 
 template <int KindA>
-void launch_compare_volumes_as(const Pipeline& a, const Pipeline& b, ComparePartial* partials, cudaStream_t s) {
-  const CompareSide sa = side_of(a), sb = side_of(b);
+void launch_compare_volumes_as(const Pipeline& a, const Pipeline& b, const CompareSide& sa, const CompareSide& sb,
+                               const uint32_t* list, const uint32_t* count, ComparePartial* partials, cudaStream_t s) {
   switch (b.config.voxel) {
     case KF_VOXEL_QUANTIZED:
       compare_volumes_kernel<KindA, KF_VOXEL_QUANTIZED>
-          <<<kCompareCtas, kCompareThreads, 0, s>>>(a.view, b.view, sa, sb, partials);
+          <<<kCompareCtas, kCompareThreads, 0, s>>>(a.view, b.view, sa, sb, list, count, partials);
       break;
     case KF_VOXEL_BF16:
-      compare_volumes_kernel<KindA, KF_VOXEL_BF16><<<kCompareCtas, kCompareThreads, 0, s>>>(a.view, b.view, sa, sb, partials);
+      compare_volumes_kernel<KindA, KF_VOXEL_BF16>
+          <<<kCompareCtas, kCompareThreads, 0, s>>>(a.view, b.view, sa, sb, list, count, partials);
       break;
     default:
       compare_volumes_kernel<KindA, KF_VOXEL_FLOAT>
-          <<<kCompareCtas, kCompareThreads, 0, s>>>(a.view, b.view, sa, sb, partials);
+          <<<kCompareCtas, kCompareThreads, 0, s>>>(a.view, b.view, sa, sb, list, count, partials);
       break;
   }
 }
 
-void launch_compare_volumes(const Pipeline& a, const Pipeline& b, ComparePartial* partials, cudaStream_t s) {
+void launch_compare_volumes(const Pipeline& a, const Pipeline& b, CompareScratch& scratch, cudaStream_t s) {
+  const CompareSide sa = side_of(a), sb = side_of(b);
+  const uint32_t blocks = a.view.bx * a.view.by * a.view.bz;
+  const uint32_t chunks = ceil_div(blocks, kChunkBricks);
+  const uint32_t ctas = ceil_div(chunks, kChunksPerCta);
+  // [masks: chunks][counts: ctas][offsets: ctas + 1][list: blocks]
+  const size_t words = static_cast<size_t>(chunks) + 2u * ctas + 1u + blocks;
+  if (scratch.live.count < words) scratch.live.resize(words);
+  uint32_t* masks = scratch.live.ptr;
+  uint32_t* counts = masks + chunks;
+  uint32_t* offsets = counts + ctas;
+  uint32_t* list = offsets + ctas + 1;
+  live_mask_kernel<<<ctas, kCompareThreads, 0, s>>>(sa, sb, blocks, masks, counts);
+  check(cudaGetLastError(), "live_mask_kernel launch");
+  live_scan_kernel<<<1, 1024, 0, s>>>(counts, ctas, offsets);
+  check(cudaGetLastError(), "live_scan_kernel launch");
+  live_list_kernel<<<ctas, kCompareThreads, 0, s>>>(masks, chunks, offsets, list);
+  check(cudaGetLastError(), "live_list_kernel launch");
   switch (a.config.voxel) {
     case KF_VOXEL_QUANTIZED:
-      launch_compare_volumes_as<KF_VOXEL_QUANTIZED>(a, b, partials, s);
+      launch_compare_volumes_as<KF_VOXEL_QUANTIZED>(a, b, sa, sb, list, offsets + ctas, scratch.partials.ptr, s);
       break;
     case KF_VOXEL_BF16:
-      launch_compare_volumes_as<KF_VOXEL_BF16>(a, b, partials, s);
+      launch_compare_volumes_as<KF_VOXEL_BF16>(a, b, sa, sb, list, offsets + ctas, scratch.partials.ptr, s);
       break;
     default:
-      launch_compare_volumes_as<KF_VOXEL_FLOAT>(a, b, partials, s);
+      launch_compare_volumes_as<KF_VOXEL_FLOAT>(a, b, sa, sb, list, offsets + ctas, scratch.partials.ptr, s);
       break;
   }
   check(cudaGetLastError(), "compare_volumes_kernel launch");
@@ -349,7 +439,7 @@ kf_status kf_compare_volumes(kf_pipeline* primary, kf_pipeline* reference, kf_vo
     prepare(s);
     // the reference's volume is read on the primary's stream after its own work
     if (&a != &b) check(cudaStreamSynchronize(b.stream), "comparison order");
-    launch_compare_volumes(a, b, s.partials.ptr, a.stream);
+    launch_compare_volumes(a, b, s, a.stream);
     const ComparePartial r = finish(s, a.stream);
     out->compared_voxels = r.compared;
     out->only_primary = r.only_primary;
