@@ -207,25 +207,56 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
     voxel_updates_per_step = (updates1.value - updates0.value) / args.steps
 
     # ---- end to end through the public API: host depth in, pose out ----------------
+    # Frames in flight (kf_frame_submit / kf_frame_result_next): every step
+    # copies its depth frame from pinned host memory into the pipeline's
+    # staging and up to the device, and reads its result (the frame's tracker
+    # state, 736 B) back to the host; up to two frames run ahead of the
+    # results read.  The host-synchronous loop (kf_frame_process per frame,
+    # the reference's loop shape) is reported beside it.
+    result_bytes = 2 * 736  # the frame graph's own result copy + the queued copy
     pipe2 = kf.Pipeline(cfg)
-    loop = kf.Reconstruction(pipe2, k)
+    loop = kf.PipelinedReconstruction(pipe2, k)
     pinned = torch.from_numpy(seq.depth.view(np.int16)).pin_memory().numpy().view(np.uint16)
-    for s in range(max(args.warmup, 3)):
-        loop.process(pinned[frame_schedule(s)])
+    warm = max(args.warmup, 3)
+    for s in range(warm):
+        loop.submit(pinned[frame_schedule(s)])
+        loop.next_result()
     stream2_ptr = C.c_void_p()
     abi.check(lib.kf_pipeline_stream(pipe2.handle, C.byref(stream2_ptr)))
     stream2 = torch.cuda.ExternalStream(stream2_ptr.value)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
+    ahead = 2
     e0.record(stream2)
     for s in range(args.steps):
-        loop.process(pinned[frame_schedule(max(args.warmup, 3) + s)])
+        loop.submit(pinned[frame_schedule(warm + s)])
+        if s >= ahead:
+            loop.next_result()
+    while len(loop.results) < warm + args.steps:
+        loop.next_result()
     e1.record(stream2)
     e1.synchronize()
     barrier()
     e2e_ms = e0.elapsed_time(e1)
-    result_bytes = C.sizeof(abi.FrameResult)
+
+    sync_pipe = kf.Pipeline(cfg)
+    sync_loop = kf.Reconstruction(sync_pipe, k)
+    for s in range(warm):
+        sync_loop.process(pinned[frame_schedule(s)])
+    sync_steps = min(args.steps, 400)
+    sync_stream_ptr = C.c_void_p()
+    abi.check(lib.kf_pipeline_stream(sync_pipe.handle, C.byref(sync_stream_ptr)))
+    sync_stream = torch.cuda.ExternalStream(sync_stream_ptr.value)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    f0.record(sync_stream)
+    for s in range(sync_steps):
+        sync_loop.process(pinned[frame_schedule(warm + s)])
+    f1.record(sync_stream)
+    f1.synchronize()
+    e2e_sync_fps = sync_steps / (f0.elapsed_time(f1) / 1e3)
+    del sync_loop, sync_pipe
 
     # accuracy of the e2e trajectory over the first pass of the sequence
     ate = None
@@ -333,7 +364,12 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded analytic RGB-D scene)",
         "config": {**workload_config(), "parallelism": f"replicas{world}"},
         "e2e": {"value": round(e2e_fps, 2), "unit": "frames/s", "h2d_bytes_per_step": frame_bytes,
-                "d2h_bytes_per_step": result_bytes},
+                "d2h_bytes_per_step": result_bytes,
+                "api": "PipelinedReconstruction.submit / next_result (kf_frame_submit, kf_frame_result_next), "
+                       "two frames in flight, pinned host depth"},
+        "e2e_synchronous": {"value": round(e2e_sync_fps * world, 2), "unit": "frames/s",
+                            "h2d_bytes_per_step": frame_bytes, "d2h_bytes_per_step": 736,
+                            "api": "Reconstruction.process (kf_frame_process, host sync per frame)"},
         "gpu_launches": int(kernels_per_frame.value) * args.steps,
         "gpu_launches_per_frame": int(kernels_per_frame.value),
         "voxel_updates_per_s": round(voxel_updates_per_step * fps, 1),

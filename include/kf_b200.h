@@ -424,7 +424,9 @@ kf_status kf_icp_normal_equations_static(const kf_level_view* live, const float*
  * width*height uint16 in `memory`; color may be NULL.  `pose` is the
  * camera_to_world the frame starts from and receives the result.  When
  * `first_frame` is set the frame is fused at `pose` without tracking
- * (Reconstruction::initialize, reconstruction.cpp:143-182). */
+ * (Reconstruction::initialize, reconstruction.cpp:143-182).  Host inputs in
+ * page-locked memory are copied to the device straight from the caller's
+ * buffers; pageable ones through the pipeline's pinned staging. */
 kf_status kf_frame_process(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker,
                            const uint16_t* depth, const uint32_t* color, uint32_t width,
                            uint32_t height, kf_intrinsics intrinsics, int32_t memory,
@@ -437,6 +439,18 @@ kf_status kf_frame_enqueue(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracke
                            uint32_t height, kf_intrinsics intrinsics, int32_t memory,
                            const uint32_t* iterations_per_level, int32_t first_frame);
 kf_status kf_frame_result_fetch(kf_pipeline* pipeline, kf_frame_result* result);
+/* Frames in flight, for loops that read every frame's result but need not
+ * wait for it before sending the next frame (the reference's loop waits,
+ * reconstruction.cpp:184-216): kf_frame_submit is kf_frame_enqueue plus a
+ * copy of the frame's result into a queue of eight; host inputs are staged
+ * while earlier frames still run.  kf_frame_result_next waits for the oldest
+ * queued frame only and returns its result; submitting a ninth frame before
+ * reading one is KF_ERR_INVALID_ARGUMENT. */
+kf_status kf_frame_submit(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker,
+                          const uint16_t* depth, const uint32_t* color, uint32_t width,
+                          uint32_t height, kf_intrinsics intrinsics, int32_t memory,
+                          const uint32_t* iterations_per_level, int32_t first_frame);
+kf_status kf_frame_result_next(kf_pipeline* pipeline, kf_frame_result* result);
 /* Kernel launches in one frame graph: the kernel nodes of the graph that the
  * last kf_frame_enqueue / kf_frame_process launched (this library's kernels;
  * copies, memsets and event records are not kernels).  No counterpart in the

@@ -6,13 +6,13 @@ Pipeline / PyramidSource / ProjectiveIcpTracker interfaces over that ABI.
 """
 
 from . import abi, learned, pipeline_set, synthetic, tum  # noqa: F401
-from .pipeline import (ICP_ITERATIONS, Batch, Pipeline, ProjectiveIcpTracker, PyramidSource,  # noqa: F401
-                       Reconstruction, SurfaceMaps, default_depth_options, default_icp_options,
+from .pipeline import (ICP_ITERATIONS, Batch, Pipeline, PipelinedReconstruction, ProjectiveIcpTracker,  # noqa: F401
+                       PyramidSource, Reconstruction, SurfaceMaps, default_depth_options, default_icp_options,
                        device_available, pipeline_config)
 
 from .pipeline_set import AblationStats, PipelineComparison, PipelineSet, SetReconstruction  # noqa: F401
 
 __all__ = ["abi", "learned", "pipeline_set", "synthetic", "tum", "Batch", "PipelineSet", "SetReconstruction",
-           "PipelineComparison", "AblationStats", "Pipeline", "PyramidSource", "ProjectiveIcpTracker", "Reconstruction",
+           "PipelineComparison", "AblationStats", "Pipeline", "PyramidSource", "ProjectiveIcpTracker", "Reconstruction", "PipelinedReconstruction",
            "SurfaceMaps", "pipeline_config", "default_depth_options", "default_icp_options",
            "device_available", "ICP_ITERATIONS"]

@@ -224,6 +224,8 @@ _PROTOTYPES = {
     "kf_frame_process": (C.c_int, [P, P, P, P, P, C.c_uint32, C.c_uint32, Intrinsics, C.c_int32, P, C.c_int32,
                                    C.POINTER(Rigid), C.POINTER(FrameResult)]),
     "kf_frame_enqueue": (C.c_int, [P, P, P, P, P, C.c_uint32, C.c_uint32, Intrinsics, C.c_int32, P, C.c_int32]),
+    "kf_frame_submit": (C.c_int, [P, P, P, P, P, C.c_uint32, C.c_uint32, Intrinsics, C.c_int32, P, C.c_int32]),
+    "kf_frame_result_next": (C.c_int, [P, C.POINTER(FrameResult)]),
     "kf_frame_result_fetch": (C.c_int, [P, C.POINTER(FrameResult)]),
     "kf_frame_set_pose": (C.c_int, [P, P, C.POINTER(Rigid)]),
     "kf_png_info": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_int32),
@@ -305,9 +307,8 @@ def rigid_from_matrix(m) -> Rigid:
 
 def matrix_from_rigid(r: Rigid):
     import numpy as np
+    v = np.frombuffer(r, dtype=np.float32, count=12)  # r[9] then t[3], no padding
     m = np.eye(4, dtype=np.float32)
-    for i in range(3):
-        for j in range(3):
-            m[i, j] = r.r[i * 3 + j]
-        m[i, 3] = r.t[i]
+    m[:3, :3] = v[:9].reshape(3, 3)
+    m[:3, 3] = v[9:]
     return m

@@ -296,6 +296,10 @@ kf_status kf_pipeline_destroy(kf_pipeline* pipeline) {
     Pipeline& p = pipeline->impl;
     if (p.stream) cudaStreamSynchronize(p.stream);
     p.clear_graphs();
+    if (p.staging_done) cudaEventDestroy(p.staging_done);
+    for (cudaEvent_t e : p.result_ready) {
+      if (e) cudaEventDestroy(e);
+    }
     if (p.stream) cudaStreamDestroy(p.stream);
     delete pipeline;
   });

@@ -145,36 +145,68 @@ Pipeline::FrameGraph& frame_graph_for(kf_pipeline* pipeline, kf_pyramid* pyramid
   return p.graphs.emplace(key, fg).first->second;
 }
 
-// The frame's inputs into the graph's fixed buffers, on stream `s`.
+// Page-locked host memory (cudaHostAlloc, cudaHostRegister, a framework's
+// pinned allocator) that a copy engine can read directly.
+bool page_locked(const void* ptr) {
+  cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, ptr) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return attr.type == cudaMemoryTypeHost;
+}
+
+// The frame's inputs into the graph's fixed buffers, on stream `s`.  Host
+// buffers go through pinned staging so the copy is a true async DMA and the
+// caller may reuse its buffer on return.  When the caller waits for the frame
+// before returning (`caller_waits`, kf_frame_process), page-locked inputs are
+// copied straight from the caller's buffers instead: no staging copy on the
+// host.
 void stage_inputs(Pipeline& p, Pyramid& pyr, const uint16_t* depth, const uint32_t* color, size_t n,
-                  int32_t memory, cudaStream_t s) {
+                  int32_t memory, cudaStream_t s, bool caller_waits = false) {
   if (memory == KF_MEMORY_DEVICE) {
     check(cudaMemcpyAsync(pyr.raw.ptr, depth, n * sizeof(uint16_t), cudaMemcpyDeviceToDevice, s), "depth copy");
     if (color) check(cudaMemcpyAsync(p.frame_color.ptr, color, n * 4, cudaMemcpyDeviceToDevice, s), "color copy");
     return;
   }
-  // Host buffers go through pinned staging so the copy is a true async DMA;
-  // wait for the previous frame's copy before overwriting the staging.
-  check(cudaStreamSynchronize(s), "staging reuse");
-  p.depth_staging.resize(n);
-  std::memcpy(p.depth_staging.ptr, depth, n * sizeof(uint16_t));
-  check(cudaMemcpyAsync(pyr.raw.ptr, p.depth_staging.ptr, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s),
-        "depth upload");
+  const bool direct_depth = caller_waits && page_locked(depth);
+  const bool direct_color = color != nullptr && caller_waits && page_locked(color);
+  const bool staged = !direct_depth || (color != nullptr && !direct_color);
+  // wait for the last upload from the staging before overwriting it (not for
+  // the frames after it: the host fills the staging while they run)
+  if (staged && p.staging_done != nullptr) check(cudaEventSynchronize(p.staging_done), "staging reuse");
+  const void* depth_src = depth;
+  if (!direct_depth) {
+    p.depth_staging.resize(n);
+    std::memcpy(p.depth_staging.ptr, depth, n * sizeof(uint16_t));
+    depth_src = p.depth_staging.ptr;
+  }
+  check(cudaMemcpyAsync(pyr.raw.ptr, depth_src, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s), "depth upload");
   if (color) {
-    p.color_staging.resize(n);
-    std::memcpy(p.color_staging.ptr, color, n * 4);
-    check(cudaMemcpyAsync(p.frame_color.ptr, p.color_staging.ptr, n * 4, cudaMemcpyHostToDevice, s), "color upload");
+    const void* color_src = color;
+    if (!direct_color) {
+      p.color_staging.resize(n);
+      std::memcpy(p.color_staging.ptr, color, n * 4);
+      color_src = p.color_staging.ptr;
+    }
+    check(cudaMemcpyAsync(p.frame_color.ptr, color_src, n * 4, cudaMemcpyHostToDevice, s), "color upload");
+  }
+  if (staged) {
+    if (p.staging_done == nullptr) {
+      check(cudaEventCreateWithFlags(&p.staging_done, cudaEventDisableTiming), "staging event");
+    }
+    check(cudaEventRecord(p.staging_done, s), "staging event");
   }
 }
 
 void enqueue(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker, const uint16_t* depth,
              const uint32_t* color, uint32_t width, uint32_t height, kf_intrinsics intrinsics, int32_t memory,
-             const uint32_t* iterations, int32_t first_frame) {
+             const uint32_t* iterations, int32_t first_frame, bool caller_waits = false) {
   require(depth != nullptr, "kf_frame_enqueue: null argument");
   Pipeline::FrameGraph& fg = frame_graph_for(pipeline, pyramid, tracker, width, height, intrinsics, iterations,
                                              first_frame, color != nullptr);
   Pipeline& p = pipeline->impl;
-  stage_inputs(p, pyramid->impl, depth, color, static_cast<size_t>(width) * height, memory, p.stream);
+  stage_inputs(p, pyramid->impl, depth, color, static_cast<size_t>(width) * height, memory, p.stream, caller_waits);
   check(cudaGraphLaunch(fg.exec, p.stream), "frame graph launch");
   p.last_frame_kernels = fg.kernels;
 }
@@ -361,6 +393,43 @@ kf_status kf_frame_enqueue(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracke
   });
 }
 
+kf_status kf_frame_submit(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker, const uint16_t* depth,
+                          const uint32_t* color, uint32_t width, uint32_t height, kf_intrinsics intrinsics,
+                          int32_t memory, const uint32_t* iterations_per_level, int32_t first_frame) {
+  return guarded([&] {
+    require(pipeline != nullptr && tracker != nullptr, "kf_frame_submit: null argument");
+    Pipeline& p = pipeline->impl;
+    require(p.results_pushed - p.results_popped < static_cast<uint64_t>(Pipeline::kResultSlots),
+            "kf_frame_submit: eight results are waiting; read one with kf_frame_result_next first");
+    enqueue(pipeline, pyramid, tracker, depth, color, width, height, intrinsics, memory, iterations_per_level,
+            first_frame);
+    // the frame's result into its own slot, after the frame on the stream
+    p.result_ring.resize(Pipeline::kResultSlots);
+    const int slot = static_cast<int>(p.results_pushed % Pipeline::kResultSlots);
+    if (p.result_ready[slot] == nullptr) {
+      check(cudaEventCreateWithFlags(&p.result_ready[slot], cudaEventDisableTiming), "result event");
+    }
+    check(cudaMemcpyAsync(p.result_ring.ptr + slot, tracker->impl.state.ptr, sizeof(IcpState), cudaMemcpyDeviceToHost,
+                          p.stream),
+          "result download");
+    check(cudaEventRecord(p.result_ready[slot], p.stream), "result event");
+    p.result_first[slot] = first_frame ? 1 : 0;
+    ++p.results_pushed;
+  });
+}
+
+kf_status kf_frame_result_next(kf_pipeline* pipeline, kf_frame_result* result) {
+  return guarded([&] {
+    require(pipeline != nullptr && result != nullptr, "kf_frame_result_next: null argument");
+    Pipeline& p = pipeline->impl;
+    require(p.results_popped < p.results_pushed, "kf_frame_result_next: no submitted frame is waiting");
+    const int slot = static_cast<int>(p.results_popped % Pipeline::kResultSlots);
+    check(cudaEventSynchronize(p.result_ready[slot]), "frame");
+    fill_result(p.result_ring.ptr[slot], p.result_first[slot], result);
+    ++p.results_popped;
+  });
+}
+
 kf_status kf_frame_result_fetch(kf_pipeline* pipeline, kf_frame_result* result) {
   return guarded([&] {
     require(pipeline != nullptr && result != nullptr, "kf_frame_result_fetch: null argument");
@@ -382,7 +451,7 @@ kf_status kf_frame_process(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracke
             "kf_frame_process: pose must be finite");
     launch_icp_set_pose(tracker->impl.state.ptr, *pose, 1, p.stream);
     enqueue(pipeline, pyramid, tracker, depth, color, width, height, intrinsics, memory, iterations_per_level,
-            first_frame);
+            first_frame, true);
     check(cudaStreamSynchronize(p.stream), "frame");
     kf_frame_result local;
     fill_result(*p.result_staging.ptr, first_frame, &local);

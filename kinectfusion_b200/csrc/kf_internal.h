@@ -325,6 +325,13 @@ struct Pipeline {
   PinnedArray<IcpState> result_staging;
   PinnedArray<uint16_t> depth_staging;
   PinnedArray<uint32_t> color_staging;
+  cudaEvent_t staging_done = nullptr;  // after the last upload from the staging buffers
+  // kf_frame_submit: the results of frames in flight, oldest first
+  static constexpr int kResultSlots = 8;
+  PinnedArray<IcpState> result_ring;
+  cudaEvent_t result_ready[kResultSlots] = {};
+  uint8_t result_first[kResultSlots] = {};
+  uint64_t results_pushed = 0, results_popped = 0;
   int frames_fused = 0;
 
   Maps& maps_for(uint32_t w, uint32_t h);

@@ -330,6 +330,35 @@ class Reconstruction:
         return result
 
 
+class PipelinedReconstruction(Reconstruction):
+    """The same loop with frames in flight (kf_frame_submit /
+    kf_frame_result_next): submit() returns once the frame is copied into the
+    pipeline's staging and launched, so the host prepares the next frame
+    while the device still works; results come back in submission order.
+    The pose stays on the device between frames (FP64), where process()
+    rounds it to float and sends it back each frame."""
+
+    RESULTS_IN_FLIGHT = 8
+
+    def submit(self, depth, color=None) -> None:
+        depth = np.ascontiguousarray(depth, dtype=np.uint16)
+        color = None if color is None else np.ascontiguousarray(color, dtype=np.uint32)
+        if self.frames == 0:
+            _check(lib().kf_frame_set_pose(self.pipeline.handle, self.tracker.handle, C.byref(self.pose)))
+        _check(lib().kf_frame_submit(self.pipeline.handle, self.pyramid.handle, self.tracker.handle, _ptr(depth),
+                                     _ptr(color), depth.shape[1], depth.shape[0], self.intrinsics,
+                                     abi.KF_MEMORY_HOST, self.iterations, 1 if self.frames == 0 else 0))
+        self.frames += 1
+
+    def next_result(self) -> abi.FrameResult:
+        result = abi.FrameResult()
+        _check(lib().kf_frame_result_next(self.pipeline.handle, C.byref(result)))
+        self.pose = result.camera_to_world
+        self.trajectory.append(abi.matrix_from_rigid(result.camera_to_world))
+        self.results.append(result)
+        return result
+
+
 class Batch:
     """Independent sequences stepped together (kf_batch_*): one graph launch
     runs one frame of every member.  Each member is a Reconstruction-like
