@@ -143,6 +143,23 @@ def profile_traffic() -> float | None:
     return None
 
 
+# ---- ranks ------------------------------------------------------------------------------
+def max_over_ranks(times_ms: list[float], dist, device: str) -> list[float]:
+    """Each timing as the slowest rank's (every rank runs its own replica over
+    the same timed region, between barriers)."""
+    import torch
+    t = torch.tensor(times_ms, dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def replica_throughput(steps: int, world: int, elapsed_ms: float) -> float:
+    """Whole-job frames/s: every rank processed `steps` frames of its own
+    sequence in at most `elapsed_ms`."""
+    return steps * world / (elapsed_ms / 1e3)
+
+
 # ---- our arm ------------------------------------------------------------------------------
 def run_ours(args, rank: int, world: int, dist) -> dict | None:
     import torch
@@ -341,15 +358,12 @@ def run_ours(args, rank: int, world: int, dist) -> dict | None:
                   "voxel_bytes": 24, "volume_gib": 3.0}
         del pipe_c
 
-    times = torch.tensor([elapsed_ms, e2e_ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    elapsed_ms, e2e_ms = times.tolist()
+    elapsed_ms, e2e_ms = max_over_ranks([elapsed_ms, e2e_ms], dist, "cuda")
     if rank != 0:
         return None
 
-    fps = args.steps * world / (elapsed_ms / 1e3)
-    e2e_fps = args.steps * world / (e2e_ms / 1e3)
+    fps = replica_throughput(args.steps, world, elapsed_ms)
+    e2e_fps = replica_throughput(args.steps, world, e2e_ms)
     peaks = measured_peaks()
     # algorithmic bytes of one integrate launch: read+write 8 B per fused voxel
     # plus the frame inputs it reads (depth 2 B + normals 12 B per pixel).
@@ -553,7 +567,8 @@ def cpu_baseline(seq, threads: int = 1, frames: int = 2) -> dict:
 # ---- reference arm -----------------------------------------------------------------------------
 def run_reference(args, rank: int) -> dict | None:
     """The reference's CPU implementation of the path (the oracle port: the
-    reference itself does not build here) on all host cores."""
+    reference's own sources need Eigen and other fetched dependencies that are
+    not installed) on all host cores."""
     if rank != 0:
         return None
     sys.path.insert(0, str(ROOT / "oracle"))

@@ -168,7 +168,7 @@ def render_frame(scene: Scene, pose: np.ndarray, rng: np.random.Generator):
 
 def make_sequence(seed: int, frames: int, max_step_m: float = 0.01,
                   max_step_deg: float = 0.5) -> Sequence:
-    """A seeded sequence (1 cm / 0.5 deg per frame by default)."""
+    """A seeded sequence (1 cm / 0.5 deg of camera motion per frame by default)."""
     rng = np.random.default_rng(seed)
     scene = make_scene(rng)
     poses = make_trajectory(rng, frames, max_step_m, max_step_deg)

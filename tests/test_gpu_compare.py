@@ -126,6 +126,27 @@ def test_volume_comparator_fresh_volume(variants, storage):
     assert compare_volumes(fresh, variants.reference).only_reference == variants.reference.observed_voxel_count()
 
 
+def test_volume_comparator_odd_resolution_all_pairs(seq):
+    # resolutions that are not multiples of 8 (edge bricks padded), dense and
+    # sparse on either side, every ordered pair against the oracle
+    res, origin = (100, 92, 84), (-1.0, -0.92, -0.5)
+    none = dict(color=abi.KF_COLOR_NONE)
+    band = dict(integration_mode=abi.KF_INTEGRATION_BAND)
+    members = [kf.Pipeline(kf.pipeline_config(res, 0.02, origin, 0.05, **none), "float"),
+               kf.Pipeline(kf.pipeline_config(res, 0.02, origin, 0.05, voxel=abi.KF_VOXEL_QUANTIZED, **none), "q"),
+               kf.Pipeline(kf.pipeline_config(res, 0.02, origin, 0.05, storage=abi.KF_STORAGE_SPARSE, **band,
+                                              **none), "sparse"),
+               kf.Pipeline(kf.pipeline_config(res, 0.02, origin, 0.05, storage=abi.KF_STORAGE_SPARSE,
+                                              voxel=abi.KF_VOXEL_BF16, **band, **none), "sparse-bf16")]
+    s = PipelineSet(members)
+    _feed(s, seq, 2)
+    for a in members:
+        for b in members:
+            c = compare_volumes(a, b)
+            o = assert_volume_parity(c, a, b)
+            assert o["compared_voxels"] > 0
+
+
 def test_volume_comparator_rejects_other_geometry(variants):
     other = kf.Pipeline(kf.pipeline_config(64, 0.02, (-0.64, -0.64, -0.5), 0.05, color=abi.KF_COLOR_NONE))
     with pytest.raises(ValueError, match="matching geometry"):
