@@ -297,6 +297,10 @@ kf_status kf_pipeline_destroy(kf_pipeline* pipeline) {
     if (p.stream) cudaStreamSynchronize(p.stream);
     p.clear_graphs();
     if (p.staging_done) cudaEventDestroy(p.staging_done);
+    for (cudaEvent_t e : {p.fork_event, p.pyramid_event, p.inputs_event}) {
+      if (e) cudaEventDestroy(e);
+    }
+    if (p.side_stream) cudaStreamDestroy(p.side_stream);
     for (cudaEvent_t e : p.result_ready) {
       if (e) cudaEventDestroy(e);
     }

@@ -33,17 +33,29 @@ __global__ void frame_begin_kernel(IcpState* st) {
 
 namespace {
 
-// Records the frame's work on `s` (stream capture).
+// Records the frame's work on `s` (stream capture).  The frame's inputs -
+// the pyramid, the integration pixel table and the depth tiles of the block
+// culling - need only the depth frame, not the pose: they form a side branch
+// of the graph (captured on the pipeline's side stream) that runs beside the
+// coarsest level's model render and ICP, and joins before the first ICP step
+// (the pyramid) and before the integration (the rest).
 void record_frame(Pipeline& p, Pyramid& pyr, Tracker& t, const Pipeline::GraphKey& key, bool has_color,
                   cudaStream_t s) {
   IcpState* st = t.state.ptr;
-  pyr.launch(s);
+  const cudaStream_t side = p.side_stream;
+  check(cudaEventRecord(p.fork_event, s), "graph fork");
+  check(cudaStreamWaitEvent(side, p.fork_event, 0), "graph fork");
+  pyr.launch(side);
+  check(cudaEventRecord(p.pyramid_event, side), "graph fork");
   const PyramidLevelBuffers& l0 = pyr.levels[0];
   const Intr k0 = intr_from(pyr.intrinsics);
   launch_pixel_table(pyr.raw.ptr, has_color ? p.frame_color.ptr : nullptr, l0.normals.ptr, pyr.width, pyr.height, k0,
-                     p.config.integration, p.config.tsdf_rule, p.pixel_table.ptr, s);
+                     p.config.integration, p.config.tsdf_rule, p.pixel_table.ptr, side);
+  launch_integrate_inputs(p, p.pixel_table.ptr, pyr.width, pyr.height, side);
+  check(cudaEventRecord(p.inputs_event, side), "graph join");
   frame_begin_kernel<<<1, 32, 0, s>>>(st);
   check(cudaGetLastError(), "frame_begin launch");
+  bool pyramid_joined = false;
   if (!key.first) {
     const uint32_t iters[4] = {key.it0, key.it1, key.it2, key.it3};
     for (int level = static_cast<int>(pyr.level_count) - 1; level >= 0; --level) {
@@ -67,11 +79,16 @@ void record_frame(Pipeline& p, Pyramid& pyr, Tracker& t, const Pipeline::GraphKe
       a.model_width = cam.width;
       a.model_height = cam.height;
       a.model_intrinsics = intr_from(cam.intrinsics);
+      if (!pyramid_joined) {
+        check(cudaStreamWaitEvent(s, p.pyramid_event, 0), "graph join");
+        pyramid_joined = true;
+      }
       for (uint32_t i = 0; i < iters[level]; ++i) launch_icp_iteration(a, st, t.partials.ptr, t.params, 1, 0, s);
       launch_icp_level_end(st, level, s);
     }
   }
-  launch_integrate(p, p.pixel_table.ptr, pyr.width, pyr.height, k0, Rigid{}, has_color, st, s);
+  check(cudaStreamWaitEvent(s, p.inputs_event, 0), "graph join");  // also joins the pyramid
+  launch_integrate(p, p.pixel_table.ptr, pyr.width, pyr.height, k0, Rigid{}, has_color, st, s, true);
   check(cudaMemcpyAsync(p.result_staging.ptr, st, sizeof(IcpState), cudaMemcpyDeviceToHost, s), "result download");
 }
 
@@ -113,6 +130,12 @@ Pipeline::FrameGraph& frame_graph_for(kf_pipeline* pipeline, kf_pyramid* pyramid
   // Size every buffer the graph touches before capture.
   for (uint32_t level = 0; level < pyr.level_count; ++level) p.maps_for(width >> level, height >> level);
   prepare_blocks(p, width, height, s);
+  if (p.side_stream == nullptr) {
+    check(cudaStreamCreateWithFlags(&p.side_stream, cudaStreamNonBlocking), "side stream");
+    check(cudaEventCreateWithFlags(&p.fork_event, cudaEventDisableTiming), "graph event");
+    check(cudaEventCreateWithFlags(&p.pyramid_event, cudaEventDisableTiming), "graph event");
+    check(cudaEventCreateWithFlags(&p.inputs_event, cudaEventDisableTiming), "graph event");
+  }
   check(cudaStreamSynchronize(s), "pre-capture sync");
   cudaGraph_t graph = nullptr;
   check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");

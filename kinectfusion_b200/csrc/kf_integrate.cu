@@ -720,8 +720,20 @@ void launch_pixel_table(const uint16_t* depth, const uint32_t* color, const floa
   check(cudaGetLastError(), "pixel_table_kernel launch");
 }
 
+void launch_integrate_inputs(Pipeline& p, const float4* table, uint32_t width, uint32_t height, cudaStream_t s) {
+  prepare_blocks(p, width, height, s);
+  if (p.config.integration.mode == KF_INTEGRATION_BAND) return;
+  // depth-tile pyramid
+  const TileLevels lv = tile_levels_of(p);
+  tile_max_kernel<<<dim3(ceil_div(lv.w[0], 16), ceil_div(lv.h[0], 16)), dim3(16, 16), 0, s>>>(
+      table, width, height, lv.w[0], lv.h[0], p.depth_tiles.ptr);
+  check(cudaGetLastError(), "tile_max_kernel launch");
+  tile_pyramid_kernel<<<1, 1024, 0, s>>>(p.depth_tiles.ptr, lv);
+  check(cudaGetLastError(), "tile_pyramid_kernel launch");
+}
+
 void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t height, Intr k, Rigid T,
-                      int has_color, const IcpState* state, cudaStream_t s) {
+                      int has_color, const IcpState* state, cudaStream_t s, bool inputs_ready) {
   prepare_blocks(p, width, height, s);
   const kf_integration_options& o = p.config.integration;
   const uint32_t blocks = p.view.bx * p.view.by * p.view.bz;
@@ -756,13 +768,8 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
       check(cudaGetLastError(), "band_compact_kernel launch");
     }
   } else {
-    // depth-tile pyramid
+    if (!inputs_ready) launch_integrate_inputs(p, table, width, height, s);
     const TileLevels lv = tile_levels_of(p);
-    tile_max_kernel<<<dim3(ceil_div(lv.w[0], 16), ceil_div(lv.h[0], 16)), dim3(16, 16), 0, s>>>(
-        table, width, height, lv.w[0], lv.h[0], p.depth_tiles.ptr);
-    check(cudaGetLastError(), "tile_max_kernel launch");
-    tile_pyramid_kernel<<<1, 1024, 0, s>>>(p.depth_tiles.ptr, lv);
-    check(cudaGetLastError(), "tile_pyramid_kernel launch");
     // block culling
     CullParams cp;
     cp.trunc_base = p.view.truncation;

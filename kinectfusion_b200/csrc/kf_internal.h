@@ -326,6 +326,9 @@ struct Pipeline {
   PinnedArray<uint16_t> depth_staging;
   PinnedArray<uint32_t> color_staging;
   cudaEvent_t staging_done = nullptr;  // after the last upload from the staging buffers
+  // the frame graph's side branch (frame inputs beside the first model render)
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t fork_event = nullptr, pyramid_event = nullptr, inputs_event = nullptr;
   // kf_frame_submit: the results of frames in flight, oldest first
   static constexpr int kResultSlots = 8;
   PinnedArray<IcpState> result_ring;
@@ -346,9 +349,14 @@ void launch_pixel_table(const uint16_t* depth, const uint32_t* color, const floa
                         cudaStream_t stream);
 // Dense full sweep.  `pose_state` (optional) overrides world_to_camera with
 // the inverse of the tracked pose and skips fusion when tracking failed.
+// With `inputs_ready` the steps of launch_integrate_inputs already ran.
 void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t height,
                       Intr intrinsics, Rigid world_to_camera, int has_color,
-                      const IcpState* pose_state, cudaStream_t stream);
+                      const IcpState* pose_state, cudaStream_t stream, bool inputs_ready = false);
+// The integration steps that need only the frame's pixel table, not the pose:
+// the depth-tile pyramid of the full sweep's block culling.
+void launch_integrate_inputs(Pipeline& p, const float4* table, uint32_t width, uint32_t height,
+                             cudaStream_t stream);
 // Allocates and clears the per-block skip and culling buffers.
 // C = A * B^T (+bias)(ReLU) on the tensor cores: A M x K, B N x K bf16
 // row-major (leading dimensions lda, ldb), C M x N fp32 (ldc).  `error`
