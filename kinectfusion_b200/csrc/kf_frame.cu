@@ -35,24 +35,28 @@ namespace {
 
 // Records the frame's work on `s` (stream capture).  The frame's inputs -
 // the pyramid, the integration pixel table and the depth tiles of the block
-// culling - need only the depth frame, not the pose: they form a side branch
-// of the graph (captured on the pipeline's side stream) that runs beside the
-// coarsest level's model render and ICP, and joins before the first ICP step
-// (the pyramid) and before the integration (the rest).
+// culling - need only the depth frame, not the pose.  With `key.fork` they
+// form a side branch of the graph (captured on the pipeline's side stream)
+// that runs beside the coarsest level's model render and ICP, and joins
+// before the first ICP step (the pyramid) and before the integration (the
+// rest); without, they run first on `s`.
 void record_frame(Pipeline& p, Pyramid& pyr, Tracker& t, const Pipeline::GraphKey& key, bool has_color,
                   cudaStream_t s) {
   IcpState* st = t.state.ptr;
-  const cudaStream_t side = p.side_stream;
-  check(cudaEventRecord(p.fork_event, s), "graph fork");
-  check(cudaStreamWaitEvent(side, p.fork_event, 0), "graph fork");
+  const bool fork = key.fork != 0;
+  const cudaStream_t side = fork ? p.side_stream : s;
+  if (fork) {
+    check(cudaEventRecord(p.fork_event, s), "graph fork");
+    check(cudaStreamWaitEvent(side, p.fork_event, 0), "graph fork");
+  }
   pyr.launch(side);
-  check(cudaEventRecord(p.pyramid_event, side), "graph fork");
+  if (fork) check(cudaEventRecord(p.pyramid_event, side), "graph fork");
   const PyramidLevelBuffers& l0 = pyr.levels[0];
   const Intr k0 = intr_from(pyr.intrinsics);
   launch_pixel_table(pyr.raw.ptr, has_color ? p.frame_color.ptr : nullptr, l0.normals.ptr, pyr.width, pyr.height, k0,
                      p.config.integration, p.config.tsdf_rule, p.pixel_table.ptr, side);
   launch_integrate_inputs(p, p.pixel_table.ptr, pyr.width, pyr.height, side);
-  check(cudaEventRecord(p.inputs_event, side), "graph join");
+  if (fork) check(cudaEventRecord(p.inputs_event, side), "graph join");
   frame_begin_kernel<<<1, 32, 0, s>>>(st);
   check(cudaGetLastError(), "frame_begin launch");
   bool pyramid_joined = false;
@@ -79,7 +83,7 @@ void record_frame(Pipeline& p, Pyramid& pyr, Tracker& t, const Pipeline::GraphKe
       a.model_width = cam.width;
       a.model_height = cam.height;
       a.model_intrinsics = intr_from(cam.intrinsics);
-      if (!pyramid_joined) {
+      if (fork && !pyramid_joined) {
         check(cudaStreamWaitEvent(s, p.pyramid_event, 0), "graph join");
         pyramid_joined = true;
       }
@@ -87,7 +91,7 @@ void record_frame(Pipeline& p, Pyramid& pyr, Tracker& t, const Pipeline::GraphKe
       launch_icp_level_end(st, level, s);
     }
   }
-  check(cudaStreamWaitEvent(s, p.inputs_event, 0), "graph join");  // also joins the pyramid
+  if (fork) check(cudaStreamWaitEvent(s, p.inputs_event, 0), "graph join");  // also joins the pyramid
   launch_integrate(p, p.pixel_table.ptr, pyr.width, pyr.height, k0, Rigid{}, has_color, st, s, true);
   check(cudaMemcpyAsync(p.result_staging.ptr, st, sizeof(IcpState), cudaMemcpyDeviceToHost, s), "result download");
 }
@@ -96,7 +100,8 @@ void record_frame(Pipeline& p, Pyramid& pyr, Tracker& t, const Pipeline::GraphKe
 // schedule, first-frame flag and colour, captured on first use.
 Pipeline::FrameGraph& frame_graph_for(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker,
                                       uint32_t width, uint32_t height, kf_intrinsics intrinsics,
-                                      const uint32_t* iterations, int32_t first_frame, bool has_color) {
+                                      const uint32_t* iterations, int32_t first_frame, bool has_color,
+                                      bool fork = true) {
   require(pipeline && pyramid && tracker, "kf_frame_enqueue: null argument");
   require(intrinsics.fx > 0.0f && intrinsics.fy > 0.0f, "Depth frame intrinsics must have positive focal lengths");
   Pipeline& p = pipeline->impl;
@@ -116,7 +121,7 @@ Pipeline::FrameGraph& frame_graph_for(kf_pipeline* pipeline, kf_pyramid* pyramid
   if (p.pixel_table.count != n) p.pixel_table.resize(n);
   if (p.frame_color.count != n) p.frame_color.resize(n);
   p.result_staging.resize(1);
-  Pipeline::GraphKey key{width, height, 0, 0, 0, 0, first_frame ? 1u : 0u, has_color ? 1u : 0u};
+  Pipeline::GraphKey key{width, height, 0, 0, 0, 0, first_frame ? 1u : 0u, has_color ? 1u : 0u, fork ? 1u : 0u};
   uint32_t* its[4] = {&key.it0, &key.it1, &key.it2, &key.it3};
   for (uint32_t l = 0; l < 4; ++l) *its[l] = (iterations != nullptr && l < pyr.level_count) ? iterations[l] : 0u;
   if (iterations == nullptr) {
@@ -130,7 +135,7 @@ Pipeline::FrameGraph& frame_graph_for(kf_pipeline* pipeline, kf_pyramid* pyramid
   // Size every buffer the graph touches before capture.
   for (uint32_t level = 0; level < pyr.level_count; ++level) p.maps_for(width >> level, height >> level);
   prepare_blocks(p, width, height, s);
-  if (p.side_stream == nullptr) {
+  if (fork && p.side_stream == nullptr) {
     check(cudaStreamCreateWithFlags(&p.side_stream, cudaStreamNonBlocking), "side stream");
     check(cudaEventCreateWithFlags(&p.fork_event, cudaEventDisableTiming), "graph event");
     check(cudaEventCreateWithFlags(&p.pyramid_event, cudaEventDisableTiming), "graph event");
@@ -287,8 +292,9 @@ void batch_step(kf_batch* b, const uint16_t* const* depths, uint32_t width, uint
   std::vector<uint64_t> key(2 * count, 0);
   for (size_t i = 0; i < count; ++i) {
     if (depths[i] == nullptr) continue;  // this member sits out the step
+    // one branch per member: the members already fill the GPU side by side
     graphs[i] = &frame_graph_for(b->pipelines[i], b->pyramids[i], b->trackers[i], width, height, intrinsics[i],
-                                 iterations, first != nullptr && first[i] != 0, false);
+                                 iterations, first != nullptr && first[i] != 0, false, false);
     key[2 * i] = reinterpret_cast<uint64_t>(graphs[i]->graph);
     key[2 * i + 1] = b->pipelines[i]->impl.graph_epoch;
   }

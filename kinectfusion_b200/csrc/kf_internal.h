@@ -296,13 +296,15 @@ struct Pipeline {
   cudaStream_t stream = nullptr;
   DeviceArray<unsigned long long> counters;  // [0] voxel updates, [1] colour updates
   cudaEvent_t kernel_start = nullptr, kernel_stop = nullptr;  // borrowed
-  // whole-frame graphs keyed by (width, height, iterations, first, colour)
+  // whole-frame graphs keyed by (width, height, iterations, first, colour, fork)
+  // fork: the frame's inputs on a side branch (standalone frames; batch
+  // members run concurrently already and keep one branch)
   struct GraphKey {
-    uint32_t w, h, it0, it1, it2, it3, first, color;
+    uint32_t w, h, it0, it1, it2, it3, first, color, fork;
     bool operator<(const GraphKey& o) const {
-      const uint32_t a[8] = {w, h, it0, it1, it2, it3, first, color};
-      const uint32_t b[8] = {o.w, o.h, o.it0, o.it1, o.it2, o.it3, o.first, o.color};
-      for (int i = 0; i < 8; ++i) {
+      const uint32_t a[9] = {w, h, it0, it1, it2, it3, first, color, fork};
+      const uint32_t b[9] = {o.w, o.h, o.it0, o.it1, o.it2, o.it3, o.first, o.color, o.fork};
+      for (int i = 0; i < 9; ++i) {
         if (a[i] != b[i]) return a[i] < b[i];
       }
       return false;
