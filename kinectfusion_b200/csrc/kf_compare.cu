@@ -3,14 +3,14 @@
 // deviation of two sets of surface maps, for the pipeline-set ablations.
 //
 // The reference downloads both volumes (Pipeline::host_view) and walks them on
-// one host core; here both stay in HBM and one pass reads each brick that
-// either volume may have observed once, and skips the others by their
-// observed bits or block allocation.  Counts and maxima are order-independent and come out exact; the
-// means divide a double sum of the float deviations by the compared count, as
-// Deviation does (comparison.hpp:64-83), with the sum taken per thread, then
-// over warps, CTAs and a final fixed-order pass: deterministic for a given
-// grid, and equal to the reference's sequential double sum to well under one
-// float ulp of the mean.
+// one host core; here both stay in HBM, and one pass reads once each brick
+// that either volume may have observed and skips the others by their
+// observed bits or block allocation.  Counts and maxima are order-independent
+// and come out exact; the means divide a double sum of the float deviations
+// by the compared count, as Deviation does (comparison.hpp:64-83), with the
+// sum taken per thread, then over warps, CTAs and a final fixed-order pass:
+// deterministic for a given grid, and equal to the reference's sequential
+// double sum to well under one float ulp of the mean.
 #include <mutex>
 
 #include "kf_internal.h"
