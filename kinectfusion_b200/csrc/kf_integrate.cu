@@ -164,10 +164,12 @@ __global__ void cull_blocks_kernel(VolumeDev v, Rigid T, Intr k, const float* __
         const int v0 = max(0, static_cast<int>(floorf(vmin - 1.5f)));
         const int v1 = min(static_cast<int>(cp.height) - 1, static_cast<int>(ceilf(vmax + 1.5f)));
         if (u0 <= u1 && v0 <= v1) {
-          // level whose tiles cover the rectangle with at most 2x2 texels
+          // the finest level whose tiles cover the rectangle with at most
+          // 4x4 texels (any level's tiles over the rectangle bound every pixel
+          // in it; finer ones bound it tighter)
           int tx0 = u0 / kTile, tx1 = u1 / kTile, ty0 = v0 / kTile, ty1 = v1 / kTile;
           uint32_t l = 0;
-          while (l + 1 < lv.count && (tx1 - tx0 > 1 || ty1 - ty0 > 1)) {
+          while (l + 1 < lv.count && (tx1 - tx0 > 3 || ty1 - ty0 > 3)) {
             tx0 >>= 1;
             tx1 >>= 1;
             ty0 >>= 1;
