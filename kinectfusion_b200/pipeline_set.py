@@ -295,8 +295,9 @@ class SetReconstruction:
     `comparisons` and, with an output directory, to ablation_stats.csv."""
 
     def __init__(self, pipeline_set: PipelineSet, intrinsics: abi.Intrinsics, output_dir=None, depth_options=None,
-                 icp_options=None, iterations=ICP_ITERATIONS):
+                 icp_options=None, iterations=ICP_ITERATIONS, frame_output=None):
         self.set = pipeline_set
+        self.frame_output = frame_output  # tum.FrameOutput: per-frame raycast images / point clouds
         self.intrinsics = intrinsics
         self.pyramids = [PyramidSource(depth_options) for _ in pipeline_set.members]
         self.trackers = [ProjectiveIcpTracker(icp_options) for _ in pipeline_set.members]
@@ -339,13 +340,20 @@ class SetReconstruction:
             self.trajectories[i].append(abi.matrix_from_rigid(r.camera_to_world))
         frame_index = self.frames
         self.frames += 1
+        # render_model_outputs (reconstruction.cpp:303-334): one viewpoint,
+        # the reference member's pose
+        writes = self.frame_output is not None and self.frame_output.writes_frames()
+        pose = results[self.set.reference_index].camera_to_world
         if self.set.should_compare(frame_index):
-            # render_model_outputs (reconstruction.cpp:303-334): one viewpoint,
-            # the reference member's pose
-            pose = results[self.set.reference_index].camera_to_world
             outputs = self.set.raycast_all(self.intrinsics, w, h, pose)
             comparisons = self.set.compare(outputs)
             self.comparisons.append((frame_index, comparisons))
             if self.stats is not None:
                 self.stats.append(frame_index, comparisons)
+            if writes:
+                for i, output in enumerate(outputs):
+                    subdirectory = "" if i == self.set.reference_index else output.name
+                    self.frame_output.write_frame(output.maps, frame_index, subdirectory)
+        elif writes:
+            self.frame_output.write_frame(self.set.raycast_reference(self.intrinsics, w, h, pose), frame_index)
         return results

@@ -209,3 +209,60 @@ def _quaternion(r: np.ndarray):
     q[k] = (r[k, i] + r[i, k]) / s
     q[3] = (r[k, j] - r[j, k]) / s
     return tuple(q)
+
+
+class FrameOutput:
+    """FrameOutput (src/app/frame_output.cpp:34-213): per-frame raycast
+    outputs written by worker threads, at most MAX_PENDING_WRITES in flight
+    (the oldest is waited for first), and mesh.ply.  Frames go to
+    `output_dir`, or `output_dir/subdirectory` for a pipeline-set member
+    other than the reference.  write_frame takes host maps (SurfaceMaps, or
+    anything with to_host(), such as pipeline_set.DeviceSurfaceMaps)."""
+
+    MAX_PENDING_WRITES = 16
+
+    def __init__(self, output_dir, write_raycast_images: bool = False, write_point_clouds: bool = False):
+        self.output_dir = pathlib.Path(output_dir)
+        self.write_raycast_images = write_raycast_images
+        self.write_point_clouds = write_point_clouds
+        self._pool = concurrent.futures.ThreadPoolExecutor(max_workers=4)
+        self._pending: list[concurrent.futures.Future] = []
+
+    def writes_frames(self) -> bool:
+        return self.write_raycast_images or self.write_point_clouds
+
+    @staticmethod
+    def frame_prefix(frame_index: int) -> str:
+        return f"frame_{frame_index:06d}"
+
+    def write_frame(self, maps, frame_index: int, subdirectory: str = "") -> None:
+        if not self.writes_frames():
+            return
+        if hasattr(maps, "to_host"):
+            maps = maps.to_host()
+        while len(self._pending) >= self.MAX_PENDING_WRITES:
+            self._pending.pop(0).result()
+        directory = self.output_dir / subdirectory if subdirectory else self.output_dir
+        directory.mkdir(parents=True, exist_ok=True)
+        prefix = directory / self.frame_prefix(frame_index)
+        if self.write_raycast_images:
+            self._pending.append(self._pool.submit(write_color_png, f"{prefix}_raycast.png", maps.colors))
+        if self.write_point_clouds:
+            self._pending.append(self._pool.submit(write_point_cloud_ply, f"{prefix}_raycast_point_cloud.ply",
+                                                   maps.points, maps.normals, maps.colors))
+
+    def write_mesh(self, mesh: dict, subdirectory: str = "") -> None:
+        directory = self.output_dir / subdirectory if subdirectory else self.output_dir
+        directory.mkdir(parents=True, exist_ok=True)
+        write_mesh_ply(directory / "mesh.ply", mesh)
+
+    def finish_pending_writes(self) -> None:
+        pending, self._pending = self._pending, []
+        for future in pending:
+            future.result()
+
+    def close(self) -> None:
+        try:
+            self.finish_pending_writes()
+        finally:
+            self._pool.shutdown(wait=True)

@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 from kinectfusion_b200 import abi, tum
+from kinectfusion_b200.pipeline import SurfaceMaps
 
 
 def _png(pixels: np.ndarray, bit_depth: int, color_type: int, filters, palette=None) -> bytes:
@@ -189,3 +190,33 @@ def test_trajectory_file(tmp_path):
     tum.write_trajectory(tmp_path / "t.txt", [pose], [0.5])
     fields = (tmp_path / "t.txt").read_text().split()
     assert fields[0] == "0.500000000" and [float(v) for v in fields[1:]] == [1, 2, 3, 0, 0, 0, 1]
+
+
+def test_frame_output_files(tmp_path):
+    # FrameOutput::write_frame / write_mesh (frame_output.cpp:123-213): the
+    # reference's frames at the root, another member's in its subdirectory
+    rng = np.random.default_rng(5)
+    pts = rng.normal(size=(6, 8, 3)).astype(np.float32)
+    nrm = rng.normal(size=(6, 8, 3)).astype(np.float32)
+    pts[0, :3] = np.nan
+    col = rng.integers(0, 2 ** 32, size=(6, 8), dtype=np.uint64).astype(np.uint32)
+    maps = SurfaceMaps(pts, nrm, col)
+    out = tum.FrameOutput(tmp_path / "out", write_raycast_images=True, write_point_clouds=True)
+    assert out.writes_frames() and tum.FrameOutput.frame_prefix(42) == "frame_000042"
+    for frame in range(20):  # more than MAX_PENDING_WRITES writes in flight
+        out.write_frame(maps, frame)
+    out.write_frame(maps, 7, subdirectory="bf16")
+    out.write_mesh({"positions": np.zeros((3, 3), np.float32), "normals": np.zeros((3, 3), np.float32),
+                    "colors": np.zeros((3, 3), np.float32), "triangles": np.array([[0, 1, 2]], np.uint32)})
+    out.close()
+    png = tmp_path / "out" / "frame_000019_raycast.png"
+    np.testing.assert_array_equal(tum.read_color_png(png), col)
+    _, counts, _ = _read_ply(tmp_path / "out" / "bf16" / "frame_000007_raycast_point_cloud.ply")
+    assert counts == {"vertex": 6 * 8 - 3}
+    assert len(list((tmp_path / "out").glob("frame_*_raycast.png"))) == 20
+    assert (tmp_path / "out" / "mesh.ply").exists()
+    # nothing written when neither output is on
+    quiet = tum.FrameOutput(tmp_path / "quiet")
+    quiet.write_frame(maps, 0)
+    quiet.close()
+    assert not (tmp_path / "quiet").exists()
