@@ -265,6 +265,11 @@ kf_status kf_pipeline_create(const kf_pipeline_config* config, kf_pipeline** out
 kf_status kf_pipeline_destroy(kf_pipeline* pipeline);
 /* Refill the volume with unobserved voxels (BasicVolume construction fill). */
 kf_status kf_pipeline_reset(kf_pipeline* pipeline);
+/* The same refill queued on the pipeline's stream without waiting for it
+ * (no reference counterpart: the reference starts a sequence by constructing
+ * a pipeline).  Frames enqueued after it see the empty volume; a new sequence
+ * starts without a host stall behind the previous one's frames in flight. */
+kf_status kf_pipeline_reset_async(kf_pipeline* pipeline);
 /* Pipeline::integrate (pipeline.hpp:75-79). */
 kf_status kf_pipeline_integrate(kf_pipeline* pipeline, const kf_frame_view* frame);
 /* Pipeline::raycast (pipeline.hpp:81): renders into `out` (host or device buffers). */
@@ -399,18 +404,21 @@ kf_status kf_icp_normal_equations(kf_tracker* tracker, const kf_level_view* live
                                   uint64_t* count);
 
 /* The same sweep without any allocation (no counterpart in the reference).
- * For callers that must not allocate device memory - code running inside
- * another framework's memory pool or a replayed CUDA graph, plug-ins whose
- * host forbids cudaMalloc after start-up, real-time loops kept off the
- * allocator: no tracker object is needed, and the per-CTA partial sums live in
- * a fixed device array (about 150 KB, present on every GPU that loads the
- * library until the process exits).  Live images of at most 1,228,800 pixels
- * (1200 CTAs of 1024 pixels) are accepted; larger ones return
- * KF_ERR_INVALID_ARGUMENT.  The first call on each device looks up the
- * array's address (make it before any stream capture).  Every call shares the
- * array: calls that overlap on the GPU (for example from two host threads)
- * race.  Runs on the legacy default stream and returns after the results are
- * copied to `sums` and `count`. */
+ * For callers that must not allocate device memory: plug-ins whose host
+ * application owns every byte of the GPU through its own memory pool (a
+ * cudaMalloc of theirs would bypass the pool's budget and can fail or evict
+ * the host's data), hosts that forbid cudaMalloc after start-up, and real-time
+ * loops that stay off the allocator because cudaMalloc may synchronise the
+ * device and stall the loop.  No tracker object is needed, and the per-CTA
+ * partial sums live in a fixed device array (about 150 KB, present on every
+ * GPU that loads the library until the process exits).  Live images of at
+ * most 1,228,800 pixels (1200 CTAs of 1024 pixels) are accepted; larger ones
+ * return KF_ERR_INVALID_ARGUMENT.  The first call on each device looks up the
+ * array's address; make that first call before any stream capture.  Every
+ * call shares the array: calls that overlap on the GPU (for example from two
+ * host threads) race.  The call is synchronous: it runs on the legacy default
+ * stream with blocking copies and returns after the results are copied to
+ * `sums` and `count`. */
 kf_status kf_icp_normal_equations_static(const kf_level_view* live, const float* model_points,
                                          const float* model_normals, uint32_t model_width,
                                          uint32_t model_height, kf_intrinsics model_intrinsics,

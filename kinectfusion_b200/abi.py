@@ -183,6 +183,7 @@ _PROTOTYPES = {
     "kf_pipeline_create": (C.c_int, [C.POINTER(PipelineConfig), C.POINTER(P)]),
     "kf_pipeline_destroy": (C.c_int, [P]),
     "kf_pipeline_reset": (C.c_int, [P]),
+    "kf_pipeline_reset_async": (C.c_int, [P]),
     "kf_pipeline_integrate": (C.c_int, [P, C.POINTER(FrameView)]),
     "kf_pipeline_raycast": (C.c_int, [P, C.POINTER(RaycastCamera), C.POINTER(SurfaceMapsView)]),
     "kf_pipeline_observed_voxel_count": (C.c_int, [P, C.POINTER(C.c_uint64)]),

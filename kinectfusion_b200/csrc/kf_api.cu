@@ -309,19 +309,29 @@ kf_status kf_pipeline_destroy(kf_pipeline* pipeline) {
   });
 }
 
+static void enqueue_reset(Pipeline& p) {
+  launch_fill_volume(p, p.stream);
+  reset_sparse(p, p.stream);
+  reset_blocks(p, p.stream);  // the raycast's skip structures describe the volume
+  if (p.band_map.count) {
+    check(cudaMemsetAsync(p.band_raw.ptr, 0, p.band_raw.bytes(), p.stream), "band bitmap reset");
+    check(cudaMemsetAsync(p.band_map.ptr, 0, p.band_map.bytes(), p.stream), "band bitmap reset");
+  }
+  check(cudaMemsetAsync(p.counters.ptr, 0, p.counters.bytes(), p.stream), "counter reset");
+}
+
 kf_status kf_pipeline_reset(kf_pipeline* pipeline) {
   return guarded([&] {
     require(pipeline != nullptr, "kf_pipeline_reset: null pipeline");
-    Pipeline& p = pipeline->impl;
-    launch_fill_volume(p, p.stream);
-    reset_sparse(p, p.stream);
-    reset_blocks(p, p.stream);  // the raycast's skip structures describe the volume
-    if (p.band_map.count) {
-      check(cudaMemsetAsync(p.band_raw.ptr, 0, p.band_raw.bytes(), p.stream), "band bitmap reset");
-      check(cudaMemsetAsync(p.band_map.ptr, 0, p.band_map.bytes(), p.stream), "band bitmap reset");
-    }
-    check(cudaMemsetAsync(p.counters.ptr, 0, p.counters.bytes(), p.stream), "counter reset");
-    check(cudaStreamSynchronize(p.stream), "volume reset");
+    enqueue_reset(pipeline->impl);
+    check(cudaStreamSynchronize(pipeline->impl.stream), "volume reset");
+  });
+}
+
+kf_status kf_pipeline_reset_async(kf_pipeline* pipeline) {
+  return guarded([&] {
+    require(pipeline != nullptr, "kf_pipeline_reset_async: null pipeline");
+    enqueue_reset(pipeline->impl);
   });
 }
 
@@ -663,6 +673,8 @@ kf_status kf_icp_normal_equations(kf_tracker* tracker, const kf_level_view* live
   return guarded([&] {
     require(tracker && live && model_points && model_normals && camera && model_world_to_camera && sums && count,
             "kf_icp_normal_equations: null argument");
+    require((live->vertices && live->normals) || static_cast<uint64_t>(live->width) * live->height == 0,
+            "kf_icp_normal_equations: null live vertex or normal map");
     Tracker& t = tracker->impl;
     IcpState* st = t.state.ptr;
     float cam[12], model[12];

@@ -979,6 +979,8 @@ extern "C" kf_status kf_icp_normal_equations_static(const kf_level_view* live, c
     require(live && model_points && model_normals && camera && model_world_to_camera && sums && count,
             "kf_icp_normal_equations_static: null argument");
     const uint64_t pixels = static_cast<uint64_t>(live->width) * live->height;
+    require((live->vertices && live->normals) || pixels == 0,
+            "kf_icp_normal_equations_static: null live vertex or normal map");
     if (pixels > kStaticMaxPixels) {
       throw InvalidArgument("kf_icp_normal_equations_static: the live image has " + std::to_string(pixels) +
                             " pixels; the static scratch holds sweeps of at most " +

@@ -173,8 +173,10 @@ class Pipeline:
         g = self.config.volume
         return g.res_x, g.res_y, g.res_z
 
-    def reset(self):
-        _check(lib().kf_pipeline_reset(self.handle))
+    def reset(self, wait: bool = True):
+        """Empty the volume; wait=False queues the refill on the pipeline's
+        stream and returns at once (kf_pipeline_reset_async)."""
+        _check(lib().kf_pipeline_reset(self.handle) if wait else lib().kf_pipeline_reset_async(self.handle))
 
     def integrate(self, depth, intrinsics, world_to_camera, color=None, normals=None):
         """Pipeline::integrate (pipeline.hpp:75-79); world_to_camera is a 4x4 or abi.Rigid."""

@@ -1,9 +1,10 @@
 """The allocation-free ICP sweep, kf_icp_normal_equations_static.
 
-Callers that cannot allocate device memory (code inside another framework's
-memory pool or a replayed CUDA graph, plug-ins whose host forbids cudaMalloc
-after start-up, real-time loops kept off the allocator) use this entry point:
-its scratch is a fixed device array instead of a tracker's buffers.  It must
+Callers that cannot allocate device memory (plug-ins whose host owns the
+GPU's memory through its own pool, hosts that forbid cudaMalloc after
+start-up, real-time loops kept off the allocator because it can stall the
+device) use this entry point: its scratch is a fixed device array instead of
+a tracker's buffers.  It must
 give the same normal equations as the allocating entry point,
 kf_icp_normal_equations, call after call.  This file sorts last so that a run
 stopping at the first failure has already run every other test.
@@ -84,12 +85,19 @@ def test_static_sweep_matches_allocating_sweep(scene, level):
 
 
 def test_static_sweep_rejects_oversized_images():
+    import torch  # device memory plumbing only
     lib = abi.load()
-    big = abi.LevelView(None, C.c_void_p(16), C.c_void_p(16), 4096, 4096, K640)
+    # One pixel past the limit, with real device maps of that size (zeros: no
+    # pixel would match), so the call stays in bounds even if it launched.
+    w, h = 1228801, 1
+    maps = [torch.zeros(w * h * 3, dtype=torch.float32, device="cuda") for _ in range(4)]
+    torch.cuda.synchronize()
+    big = abi.LevelView(None, C.c_void_p(maps[0].data_ptr()), C.c_void_p(maps[1].data_ptr()), w, h, K640)
     sums = np.zeros(29, dtype=np.float32)
     count = C.c_uint64()
     rigid = abi.rigid_from_matrix(np.eye(4))
-    status = lib.kf_icp_normal_equations_static(C.byref(big), C.c_void_p(16), C.c_void_p(16), 4096, 4096, K640,
+    status = lib.kf_icp_normal_equations_static(C.byref(big), C.c_void_p(maps[2].data_ptr()),
+                                                C.c_void_p(maps[3].data_ptr()), w, h, K640,
                                                 C.byref(rigid), C.byref(rigid), 0.05, 0.9,
                                                 sums.ctypes.data_as(C.c_void_p), C.byref(count))
     assert status == abi.KF_ERR_INVALID_ARGUMENT
