@@ -5,14 +5,15 @@
  * sm_100a kernels in kinectfusion_b200/: tests, the smoke check and the CPU
  * baseline leg of bench.py may call it; the product path never does.
  *
- * The reference's own CPU code cannot be compiled here: every translation
- * unit includes Eigen (Dependencies.cmake:16-22), which is not installed.
  * This file restates the host algorithms function by function, in IEEE
  * single precision with the reference's operation order (built with
  * -ffp-contract=off, like an x86-64 build without FMA), citing the reference
- * file:line each function follows.  The restatement is pinned against the
+ * file:line each function follows.  It is pinned two ways: against the
  * reference's own known-answer tests (test/tests.cpp), re-expressed in
- * tests/test_oracle_pins.py.
+ * tests/test_oracle_pins.py, and against the reference itself - its CPU
+ * translation units compiled from source with an Eigen stand-in
+ * (oracle/ref_build.sh -> oracle/_ref/libkf_ref.so) and compared on the same
+ * inputs in tests/test_oracle_vs_reference.py.
  */
 #ifndef KF_ORACLE_H
 #define KF_ORACLE_H
