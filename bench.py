@@ -677,66 +677,175 @@ def run_batch(args) -> dict:
             "clocks": clocks.summary()}
 
 
-# ---- CPU baseline (the oracle port, bounded sample) -----------------------------------------
-def cpu_baseline(seq, threads: int = 1, frames: int = 2) -> dict:
+# ---- CPU baseline (the reference's own host code, bounded sample) ----------------------------
+def cpu_baseline(seq, frames: int = 2) -> dict:
+    """The reference's host path on one core (oracle/_ref/libkf_ref.so, its
+    own sources compiled here; single-threaded by construction) over a
+    bounded sample: the first frame fused, then `frames` tracked frames of
+    the same 512^3 workload.  Falls back to the oracle port, also on one
+    core, when the library was not built."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import kf_oracle as ko
+    import kf_ref as kr
+    import kinectfusion_b200 as kf
     from kinectfusion_b200 import abi, synthetic
 
     k = abi.Intrinsics(synthetic.FX, synthetic.FY, synthetic.CX, synthetic.CY)
-    vol = ko.OracleVolume(RES, VOXEL, ORIGIN, TRUNC)
     pose = np.eye(4, dtype=np.float32)
-    args = (ko.depth_options(), ko.integration_options(), ko.raycast_options(), ko.icp_options())
-    ko.track_frame(vol, seq.depth[0], k, pose, *args, threads=threads, first=True)
+    if kr.available():
+        model = kr.RefPipeline(kf.pipeline_config(RES, VOXEL, ORIGIN, TRUNC, color=abi.KF_COLOR_NONE,
+                                                  rule=abi.KF_RULE_ANGLE_WEIGHTED))
+
+        def frame(i, first=False):
+            return model.track_frame(seq.depth[i], k, pose, ko.depth_options(), ko.icp_options(), first=first)[0]
+        kind, what = "reference", "the reference's own host code (oracle/_ref/libkf_ref.so), 1 thread"
+    else:
+        vol = ko.OracleVolume(RES, VOXEL, ORIGIN, TRUNC)
+        opts = (ko.depth_options(), ko.integration_options(), ko.raycast_options(), ko.icp_options())
+
+        def frame(i, first=False):
+            return ko.track_frame(vol, seq.depth[i], k, pose, *opts, threads=1, first=first)[0]
+        kind, what = "port", "the CPU oracle port, 1 thread (oracle/_ref was not built)"
+    pose = frame(0, True)
     t0 = time.perf_counter()
     for f in range(1, 1 + frames):
-        pose, _, _ = ko.track_frame(vol, seq.depth[f], k, pose, *args, threads=threads)
+        pose = frame(f)
     dt = time.perf_counter() - t0
-    return {"value": round(frames / dt, 4), "unit": "frames/s", "cores": threads, "kind": "port",
+    return {"value": round(frames / dt, 4), "unit": "frames/s", "cores": 1, "kind": kind,
             "host_cores": os.cpu_count(),
-            "sample": f"{frames} tracked frames of the same 512^3 workload (after one fused first frame) "
-                      f"on the CPU oracle, {threads} thread(s)"}
+            "sample": f"{frames} tracked frames of the same 512^3 workload (after one fused first frame), {what}"}
 
 
 # ---- reference arm -----------------------------------------------------------------------------
 def run_reference(args, rank: int) -> dict | None:
-    """The reference's CPU implementation of the path (the oracle port: the
-    reference's own sources need Eigen and other fetched dependencies that are
-    not installed) on all host cores."""
+    """The reference's CPU implementation of the path: its own host code
+    (src/kinectfusion/*.cpp compiled from source into oracle/_ref/libkf_ref.so
+    by oracle/ref_build.sh), driven frame by frame as
+    Reconstruction::process_frame does, on the same fresh 30-frame sequence
+    and 512^3 workload as our arm.  The reference's host path is
+    single-threaded by construction (plain loops, README.md:109-111), so it
+    runs on one core.  Each step is one frame (about 3.5 s); the run is
+    bounded to KF_REFERENCE_MAX_FRAMES frames in total (default 30).  Falls
+    back to the oracle port (kf_oracle.c) when the library was not built."""
     if rank != 0:
         return None
     sys.path.insert(0, str(ROOT / "oracle"))
     import kf_oracle as ko
+    import kf_ref as kr
+    import kinectfusion_b200 as kf
     from kinectfusion_b200 import abi, synthetic
 
-    threads = os.cpu_count() or 1
     seq = synthetic.make_sequence(seed=1000, frames=SEQ_FRAMES)
     k = abi.Intrinsics(synthetic.FX, synthetic.FY, synthetic.CX, synthetic.CY)
-    vol = ko.OracleVolume(RES, VOXEL, ORIGIN, TRUNC)
-    pose = np.eye(4, dtype=np.float32)
-    opts = (ko.depth_options(), ko.integration_options(), ko.raycast_options(), ko.icp_options())
-    ko.track_frame(vol, seq.depth[0], k, pose, *opts, threads=threads, first=True)
-    steps, warmup = args.steps, args.warmup
-    # bound the run to a few minutes: one frame is ~1-2 s on 8 cores
-    budget = int(os.environ.get("KF_REFERENCE_MAX_FRAMES", "40"))
+    steps, warmup = args.steps, max(1, args.warmup)
+    budget = int(os.environ.get("KF_REFERENCE_MAX_FRAMES", "30"))
     if steps + warmup > budget:
-        warmup = min(warmup, 3)
+        warmup = min(warmup, 2)
         steps = max(1, budget - warmup)
+    pose = np.eye(4, dtype=np.float32)
+    if kr.available():
+        kind, cores = "reference", 1
+        cfg = kf.pipeline_config(RES, VOXEL, ORIGIN, TRUNC, color=abi.KF_COLOR_NONE, rule=abi.KF_RULE_ANGLE_WEIGHTED)
+        model = kr.RefPipeline(cfg)
+
+        def frame(i: int, first: bool):
+            nonlocal pose
+            pose, _, _ = model.track_frame(seq.depth[i], k, pose, ko.depth_options(), ko.icp_options(), first=first)
+        what = "the reference's own host code (oracle/_ref/libkf_ref.so, compiled from its sources), 1 thread"
+    else:
+        kind, cores = "port", os.cpu_count() or 1
+        vol = ko.OracleVolume(RES, VOXEL, ORIGIN, TRUNC)
+        opts = (ko.depth_options(), ko.integration_options(), ko.raycast_options(), ko.icp_options())
+
+        def frame(i: int, first: bool):
+            nonlocal pose
+            pose, _, _ = ko.track_frame(vol, seq.depth[i], k, pose, *opts, threads=cores, first=first)
+        what = f"the CPU oracle port ({cores} OpenMP threads; oracle/_ref was not built)"
+    frame(0, True)  # the first frame is fused without tracking
     for s in range(1, 1 + warmup):
-        pose, _, _ = ko.track_frame(vol, seq.depth[frame_schedule(s)], k, pose, *opts, threads=threads)
+        frame(s, False)
     t0 = time.perf_counter()
     for s in range(steps):
-        pose, _, _ = ko.track_frame(vol, seq.depth[frame_schedule(1 + warmup + s)], k, pose, *opts, threads=threads)
+        frame((1 + warmup + s) % SEQ_FRAMES, False)
     dt = time.perf_counter() - t0
     fps = steps / dt
     return {"impl": "reference", "metric": METRIC, "value": round(fps, 4), "unit": "frames/s", "n_gpus": 0,
             "steps": steps, "warmup": warmup, "ms_per_step": round(dt / steps * 1e3, 2), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded analytic RGB-D scene)",
-            "config": {**workload_config(), "parallelism": f"cpu{threads}"},
-            "cpu_baseline": {"value": round(fps, 4), "unit": "frames/s", "cores": threads, "kind": "port",
-                             "sample": f"{steps} tracked frames of the 512^3 workload on the CPU oracle "
-                                       f"({threads} OpenMP threads)"},
+            "config": {**workload_config(), "parallelism": f"cpu{cores}"},
+            "cpu_baseline": {"value": round(fps, 4), "unit": "frames/s", "cores": cores, "kind": kind,
+                             "host_cores": os.cpu_count(),
+                             "sample": f"frames 1..{warmup + steps} of the first 30-frame sequence after its fused "
+                                       f"first frame ({warmup} untimed), {what}"},
             "e2e": {"value": round(fps, 4), "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def run_reference_cuda(args) -> dict:
+    """The reference's own CUDA pipeline on this GPU: src/kinectfusion/cuda/*.cu
+    built for sm_100a from its sources (oracle/_ref/libkf_ref_cuda.so), run as
+    its app's frame loop (Reconstruction::process_frame with --space cuda
+    --preload: host frames uploaded by its device pyramid source, its device
+    model renders, its device correspondence sweeps).  Timed by the host clock
+    around the loop, as the reference's own fps line is
+    (reconstruction.cpp:117-138), over the same fresh 30-frame passes as our
+    arm; every row also reports our arm's host-frame loop on the same frames
+    and clock for the ratio."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import kf_oracle as ko
+    import kf_ref as kr
+    import kinectfusion_b200 as kf
+    from kinectfusion_b200 import abi, synthetic
+
+    k = abi.Intrinsics(synthetic.FX, synthetic.FY, synthetic.CX, synthetic.CY)
+    passes = max(1, args.steps // SEQ_FRAMES)
+    seqs = [synthetic.make_sequence(seed=1000 + i, frames=SEQ_FRAMES) for i in range(min(passes, 4))]
+    rows = []
+    for name, color, device_solve in (("default (colour float, host solve)", abi.KF_COLOR_FLOAT, False),
+                                      ("--color none", abi.KF_COLOR_NONE, False),
+                                      ("--color none --icp-device-solve", abi.KF_COLOR_NONE, True)):
+        cfg = kf.pipeline_config(RES, VOXEL, ORIGIN, TRUNC, color=color, rule=abi.KF_RULE_ANGLE_WEIGHTED)
+        timings = {}
+        for impl in ("reference", "ours"):
+            total, frames, tracked = 0.0, 0, 0
+            for p in range(passes):
+                q = seqs[p % len(seqs)]
+                if impl == "reference":
+                    loop = kr.RefDevicePipeline(cfg, ko.depth_options(), ko.icp_options(), device_solve=device_solve)
+                    run = lambda f: loop.process(q.depth[f], k, q.color[f] if color == abi.KF_COLOR_FLOAT else None)[0]
+                    sync = kr.RefDevicePipeline.synchronize
+                else:
+                    loop = kf.Reconstruction(kf.Pipeline(cfg), k)
+                    run = lambda f: bool(loop.process(q.depth[f], q.color[f] if color == abi.KF_COLOR_FLOAT
+                                                      else None).tracked)
+                    sync = lambda: None  # process() returns after the frame's result is on the host
+                if p == 0:  # warm-up pass on the same pipeline object kind
+                    for f in range(3):
+                        run(f)
+                    sync()
+                    del loop
+                    loop = (kr.RefDevicePipeline(cfg, ko.depth_options(), ko.icp_options(), device_solve=device_solve)
+                            if impl == "reference" else kf.Reconstruction(kf.Pipeline(cfg), k))
+                sync()
+                t0 = time.perf_counter()
+                for f in range(SEQ_FRAMES):
+                    tracked += int(run(f))
+                sync()
+                total += time.perf_counter() - t0
+                frames += SEQ_FRAMES
+                del loop
+            timings[impl] = {"fps": round(frames / total, 1), "frames": frames, "tracked": tracked}
+        rows.append({"flags": name, "reference_cuda_fps": timings["reference"]["fps"],
+                     "ours_host_frames_fps": timings["ours"]["fps"],
+                     "ratio": round(timings["ours"]["fps"] / timings["reference"]["fps"], 2),
+                     "tracked": [timings["reference"]["tracked"], timings["ours"]["tracked"]],
+                     "frames": frames})
+    return {"metric": "frames/s, the reference's own CUDA pipeline on this B200 (640x480, 512^3)",
+            "value": rows[1]["reference_cuda_fps"], "unit": "frames/s", "n_gpus": 1, "steps": passes * SEQ_FRAMES,
+            "warmup": 3, "higher_is_better": True, "scaling": "none", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded analytic RGB-D scene)",
+            "config": {**workload_config(), "timing": "host clock around each fresh 30-frame pass (the reference's "
+                                                     "own fps line), host frames in, both implementations"},
+            "rows": rows}
 
 
 # The reference's published ablation rows (README.md:199-214, RTX 5080, TUM
@@ -960,6 +1069,66 @@ def run_compare(args) -> dict:
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),
     }
+
+
+def run_integrate(args) -> dict:
+    """The integration kernel alone on the headline geometry: one fresh dense
+    512^3 float volume (1 GiB, larger than L2; about 1.1 GB on the device in
+    all), the first 30-frame sequence integrated at its ground-truth poses
+    (pixel table, depth tiles, block culling, integrate_blocks_kernel,
+    stencil bits per frame), CUDA events around integrate_blocks_kernel only.
+    The small, single-pipeline entry point that ncu captures target."""
+    import torch
+
+    import kinectfusion_b200 as kf
+    from kinectfusion_b200 import abi, synthetic
+
+    lib = abi.load()
+    seq = synthetic.make_sequence(seed=1000, frames=SEQ_FRAMES)
+    k = abi.Intrinsics(synthetic.FX, synthetic.FY, synthetic.CX, synthetic.CY)
+    cfg = kf.pipeline_config(RES, VOXEL, ORIGIN, TRUNC, color=abi.KF_COLOR_NONE, rule=abi.KF_RULE_ANGLE_WEIGHTED)
+    pipe = kf.Pipeline(cfg)
+    sp = C.c_void_p()
+    abi.check(lib.kf_pipeline_stream(pipe.handle, C.byref(sp)))
+    stream = torch.cuda.ExternalStream(sp.value)
+    pyr = kf.PyramidSource()
+    normals = []
+    for f in range(SEQ_FRAMES):
+        pyr.build(seq.depth[f], k)
+        normals.append(pyr.download_level(0)["normals"])
+    ev_a, ev_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev_a.record(stream)
+    ev_b.record(stream)
+    abi.check(lib.kf_pipeline_set_kernel_events(pipe.handle, C.c_void_p(ev_a.cuda_event), C.c_void_p(ev_b.cuda_event)))
+    frames = min(max(args.steps, 1), SEQ_FRAMES)
+    ms, updates = [], []
+    for f in range(frames):
+        u0 = C.c_uint64()
+        abi.check(lib.kf_pipeline_update_counts(pipe.handle, C.byref(u0), None))
+        pipe.integrate(seq.depth[f], k, np.linalg.inv(seq.poses[f]), normals=normals[f])
+        u1 = C.c_uint64()
+        abi.check(lib.kf_pipeline_update_counts(pipe.handle, C.byref(u1), None))
+        ms.append(ev_a.elapsed_time(ev_b))
+        updates.append(u1.value - u0.value)
+    abi.check(lib.kf_pipeline_set_kernel_events(pipe.handle, None, None))
+    listed = C.c_uint64()
+    abi.check(lib.kf_pipeline_listed_blocks(pipe.handle, C.byref(listed)))
+    timed = slice(1, None) if frames > 1 else slice(None)
+    alg = float(np.mean(updates[timed])) * 16 + 640 * 480 * 14
+    kernel_s = float(np.mean(ms[timed])) / 1e3
+    peaks = measured_peaks()
+    achieved = alg / kernel_s / 1e9
+    return {"metric": "integrate_blocks_kernel GB/s of algorithmic traffic (640x480 into 512^3 float)",
+            "value": round(achieved, 1), "unit": "GB/s", "n_gpus": 1, "steps": frames, "warmup": 1,
+            "ms_per_step": round(kernel_s * 1e3, 4), "higher_is_better": True, "scaling": "none",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded analytic RGB-D scene)",
+            "config": {"workload": "one fresh dense 512^3 float volume, frames 0..N-1 of the first sequence "
+                                   "integrated at ground-truth poses, angle-weighted, colour off"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                         "frac": round(achieved / peaks.get("hbm_gbs", 6650.0), 4),
+                         "alg_bytes_per_launch": alg, "launch_ms": round(kernel_s * 1e3, 4)},
+            "per_frame_ms": [round(m, 4) for m in ms], "voxel_updates": updates,
+            "listed_blocks_last_frame": int(listed.value)}
 
 
 def run_gemm(args) -> dict:
@@ -1196,12 +1365,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
-    ap.add_argument("--config", choices=["cfg2", "batch16", "learned", "sparse", "ablations", "gemm", "compare"],
+    ap.add_argument("--config", choices=["cfg2", "batch16", "learned", "sparse", "ablations", "gemm", "compare",
+                                         "reference_cuda", "integrate"],
                     default="cfg2",
                     help="cfg2: the headline 512^3 workload (default); batch16: 16 sequences batched; "
                          "learned: the learned ICP warm start against constant velocity; sparse: cfg3, "
                          "a 2048^3 sparse domain; ablations: the reference's ablation flags; compare: a "
-                         "pipeline set compared every frame")
+                         "pipeline set compared every frame; reference_cuda: the reference's own CUDA "
+                         "pipeline timed on this GPU beside ours")
     ap.add_argument("--sparse-frames", type=int, default=300)
     ap.add_argument("--gemm-size", type=int, default=8192)
     ap.add_argument("--compare-res", type=int, default=RES)
@@ -1225,6 +1396,10 @@ def main():
         line = run_gemm(args) if rank == 0 else None
     elif args.config == "compare":
         line = run_compare(args) if rank == 0 else None
+    elif args.config == "reference_cuda":
+        line = run_reference_cuda(args) if rank == 0 else None
+    elif args.config == "integrate":
+        line = run_integrate(args) if rank == 0 else None
     else:
         if world > 1:
             import datetime

@@ -219,6 +219,10 @@ typedef struct {
   int32_t status[4];    /* per pyramid level, KF_ICP_* (index = level) */
   int32_t iterations[4];
   uint64_t correspondences[4];
+  /* the world_to_camera the frame was integrated at: the FP64 inverse of the
+   * tracked pose rounded to float (the reference inverts its float pose,
+   * reconstruction.cpp:274; the two agree to rounding) */
+  kf_rigid world_to_camera;
 } kf_frame_result;
 
 /* Welded triangle mesh (MarchingCubes::Mesh, marching_cubes.hpp:20-25). */
@@ -295,6 +299,13 @@ kf_status kf_pipeline_listed_blocks(kf_pipeline* pipeline, uint64_t* blocks);
 /* Sparse storage: the block-slot grid (BlockRep::grid, block_rep.hpp:26-110),
  * one uint32 per 8^3 block in x-major block order, 0xFFFFFFFF = unallocated. */
 kf_status kf_pipeline_download_block_grid(kf_pipeline* pipeline, uint32_t* grid, size_t count);
+/* The sparse block pool: capacity blocks of 512 raw voxels (slot order, each
+ * block's voxels z*64 + y*8 + x, the reference's SparseVolumeView pool layout,
+ * block_rep.hpp:93-100); `bytes` = capacity * 512 * voxel bytes.  With the
+ * block grid it is the whole sparse volume without a dense expansion (no
+ * reference counterpart: the reference exposes it only as host_view's dense
+ * staging copy). */
+kf_status kf_pipeline_download_pool(kf_pipeline* pipeline, void* voxels, size_t bytes);
 /* band-march backend: the dilated band bitmap the raycast reads
  * (BasicBandBitmap::view, occupancy.hpp:262-267), one bit per 8^3 block in
  * z-major order (((x * blocks_y) + y) * blocks_z + z), count =
@@ -364,8 +375,8 @@ kf_status kf_gemm_bf16(const void* a, const void* b, float* c, int32_t m, int32_
 /* ---- launch shapes and the autotuner (no counterpart in the reference) ----
  * Shapes that leave every output bit unchanged: the march kernel's CTA
  * (raycast_block_x * raycast_block_y <= 64 threads), the fusion grid, and
- * the lanes that march each ray together (1, 2 or 4; a warp then holds 32,
- * 16 or 8 rays) for renders of at most 20,000 rays, at most 80,000 rays,
+ * the lanes that march each ray together (1, 2, 4, 8, 16 or 32; a warp then
+ * holds 32 down to 1 rays) for renders of at most 20,000 rays, at most 80,000 rays,
  * and more.  Small renders have too few rays to fill the GPU one lane per
  * ray; with several lanes a ray takes up to that many samples per round. */
 typedef struct {

@@ -136,7 +136,8 @@ class IcpOutcome(C.Structure):
 
 class FrameResult(C.Structure):
     _fields_ = [("camera_to_world", Rigid), ("tracked", C.c_int32), ("status", C.c_int32 * 4),
-                ("iterations", C.c_int32 * 4), ("correspondences", C.c_uint64 * 4)]
+                ("iterations", C.c_int32 * 4), ("correspondences", C.c_uint64 * 4),
+                ("world_to_camera", Rigid)]
 
 
 class Mesh(C.Structure):
@@ -189,6 +190,7 @@ _PROTOTYPES = {
     "kf_pipeline_observed_voxel_count": (C.c_int, [P, C.POINTER(C.c_uint64)]),
     "kf_pipeline_download_volume": (C.c_int, [P, P, P, P]),
     "kf_pipeline_download_raw": (C.c_int, [P, P, C.c_size_t, P, C.c_size_t]),
+    "kf_pipeline_download_pool": (C.c_int, [P, P, C.c_size_t]),
     "kf_pipeline_extract_mesh": (C.c_int, [P, C.c_float, C.POINTER(Mesh)]),
     "kf_frame_kernel_count": (C.c_int, [P, C.POINTER(C.c_uint32)]),
     "kf_batch_create": (C.c_int, [P, P, P, C.c_uint32, C.POINTER(P)]),

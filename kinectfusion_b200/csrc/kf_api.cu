@@ -484,6 +484,17 @@ kf_status kf_pipeline_download_block_grid(kf_pipeline* pipeline, uint32_t* grid,
   });
 }
 
+kf_status kf_pipeline_download_pool(kf_pipeline* pipeline, void* voxels, size_t bytes) {
+  return guarded([&] {
+    require(pipeline != nullptr && voxels != nullptr, "kf_pipeline_download_pool: null argument");
+    Pipeline& p = pipeline->impl;
+    require(p.grid.count != 0, "kf_pipeline_download_pool: the pipeline is not sparse");
+    require(bytes == p.sparse_capacity * 512u * p.voxel_bytes, "kf_pipeline_download_pool: pool size mismatch");
+    check(cudaStreamSynchronize(p.stream), "pool download sync");
+    check(cudaMemcpy(voxels, p.voxels.ptr, bytes, cudaMemcpyDeviceToHost), "pool download");
+  });
+}
+
 kf_status kf_pipeline_download_band_bitmap(kf_pipeline* pipeline, uint32_t* words, size_t count) {
   return guarded([&] {
     require(pipeline != nullptr && words != nullptr, "kf_pipeline_download_band_bitmap: null argument");

@@ -245,6 +245,8 @@ void fill_result(const IcpState& st, int first, kf_frame_result* r) {
     r->camera_to_world.t[i] = static_cast<float>(st.pose[i * 4 + 3]);
   }
   r->tracked = st.failed ? 0 : 1;
+  std::memcpy(r->world_to_camera.r, st.world_to_camera, 9 * sizeof(float));
+  std::memcpy(r->world_to_camera.t, st.world_to_camera + 9, 3 * sizeof(float));
   for (int l = 0; l < 4; ++l) {
     r->status[l] = first ? KF_ICP_NOT_RUN : st.level_status[l];
     r->iterations[l] = first ? 0 : st.level_iterations[l];

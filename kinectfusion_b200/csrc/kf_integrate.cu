@@ -197,9 +197,53 @@ __global__ void cull_blocks_kernel(VolumeDev v, Rigid T, Intr k, const float* __
   if (keep) list[base + __popc(ballot & ((1u << lane) - 1u))] = block;
 }
 
+// The pixel lround(project(K, p)) of a camera point, as observe() picks it
+// (tsdf_integration.hpp:196-205), decided without the projection's two IEEE
+// divisions where that cannot change the answer: 1 = in the image at
+// (rx, ry), -1 = no pixel (behind the camera or outside the image), 0 = too
+// close to a rounding boundary (k + 0.5) to tell - the caller then runs the
+// exact quotient.  The estimate uses __fdividef (at most 2 ulp): below 2048
+// in magnitude it is within 1.3e-3 pixel of the exact value, so a margin of
+// 4e-3 pixel decides exactly; beyond that the point is outside any image
+// this path accepts (width and height up to 2048; wider images always take
+// the exact path).  Rounding to nearest even equals lround away from the
+// half-way points.
+__device__ __forceinline__ int pixel_estimate(const Intr& k, f3 p, uint32_t width, uint32_t height, uint32_t& rx,
+                                              uint32_t& ry) {
+  if (!(p.z > 0.0f)) return -1;
+  if (!(p.z >= 1e-6f) || width > 2048u || height > 2048u) return 0;
+  const float ax = __fdividef(k.fx * p.x, p.z) + k.cx;
+  const float ay = __fdividef(k.fy * p.y, p.z) + k.cy;
+  if (!(fabsf(ax) < 2048.0f && fabsf(ay) < 2048.0f)) return -1;
+  const float nx = rintf(ax), ny = rintf(ay);
+  if (fabsf(ax - nx) > 0.5f - 4e-3f || fabsf(ay - ny) > 0.5f - 4e-3f) return 0;
+  const int ix = __float2int_rn(nx), iy = __float2int_rn(ny);
+  if (static_cast<uint32_t>(ix) >= width || static_cast<uint32_t>(iy) >= height) return -1;
+  rx = static_cast<uint32_t>(ix);
+  ry = static_cast<uint32_t>(iy);
+  return 1;
+}
+
+// Where the projective sdf = d - |p| / lambda falls: -1 certainly below
+// -truncation (no update), +1 certainly at or above +truncation (the update
+// writes tsdf exactly 1), 0 undecided (the exact expression runs).  |p| and
+// the quotient are estimated with rsqrtf and __fdividef (relative error below
+// 1e-6 together); the margin is 1e-4 m plus 1e-6 of the distance, far above
+// that error.
+__device__ __forceinline__ int sdf_region(f3 p, float d, float lambda, float truncation) {
+  const float s2 = dot(p, p);
+  if (!(s2 > 1e-30f) || !(lambda >= 1.0f)) return 0;
+  const float dist = __fdividef(s2 * rsqrtf(s2), lambda);
+  const float est = d - dist;
+  const float margin = 1e-4f + 1e-6f * dist;
+  if (est < -truncation - margin) return -1;
+  if (est > truncation + margin) return 1;
+  return 0;
+}
+
 // Step 3: one CTA per listed block, four voxels (along z) per thread.
 template <int Kind, bool Color>
-__global__ void __launch_bounds__(kBlockThreads)
+__global__ void __launch_bounds__(kBlockThreads, 8)
     integrate_blocks_kernel(VolumeDev v, const float4* __restrict__ table, uint32_t width, uint32_t height, Intr k,
                             Rigid T, IntegParams ip, const IcpState* __restrict__ state,
                             const uint32_t* __restrict__ list, const unsigned* __restrict__ count,
@@ -214,6 +258,25 @@ __global__ void __launch_bounds__(kBlockThreads)
   }
   Raw* __restrict__ voxels = reinterpret_cast<Raw*>(v.voxels);
   const unsigned n = *count;
+  // Per block, two passes over its 512 voxels (thread t: x = t & 7,
+  // y = (t >> 3) & 7, z = 4 (t >> 6) + i, i < 4):
+  //  A. every voxel: camera point, pixel, table entry, and the sdf's region
+  //     from an error-bounded estimate (sdf_region).  Voxels certainly behind
+  //     the band are done; voxels certainly in front of it whose stored tsdf
+  //     is exactly 1 fuse to exactly 1 without a division.  Everything else
+  //     (including voxels whose pixel sits at a rounding boundary of the
+  //     estimate) goes to the block's queue in shared memory.
+  //  B. the queue, densely, one voxel per thread: the exact sdf and the
+  //     exact weighted average.
+  // Both passes set the voxel's bits in shared masks (bit v of the 512-bit
+  // masks, v = z * 64 + y * 8 + x), which the raycast's skip bits take
+  // afterwards.  The work per voxel is the host expression either way, so
+  // the stored bits are the same; the queue only keeps a warp's lanes busy
+  // with the voxels that need the long exact path.
+  __shared__ uint32_t s_fused[16], s_one[16];
+  __shared__ unsigned s_queued;
+  __shared__ uint16_t s_queue_voxel[512];
+  __shared__ float4 s_queue_table[512];
   const uint32_t lx = threadIdx.x & 7u, ly = (threadIdx.x >> 3) & 7u, lz = (threadIdx.x >> 6) * 4u;
   unsigned updates = 0, color_updates = 0;
   for (unsigned item = blockIdx.x; item < n; item += gridDim.x) {
@@ -221,87 +284,172 @@ __global__ void __launch_bounds__(kBlockThreads)
     // sparse volumes: listed blocks are allocated (SparseVolumeView::find_voxel)
     const uint32_t slot = v.grid != nullptr ? __ldg(v.grid + block) : block;
     const uint32_t bxi = block % v.bx, byi = (block / v.bx) % v.by, bzi = block / (v.bx * v.by);
-    const uint32_t x = bxi * 8 + lx, y = byi * 8 + ly;
-    uint32_t fused_z = 0;  // bit i: voxel z = lz + i fused this frame
-    uint32_t one_z = 0;    // bit i: voxel z = lz + i now observed with tsdf exactly 1
+    if (threadIdx.x < 16) {
+      s_fused[threadIdx.x] = 0u;
+      s_one[threadIdx.x] = 0u;
+    }
+    if (threadIdx.x == 0) s_queued = 0u;
+    __syncthreads();
+    Raw* __restrict__ brick = voxels + static_cast<size_t>(slot) * 512;
+    // ---- pass A ------------------------------------------------------------
+    {
+      const uint32_t x = bxi * 8 + lx, y = byi * 8 + ly;
+      f3 cp[4];
+      float4 tb[4];
+      uint32_t seen = 0;     // bit i: voxel i projects into the image
+      uint32_t unknown = 0;  // bit i: voxel i's pixel needs the exact quotient
+      // IntegrationContext::observe's pixel and table entry
+      // (tsdf_integration.hpp:183-205), the four gathers in flight together
 #pragma unroll
-    for (uint32_t i = 0; i < 4; ++i) {
-      const uint32_t z = bzi * 8 + lz + i;
-      if (x < v.rx && y < v.ry && z < v.rz) {
-        // IntegrationContext::observe (tsdf_integration.hpp:183-224)
-        const f3 cp = apply(T, cell_center(v, x, y, z));
-        if (cp.z > 0.0f) {
-          float px, py;
-          project(k, cp, px, py);
-          const long rx = lroundf(px), ry = lroundf(py);
-          if (rx >= 0 && ry >= 0 && rx < static_cast<long>(width) && ry < static_cast<long>(height)) {
-            const float4 tb = __ldg(table + (static_cast<size_t>(ry) * width + static_cast<size_t>(rx)));
-            const float sd = tb.x;
-            if (!isnan(sd)) {
-              const float truncation =
-                  ip.distance_scaled_truncation ? v.truncation + (ip.truncation_distance_scale * sd) : v.truncation;
-              const float sdf = ip.projective_distance ? sd - (norm(cp) / tb.y) : sd - cp.z;
-              const float ow = tb.z;
-              if (!(sdf < -truncation) && ow > 0.0f) {
-                const float tsdf = clampf(sdf / truncation, -1.0f, 1.0f);
-                // BasicVoxel::fused (volume.hpp:137-146)
-                const size_t index = static_cast<size_t>(slot) * 512 + brick_offset(x, y, z);
-                const Raw old = voxels[index];
-                const float t0 = VT::tsdf(old);
-                const float w0 = VT::weight(old);
-                const float avg = ((t0 * w0) + (tsdf * ow)) / (w0 + ow);
-                const float sum_w = w0 + ow;
-                const Raw fused = VT::encode(avg, ip.max_weight < sum_w ? ip.max_weight : sum_w);
-                voxels[index] = fused;
-                ++updates;
-                fused_z |= 1u << i;
-                if (VT::tsdf(fused) == 1.0f) one_z |= 1u << i;
-                if constexpr (Color) {
-                  if (ip.has_color && sdf <= truncation * 0.5f) {
-                    // ColorVoxel::fused (volume.hpp:160-170)
-                    ++color_updates;
-                    const float4 cv = v.colors[index];
-                    const f3 c = color_from_pixel(__float_as_uint(tb.w));
-                    const f3 avgc = ((make(cv.x, cv.y, cv.z) * cv.w) + (c * ow)) / (cv.w + ow);
-                    const float cw = cv.w + ow;
-                    v.colors[index] = make_float4(avgc.x, avgc.y, avgc.z, ip.max_weight < cw ? ip.max_weight : cw);
-                  }
-                }
-              }
-            }
+      for (uint32_t i = 0; i < 4; ++i) {
+        const uint32_t z = bzi * 8 + lz + i;
+        tb[i] = make_float4(kNaN, 0.0f, 0.0f, 0.0f);
+        cp[i] = make(0.0f, 0.0f, 0.0f);
+        if (x < v.rx && y < v.ry && z < v.rz) {
+          cp[i] = apply(T, cell_center(v, x, y, z));
+          uint32_t rx = 0, ry = 0;
+          const int pe = pixel_estimate(k, cp[i], width, height, rx, ry);
+          if (pe > 0) {
+            tb[i] = __ldg(table + (static_cast<size_t>(ry) * width + rx));
+            seen |= 1u << i;
+          } else if (pe == 0) {
+            unknown |= 1u << i;
           }
         }
       }
-    }
-    // ---- skip bits of the raycast ---------------------------------------
-    // Per voxel: `one` (observed with tsdf exactly 1) and `observed`.  A
-    // brick layer z is 16 bytes: words 4z, 4z+1 hold `one`, 4z+2, 4z+3 hold
-    // `observed`, bit (y & 3) * 8 + x of word (y >> 2).  A warp holds 32
-    // consecutive voxels of one layer half for each of its four z, i.e.
-    // exactly one word: ballots give the new bits of the voxels fused this
-    // frame, the other bits are kept.
-    if (voxel_bits == nullptr) continue;  // no skip structures (sparse storage)
-    uint32_t* bits = voxel_bits + static_cast<size_t>(block) * 32u;
-    const uint32_t half = (threadIdx.x >> 5) & 1u;
-    uint32_t changed = 0u;
+      // the sdf's region (tsdf_integration.hpp:206-224): -1 no update, 1 in
+      // front of the band (tsdf exactly 1), 0 needs the exact sdf
+      int region[4];
 #pragma unroll
-    for (uint32_t i = 0; i < 4; ++i) {
-      const uint32_t fused = __ballot_sync(0xFFFFFFFFu, (fused_z >> i) & 1u);
-      const uint32_t ones = __ballot_sync(0xFFFFFFFFu, (one_z >> i) & 1u);
-      if ((threadIdx.x & 31u) == 0 && fused != 0u) {
-        const uint32_t w = 4u * (lz + i) + half;
-        const uint32_t old_one = __ldcg(bits + w), old_obs = __ldcg(bits + w + 2u);
-        const uint32_t one = (old_one & ~fused) | (ones & fused);
-        const uint32_t obs = old_obs | fused;
-        if (one != old_one || obs != old_obs) {
-          bits[w] = one;
-          bits[w + 2u] = obs;
-          changed = 1u;
+      for (uint32_t i = 0; i < 4; ++i) {
+        region[i] = -1;
+        if (!((seen >> i) & 1u)) continue;
+        const float sd = tb[i].x;
+        if (isnan(sd) || !(tb[i].z > 0.0f)) continue;
+        const float truncation =
+            ip.distance_scaled_truncation ? v.truncation + (ip.truncation_distance_scale * sd) : v.truncation;
+        if (ip.projective_distance) {
+          region[i] = sdf_region(cp[i], sd, tb[i].y, truncation);
+        } else {
+          const float d = sd - cp[i].z;  // exact already
+          region[i] = d < -truncation ? -1 : (d >= truncation ? 1 : 0);
+        }
+      }
+      Raw old[4];
+#pragma unroll
+      for (uint32_t i = 0; i < 4; ++i) {
+        if (region[i] > 0) old[i] = brick[(lz + i) * 64u + ly * 8u + lx];
+      }
+#pragma unroll
+      for (uint32_t i = 0; i < 4; ++i) {
+        const uint32_t vi = (lz + i) * 64u + ly * 8u + lx;
+        if ((unknown >> i) & 1u) {
+          const unsigned q = atomicAdd(&s_queued, 1u);
+          s_queue_voxel[q] = static_cast<uint16_t>(vi | 0x4000u);
+          continue;
+        }
+        if (region[i] < 0) continue;
+        if (region[i] > 0 && VT::tsdf(old[i]) == 1.0f) {
+          // sdf >= truncation: clamp(sdf / truncation) is exactly 1, and
+          // (1 * w0 + 1 * ow) / (w0 + ow) is exactly 1 (BasicVoxel::fused,
+          // volume.hpp:137-146); no colour update (sdf > truncation / 2)
+          const float sum_w = VT::weight(old[i]) + tb[i].z;
+          const Raw fused = VT::encode(1.0f, ip.max_weight < sum_w ? ip.max_weight : sum_w);
+          brick[vi] = fused;
+          ++updates;
+          atomicOr(&s_fused[vi >> 5], 1u << (vi & 31u));
+          if (VT::tsdf(fused) == 1.0f) atomicOr(&s_one[vi >> 5], 1u << (vi & 31u));
+        } else {
+          const unsigned q = atomicAdd(&s_queued, 1u);
+          s_queue_voxel[q] = static_cast<uint16_t>(vi | (region[i] > 0 ? 0x8000u : 0u));
+          s_queue_table[q] = tb[i];
         }
       }
     }
-    if (__syncthreads_or(changed != 0u) && threadIdx.x == 0) {
-      atomicOr(dirty_bits + (block >> 5), 1u << (block & 31u));
+    __syncthreads();
+    // ---- pass B: the queued voxels, exact ----------------------------------
+    const unsigned queued = s_queued;
+    for (unsigned q = threadIdx.x; q < queued; q += kBlockThreads) {
+      const uint32_t tag = s_queue_voxel[q];
+      const uint32_t vi = tag & 0x1FFu;
+      const bool front = (tag & 0x8000u) != 0u;
+      const uint32_t x = bxi * 8 + (vi & 7u), y = byi * 8 + ((vi >> 3) & 7u), z = bzi * 8 + (vi >> 6);
+      const f3 cp = apply(T, cell_center(v, x, y, z));
+      float4 tb;
+      if (tag & 0x4000u) {
+        // the exact pixel (tsdf_integration.hpp:196-205) and its table entry
+        float px, py;
+        project(k, cp, px, py);
+        const long rx = lroundf(px), ry = lroundf(py);
+        if (!(rx >= 0 && ry >= 0 && rx < static_cast<long>(width) && ry < static_cast<long>(height))) continue;
+        tb = __ldg(table + (static_cast<size_t>(ry) * width + static_cast<size_t>(rx)));
+        if (isnan(tb.x) || !(tb.z > 0.0f)) continue;
+      } else {
+        tb = s_queue_table[q];
+      }
+      const float sd = tb.x, ow = tb.z;
+      const float truncation =
+          ip.distance_scaled_truncation ? v.truncation + (ip.truncation_distance_scale * sd) : v.truncation;
+      float tsdf = 1.0f, sdf = 0.0f;
+      if (!front) {
+        sdf = ip.projective_distance ? sd - (norm(cp) / tb.y) : sd - cp.z;
+        if (sdf < -truncation) continue;
+        tsdf = clampf(sdf / truncation, -1.0f, 1.0f);
+      }
+      // ClassicTsdf / AngleWeightedTsdf::update -> BasicVoxel::fused
+      // (tsdf_integration.hpp:287-342, volume.hpp:137-146)
+      const Raw old = brick[vi];
+      const float t0 = VT::tsdf(old);
+      const float w0 = VT::weight(old);
+      const float sum_w = w0 + ow;
+      const float avg = ((t0 * w0) + (tsdf * ow)) / sum_w;
+      const Raw fused = VT::encode(avg, ip.max_weight < sum_w ? ip.max_weight : sum_w);
+      brick[vi] = fused;
+      ++updates;
+      atomicOr(&s_fused[vi >> 5], 1u << (vi & 31u));
+      if (VT::tsdf(fused) == 1.0f) atomicOr(&s_one[vi >> 5], 1u << (vi & 31u));
+      if constexpr (Color) {
+        if (ip.has_color && !front && sdf <= truncation * 0.5f) {
+          // ColorVoxel::fused (volume.hpp:160-170)
+          ++color_updates;
+          float4* __restrict__ cbrick = v.colors + static_cast<size_t>(slot) * 512;
+          const float4 cv = cbrick[vi];
+          const f3 c = color_from_pixel(__float_as_uint(tb.w));
+          const f3 avgc = ((make(cv.x, cv.y, cv.z) * cv.w) + (c * ow)) / (cv.w + ow);
+          const float cw = cv.w + ow;
+          cbrick[vi] = make_float4(avgc.x, avgc.y, avgc.z, ip.max_weight < cw ? ip.max_weight : cw);
+        }
+      }
+    }
+    __syncthreads();
+    // ---- skip bits of the raycast ---------------------------------------
+    // Per voxel: `one` (observed with tsdf exactly 1) and `observed`.  A
+    // brick layer z is 16 bytes: words 4z, 4z+1 hold `one`, 4z+2, 4z+3 hold
+    // `observed`, bit (y & 3) * 8 + x of word (y >> 2) - mask word w of the
+    // shared masks is layer w >> 1, half w & 1.  The voxels fused this frame
+    // take their new bits, the others keep theirs.
+    if (voxel_bits != nullptr) {
+      uint32_t* bits = voxel_bits + static_cast<size_t>(block) * 32u;
+      uint32_t changed = 0u;
+      if (threadIdx.x < 16) {
+        const uint32_t fused = s_fused[threadIdx.x];
+        if (fused != 0u) {
+          const uint32_t w = 4u * (threadIdx.x >> 1) + (threadIdx.x & 1u);
+          const uint32_t old_one = __ldcg(bits + w), old_obs = __ldcg(bits + w + 2u);
+          const uint32_t one = (old_one & ~fused) | (s_one[threadIdx.x] & fused);
+          const uint32_t obs = old_obs | fused;
+          if (one != old_one || obs != old_obs) {
+            bits[w] = one;
+            bits[w + 2u] = obs;
+            changed = 1u;
+          }
+        }
+      }
+      if (__syncthreads_or(changed != 0u) && threadIdx.x == 0) {
+        atomicOr(dirty_bits + (block >> 5), 1u << (block & 31u));
+      }
+    } else {
+      __syncthreads();  // the masks and the queue are reused by the next block
     }
   }
   const unsigned total = __reduce_add_sync(0xFFFFFFFFu, updates);

@@ -44,12 +44,13 @@ struct RaycastParams {
 
 // Pixel tile of one warp that holds `rays` rays (lanes 0..rays-1; the other
 // lanes start done and lend themselves to the live rays' cooperative rounds):
-// 16 rays -> 4 x 4 pixels, 8 rays -> 4 x 2.  A CTA stacks its warps in y.
+// 16 rays -> 4 x 4 pixels, 8 -> 4 x 2, 4 -> 4 x 1, 2 -> 2 x 1, 1 -> 1 x 1.
+// A CTA stacks its warps in y.
 __device__ __forceinline__ void warp_tile_pixel(uint32_t rays, uint32_t& col, uint32_t& row, bool& has_ray) {
   const uint32_t tid = threadIdx.y * blockDim.x + threadIdx.x;
   const uint32_t warp = tid >> 5, lane = tid & 31u;
   const uint32_t warps = (blockDim.x * blockDim.y) >> 5;
-  const uint32_t tw = 4u, th = rays / 4u;
+  const uint32_t tw = rays < 4u ? rays : 4u, th = rays / tw;
   col = blockIdx.x * tw + (lane % tw);
   row = (blockIdx.y * warps + warp) * th + (lane / tw) % th;
   has_ray = lane < rays;
@@ -800,9 +801,10 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
   dim3 block(p.raycast_block_x, p.raycast_block_y);
   dim3 grid(ceil_div(cam.width, block.x), ceil_div(cam.height, block.y));
   if (rp.rays_per_warp < 32u) {
-    // two warps per CTA, each a 4 x (rays / 4) pixel tile
+    // two warps per CTA, each a tw x th pixel tile (warp_tile_pixel)
+    const uint32_t tw = rp.rays_per_warp < 4u ? rp.rays_per_warp : 4u, th = rp.rays_per_warp / tw;
     block = dim3(64, 1);
-    grid = dim3(ceil_div(cam.width, 4u), ceil_div(cam.height, 2u * (rp.rays_per_warp / 4u)));
+    grid = dim3(ceil_div(cam.width, tw), ceil_div(cam.height, 2u * th));
   }
   // the skip structures exist once a full-sweep integration prepared them
   const uint32_t* voxel_bits = p.brick_class.count && p.view.grid == nullptr ? p.voxel_bits.ptr : nullptr;

@@ -81,8 +81,8 @@ void validate(const kf_launch_shapes& s) {
           "Raycast CTA shape must have 1..64 threads");
   require(s.integrate_ctas > 0 && s.integrate_ctas <= 65535u, "Fusion grid must have 1..65535 CTAs");
   for (int i = 0; i < 3; ++i) {
-    require(s.raycast_lanes[i] == 1 || s.raycast_lanes[i] == 2 || s.raycast_lanes[i] == 4,
-            "Lanes per ray must be 1, 2 or 4");
+    const uint32_t l = s.raycast_lanes[i];
+    require(l >= 1 && l <= 32 && (l & (l - 1)) == 0, "Lanes per ray must be 1, 2, 4, 8, 16 or 32");
   }
 }
 
@@ -144,7 +144,7 @@ kf_status kf_pipeline_autotune(kf_pipeline* pipeline, const uint16_t* frames, ui
     }
     // lanes per ray of each render-size class (one class at a time)
     for (int cls = 0; cls < 3; ++cls) {
-      for (uint32_t lanes : {1u, 2u, 4u}) {
+      for (uint32_t lanes : {1u, 2u, 4u, 8u, 16u, 32u}) {
         if (lanes == best.raycast_lanes[cls]) continue;
         kf_launch_shapes c = best;
         c.raycast_lanes[cls] = lanes;

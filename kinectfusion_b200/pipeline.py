@@ -234,6 +234,17 @@ class Pipeline:
         _check(lib().kf_pipeline_download_raw(self.handle, _ptr(raw), raw.nbytes, None, 0))
         return raw
 
+    def download_pool(self) -> np.ndarray:
+        """Sparse storage: the raw block pool, (capacity, 512) voxels in slot
+        order (kf_pipeline_download_pool)."""
+        _, capacity = self.block_stats()
+        if self.config.voxel == abi.KF_VOXEL_FLOAT:
+            raw = np.empty((capacity, 512, 2), dtype=np.float32)
+        else:
+            raw = np.empty((capacity, 512), dtype=np.uint32)
+        _check(lib().kf_pipeline_download_pool(self.handle, _ptr(raw), raw.nbytes))
+        return raw
+
     def launch_shapes(self) -> abi.LaunchShapes:
         shapes = abi.LaunchShapes()
         _check(lib().kf_pipeline_get_launch_shapes(self.handle, C.byref(shapes)))

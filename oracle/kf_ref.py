@@ -223,3 +223,107 @@ def icp_estimate(live_v, live_n, model_p, model_n, k, model_camera_to_world, ini
                                    C.byref(k), C.byref(_rigid(model_camera_to_world)), C.byref(_rigid(initial)),
                                    iterations, C.byref(options), C.byref(out)))
     return out
+
+
+# ---- the reference's CUDA pipeline (libkf_ref_cuda.so) --------------------------------------
+LIB_CUDA = HERE / "_ref" / "libkf_ref_cuda.so"
+_lib_cuda = None
+
+
+def cuda_available() -> bool:
+    return LIB_CUDA.exists()
+
+
+def load_cuda() -> C.CDLL:
+    """The reference built with its CUDA path (src/kinectfusion/cuda/*.cu for
+    sm_100a).  Loaded into its own handle; it shares no state with the
+    host-only library."""
+    global _lib_cuda
+    if _lib_cuda is not None:
+        return _lib_cuda
+    if not LIB_CUDA.exists():
+        raise FileNotFoundError(f"{LIB_CUDA} is not built")
+    lib = C.CDLL(str(LIB_CUDA))
+    sig = {
+        "kfr_last_error": (C.c_char_p, []),
+        "kfr_dev_available": (C.c_int, []),
+        "kfr_dev_create": (C.c_int, [C.POINTER(abi.PipelineConfig), C.POINTER(abi.DepthOptions),
+                                     C.POINTER(abi.IcpOptions), C.c_int32, C.c_int32, C.POINTER(P)]),
+        "kfr_dev_destroy": (None, [P]),
+        "kfr_dev_frame": (C.c_int, [P, P, P, C.c_uint32, C.c_uint32, C.POINTER(abi.Intrinsics), P, C.c_int32,
+                                    C.POINTER(abi.Rigid), C.POINTER(C.c_int32), P]),
+        "kfr_dev_raycast": (C.c_int, [P, C.POINTER(abi.Intrinsics), C.c_uint32, C.c_uint32, C.POINTER(abi.Rigid),
+                                      P, P, P]),
+        "kfr_dev_host_view": (C.c_int, [P, P]),
+        "kfr_dev_observed": (C.c_uint64, [P]),
+        "kfr_dev_synchronize": (C.c_int, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype, fn.argtypes = res, args
+    _lib_cuda = lib
+    return lib
+
+
+def _check_cuda(rc: int):
+    if rc != 0:
+        raise RuntimeError("reference (CUDA): " + load_cuda().kfr_last_error().decode())
+
+
+class RefDevicePipeline:
+    """The reference's --space cuda pipeline (Pipeline::create with
+    MemorySpace::kDevice, the device PyramidSource, ProjectiveIcpTracker) run
+    frame by frame as Reconstruction::process_frame does.  device_solve and
+    capture_graph are its --icp-device-solve / --icp-capture-graph switches."""
+
+    def __init__(self, config: abi.PipelineConfig, depth_options: abi.DepthOptions, icp_options: abi.IcpOptions,
+                 device_solve: bool = False, capture_graph: bool = False, iterations=(10, 5, 4)):
+        lib = load_cuda()
+        h = C.c_void_p()
+        _check_cuda(lib.kfr_dev_create(C.byref(config), C.byref(depth_options), C.byref(icp_options),
+                                       int(device_solve), int(capture_graph), C.byref(h)))
+        self.handle = h
+        self.config = config
+        self.iterations = np.array(list(iterations) + [4] * (4 - len(iterations)), dtype=np.uint32)
+        self.pose = abi.rigid_from_matrix(np.eye(4))
+        self.frames = 0
+        self.trajectory = []
+
+    def __del__(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            load_cuda().kfr_dev_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def process(self, depth, intrinsics, color=None):
+        depth = np.ascontiguousarray(depth, dtype=np.uint16)
+        color = None if color is None else np.ascontiguousarray(color, dtype=np.uint32)
+        tracked = C.c_int32()
+        status = np.zeros(4, np.int32)
+        _check_cuda(load_cuda().kfr_dev_frame(self.handle, _ptr(depth), _ptr(color), depth.shape[1], depth.shape[0],
+                                              C.byref(intrinsics), _ptr(self.iterations), 1 if self.frames == 0 else 0,
+                                              C.byref(self.pose), C.byref(tracked), _ptr(status)))
+        self.frames += 1
+        self.trajectory.append(abi.matrix_from_rigid(self.pose))
+        return bool(tracked.value), status
+
+    def raycast(self, k, width, height, camera_to_world):
+        points = np.zeros((height, width, 3), np.float32)
+        normals = np.zeros((height, width, 3), np.float32)
+        colors = np.zeros((height, width), np.uint32)
+        _check_cuda(load_cuda().kfr_dev_raycast(self.handle, C.byref(k), width, height,
+                                                C.byref(_rigid(camera_to_world)), _ptr(points), _ptr(normals),
+                                                _ptr(colors)))
+        return points, normals, colors
+
+    def host_view(self) -> np.ndarray:
+        g = self.config.volume
+        out = np.zeros((g.res_x * g.res_y * g.res_z, 2), np.float32)
+        _check_cuda(load_cuda().kfr_dev_host_view(self.handle, _ptr(out)))
+        return out
+
+    def observed_voxel_count(self) -> int:
+        return int(load_cuda().kfr_dev_observed(self.handle))
+
+    @staticmethod
+    def synchronize():
+        _check_cuda(load_cuda().kfr_dev_synchronize())

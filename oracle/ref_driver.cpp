@@ -321,8 +321,13 @@ class IcpConsumer final : public kf::TrackingSurfaceConsumer {
   void consume(const kf::HostTrackingSurfaces& surfaces) override {
     outcome_ = tracker_.estimate_pose(surfaces, intrinsics_, pose_, iterations_);
   }
-  void consume(const kf::DeviceTrackingSurfaces&) override {
-    throw std::logic_error("host surfaces only");
+  void consume(const kf::DeviceTrackingSurfaces& surfaces) override {
+#ifdef KF_REF_CUDA
+    outcome_ = tracker_.estimate_pose(surfaces, intrinsics_, pose_, iterations_);
+#else
+    (void)surfaces;
+    throw std::logic_error("host surfaces only: this build has no CUDA path");
+#endif
   }
   const kf::IcpOutcome& outcome() const { return outcome_; }
 
@@ -564,3 +569,148 @@ int kfr_track_frame(kfr_pipeline* p, const uint16_t* depth, const uint32_t* colo
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The reference's own CUDA pipeline (built only into libkf_ref_cuda.so, with
+// the reference's src/kinectfusion/cuda/*.cu): Pipeline::create with
+// MemorySpace::kDevice (device_pipeline.cu), the device PyramidSource
+// (depth_processing.cu) and ProjectiveIcpTracker's device correspondence
+// sweep, driven by the loop of Reconstruction::process_frame.  Used to time
+// the reference's GPU path on the same GPU and to compare outputs.
+#ifdef KF_REF_CUDA
+#include <cuda_runtime_api.h>
+
+struct kfr_device {
+  kf::PipelineConfig config;
+  std::unique_ptr<kf::Pipeline> pipeline;
+  std::unique_ptr<kf::PyramidSource> pyramid;
+  std::unique_ptr<kf::ProjectiveIcpTracker> tracker;
+  kf::image_proc::DepthImage depth;
+  kf::image_proc::ColorImage color;
+};
+
+extern "C" {
+
+int kfr_dev_available(void) {
+  int count = 0;
+  return cudaGetDeviceCount(&count) == cudaSuccess && count > 0 ? 1 : 0;
+}
+
+// device_solve / capture_graph: the reference's --icp-device-solve and
+// --icp-capture-graph switches (app_options.cpp:138-141).
+int kfr_dev_create(const kf_pipeline_config* config, const kf_depth_options* depth_options,
+                   const kf_icp_options* icp_options, int32_t device_solve, int32_t capture_graph, kfr_device** out) {
+  return guarded([&] {
+    auto d = std::make_unique<kfr_device>();
+    d->config = to_config(*config);
+    d->config.space = kf::MemorySpace::kDevice;
+    kf::Pipeline::Creation creation = kf::Pipeline::create(d->config);
+    if (creation.space != kf::MemorySpace::kDevice) {
+      throw std::runtime_error("reference device pipeline unavailable: " + creation.fallback_reason);
+    }
+    d->pipeline = std::move(creation.pipeline);
+    kf::PyramidSource::Creation pyr = kf::PyramidSource::create(kf::MemorySpace::kDevice,
+                                                                to_depth_options(*depth_options));
+    if (!pyr.fallback_reason.empty()) throw std::runtime_error(pyr.fallback_reason);
+    d->pyramid = std::move(pyr.source);
+    kf::ProjectiveIcpOptions icp = to_icp_options(*icp_options);
+    icp.device_solve = device_solve != 0;
+    icp.device_graph_build = capture_graph ? kf::IcpGraphBuild::kCaptured : kf::IcpGraphBuild::kExplicit;
+    d->tracker = std::make_unique<kf::ProjectiveIcpTracker>(icp);
+    *out = d.release();
+  });
+}
+
+void kfr_dev_destroy(kfr_device* d) { delete d; }
+
+// One frame of Reconstruction::process_frame on the reference's device path
+// (reconstruction.cpp:184-277): the host frame is uploaded by the device
+// pyramid source, each level renders the model on the device and tracks
+// (host or device solve), the frame is integrated from the pyramid's upload.
+int kfr_dev_frame(kfr_device* d, const uint16_t* depth, const uint32_t* color, uint32_t width, uint32_t height,
+                  const kf_intrinsics* intrinsics, const uint32_t* iterations_per_level, int32_t first,
+                  kf_rigid* pose, int32_t* tracked, int32_t* level_status) {
+  return guarded([&] {
+    if (d->depth.width() != width || d->depth.height() != height) {
+      d->depth = kf::image_proc::DepthImage{width, height};
+      d->color = kf::image_proc::ColorImage{width, height};
+    }
+    std::memcpy(d->depth.data().data(), depth, static_cast<std::size_t>(width) * height * sizeof(uint16_t));
+    if (color != nullptr) {
+      std::memcpy(d->color.data().data(), color, static_cast<std::size_t>(width) * height * sizeof(uint32_t));
+    }
+    const kf::CameraIntrinsics k = to_intrinsics(*intrinsics);
+    const std::size_t levels = d->pyramid->build(d->depth, k);
+    Eigen::Matrix4f camera_to_world = to_matrix(*pose);
+    for (int l = 0; l < 4; ++l) level_status[l] = KF_ICP_NOT_RUN;
+    bool ok = levels > 0;
+    if (!first && ok) {
+      Eigen::Matrix4f tracked_pose = camera_to_world;
+      for (std::size_t level_index = levels; level_index-- > 0;) {
+        const unsigned int scale = 1U << level_index;
+        const kf::RaycastCamera camera{.intrinsics = k.scaled(static_cast<unsigned int>(level_index)),
+                                       .width = width / scale,
+                                       .height = height / scale,
+                                       .camera_to_world = tracked_pose};
+        const kf::PyramidLevel level = d->pyramid->level(level_index);
+        IcpConsumer consumer{*d->tracker, level.intrinsics, tracked_pose, iterations_per_level[level_index]};
+        d->pipeline->track(camera, level, consumer);
+        const kf::IcpOutcome& outcome = consumer.outcome();
+        level_status[level_index] = status_of(outcome);
+        tracked_pose = outcome.pose;
+        if (!outcome.result) {
+          ok = false;
+          break;
+        }
+      }
+      camera_to_world = tracked_pose;
+    }
+    if (ok) {
+      kf::DepthFrame frame{.depth = &d->depth,
+                           .color = color != nullptr ? &d->color : nullptr,
+                           .normals = d->pyramid->host_normals(),
+                           .intrinsics = k};
+      const kf::DeviceDepthFrame* upload = d->pyramid->device_frame(frame);
+      frame.world_to_camera = camera_to_world.inverse();
+      d->pipeline->integrate(frame, upload);
+    }
+    *pose = to_rigid(camera_to_world);
+    *tracked = ok ? 1 : 0;
+  });
+}
+
+int kfr_dev_raycast(kfr_device* d, const kf_intrinsics* intrinsics, uint32_t width, uint32_t height,
+                    const kf_rigid* camera_to_world, float* points, float* normals, uint32_t* colors) {
+  return guarded([&] {
+    const kf::RaycastCamera camera{.intrinsics = to_intrinsics(*intrinsics),
+                                   .width = width,
+                                   .height = height,
+                                   .camera_to_world = to_matrix(*camera_to_world)};
+    const kf::SurfaceMaps maps = d->pipeline->raycast(camera);
+    copy_vec3_image(maps.points, points);
+    copy_vec3_image(maps.normals, normals);
+    if (colors != nullptr) {
+      std::memcpy(colors, maps.colors.data().data(), maps.colors.data().size() * sizeof(uint32_t));
+    }
+  });
+}
+
+// Pipeline::host_view: the dense float (tsdf, weight) volume, x fastest.
+int kfr_dev_host_view(kfr_device* d, float* voxels) {
+  return guarded([&] {
+    std::optional<kf::HostVolume> staging;
+    const kf::ConstHostVolumeView v = d->pipeline->host_view(staging);
+    std::memcpy(voxels, v.voxels, v.voxel_count() * sizeof(kf::Voxel));
+  });
+}
+
+uint64_t kfr_dev_observed(const kfr_device* d) { return d->pipeline->observed_voxel_count(); }
+
+int kfr_dev_synchronize(void) {
+  return guarded([&] {
+    if (cudaDeviceSynchronize() != cudaSuccess) throw std::runtime_error("cudaDeviceSynchronize failed");
+  });
+}
+
+}  // extern "C"
+#endif  // KF_REF_CUDA

@@ -25,6 +25,7 @@ def test_struct_sizes_match_header_layout():
     assert C.sizeof(abi.Intrinsics) == 16
     assert C.sizeof(abi.VolumeGeometry) == 32
     assert C.sizeof(abi.FrameView) == 8 * 3 + 8 + 16 + 48 + 4 + 4
+    assert C.sizeof(abi.FrameResult) == 48 + 4 + 16 + 16 + 4 + 32 + 48  # 4 B of padding before the u64s
 
 
 def test_defaults_mirror_reference():
