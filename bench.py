@@ -785,11 +785,13 @@ def run_reference_cuda(args) -> dict:
     built for sm_100a from its sources (oracle/_ref/libkf_ref_cuda.so), run as
     its app's frame loop (Reconstruction::process_frame with --space cuda
     --preload: host frames uploaded by its device pyramid source, its device
-    model renders, its device correspondence sweeps).  Timed by the host clock
-    around the loop, as the reference's own fps line is
-    (reconstruction.cpp:117-138), over the same fresh 30-frame passes as our
-    arm; every row also reports our arm's host-frame loop on the same frames
-    and clock for the ratio."""
+    model renders, its device correspondence sweeps).  Beside it, on the same
+    frames and clock: the same reference loop with its device seams taken by
+    this project's drop-in glue (kinectfusion_b200/glue/b200_backend.cpp over
+    libkf_b200.so, oracle/_ref/libkf_ref_b200.so) and this project's own
+    host-frame loop (kf_frame_process).  Timed by the host clock around each
+    fresh 30-frame pass, as the reference's own fps line is
+    (reconstruction.cpp:117-138)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import kf_oracle as ko
     import kf_ref as kr
@@ -799,52 +801,72 @@ def run_reference_cuda(args) -> dict:
     k = abi.Intrinsics(synthetic.FX, synthetic.FY, synthetic.CX, synthetic.CY)
     passes = max(1, args.steps // SEQ_FRAMES)
     seqs = [synthetic.make_sequence(seed=1000 + i, frames=SEQ_FRAMES) for i in range(min(passes, 4))]
+
+    class Ours:
+        def __init__(self, cfg):
+            self.loop = kf.Reconstruction(kf.Pipeline(cfg), k)
+
+        def process(self, depth, color):
+            return bool(self.loop.process(depth, color).tracked)
+
+        def synchronize(self):
+            pass  # process() returns after the frame's result is on the host
+
+    class Reference:
+        def __init__(self, cfg, backend, device_solve):
+            self.loop = kr.RefDevicePipeline(cfg, ko.depth_options(), ko.icp_options(), device_solve=device_solve,
+                                             backend=backend)
+
+        def process(self, depth, color):
+            return self.loop.process(depth, k, color)[0]
+
+        def synchronize(self):
+            self.loop.synchronize()
+
     rows = []
     for name, color, device_solve in (("default (colour float, host solve)", abi.KF_COLOR_FLOAT, False),
                                       ("--color none", abi.KF_COLOR_NONE, False),
                                       ("--color none --icp-device-solve", abi.KF_COLOR_NONE, True)):
         cfg = kf.pipeline_config(RES, VOXEL, ORIGIN, TRUNC, color=color, rule=abi.KF_RULE_ANGLE_WEIGHTED)
+        makers = {"reference_cuda": lambda: Reference(cfg, "cuda", device_solve),
+                  "reference_over_glue": lambda: Reference(cfg, "glue", device_solve),
+                  "ours": lambda: Ours(cfg)}
         timings = {}
-        for impl in ("reference", "ours"):
+        for impl, make in makers.items():
+            if impl == "reference_over_glue" and not kr.cuda_available("glue"):
+                continue
+            warm = make()  # warm-up pass of three frames on a throwaway instance
+            for f in range(3):
+                warm.process(seqs[0].depth[f], seqs[0].color[f] if color == abi.KF_COLOR_FLOAT else None)
+            warm.synchronize()
+            del warm
             total, frames, tracked = 0.0, 0, 0
             for p in range(passes):
                 q = seqs[p % len(seqs)]
-                if impl == "reference":
-                    loop = kr.RefDevicePipeline(cfg, ko.depth_options(), ko.icp_options(), device_solve=device_solve)
-                    run = lambda f: loop.process(q.depth[f], k, q.color[f] if color == abi.KF_COLOR_FLOAT else None)[0]
-                    sync = kr.RefDevicePipeline.synchronize
-                else:
-                    loop = kf.Reconstruction(kf.Pipeline(cfg), k)
-                    run = lambda f: bool(loop.process(q.depth[f], q.color[f] if color == abi.KF_COLOR_FLOAT
-                                                      else None).tracked)
-                    sync = lambda: None  # process() returns after the frame's result is on the host
-                if p == 0:  # warm-up pass on the same pipeline object kind
-                    for f in range(3):
-                        run(f)
-                    sync()
-                    del loop
-                    loop = (kr.RefDevicePipeline(cfg, ko.depth_options(), ko.icp_options(), device_solve=device_solve)
-                            if impl == "reference" else kf.Reconstruction(kf.Pipeline(cfg), k))
-                sync()
+                loop = make()
+                loop.synchronize()
                 t0 = time.perf_counter()
                 for f in range(SEQ_FRAMES):
-                    tracked += int(run(f))
-                sync()
+                    tracked += int(loop.process(q.depth[f], q.color[f] if color == abi.KF_COLOR_FLOAT else None))
+                loop.synchronize()
                 total += time.perf_counter() - t0
                 frames += SEQ_FRAMES
                 del loop
-            timings[impl] = {"fps": round(frames / total, 1), "frames": frames, "tracked": tracked}
-        rows.append({"flags": name, "reference_cuda_fps": timings["reference"]["fps"],
-                     "ours_host_frames_fps": timings["ours"]["fps"],
-                     "ratio": round(timings["ours"]["fps"] / timings["reference"]["fps"], 2),
-                     "tracked": [timings["reference"]["tracked"], timings["ours"]["tracked"]],
-                     "frames": frames})
+            timings[impl] = {"fps": round(frames / total, 1), "tracked": tracked}
+        row = {"flags": name, "frames": frames,
+               **{f"{impl}_fps": t["fps"] for impl, t in timings.items()},
+               "tracked": {impl: t["tracked"] for impl, t in timings.items()},
+               "ours_over_reference_cuda": round(timings["ours"]["fps"] / timings["reference_cuda"]["fps"], 2)}
+        if "reference_over_glue" in timings:
+            row["glue_over_reference_cuda"] = round(timings["reference_over_glue"]["fps"] /
+                                                    timings["reference_cuda"]["fps"], 2)
+        rows.append(row)
     return {"metric": "frames/s, the reference's own CUDA pipeline on this B200 (640x480, 512^3)",
             "value": rows[1]["reference_cuda_fps"], "unit": "frames/s", "n_gpus": 1, "steps": passes * SEQ_FRAMES,
             "warmup": 3, "higher_is_better": True, "scaling": "none", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded analytic RGB-D scene)",
             "config": {**workload_config(), "timing": "host clock around each fresh 30-frame pass (the reference's "
-                                                     "own fps line), host frames in, both implementations"},
+                                                     "own fps line), host frames in, every implementation"},
             "rows": rows}
 
 

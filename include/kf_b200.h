@@ -260,6 +260,11 @@ kf_status kf_pyramid_build(kf_pyramid* pyramid, const uint16_t* depth, uint32_t 
                            uint32_t* level_count);
 /* PyramidSource::level (depth_processing.hpp:437): device views, valid until the next build. */
 kf_status kf_pyramid_level(const kf_pyramid* pyramid, uint32_t index, kf_level_view* out);
+/* The unfiltered depth of the last build on the device (width*height u16,
+ * valid until the next build): the upload PyramidSource::device_frame hands
+ * to integration so the frame crosses to the device once
+ * (depth_processing.hpp:451-453, depth_processing.cu:149-157). */
+kf_status kf_pyramid_raw_depth(const kf_pyramid* pyramid, const uint16_t** depth);
 /* Host copies of one level (any pointer may be NULL). */
 kf_status kf_pyramid_download_level(const kf_pyramid* pyramid, uint32_t index, uint16_t* depth,
                                     float* vertices, float* normals);
@@ -404,6 +409,24 @@ kf_status kf_tracker_destroy(kf_tracker* tracker);
 kf_status kf_pipeline_track(kf_pipeline* pipeline, kf_tracker* tracker,
                             const kf_raycast_camera* camera, const kf_level_view* live,
                             uint32_t iterations, kf_icp_outcome* outcome);
+/* The model render of Pipeline::track (pipeline.hpp:83-85,
+ * device_pipeline.cu:133-136): the volume raycast at `camera` into the
+ * pipeline's cached device maps of that extent; `out` receives their device
+ * views (KF_MEMORY_DEVICE), valid until the next render of the same extent. */
+kf_status kf_pipeline_render_model(kf_pipeline* pipeline, const kf_raycast_camera* camera,
+                                   kf_surface_maps* out);
+/* The whole-level device Gauss-Newton loop over given device maps
+ * (BasicDeviceCorrespondenceSweep::run_loop, icp_correspondence.hpp:366-369,
+ * icp_correspondence.cu:397-439): `iterations` steps from
+ * initial_camera_to_world against the model rendered with model_intrinsics
+ * at model_world_to_camera's inverse, with the tracker's options, one host
+ * sync at the end.  sums (29 floats, may be NULL) receives the normal
+ * equations of the last step. */
+kf_status kf_icp_level(kf_tracker* tracker, const kf_level_view* live, const float* model_points,
+                       const float* model_normals, uint32_t model_width, uint32_t model_height,
+                       kf_intrinsics model_intrinsics, const kf_rigid* model_world_to_camera,
+                       const kf_rigid* initial_camera_to_world, uint32_t iterations, kf_icp_outcome* outcome,
+                       float* sums);
 /* One correspondence sweep (BasicDeviceCorrespondenceSweep::run,
  * icp_correspondence.cu:572-597): fills sums[29] (21 JtJ + 6 Jtr + distance
  * sum + squared residual sum) and the match count.  Device views. */

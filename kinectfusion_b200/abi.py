@@ -191,6 +191,10 @@ _PROTOTYPES = {
     "kf_pipeline_download_volume": (C.c_int, [P, P, P, P]),
     "kf_pipeline_download_raw": (C.c_int, [P, P, C.c_size_t, P, C.c_size_t]),
     "kf_pipeline_download_pool": (C.c_int, [P, P, C.c_size_t]),
+    "kf_pyramid_raw_depth": (C.c_int, [P, C.POINTER(C.c_void_p)]),
+    "kf_pipeline_render_model": (C.c_int, [P, C.POINTER(RaycastCamera), C.POINTER(SurfaceMapsView)]),
+    "kf_icp_level": (C.c_int, [P, C.POINTER(LevelView), P, P, C.c_uint32, C.c_uint32, Intrinsics, C.POINTER(Rigid),
+                               C.POINTER(Rigid), C.c_uint32, C.POINTER(IcpOutcome), P]),
     "kf_pipeline_extract_mesh": (C.c_int, [P, C.c_float, C.POINTER(Mesh)]),
     "kf_frame_kernel_count": (C.c_int, [P, C.POINTER(C.c_uint32)]),
     "kf_batch_create": (C.c_int, [P, P, P, C.c_uint32, C.POINTER(P)]),

@@ -244,7 +244,11 @@ kf_status kf_pipeline_create(const kf_pipeline_config* config, kf_pipeline** out
         p.sparse_capacity = c.sparse_block_capacity != 0 ? c.sparse_block_capacity : blocks / 4;
         require(p.sparse_capacity > 0 && p.sparse_capacity < 0xFFFFFFFFull, "Sparse block capacity out of range");
         p.voxel_count = p.sparse_capacity * 512;
-        p.grid.resize(blocks);
+        // the voxel-block hash: a power of two >= 2 x capacity entries
+        uint64_t entries = 1024;
+        while (entries < 2 * p.sparse_capacity) entries <<= 1;
+        require(entries <= (1ull << 32), "Sparse block capacity out of range");
+        p.block_table.resize(entries);
         p.null_bricks.resize(blocks);
         p.slot_block.resize(p.sparse_capacity);
         p.allocated.resize(2);
@@ -257,7 +261,8 @@ kf_status kf_pipeline_create(const kf_pipeline_config* config, kf_pipeline** out
       VolumeDev& v = p.view;
       v.voxels = p.voxels.ptr;
       v.colors = c.color == KF_COLOR_FLOAT ? p.colors.ptr : nullptr;
-      v.grid = c.storage == KF_STORAGE_SPARSE ? p.grid.ptr : nullptr;
+      v.table = c.storage == KF_STORAGE_SPARSE ? p.block_table.ptr : nullptr;
+      v.table_mask = c.storage == KF_STORAGE_SPARSE ? static_cast<uint32_t>(p.block_table.count - 1) : 0u;
       v.rx = g.res_x;
       v.ry = g.res_y;
       v.rz = g.res_z;
@@ -393,22 +398,34 @@ kf_status kf_pipeline_observed_voxel_count(kf_pipeline* pipeline, uint64_t* coun
 }
 
 namespace {
+// The block -> slot map of a sparse volume as a dense host array (one entry
+// per block, kUnallocated when none), expanded from the device's voxel-block
+// hash: the layout of the reference's block grid (block_rep.hpp:26-39).
+std::vector<uint32_t> host_block_grid(const Pipeline& p) {
+  std::vector<unsigned long long> table(p.block_table.count);
+  check(cudaMemcpy(table.data(), p.block_table.ptr, table.size() * sizeof(unsigned long long),
+                   cudaMemcpyDeviceToHost), "block table download");
+  std::vector<uint32_t> grid(static_cast<size_t>(p.view.bx) * p.view.by * p.view.bz, kUnallocated);
+  for (const unsigned long long e : table) {
+    if (e == kEmptyEntry) continue;
+    const uint32_t block = static_cast<uint32_t>(e >> 32);
+    if (block < grid.size()) grid[block] = static_cast<uint32_t>(e);
+  }
+  return grid;
+}
+
 // Copies the bricked device volume to the host in the reference's x-fastest
 // order (Size3::flatten, vector.hpp:61-67): elem_bytes per voxel.  Sparse
-// volumes resolve each block through the grid; unallocated blocks read as
+// volumes resolve each block through the block table; unallocated blocks read as
 // `unallocated` (elem_bytes of an unobserved voxel).
 void download_dense(const Pipeline& p, const void* device, size_t elem_bytes, void* out, const void* unallocated) {
   const kf_volume_geometry& g = p.config.volume;
   const uint64_t bx = (g.res_x + 7) / 8, by = (g.res_y + 7) / 8, bz = (g.res_z + 7) / 8;
-  const bool sparse = p.view.grid != nullptr;
+  const bool sparse = p.view.table != nullptr;
   std::vector<uint8_t> raw((sparse ? p.sparse_capacity : bx * by * bz) * 512 * elem_bytes);
   check(cudaMemcpy(raw.data(), device, raw.size(), cudaMemcpyDeviceToHost), "volume download");
   std::vector<uint32_t> grid;
-  if (sparse) {
-    grid.resize(bx * by * bz);
-    check(cudaMemcpy(grid.data(), p.grid.ptr, grid.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost),
-          "grid download");
-  }
+  if (sparse) grid = host_block_grid(p);
   uint8_t* dst = static_cast<uint8_t*>(out);
   for (uint64_t z = 0; z < g.res_z; ++z) {
     for (uint64_t y = 0; y < g.res_y; ++y) {
@@ -477,10 +494,12 @@ kf_status kf_pipeline_download_block_grid(kf_pipeline* pipeline, uint32_t* grid,
   return guarded([&] {
     require(pipeline != nullptr && grid != nullptr, "kf_pipeline_download_block_grid: null argument");
     Pipeline& p = pipeline->impl;
-    require(p.grid.count != 0, "kf_pipeline_download_block_grid: the pipeline is not sparse");
-    require(count == p.grid.count, "kf_pipeline_download_block_grid: grid size mismatch");
+    require(p.block_table.count != 0, "kf_pipeline_download_block_grid: the pipeline is not sparse");
+    require(count == static_cast<size_t>(p.view.bx) * p.view.by * p.view.bz,
+            "kf_pipeline_download_block_grid: grid size mismatch");
     check(cudaStreamSynchronize(p.stream), "grid download sync");
-    check(cudaMemcpy(grid, p.grid.ptr, count * sizeof(uint32_t), cudaMemcpyDeviceToHost), "grid download");
+    const std::vector<uint32_t> dense = host_block_grid(p);
+    std::memcpy(grid, dense.data(), count * sizeof(uint32_t));
   });
 }
 
@@ -488,7 +507,7 @@ kf_status kf_pipeline_download_pool(kf_pipeline* pipeline, void* voxels, size_t 
   return guarded([&] {
     require(pipeline != nullptr && voxels != nullptr, "kf_pipeline_download_pool: null argument");
     Pipeline& p = pipeline->impl;
-    require(p.grid.count != 0, "kf_pipeline_download_pool: the pipeline is not sparse");
+    require(p.block_table.count != 0, "kf_pipeline_download_pool: the pipeline is not sparse");
     require(bytes == p.sparse_capacity * 512u * p.voxel_bytes, "kf_pipeline_download_pool: pool size mismatch");
     check(cudaStreamSynchronize(p.stream), "pool download sync");
     check(cudaMemcpy(voxels, p.voxels.ptr, bytes, cudaMemcpyDeviceToHost), "pool download");
@@ -674,6 +693,67 @@ kf_status kf_pipeline_track(kf_pipeline* pipeline, kf_tracker* tracker, const kf
     check(cudaMemcpyAsync(t.staging.ptr, st, sizeof(IcpState), cudaMemcpyDeviceToHost, s), "ICP result download");
     check(cudaStreamSynchronize(s), "track");
     fill_outcome(*t.staging.ptr, outcome);
+  });
+}
+
+kf_status kf_pipeline_render_model(kf_pipeline* pipeline, const kf_raycast_camera* camera, kf_surface_maps* out) {
+  return guarded([&] {
+    require(pipeline && camera && out, "kf_pipeline_render_model: null argument");
+    validate_camera(*camera);
+    Pipeline& p = pipeline->impl;
+    Pipeline::Maps& m = p.maps_for(camera->width, camera->height);
+    launch_raycast(p, *camera, m.points.ptr, m.normals.ptr, m.colors.ptr, nullptr, p.stream);
+    check(cudaStreamSynchronize(p.stream), "model render");
+    out->points = m.points.ptr;
+    out->normals = m.normals.ptr;
+    out->colors = m.colors.ptr;
+    out->width = camera->width;
+    out->height = camera->height;
+    out->memory = KF_MEMORY_DEVICE;
+  });
+}
+
+kf_status kf_icp_level(kf_tracker* tracker, const kf_level_view* live, const float* model_points,
+                       const float* model_normals, uint32_t model_width, uint32_t model_height,
+                       kf_intrinsics model_intrinsics, const kf_rigid* model_world_to_camera,
+                       const kf_rigid* initial_camera_to_world, uint32_t iterations, kf_icp_outcome* outcome,
+                       float* sums) {
+  return guarded([&] {
+    require(tracker && live && model_points && model_normals && model_world_to_camera && initial_camera_to_world &&
+                outcome,
+            "kf_icp_level: null argument");
+    require((live->vertices && live->normals) || static_cast<uint64_t>(live->width) * live->height == 0,
+            "kf_icp_level: null live vertex or normal map");
+    Tracker& t = tracker->impl;
+    IcpState* st = t.state.ptr;
+    cudaStream_t s = 0;  // the legacy stream, ordered with the caller's device maps
+    launch_icp_set_pose(st, *initial_camera_to_world, 1, s);
+    launch_icp_level_begin(st, t.params.damping_lambda, s);
+    // the model transform is fixed for the level (IcpIterationTransforms)
+    float model[12];
+    std::memcpy(model, model_world_to_camera->r, 9 * sizeof(float));
+    std::memcpy(model + 9, model_world_to_camera->t, 3 * sizeof(float));
+    check(cudaMemcpyAsync(reinterpret_cast<char*>(st) + offsetof(IcpState, model), model, sizeof(model),
+                          cudaMemcpyHostToDevice, s),
+          "model upload");
+    IcpLevelArgs a;
+    a.live_vertices = live->vertices;
+    a.live_normals = live->normals;
+    a.live_width = live->width;
+    a.live_height = live->height;
+    a.model_points = model_points;
+    a.model_normals = model_normals;
+    a.model_width = model_width;
+    a.model_height = model_height;
+    a.model_intrinsics = intr_from(model_intrinsics);
+    if (static_cast<size_t>(live->width) * live->height > 0) {
+      for (uint32_t i = 0; i < iterations; ++i) launch_icp_iteration(a, st, t.partials.ptr, t.params, 1, 1, s);
+    }
+    launch_icp_level_end(st, -1, s);
+    check(cudaMemcpyAsync(t.staging.ptr, st, sizeof(IcpState), cudaMemcpyDeviceToHost, s), "ICP result download");
+    check(cudaStreamSynchronize(s), "ICP level");
+    fill_outcome(*t.staging.ptr, outcome);
+    if (sums) std::memcpy(sums, t.staging.ptr->sums, kIcpSums * sizeof(float));
   });
 }
 

@@ -155,11 +155,14 @@ struct VoxelTraits<KF_VOXEL_BF16> {
 };
 
 // Device view of one volume (VolumeView / SparseVolumeView, volume.hpp:291-356,
-// block_rep.hpp:26-110).  Sparse volumes resolve blocks through `grid`.
+// block_rep.hpp:26-110).  Sparse volumes resolve blocks through the block table.
 struct VolumeDev {
   void* voxels;
   float4* colors;       // nullptr when the color facet is off
-  const uint32_t* grid; // nullptr for dense storage
+  // sparse storage: the voxel-block hash (block_table_lookup); nullptr for
+  // dense storage
+  const unsigned long long* table;
+  uint32_t table_mask;  // entries - 1 (entries a power of two)
   uint32_t rx, ry, rz;
   uint32_t bx, by, bz;  // block extent
   float voxel_size;
@@ -170,11 +173,46 @@ struct VolumeDev {
 
 constexpr uint32_t kUnallocated = 0xFFFFFFFFu;
 
+// The voxel-block hash of sparse storage (the reference's BlockRep maps
+// blocks to pool slots through a dense grid of block slots,
+// block_rep.hpp:26-110; here an open-addressing table whose size follows the
+// pool, not the domain).  Entry = (block << 32) | slot, kEmptyEntry when
+// free; linear probing from the block's hash.  Entries are only ever added
+// (by the allocation pass, atomicCAS on an empty entry) and the table has at
+// least twice as many entries as the pool has slots, so a probe sequence
+// always reaches the block's entry or an empty one; every loop is bounded by
+// the table size all the same.
+constexpr unsigned long long kEmptyEntry = ~0ull;
+
+__host__ __device__ __forceinline__ uint32_t block_hash(uint32_t block) {
+  // murmur3's 32-bit finaliser: neighbouring blocks land far apart
+  uint32_t h = block;
+  h ^= h >> 16;
+  h *= 0x85EBCA6Bu;
+  h ^= h >> 13;
+  h *= 0xC2B2AE35u;
+  h ^= h >> 16;
+  return h;
+}
+
+// Slot of `block`, or kUnallocated.  For kernels that only read the table.
+__device__ __forceinline__ uint32_t block_table_lookup(const unsigned long long* __restrict__ table, uint32_t mask,
+                                                       uint32_t block) {
+  uint32_t h = block_hash(block) & mask;
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const unsigned long long e = __ldg(table + h);
+    if (e == kEmptyEntry) return kUnallocated;
+    if (static_cast<uint32_t>(e >> 32) == block) return static_cast<uint32_t>(e);
+    h = (h + 1u) & mask;
+  }
+  return kUnallocated;
+}
+
 // Voxel storage is bricked: 8x8x8 bricks of 512 contiguous voxels, voxel
 // (x, y, z) at brick slot * 512 + ((z & 7) * 8 + (y & 7)) * 8 + (x & 7) (the
 // intra-block order of BlockGrid::intra_of_voxel, grid.hpp:54-69).  Dense
 // volumes place brick b (x-major block index) at slot b; sparse volumes look
-// the slot up in `grid`.  A trilinear stencil or an 8-voxel walk along any
+// the slot up in the block table.  A trilinear stencil or an 8-voxel walk along any
 // axis stays inside one or two 4 KB bricks, where the reference's
 // x-fastest layout puts z-neighbours a whole slice (2 MB at 512^3) apart.
 __device__ __forceinline__ uint32_t brick_offset(uint32_t x, uint32_t y, uint32_t z) {
@@ -184,10 +222,10 @@ __device__ __forceinline__ uint32_t brick_offset(uint32_t x, uint32_t y, uint32_
 // Storage index of an in-bounds voxel, or -1 when its block is not allocated.
 __device__ __forceinline__ long long storage_index(const VolumeDev& v, uint32_t x, uint32_t y, uint32_t z) {
   const uint32_t block = ((z >> 3) * v.by + (y >> 3)) * v.bx + (x >> 3);
-  if (v.grid == nullptr) {
+  if (v.table == nullptr) {
     return static_cast<long long>(block) * 512 + brick_offset(x, y, z);
   }
-  const uint32_t slot = __ldg(v.grid + block);
+  const uint32_t slot = block_table_lookup(v.table, v.table_mask, block);
   if (slot == kUnallocated) return -1;
   return static_cast<long long>(slot) * 512 + brick_offset(x, y, z);
 }

@@ -135,19 +135,20 @@ __device__ __forceinline__ void compare_voxel(typename VoxelTraits<KindA>::Raw a
 // sparse volume holds observed voxels only in allocated blocks.  A dense
 // volume that no integration touched yet (no bits allocated) holds none.
 struct CompareSide {
-  const uint32_t* grid;   // sparse: block -> slot
+  const unsigned long long* table;  // sparse: the voxel-block hash (block -> slot)
+  uint32_t table_mask;
   const uint4* observed;  // dense
   uint32_t fresh;         // dense, never integrated
 };
 
 __device__ __forceinline__ uint32_t slot_of(const CompareSide& s, uint32_t blk) {
   if (s.fresh) return kUnallocated;  // every voxel reads as unobserved
-  return s.grid == nullptr ? blk : __ldg(s.grid + blk);
+  return s.table == nullptr ? blk : block_table_lookup(s.table, s.table_mask, blk);
 }
 
 __device__ __forceinline__ bool may_hold_observed(const CompareSide& s, uint32_t blk) {
   if (s.fresh) return false;
-  if (s.grid != nullptr) return __ldg(s.grid + blk) != kUnallocated;
+  if (s.table != nullptr) return block_table_lookup(s.table, s.table_mask, blk) != kUnallocated;
   // the upper 8 bytes of each layer's 16: its two observed words
   const uint2* layers = reinterpret_cast<const uint2*>(s.observed + static_cast<size_t>(blk) * 8u);
   uint32_t any = 0u;
@@ -354,8 +355,9 @@ float mean_of(double sum, unsigned long long count) {
 
 CompareSide side_of(const Pipeline& p) {
   CompareSide side{};
-  side.grid = p.view.grid;
-  if (p.view.grid == nullptr) {
+  side.table = p.view.table;
+  side.table_mask = p.view.table_mask;
+  if (p.view.table == nullptr) {
     // the bits exist from the first integration on (prepare_blocks runs
     // before every integration of a dense volume)
     side.observed = p.voxel_bits.count ? reinterpret_cast<const uint4*>(p.voxel_bits.ptr) : nullptr;

@@ -243,7 +243,7 @@ __device__ __forceinline__ int sdf_region(f3 p, float d, float lambda, float tru
 
 // Step 3: one CTA per listed block, four voxels (along z) per thread.
 template <int Kind, bool Color>
-__global__ void __launch_bounds__(kBlockThreads, 8)
+__global__ void __launch_bounds__(kBlockThreads, 10)
     integrate_blocks_kernel(VolumeDev v, const float4* __restrict__ table, uint32_t width, uint32_t height, Intr k,
                             Rigid T, IntegParams ip, const IcpState* __restrict__ state,
                             const uint32_t* __restrict__ list, const unsigned* __restrict__ count,
@@ -282,7 +282,7 @@ __global__ void __launch_bounds__(kBlockThreads, 8)
   for (unsigned item = blockIdx.x; item < n; item += gridDim.x) {
     const uint32_t block = list[item];
     // sparse volumes: listed blocks are allocated (SparseVolumeView::find_voxel)
-    const uint32_t slot = v.grid != nullptr ? __ldg(v.grid + block) : block;
+    const uint32_t slot = v.table != nullptr ? block_table_lookup(v.table, v.table_mask, block) : block;
     const uint32_t bxi = block % v.bx, byi = (block / v.bx) % v.by, bzi = block / (v.bx * v.by);
     if (threadIdx.x < 16) {
       s_fused[threadIdx.x] = 0u;
@@ -536,6 +536,32 @@ __global__ void stencil_bits_kernel(const uint4* __restrict__ voxel_bits, uint4*
   }
 }
 
+// Per group of 4 x 4 x 4 bricks (32^3 voxels): 1 when every brick of the
+// group has class 1 (every stencil nullopt), 2 when every one has class 2
+// (every stencil exactly 1.0), 0 otherwise; bricks past the volume's brick
+// extent are not part of a group.  The raycast crosses such a group in one
+// go, as it crosses a single brick of that class.
+__global__ void group_class_kernel(const uint8_t* __restrict__ brick_class, uint32_t bx, uint32_t by, uint32_t bz,
+                                   uint8_t* __restrict__ group_class, const IcpState* __restrict__ state) {
+  if (state != nullptr && state->failed) return;  // no integration this frame: the classes stand
+  const uint32_t gx = (bx + 3u) >> 2, gy = (by + 3u) >> 2, gz = (bz + 3u) >> 2;
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= gx * gy * gz) return;
+  const uint32_t x0 = (g % gx) * 4u, y0 = ((g / gx) % gy) * 4u, z0 = (g / (gx * gy)) * 4u;
+  uint32_t first = 0xFFu;
+  bool same = true;
+  for (uint32_t z = z0; z < min(z0 + 4u, bz); ++z) {
+    for (uint32_t y = y0; y < min(y0 + 4u, by); ++y) {
+      for (uint32_t x = x0; x < min(x0 + 4u, bx); ++x) {
+        const uint32_t c = brick_class[(static_cast<size_t>(z) * by + y) * bx + x];
+        if (first == 0xFFu) first = c;
+        same = same && c == first;
+      }
+    }
+  }
+  group_class[g] = static_cast<uint8_t>(same && (first == 1u || first == 2u) ? first : 0u);
+}
+
 // ---- band integration (BandIntegrationSweep<kDevice>, tsdf_integration.cu:
 // 240-291; TruncationBandWalk::visit_pixel, tsdf_integration.hpp:384-426) ----
 // One thread per pixel walks its truncation band [d - band, d + band] along
@@ -606,16 +632,18 @@ __global__ void band_compact_kernel(const uint32_t* __restrict__ bits, uint32_t 
 
 // ---- sparse allocation (BlockRep<kDevice>::integrate, block_rep.cu:100-152) ----
 // The reference allocates marked blocks first come, first served (atomicAdd
-// on the slot counter, block_rep.cu:18-41).  Here slots go to the newly
-// marked blocks in block-index order (a scan over the marked words), so the
-// allocation is deterministic; as in the reference every attempt counts, a
-// block past the capacity stays unallocated and its updates are dropped.
+// on the slot counter, block_rep.cu:18-41) into a dense grid of block slots.
+// Here slots go to the newly marked blocks in block-index order (a scan over
+// the marked words), so the allocation is deterministic, and each new block
+// is inserted into the voxel-block hash with atomicCAS; as in the reference
+// every attempt counts, a block past the capacity stays unallocated and its
+// updates are dropped.
 constexpr int kAllocWords = 1024;  // words per CTA of the allocation scan
 
 // Marked blocks not allocated yet, and their count per word.
-__global__ void sparse_new_kernel(const uint32_t* __restrict__ marked, const uint32_t* __restrict__ grid,
-                                  uint32_t words, uint32_t* __restrict__ new_bits, uint32_t* __restrict__ counts,
-                                  const IcpState* __restrict__ state) {
+__global__ void sparse_new_kernel(const uint32_t* __restrict__ marked, const unsigned long long* __restrict__ table,
+                                  uint32_t table_mask, uint32_t words, uint32_t* __restrict__ new_bits,
+                                  uint32_t* __restrict__ counts, const IcpState* __restrict__ state) {
   if (state != nullptr && state->failed) return;
   const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= words) return;
@@ -623,7 +651,7 @@ __global__ void sparse_new_kernel(const uint32_t* __restrict__ marked, const uin
   while (m != 0u) {
     const uint32_t b = static_cast<uint32_t>(__ffs(m) - 1);
     m &= m - 1u;
-    if (grid[w * 32u + b] == kUnallocated) fresh |= 1u << b;
+    if (block_table_lookup(table, table_mask, w * 32u + b) == kUnallocated) fresh |= 1u << b;
   }
   new_bits[w] = fresh;
   counts[w] = static_cast<uint32_t>(__popc(fresh));
@@ -712,21 +740,31 @@ __global__ void __launch_bounds__(1024)
 __global__ void sparse_assign_kernel(const uint32_t* __restrict__ marked, const uint32_t* __restrict__ new_bits,
                                      const uint32_t* __restrict__ prefix, const uint32_t* __restrict__ cta_prefix,
                                      uint32_t words, const unsigned long long* __restrict__ allocated,
-                                     unsigned long long capacity, uint32_t* __restrict__ grid,
-                                     uint32_t* __restrict__ slot_block, uint32_t* __restrict__ list,
+                                     unsigned long long capacity, unsigned long long* __restrict__ table,
+                                     uint32_t table_mask, uint32_t* __restrict__ slot_block, uint32_t* __restrict__ list,
                                      unsigned* __restrict__ count, uint8_t* __restrict__ null_bricks, uint32_t bx,
                                      uint32_t by, uint32_t bz, const IcpState* __restrict__ state) {
   if (state != nullptr && state->failed) return;
   const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= words) return;
-  uint32_t fresh = new_bits[w];
+  const uint32_t fresh_bits = new_bits[w];
+  uint32_t fresh = fresh_bits, granted = 0u;
   unsigned long long slot = allocated[1] + cta_prefix[w / kAllocWords] + prefix[w];
   while (fresh != 0u) {
     const uint32_t b = static_cast<uint32_t>(__ffs(fresh) - 1);
     fresh &= fresh - 1u;
     if (slot < capacity) {
       const uint32_t block = w * 32u + b;
-      grid[block] = static_cast<uint32_t>(slot);
+      // insert (block, slot): the first empty entry of the block's probe
+      // sequence (the table is at most half full)
+      const unsigned long long entry = (static_cast<unsigned long long>(block) << 32) | slot;
+      uint32_t h = block_hash(block) & table_mask;
+      for (uint32_t probe = 0; probe <= table_mask; ++probe) {
+        const unsigned long long prev = atomicCAS(table + h, kEmptyEntry, entry);
+        if (prev == kEmptyEntry || prev == entry) break;
+        h = (h + 1u) & table_mask;
+      }
+      granted |= 1u << b;
       slot_block[slot] = block;
       // the stencils that can reach this block are no longer all nullopt
       const int x = static_cast<int>(block % bx), y = static_cast<int>((block / bx) % by),
@@ -740,12 +778,8 @@ __global__ void sparse_assign_kernel(const uint32_t* __restrict__ marked, const 
     }
     ++slot;
   }
-  uint32_t m = marked[w], usable = 0u;
-  while (m != 0u) {
-    const uint32_t b = static_cast<uint32_t>(__ffs(m) - 1);
-    m &= m - 1u;
-    if (grid[w * 32u + b] != kUnallocated) usable |= 1u << b;
-  }
+  // the marked blocks allocated before this frame, and the new ones granted a slot
+  uint32_t usable = (marked[w] & ~fresh_bits) | granted;
   if (usable == 0u) return;
   const unsigned base = atomicAdd(count, static_cast<unsigned>(__popc(usable)));
   unsigned n = 0;
@@ -812,11 +846,12 @@ void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t s
     p.block_count.resize(1);
     p.brick_dirty.resize(words);
     p.band_bits.resize(words);
-    if (p.view.grid == nullptr) {
+    if (p.view.table == nullptr) {
       // the raycast's skip structures (dense storage only)
       p.voxel_bits.resize(static_cast<size_t>(blocks) * 32u);
       p.stencil_bits.resize(static_cast<size_t>(blocks) * 32u);
       p.brick_class.resize(blocks);
+      p.group_class.resize(static_cast<size_t>((p.view.bx + 3) / 4) * ((p.view.by + 3) / 4) * ((p.view.bz + 3) / 4));
     } else {
       p.new_bits.resize(words);
       p.word_prefix.resize(words);
@@ -850,12 +885,13 @@ void reset_blocks(Pipeline& p, cudaStream_t s) {
   check(cudaMemsetAsync(p.voxel_bits.ptr, 0, p.voxel_bits.bytes(), s), "skip bits reset");
   check(cudaMemsetAsync(p.stencil_bits.ptr, 0, p.stencil_bits.bytes(), s), "skip bits reset");
   check(cudaMemsetAsync(p.brick_class.ptr, 1, p.brick_class.bytes(), s), "skip bits reset");
+  check(cudaMemsetAsync(p.group_class.ptr, 1, p.group_class.bytes(), s), "skip bits reset");
 }
 
 void reset_sparse(Pipeline& p, cudaStream_t s) {
-  if (p.grid.count == 0) return;
-  check(cudaMemsetAsync(p.grid.ptr, 0xFF, p.grid.bytes(), s), "sparse grid reset");
-  check(cudaMemsetAsync(p.null_bricks.ptr, 1, p.null_bricks.bytes(), s), "sparse grid reset");
+  if (p.block_table.count == 0) return;
+  check(cudaMemsetAsync(p.block_table.ptr, 0xFF, p.block_table.bytes(), s), "block table reset");  // kEmptyEntry
+  check(cudaMemsetAsync(p.null_bricks.ptr, 1, p.null_bricks.bytes(), s), "sparse null bricks reset");
   check(cudaMemsetAsync(p.allocated.ptr, 0, p.allocated.bytes(), s), "sparse counter reset");
 }
 
@@ -897,11 +933,11 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
         p.view, state, p.band_bits.ptr);
     check(cudaGetLastError(), "band_mark_kernel launch");
     const uint32_t words = static_cast<uint32_t>(p.band_bits.count);
-    if (p.view.grid != nullptr) {
+    if (p.view.table != nullptr) {
       // sparse: allocate the newly marked blocks, list the allocated ones
       const uint32_t ctas = ceil_div(words, static_cast<uint32_t>(kAllocWords));
-      sparse_new_kernel<<<ceil_div(words, 256), 256, 0, s>>>(p.band_bits.ptr, p.grid.ptr, words, p.new_bits.ptr,
-                                                             p.word_prefix.ptr, state);
+      sparse_new_kernel<<<ceil_div(words, 256), 256, 0, s>>>(p.band_bits.ptr, p.block_table.ptr, p.view.table_mask,
+                                                             words, p.new_bits.ptr, p.word_prefix.ptr, state);
       check(cudaGetLastError(), "sparse_new_kernel launch");
       sparse_scan_local_kernel<<<ctas, kAllocWords, 0, s>>>(p.word_prefix.ptr, words, p.cta_prefix.ptr, state);
       check(cudaGetLastError(), "sparse_scan_local_kernel launch");
@@ -909,7 +945,8 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
       check(cudaGetLastError(), "sparse_scan_top_kernel launch");
       sparse_assign_kernel<<<ceil_div(words, 256), 256, 0, s>>>(
           p.band_bits.ptr, p.new_bits.ptr, p.word_prefix.ptr, p.cta_prefix.ptr, words, p.allocated.ptr,
-          p.sparse_capacity, p.grid.ptr, p.slot_block.ptr, p.block_list.ptr, p.block_count.ptr, p.null_bricks.ptr,
+          p.sparse_capacity, p.block_table.ptr, p.view.table_mask, p.slot_block.ptr, p.block_list.ptr,
+          p.block_count.ptr, p.null_bricks.ptr,
           p.view.bx, p.view.by, p.view.bz, state);
       check(cudaGetLastError(), "sparse_assign_kernel launch");
     } else {
@@ -963,6 +1000,10 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
       p.brick_class.ptr, p.brick_dirty.ptr, p.view.bx, p.view.by, p.view.bz, p.config.raycast.corner_policy == KF_CORNERS_REQUIRE_ALL,
       state);
   check(cudaGetLastError(), "stencil_bits_kernel launch");
+  const uint32_t groups = static_cast<uint32_t>(p.group_class.count);
+  group_class_kernel<<<ceil_div(groups, 256u), 256, 0, s>>>(p.brick_class.ptr, p.view.bx, p.view.by, p.view.bz,
+                                                             p.group_class.ptr, state);
+  check(cudaGetLastError(), "group_class_kernel launch");
 }
 
 void launch_fill_volume(Pipeline& p, cudaStream_t s) {

@@ -261,6 +261,9 @@ struct Pipeline {
   // Per brick: 1 = every stencil based in the brick is nullopt, 2 = every
   // one is exactly 1.0 (all eight corners observed with tsdf exactly 1).
   DeviceArray<uint8_t> brick_class;
+  // Per group of 4x4x4 bricks: the class shared by all of its bricks (1 or
+  // 2), or 0 (group_class_kernel); the raycast crosses such a group at once.
+  DeviceArray<uint8_t> group_class;
   DeviceArray<uint32_t> band_bits;       // band integration: blocks the bands cross
   // band-march raycast (BasicBandBitmap, occupancy.hpp:240-278): block bits
   // in z-major order (32 z-blocks per word), raw and 3^3-dilated; rebuilt
@@ -269,9 +272,10 @@ struct Pipeline {
   // sparse storage: per block b (x-major), 1 while the blocks b + {0,1}^3 are
   // all unallocated (every trilinear stencil based in b is then nullopt)
   DeviceArray<uint8_t> null_bricks;
-  // Sparse storage (BlockRep, block_rep.hpp:26-110): a slot per 8^3 block in
-  // `grid` (kUnallocated when none), `sparse_capacity` slots in the pools.
-  DeviceArray<uint32_t> grid;
+  // Sparse storage (BlockRep, block_rep.hpp:26-110): the voxel-block hash
+  // (block -> slot, kf_common.cuh block_table_lookup) of 2^k >= 2 x capacity
+  // entries, `sparse_capacity` slots in the pools.
+  DeviceArray<unsigned long long> block_table;
   DeviceArray<uint32_t> slot_block;      // block of each allocated slot
   DeviceArray<unsigned long long> allocated;  // [0] attempts so far (overflow included), [1] this frame's base
   DeviceArray<uint32_t> new_bits, word_prefix, cta_prefix;
@@ -319,7 +323,7 @@ struct Pipeline {
   uint64_t graph_epoch = 0;  // bumped whenever the frame graphs are dropped
   // Launch shapes the autotuner may change (none of them changes a result bit)
   uint32_t raycast_block_x = 8, raycast_block_y = 8;  // march CTA, at most 64 threads
-  uint32_t integrate_ctas = 148 * 12;                 // fusion grid (grid-strided over listed blocks)
+  uint32_t integrate_ctas = 148 * 32;                 // fusion grid (grid-strided over listed blocks)
   uint32_t raycast_lanes[3] = {4, 4, 1};              // lanes per ray: <= 20,000 rays, <= 80,000, more
   uint32_t last_frame_kernels = 0;
   kf_pyramid* graph_pyramid = nullptr;

@@ -196,16 +196,22 @@ __global__ void __launch_bounds__(512)
 }
 
 // Allocated blocks of a sparse grid, in block order.
-__global__ void allocated_flags_kernel(const uint32_t* __restrict__ grid, uint32_t blocks,
+// Sparse storage: flag the block of every used pool slot (the slots are
+// handed out in order, min(attempts, capacity) of them).
+__global__ void allocated_flags_kernel(const uint32_t* __restrict__ slot_block,
+                                       const unsigned long long* __restrict__ allocated, unsigned long long capacity,
                                        uint32_t* __restrict__ flags) {
-  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < blocks) flags[b] = grid[b] != kUnallocated ? 1u : 0u;
+  const unsigned long long used = allocated[0] < capacity ? allocated[0] : capacity;
+  for (unsigned long long s = blockIdx.x * static_cast<unsigned long long>(blockDim.x) + threadIdx.x; s < used;
+       s += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+    flags[slot_block[s]] = 1u;
+  }
 }
 
-__global__ void allocated_list_kernel(const uint32_t* __restrict__ grid, const uint32_t* __restrict__ position,
+__global__ void allocated_list_kernel(const uint32_t* __restrict__ flags, const uint32_t* __restrict__ position,
                                       uint32_t blocks, uint32_t* __restrict__ list) {
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < blocks && grid[b] != kUnallocated) list[position[b]] = b;
+  if (b < blocks && flags[b] != 0u) list[position[b]] = b;
 }
 
 // Exclusive scan of n values (or of their popcounts) in blocks of
@@ -370,7 +376,7 @@ void fill_missing_normals(kf_mesh& m) {
 template <int Kind>
 void extract_typed(Pipeline& p, float min_weight, kf_mesh& out, cudaStream_t s) {
   const VolumeDev& v = p.view;
-  const bool sparse = v.grid != nullptr;
+  const bool sparse = v.table != nullptr;
   // edge keys: storage index of the near voxel * 3 + axis
   const unsigned long long keys = static_cast<unsigned long long>(p.voxel_count) * 3ull;
   const unsigned long long words64 = (keys + 31ull) / 32ull;
@@ -384,12 +390,13 @@ void extract_typed(Pipeline& p, float min_weight, kf_mesh& out, cudaStream_t s) 
   if (sparse) {
     const uint32_t blocks = v.bx * v.by * v.bz;
     DeviceArray<uint32_t> flags(blocks), position(blocks);
-    allocated_flags_kernel<<<ceil_div(blocks, 256), 256, 0, s>>>(v.grid, blocks, flags.ptr);
+    check(cudaMemsetAsync(flags.ptr, 0, flags.bytes(), s), "allocated flags");
+    allocated_flags_kernel<<<148 * 4, 256, 0, s>>>(p.slot_block.ptr, p.allocated.ptr, p.sparse_capacity, flags.ptr);
     check(cudaGetLastError(), "allocated_flags_kernel launch");
     units = exclusive_scan(flags.ptr, position.ptr, blocks, false, s);
     if (units == 0) return;
     block_list.resize(units);
-    allocated_list_kernel<<<ceil_div(blocks, 256), 256, 0, s>>>(v.grid, position.ptr, blocks, block_list.ptr);
+    allocated_list_kernel<<<ceil_div(blocks, 256), 256, 0, s>>>(flags.ptr, position.ptr, blocks, block_list.ptr);
     check(cudaGetLastError(), "allocated_list_kernel launch");
   }
   DeviceArray<uint32_t> edge_words(words), word_first(words), unit_tris(units), unit_first(units);

@@ -284,6 +284,15 @@ kf_status kf_pyramid_level(const kf_pyramid* pyramid, uint32_t index, kf_level_v
   });
 }
 
+kf_status kf_pyramid_raw_depth(const kf_pyramid* pyramid, const uint16_t** depth) {
+  return guarded([&] {
+    require(pyramid != nullptr && depth != nullptr, "kf_pyramid_raw_depth: null argument");
+    const Pyramid& p = pyramid->impl;
+    require(p.level_count > 0, "kf_pyramid_raw_depth: no frame built yet");
+    *depth = p.raw.ptr;
+  });
+}
+
 kf_status kf_pyramid_download_level(const kf_pyramid* pyramid, uint32_t index, uint16_t* depth,
                                     float* vertices, float* normals) {
   return guarded([&] {

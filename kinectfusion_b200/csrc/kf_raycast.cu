@@ -166,11 +166,13 @@ __device__ __forceinline__ int record_class(uint4 r, uint32_t bit) {
 // (voxels) shrinks the box by more than the rounding that separates this
 // line from the march's own sample positions, so every sample before the
 // returned parameter has its base in the brick.
+// `size` is the box's edge in voxels: 8 for a brick, 32 for a group of 4^3
+// bricks (the box of group (bxi, byi, bzi) is [32b + 0.5, 32b + 32.5)).
 __device__ __forceinline__ float brick_exit(const VolumeDev& v, f3 g0, f3 inv_gdir, uint32_t bxi, uint32_t byi,
-                                            uint32_t bzi, bool clip, float margin) {
-  auto axis = [margin, clip](float g, float inv, uint32_t b, uint32_t extent) {
-    const float lo = static_cast<float>(b * 8u) + 0.5f + margin;
-    float hi = static_cast<float>(b * 8u) + 8.5f - margin;
+                                            uint32_t bzi, bool clip, float margin, uint32_t size = 8u) {
+  auto axis = [margin, clip, size](float g, float inv, uint32_t b, uint32_t extent) {
+    const float lo = static_cast<float>(b * size) + 0.5f + margin;
+    float hi = static_cast<float>(b * size + size) + 0.5f - margin;
     if (clip) hi = fminf(hi, static_cast<float>(extent) - margin);
     return ((inv >= 0.0f ? hi : lo) - g) * inv;
   };
@@ -187,12 +189,14 @@ enum : int { kNone = 0, kFound = 1, kStop = 2 };
 // 176-205): kNull or kValue with its value in `tsdf`.  With the skip
 // structures, a sample the stencil bits decide needs no corner gather, and
 // `jump` gets its brick (bit 31 | x | y << 10 | z << 20) when every stencil
-// of that brick has the sample's class.
+// of that brick has the sample's class, or its group of 4^3 bricks (bits 31
+// and 30 | group x | y << 10 | z << 20) when every brick of the group does.
 template <int Kind>
 __device__ __forceinline__ int march_sample(const Sampler<Kind>& s, const VolumeDev& v,
                                             const uint32_t* __restrict__ voxel_bits,
                                             const uint4* __restrict__ stencil_bits,
                                             const uint8_t* __restrict__ brick_class,
+                                            const uint8_t* __restrict__ group_class,
                                             const uint8_t* __restrict__ null_bricks, int policy, f3 point,
                                             float& tsdf, uint32_t& jump) {
   jump = 0u;
@@ -232,6 +236,13 @@ __device__ __forceinline__ int march_sample(const Sampler<Kind>& s, const Volume
     if (cls != 0) {
       if (summary == (cls == 1 ? 2 : 1) && slot.bx < 1024u && slot.by < 1024u && slot.bz < 1024u) {
         jump = 0x80000000u | slot.bx | (slot.by << 10) | (slot.bz << 20);
+        if (group_class != nullptr) {
+          const uint32_t gx = (v.bx + 3u) >> 2, gy = (v.by + 3u) >> 2;
+          const uint32_t gxi = slot.bx >> 2, gyi = slot.by >> 2, gzi = slot.bz >> 2;
+          if (__ldg(group_class + (static_cast<size_t>(gzi) * gy + gyi) * gx + gxi) == summary) {
+            jump = 0xC0000000u | gxi | (gyi << 10) | (gzi << 20);
+          }
+        }
       }
       if (cls == 2) return kNull;
       tsdf = 1.0f;
@@ -292,7 +303,8 @@ __device__ __forceinline__ void box_range(const VolumeDev& v, f3 o, f3 d, float&
 template <int Kind>
 __global__ void __launch_bounds__(64)
     raycast_kernel(VolumeDev v, const uint32_t* __restrict__ voxel_bits, const uint4* __restrict__ stencil_bits,
-                   const uint8_t* __restrict__ brick_class, const uint8_t* __restrict__ null_bricks,
+                   const uint8_t* __restrict__ brick_class, const uint8_t* __restrict__ group_class,
+                   const uint8_t* __restrict__ null_bricks,
                    RaycastParams rp, Intr k, uint32_t width,
                    uint32_t height, Rigid pose, const IcpState* __restrict__ state, float* __restrict__ points) {
   if (state != nullptr) {
@@ -383,7 +395,7 @@ __global__ void __launch_bounds__(64)
     float last = r, next = r + step;
     if (jump != 0u) {
       const float t_exit = brick_exit(v, g0, inv_gdir, jump & 1023u, (jump >> 10) & 1023u, (jump >> 20) & 1023u,
-                                      kind == kValue, margin);
+                                      kind == kValue, margin, (jump & 0x40000000u) ? 32u : 8u);
       while (next < t_exit && next <= rp.max_depth && !(next > t_out)) {
         last = next;
         next += step;
@@ -410,7 +422,7 @@ __global__ void __launch_bounds__(64)
         f3 point = make(0.0f, 0.0f, 0.0f);
         if (r <= rp.max_depth && !(r > t_out)) {
           point = pose.t + (dir * r);
-          kind = march_sample(s, v, voxel_bits, stencil_bits, brick_class, null_bricks, rp.policy, point, tsdf, jump);
+          kind = march_sample(s, v, voxel_bits, stencil_bits, brick_class, group_class, null_bricks, rp.policy, point, tsdf, jump);
         }
         f3 surf = make(0.0f, 0.0f, 0.0f);
         const int event = sample_event(kind, tsdf, point, have_prev, prev_tsdf, prev_point, surf);
@@ -451,7 +463,7 @@ __global__ void __launch_bounds__(64)
     f3 point = make(0.0f, 0.0f, 0.0f);
     if (active && r <= rp.max_depth && !(r > o_tout)) {
       point = pose.t + (o_dir * r);
-      kind = march_sample(s, v, voxel_bits, stencil_bits, brick_class, null_bricks, rp.policy, point, tsdf, jump);
+      kind = march_sample(s, v, voxel_bits, stencil_bits, brick_class, group_class, null_bricks, rp.policy, point, tsdf, jump);
     }
     // the state before this sample: the previous lane's sample, or the ray's
     const int up_kind = __shfl_up_sync(0xFFFFFFFFu, kind, 1);
@@ -807,7 +819,7 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
     grid = dim3(ceil_div(cam.width, tw), ceil_div(cam.height, 2u * th));
   }
   // the skip structures exist once a full-sweep integration prepared them
-  const uint32_t* voxel_bits = p.brick_class.count && p.view.grid == nullptr ? p.voxel_bits.ptr : nullptr;
+  const uint32_t* voxel_bits = p.brick_class.count && p.view.table == nullptr ? p.voxel_bits.ptr : nullptr;
   const uint4* stencil_bits = reinterpret_cast<const uint4*>(p.stencil_bits.ptr);
   const Rigid pose = rigid_from(cam.camera_to_world);
   if (p.config.raycast_backend == KF_RAYCAST_BAND_MARCH) {
@@ -816,8 +828,10 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
                                                    cam.height, pose, state, points);
     check(cudaGetLastError(), "band_march_kernel launch");
   } else {
-    const uint8_t* null_bricks = p.view.grid != nullptr ? p.null_bricks.ptr : nullptr;
-    raycast_kernel<Kind><<<grid, block, 0, s>>>(p.view, voxel_bits, stencil_bits, p.brick_class.ptr, null_bricks, rp,
+    const uint8_t* null_bricks = p.view.table != nullptr ? p.null_bricks.ptr : nullptr;
+    const uint8_t* group_class = voxel_bits != nullptr && p.group_class.count ? p.group_class.ptr : nullptr;
+    raycast_kernel<Kind><<<grid, block, 0, s>>>(p.view, voxel_bits, stencil_bits, p.brick_class.ptr, group_class,
+                                                null_bricks, rp,
                                                 intr_from(cam.intrinsics), cam.width, cam.height, pose, state,
                                                 points);
     check(cudaGetLastError(), "raycast_kernel launch");

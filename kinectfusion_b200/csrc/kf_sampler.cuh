@@ -46,15 +46,18 @@ struct Sampler {
     const f3 fr = gg - fl;
     float acc = 0.0f, ws = 0.0f;
     int valid = 0;
-    if (v.grid == nullptr && bx >= 0 && by >= 0 && bz >= 0 && (bx & 7) != 7 && (by & 7) != 7 && (bz & 7) != 7 &&
+    if (bx >= 0 && by >= 0 && bz >= 0 && (bx & 7) != 7 && (by & 7) != 7 && (bz & 7) != 7 &&
         bx + 1 < static_cast<int>(v.rx) && by + 1 < static_cast<int>(v.ry) && bz + 1 < static_cast<int>(v.rz)) {
-      // Dense, all eight corners in one brick: fixed offsets from the base
-      // voxel, loads issued together, blended in the reference corner order.
-      const Raw* b = reinterpret_cast<const Raw*>(v.voxels) +
-                     storage_index(v, static_cast<uint32_t>(bx), static_cast<uint32_t>(by), static_cast<uint32_t>(bz));
+      // All eight corners in one brick: one storage lookup (sparse storage:
+      // one block-table probe; an unallocated block has no corner), fixed
+      // offsets from the base voxel, loads issued together, blended in the
+      // reference corner order.
+      const long long base =
+          storage_index(v, static_cast<uint32_t>(bx), static_cast<uint32_t>(by), static_cast<uint32_t>(bz));
+      const Raw* b = reinterpret_cast<const Raw*>(v.voxels) + (base < 0 ? 0 : base);
       Raw r[8];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) r[c] = __ldg(b + ((c >> 2) * 64 + ((c >> 1) & 1) * 8 + (c & 1)));
+      for (int c = 0; c < 8; ++c) r[c] = base < 0 ? VT::unobserved() : __ldg(b + ((c >> 2) * 64 + ((c >> 1) & 1) * 8 + (c & 1)));
 #pragma unroll
       for (int c = 0; c < 8; ++c) {
         if (!VT::observed(r[c]) || !VT::finite(r[c])) continue;

@@ -156,7 +156,7 @@ kf_status kf_pipeline_autotune(kf_pipeline* pipeline, const uint16_t* frames, ui
         }
       }
     }
-    const uint32_t grids[] = {148 * 4, 148 * 8, 148 * 12, 148 * 16, 148 * 24};
+    const uint32_t grids[] = {148 * 8, 148 * 16, 148 * 24, 148 * 32, 148 * 48};
     for (uint32_t g : grids) {
       kf_launch_shapes c = best;
       c.integrate_ctas = g;

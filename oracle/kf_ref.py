@@ -227,23 +227,27 @@ def icp_estimate(live_v, live_n, model_p, model_n, k, model_camera_to_world, ini
 
 # ---- the reference's CUDA pipeline (libkf_ref_cuda.so) --------------------------------------
 LIB_CUDA = HERE / "_ref" / "libkf_ref_cuda.so"
-_lib_cuda = None
+# the reference's host code with its device seams taken by
+# kinectfusion_b200/glue/b200_backend.cpp over this project's library
+LIB_GLUE = HERE / "_ref" / "libkf_ref_b200.so"
+_lib_cuda = {}
 
 
-def cuda_available() -> bool:
-    return LIB_CUDA.exists()
+def cuda_available(backend: str = "cuda") -> bool:
+    return (LIB_CUDA if backend == "cuda" else LIB_GLUE).exists()
 
 
-def load_cuda() -> C.CDLL:
-    """The reference built with its CUDA path (src/kinectfusion/cuda/*.cu for
-    sm_100a).  Loaded into its own handle; it shares no state with the
-    host-only library."""
-    global _lib_cuda
-    if _lib_cuda is not None:
-        return _lib_cuda
-    if not LIB_CUDA.exists():
-        raise FileNotFoundError(f"{LIB_CUDA} is not built")
-    lib = C.CDLL(str(LIB_CUDA))
+def load_cuda(backend: str = "cuda") -> C.CDLL:
+    """backend "cuda": the reference built with its own CUDA path
+    (src/kinectfusion/cuda/*.cu for sm_100a); "glue": the reference's host
+    code over this project's library through the drop-in glue.  Each is
+    loaded into its own handle."""
+    if backend in _lib_cuda:
+        return _lib_cuda[backend]
+    path = LIB_CUDA if backend == "cuda" else LIB_GLUE
+    if not path.exists():
+        raise FileNotFoundError(f"{path} is not built")
+    lib = C.CDLL(str(path))
     sig = {
         "kfr_last_error": (C.c_char_p, []),
         "kfr_dev_available": (C.c_int, []),
@@ -261,13 +265,8 @@ def load_cuda() -> C.CDLL:
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
         fn.restype, fn.argtypes = res, args
-    _lib_cuda = lib
+    _lib_cuda[backend] = lib
     return lib
-
-
-def _check_cuda(rc: int):
-    if rc != 0:
-        raise RuntimeError("reference (CUDA): " + load_cuda().kfr_last_error().decode())
 
 
 class RefDevicePipeline:
@@ -277,11 +276,12 @@ class RefDevicePipeline:
     capture_graph are its --icp-device-solve / --icp-capture-graph switches."""
 
     def __init__(self, config: abi.PipelineConfig, depth_options: abi.DepthOptions, icp_options: abi.IcpOptions,
-                 device_solve: bool = False, capture_graph: bool = False, iterations=(10, 5, 4)):
-        lib = load_cuda()
+                 device_solve: bool = False, capture_graph: bool = False, iterations=(10, 5, 4),
+                 backend: str = "cuda"):
+        self.lib = load_cuda(backend)
         h = C.c_void_p()
-        _check_cuda(lib.kfr_dev_create(C.byref(config), C.byref(depth_options), C.byref(icp_options),
-                                       int(device_solve), int(capture_graph), C.byref(h)))
+        self._check(self.lib.kfr_dev_create(C.byref(config), C.byref(depth_options), C.byref(icp_options),
+                                            int(device_solve), int(capture_graph), C.byref(h)))
         self.handle = h
         self.config = config
         self.iterations = np.array(list(iterations) + [4] * (4 - len(iterations)), dtype=np.uint32)
@@ -289,9 +289,13 @@ class RefDevicePipeline:
         self.frames = 0
         self.trajectory = []
 
+    def _check(self, rc: int):
+        if rc != 0:
+            raise RuntimeError("reference (device): " + self.lib.kfr_last_error().decode())
+
     def __del__(self):
         if getattr(self, "handle", None) and self.handle.value:
-            load_cuda().kfr_dev_destroy(self.handle)
+            self.lib.kfr_dev_destroy(self.handle)
             self.handle = C.c_void_p()
 
     def process(self, depth, intrinsics, color=None):
@@ -299,7 +303,7 @@ class RefDevicePipeline:
         color = None if color is None else np.ascontiguousarray(color, dtype=np.uint32)
         tracked = C.c_int32()
         status = np.zeros(4, np.int32)
-        _check_cuda(load_cuda().kfr_dev_frame(self.handle, _ptr(depth), _ptr(color), depth.shape[1], depth.shape[0],
+        self._check(self.lib.kfr_dev_frame(self.handle, _ptr(depth), _ptr(color), depth.shape[1], depth.shape[0],
                                               C.byref(intrinsics), _ptr(self.iterations), 1 if self.frames == 0 else 0,
                                               C.byref(self.pose), C.byref(tracked), _ptr(status)))
         self.frames += 1
@@ -310,7 +314,7 @@ class RefDevicePipeline:
         points = np.zeros((height, width, 3), np.float32)
         normals = np.zeros((height, width, 3), np.float32)
         colors = np.zeros((height, width), np.uint32)
-        _check_cuda(load_cuda().kfr_dev_raycast(self.handle, C.byref(k), width, height,
+        self._check(self.lib.kfr_dev_raycast(self.handle, C.byref(k), width, height,
                                                 C.byref(_rigid(camera_to_world)), _ptr(points), _ptr(normals),
                                                 _ptr(colors)))
         return points, normals, colors
@@ -318,12 +322,11 @@ class RefDevicePipeline:
     def host_view(self) -> np.ndarray:
         g = self.config.volume
         out = np.zeros((g.res_x * g.res_y * g.res_z, 2), np.float32)
-        _check_cuda(load_cuda().kfr_dev_host_view(self.handle, _ptr(out)))
+        self._check(self.lib.kfr_dev_host_view(self.handle, _ptr(out)))
         return out
 
     def observed_voxel_count(self) -> int:
-        return int(load_cuda().kfr_dev_observed(self.handle))
+        return int(self.lib.kfr_dev_observed(self.handle))
 
-    @staticmethod
-    def synchronize():
-        _check_cuda(load_cuda().kfr_dev_synchronize())
+    def synchronize(self):
+        self._check(self.lib.kfr_dev_synchronize())

@@ -5,7 +5,10 @@
 #   oracle/_ref/libkf_ref_cuda.so  the same plus its CUDA path
 #                                  (src/kinectfusion/cuda/*.cu, sm_100a) - the
 #                                  reference's GPU pipeline, timed on the same
-#                                  GPU as a comparison row.
+#                                  GPU as a comparison row;
+#   oracle/_ref/libkf_ref_b200.so  its host code with the device seams of
+#                                  kinectfusion_b200/glue/b200_backend.cpp over
+#                                  this library (the drop-in build).
 #
 # TEST INFRASTRUCTURE ONLY.  Compiles the reference's translation units where
 # they lie, read-only, under $KF_REFERENCE (default /root/reference) -
@@ -80,6 +83,31 @@ build_cuda() {
   rm -rf "$obj"
 }
 
+# The reference's own host code with its device seams taken by this
+# project's glue (kinectfusion_b200/glue/b200_backend.cpp) over
+# kinectfusion_b200/libkf_b200.so: the reference's loop running on this
+# library, as a maintainer's drop-in build would.
+build_glue() {
+  local obj="$OUT/obj_glue"
+  mkdir -p "$obj"
+  local pids=()
+  for tu in "${TUS[@]}"; do
+    "$CXX" "${HOST_FLAGS[@]}" -DKINECTFUSION_HAS_CUDA -I/usr/local/cuda/include \
+      -c "$REF/src/kinectfusion/$tu.cpp" -o "$obj/$tu.o" & pids+=($!)
+  done
+  "$CXX" "${HOST_FLAGS[@]}" -DKINECTFUSION_HAS_CUDA -DKF_REF_CUDA -I/usr/local/cuda/include \
+    -c "$HERE/ref_driver.cpp" -o "$obj/ref_driver.o" & pids+=($!)
+  "$CXX" "${HOST_FLAGS[@]}" -DKINECTFUSION_HAS_CUDA -I"$HERE/../include" \
+    -c "$HERE/../kinectfusion_b200/glue/b200_backend.cpp" -o "$obj/b200_backend.o" & pids+=($!)
+  for p in "${pids[@]}"; do wait "$p"; done
+  "$CXX" -shared -o "$OUT/libkf_ref_b200.so.tmp" "$obj"/*.o -L"$HERE/../kinectfusion_b200" -lkf_b200 \
+    -Wl,-rpath,'$ORIGIN/../../kinectfusion_b200' -L/usr/local/cuda/lib64 -lcudart -Wl,-rpath,/usr/local/cuda/lib64
+  mv "$OUT/libkf_ref_b200.so.tmp" "$OUT/libkf_ref_b200.so"
+  rm -rf "$obj"
+}
+
 if stale "$OUT/libkf_ref.so"; then build_host; fi
 if [ -x "$NVCC" ] && stale "$OUT/libkf_ref_cuda.so"; then build_cuda; fi
+INPUTS+=("$HERE/../kinectfusion_b200/glue/b200_backend.cpp" "$HERE/../kinectfusion_b200/libkf_b200.so")
+if [ -f "$HERE/../kinectfusion_b200/libkf_b200.so" ] && stale "$OUT/libkf_ref_b200.so"; then build_glue; fi
 echo "$OUT/libkf_ref.so"
