@@ -213,7 +213,9 @@ class B200Pipeline final : public Pipeline {
     staging.emplace(geometry_);
     const HostVolumeView v = staging->view();
     const std::size_t n = v.voxel_count();
-    std::vector<float> tsdf(n), weight(n), color(v.colors != nullptr ? n * 4 : 0);
+    // A colourless storage leaves the staging volume's colour facet as
+    // allocated, as materialize does (volume_representation.hpp:119-129).
+    std::vector<float> tsdf(n), weight(n), color(has_color_ && v.colors != nullptr ? n * 4 : 0);
     check(kf_pipeline_download_volume(handle_, tsdf.data(), weight.data(), color.empty() ? nullptr : color.data()));
     for (std::size_t i = 0; i < n; ++i) v.voxels[i] = Voxel{.distance = tsdf[i], .weight = weight[i]};
     if (!color.empty()) {
