@@ -403,6 +403,15 @@ kf_status kf_pipeline_autotune(kf_pipeline* pipeline, const uint16_t* frames, ui
  * (icp_optimizer.hpp:115-116, icp_optimizer.cpp:58-76) with the device solve. */
 kf_status kf_tracker_create(const kf_icp_options* options, kf_tracker** out);
 kf_status kf_tracker_destroy(kf_tracker* tracker);
+/* Test hook of the bounded device waits (no reference counterpart).  Each
+ * ICP level runs as one cooperative kernel whose CTAs meet at a grid barrier
+ * once per Gauss-Newton step; every wait there gives up after 250 ms.  This
+ * arms the tracker so that the barrier of its next level never completes
+ * (its arrival count is set beyond any grid): the waits run out, the frame
+ * is marked failed (no integration), and the call that reads the result
+ * returns KF_ERR_DEVICE_TIMEOUT and clears the barrier, after which the
+ * tracker runs normally.  Call it with no work of the tracker in flight. */
+kf_status kf_tracker_stall_next_level(kf_tracker* tracker);
 /* Renders the model at `camera` and tracks `live` against it for `iterations`
  * Gauss-Newton steps starting from camera->camera_to_world
  * (Pipeline::track, pipeline.hpp:84-85 + IcpConsumer, reconstruction.cpp:63-67). */

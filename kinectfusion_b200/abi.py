@@ -221,6 +221,7 @@ _PROTOTYPES = {
                                           C.POINTER(SurfaceMapsComparison)]),
     "kf_tracker_create": (C.c_int, [C.POINTER(IcpOptions), C.POINTER(P)]),
     "kf_tracker_destroy": (C.c_int, [P]),
+    "kf_tracker_stall_next_level": (C.c_int, [P]),
     "kf_pipeline_track": (C.c_int, [P, P, C.POINTER(RaycastCamera), C.POINTER(LevelView), C.c_uint32,
                                     C.POINTER(IcpOutcome)]),
     "kf_icp_normal_equations": (C.c_int, [P, C.POINTER(LevelView), P, P, C.c_uint32, C.c_uint32, Intrinsics,

@@ -642,7 +642,7 @@ kf_status kf_tracker_create(const kf_icp_options* options, kf_tracker** out) {
       t->impl.options = *options;
       t->impl.params = icp_params_from(*options);
       t->impl.state.resize(1);
-      t->impl.partials.resize(static_cast<size_t>(kIcpMaxGrid) * kIcpSlot);
+      t->impl.partials.resize(2 * static_cast<size_t>(kIcpMaxGrid) * kIcpSlot);
       t->impl.staging.resize(1);
       prepare_icp_kernels();
       check(cudaMemset(t->impl.state.ptr, 0, sizeof(IcpState)), "tracker state init");
@@ -661,6 +661,17 @@ kf_status kf_tracker_destroy(kf_tracker* tracker) {
   return guarded([&] { delete tracker; });
 }
 
+kf_status kf_tracker_stall_next_level(kf_tracker* tracker) {
+  return guarded([&] {
+    require(tracker != nullptr, "kf_tracker_stall_next_level: null tracker");
+    const unsigned beyond_any_grid = 0x80000000u;
+    check(cudaMemcpy(reinterpret_cast<char*>(tracker->impl.state.ptr) + offsetof(IcpState, barrier) +
+                         offsetof(IcpBarrier, count),
+                     &beyond_any_grid, sizeof(beyond_any_grid), cudaMemcpyHostToDevice),
+          "barrier stall");
+  });
+}
+
 kf_status kf_pipeline_track(kf_pipeline* pipeline, kf_tracker* tracker, const kf_raycast_camera* camera,
                             const kf_level_view* live, uint32_t iterations, kf_icp_outcome* outcome) {
   return guarded([&] {
@@ -675,7 +686,6 @@ kf_status kf_pipeline_track(kf_pipeline* pipeline, kf_tracker* tracker, const kf
     // initial pose.
     launch_icp_set_pose(st, camera->camera_to_world, 1, s);
     launch_raycast(p, *camera, m.points.ptr, m.normals.ptr, m.colors.ptr, nullptr, s);
-    launch_icp_level_begin(st, t.params.damping_lambda, s);
     IcpLevelArgs a;
     a.live_vertices = live->vertices;
     a.live_normals = live->normals;
@@ -686,12 +696,11 @@ kf_status kf_pipeline_track(kf_pipeline* pipeline, kf_tracker* tracker, const kf
     a.model_width = camera->width;
     a.model_height = camera->height;
     a.model_intrinsics = intr_from(camera->intrinsics);
-    if (static_cast<size_t>(live->width) * live->height > 0) {
-      for (uint32_t i = 0; i < iterations; ++i) launch_icp_iteration(a, st, t.partials.ptr, t.params, 1, 1, s);
-    }
-    launch_icp_level_end(st, -1, s);
+    const uint32_t steps = static_cast<size_t>(live->width) * live->height > 0 ? iterations : 0u;
+    launch_icp_level(a, st, t.partials.ptr, t.params, steps, -1, 1, 1, s);
     check(cudaMemcpyAsync(t.staging.ptr, st, sizeof(IcpState), cudaMemcpyDeviceToHost, s), "ICP result download");
     check(cudaStreamSynchronize(s), "track");
+    check_icp_barrier(*t.staging.ptr, st, s);
     fill_outcome(*t.staging.ptr, outcome);
   });
 }
@@ -746,12 +755,12 @@ kf_status kf_icp_level(kf_tracker* tracker, const kf_level_view* live, const flo
     a.model_width = model_width;
     a.model_height = model_height;
     a.model_intrinsics = intr_from(model_intrinsics);
-    if (static_cast<size_t>(live->width) * live->height > 0) {
-      for (uint32_t i = 0; i < iterations; ++i) launch_icp_iteration(a, st, t.partials.ptr, t.params, 1, 1, s);
-    }
-    launch_icp_level_end(st, -1, s);
+    // the level start ran above (the model transform replaced after it)
+    const uint32_t steps = static_cast<size_t>(live->width) * live->height > 0 ? iterations : 0u;
+    launch_icp_level(a, st, t.partials.ptr, t.params, steps, -1, 0, 1, s);
     check(cudaMemcpyAsync(t.staging.ptr, st, sizeof(IcpState), cudaMemcpyDeviceToHost, s), "ICP result download");
     check(cudaStreamSynchronize(s), "ICP level");
+    check_icp_barrier(*t.staging.ptr, st, s);
     fill_outcome(*t.staging.ptr, outcome);
     if (sums) std::memcpy(sums, t.staging.ptr->sums, kIcpSums * sizeof(float));
   });

@@ -1,9 +1,10 @@
 // kf_frame.cu - the whole per-frame pipeline as one CUDA graph
 // (Reconstruction::process_frame, reconstruction.cpp:184-277):
 //   depth upload -> bilateral + 3-level pyramid -> integration pixel table ->
-//   for level 2, 1, 0: [ICP level begin, model raycast at the current
-//   estimate, N Gauss-Newton steps, level end] -> integrate at the tracked
-//   pose (skipped on a tracking failure) -> result download.
+//   for level 2, 1, 0: [model raycast at the current estimate, one
+//   cooperative kernel running the level's N Gauss-Newton steps] ->
+//   integrate at the tracked pose (skipped on a tracking failure) -> result
+//   download.
 // One graph launch and at most one host synchronisation per frame.  The
 // reference syncs once per ICP iteration (icp_correspondence.cu:589-596).
 #include <cstring>
@@ -70,7 +71,6 @@ void record_frame(Pipeline& p, Pyramid& pyr, Tracker& t, const Pipeline::GraphKe
       cam.width = pyr.width >> level;
       cam.height = pyr.height >> level;
       std::memset(&cam.camera_to_world, 0, sizeof(cam.camera_to_world));
-      launch_icp_level_begin(st, t.params.damping_lambda, s);
       Pipeline::Maps& m = p.maps_for(cam.width, cam.height);
       launch_raycast(p, cam, m.points.ptr, m.normals.ptr, m.colors.ptr, st, s);
       IcpLevelArgs a;
@@ -87,8 +87,10 @@ void record_frame(Pipeline& p, Pyramid& pyr, Tracker& t, const Pipeline::GraphKe
         check(cudaStreamWaitEvent(s, p.pyramid_event, 0), "graph join");
         pyramid_joined = true;
       }
-      for (uint32_t i = 0; i < iters[level]; ++i) launch_icp_iteration(a, st, t.partials.ptr, t.params, 1, 0, s);
-      launch_icp_level_end(st, level, s);
+      // the level's start, steps and end in one cooperative launch; the
+      // render above used the camera the previous level (or the frame
+      // start) left, which is the level start's camera
+      launch_icp_level(a, st, t.partials.ptr, t.params, iters[level], level, 1, 0, s);
     }
   }
   if (fork) check(cudaStreamWaitEvent(s, p.inputs_event, 0), "graph join");  // also joins the pyramid
@@ -239,7 +241,10 @@ void enqueue(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker, co
   p.last_frame_kernels = fg.kernels;
 }
 
-void fill_result(const IcpState& st, int first, kf_frame_result* r) {
+// `device` is the tracker state the frame ran on: a grid barrier that gave
+// up during the frame is cleared there and reported as an error.
+void fill_result(const IcpState& st, int first, kf_frame_result* r, IcpState* device, cudaStream_t s) {
+  if (device != nullptr) check_icp_barrier(st, device, s);
   for (int i = 0; i < 3; ++i) {
     for (int j = 0; j < 3; ++j) r->camera_to_world.r[i * 3 + j] = static_cast<float>(st.pose[i * 4 + j]);
     r->camera_to_world.t[i] = static_cast<float>(st.pose[i * 4 + 3]);
@@ -456,7 +461,8 @@ kf_status kf_frame_result_next(kf_pipeline* pipeline, kf_frame_result* result) {
     require(p.results_popped < p.results_pushed, "kf_frame_result_next: no submitted frame is waiting");
     const int slot = static_cast<int>(p.results_popped % Pipeline::kResultSlots);
     check(cudaEventSynchronize(p.result_ready[slot]), "frame");
-    fill_result(p.result_ring.ptr[slot], p.result_first[slot], result);
+    fill_result(p.result_ring.ptr[slot], p.result_first[slot], result,
+                p.graph_tracker ? p.graph_tracker->impl.state.ptr : nullptr, p.stream);
     ++p.results_popped;
   });
 }
@@ -467,7 +473,8 @@ kf_status kf_frame_result_fetch(kf_pipeline* pipeline, kf_frame_result* result) 
     Pipeline& p = pipeline->impl;
     check(cudaStreamSynchronize(p.stream), "frame");
     require(p.result_staging.ptr != nullptr, "kf_frame_result_fetch: no frame was processed");
-    fill_result(*p.result_staging.ptr, 0, result);
+    fill_result(*p.result_staging.ptr, 0, result, p.graph_tracker ? p.graph_tracker->impl.state.ptr : nullptr,
+                p.stream);
   });
 }
 
@@ -485,7 +492,7 @@ kf_status kf_frame_process(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracke
             first_frame, true);
     check(cudaStreamSynchronize(p.stream), "frame");
     kf_frame_result local;
-    fill_result(*p.result_staging.ptr, first_frame, &local);
+    fill_result(*p.result_staging.ptr, first_frame, &local, tracker->impl.state.ptr, p.stream);
     *pose = local.camera_to_world;
     if (result) *result = local;
   });

@@ -18,7 +18,9 @@
 //     icp_correspondence.cu:68-78).
 // The reference reduces with FP32 atomics (non-deterministic,
 // icp_correspondence.cu:131-145); this reduction is deterministic.
+#include <atomic>
 #include <cmath>
+#include <cstddef>
 
 #include "kf_internal.h"
 
@@ -501,29 +503,20 @@ __device__ __noinline__ void gauss_newton_step(IcpState* st, const float* sums_i
   }
 }
 
-// Two CTAs per SM (the FP64 solve is a separate function and spills there,
-// not here).  Pix live pixels per thread and grid step.
-template <bool Solve, int Pix>
-__global__ void __launch_bounds__(kIcpBlock, 2)
-    icp_iteration_kernel(IcpLevelArgs a, IcpState* __restrict__ st, float* __restrict__ partials, IcpParams p,
-                         int want_values) {
-  __shared__ int s_flag;
-  __shared__ float s_warp[kIcpBlock / 32][kIcpSlot];
-  __shared__ float s_total[kIcpSlot];
-  __shared__ unsigned long long s_count;
-  if (threadIdx.x == 0) s_flag = (st->status != kIcpRunning);
-  __syncthreads();
-  if (s_flag) return;
-
-  const Rigid cam = rigid_load(st->camera);
-  const Rigid model = rigid_load(st->model);
+// One CTA's share of a correspondence sweep: CTA `cta` of `ctas` associates
+// its pixels (Pix per thread and grid step) and writes its partial slot - the
+// 29 sums and, as integer bits in slot kIcpSums, the matched pixel count.
+template <int Pix>
+__device__ __forceinline__ void sweep_cta(const IcpLevelArgs& a, const Rigid& cam, const Rigid& model,
+                                          const IcpParams& p, unsigned cta, unsigned ctas, float* __restrict__ slot,
+                                          float (&s_warp)[kIcpBlock / 32][kIcpSlot]) {
   // acc[0..28]: the 29 sums, acc[29]: matched pixels, acc[30..31]: padding
   float acc[32];
 #pragma unroll
   for (int i = 0; i < 32; ++i) acc[i] = 0.0f;
   const uint32_t pixels = a.live_width * a.live_height;
-  const uint32_t stride = gridDim.x * kIcpBlock;
-  for (uint32_t first = blockIdx.x * kIcpBlock + threadIdx.x; first < pixels; first += stride * Pix) {
+  const uint32_t stride = ctas * kIcpBlock;
+  for (uint32_t first = cta * kIcpBlock + threadIdx.x; first < pixels; first += stride * Pix) {
     // Pix pixels per thread, each step of the association issued for all of
     // them before the next, so their memory latencies overlap
     f3 src[Pix], lnr[Pix];
@@ -604,39 +597,40 @@ __global__ void __launch_bounds__(kIcpBlock, 2)
     float sum = 0.0f;
     for (int w = 0; w < kIcpBlock / 32; ++w) sum += s_warp[w][threadIdx.x];
     // the count travels as integer bits in slot kIcpSums
-    partials[blockIdx.x * kIcpSlot + threadIdx.x] =
-        threadIdx.x == kIcpSums ? __uint_as_float(static_cast<unsigned>(sum)) : sum;
+    slot[threadIdx.x] = threadIdx.x == kIcpSums ? __uint_as_float(static_cast<unsigned>(sum)) : sum;
     __threadfence();
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned ticket = atomicAdd(&st->arrived, 1u);
-    s_flag = (ticket == gridDim.x - 1) ? 1 : 0;
-  }
-  __syncthreads();
-  if (!s_flag) return;
-  __threadfence();
-  // Last CTA: deterministic Kahan-compensated combine of the CTA partials.
-  // Thread (sum i, segment g) compensates over CTAs g, g+8, g+16, ... then
-  // the eight segment results of each sum are combined in segment order.
-  __shared__ float s_seg_sum[8][kIcpSlot];
-  __shared__ float s_seg_comp[8][kIcpSlot];
-  // Stage every partial in shared memory: independent coalesced loads, eight
-  // in flight per thread.
-  extern __shared__ float s_parts[];
+}
+
+// Shared memory of the combine: the eight segment sums and compensations.
+struct CombineShared {
+  float seg_sum[8][kIcpSlot];
+  float seg_comp[8][kIcpSlot];
+  float total[kIcpSlot];
+  unsigned long long count;
+};
+
+// Deterministic Kahan-compensated combine of `ctas` partial slots, by all
+// threads of the CTA: every slot is staged in shared memory (`staged`, ctas x
+// kIcpSlot floats; independent coalesced L2 loads, eight in flight per
+// thread), then thread (sum i, segment g) compensates over slots g, g+8,
+// g+16, ... and the eight segment results of each sum are combined in
+// segment order.  Ends with c.total / c.count valid after a barrier.
+__device__ __forceinline__ void combine_slots(const float* __restrict__ slots, unsigned ctas, float* staged,
+                                              CombineShared& c) {
   {
-    const unsigned n = gridDim.x * kIcpSlot;
+    const unsigned n = ctas * kIcpSlot;
     for (unsigned e0 = threadIdx.x; e0 < n; e0 += 8 * kIcpBlock) {
       float v[8];
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         const unsigned e = e0 + u * kIcpBlock;
-        v[u] = e < n ? __ldcg(partials + e) : 0.0f;
+        v[u] = e < n ? __ldcg(slots + e) : 0.0f;
       }
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         const unsigned e = e0 + u * kIcpBlock;
-        if (e < n) s_parts[e] = v[u];
+        if (e < n) staged[e] = v[u];
       }
     }
   }
@@ -645,46 +639,76 @@ __global__ void __launch_bounds__(kIcpBlock, 2)
     const unsigned i = threadIdx.x % kIcpSlot, g = threadIdx.x / kIcpSlot;  // 8 x 32 threads
     if (i < kIcpSums) {
       float sum = 0.0f, comp = 0.0f;
-      for (unsigned b = g; b < gridDim.x; b += 8) {
-        const float y = s_parts[b * kIcpSlot + i] - comp;
+      for (unsigned b = g; b < ctas; b += 8) {
+        const float y = staged[b * kIcpSlot + i] - comp;
         const float t = sum + y;
         comp = (t - sum) - y;
         sum = t;
       }
-      s_seg_sum[g][i] = sum;
-      s_seg_comp[g][i] = comp;
+      c.seg_sum[g][i] = sum;
+      c.seg_comp[g][i] = comp;
     } else if (i == kIcpSums) {
-      unsigned c = 0;
-      for (unsigned b = g; b < gridDim.x; b += 8) c += __float_as_uint(s_parts[b * kIcpSlot + kIcpSums]);
-      s_seg_sum[g][i] = __uint_as_float(c);
+      unsigned n = 0;
+      for (unsigned b = g; b < ctas; b += 8) n += __float_as_uint(staged[b * kIcpSlot + kIcpSums]);
+      c.seg_sum[g][i] = __uint_as_float(n);
     }
   }
   __syncthreads();
   if (threadIdx.x < kIcpSums) {
     float sum = 0.0f, comp = 0.0f;
     for (int g = 0; g < 8; ++g) {
-      const float y = (s_seg_sum[g][threadIdx.x] - s_seg_comp[g][threadIdx.x]) - comp;
+      const float y = (c.seg_sum[g][threadIdx.x] - c.seg_comp[g][threadIdx.x]) - comp;
       const float t = sum + y;
       comp = (t - sum) - y;
       sum = t;
     }
-    s_total[threadIdx.x] = sum;
+    c.total[threadIdx.x] = sum;
   } else if (threadIdx.x == kIcpSums) {
-    unsigned long long c = 0;
-    for (int g = 0; g < 8; ++g) c += __float_as_uint(s_seg_sum[g][kIcpSums]);
-    s_count = c;
+    unsigned long long n = 0;
+    for (int g = 0; g < 8; ++g) n += __float_as_uint(c.seg_sum[g][kIcpSums]);
+    c.count = n;
   }
   __syncthreads();
+}
+
+// Two CTAs per SM (the FP64 solve is a separate function and spills there,
+// not here).  Pix live pixels per thread and grid step.  One sweep per
+// launch; the last CTA to arrive (an atomic ticket, no waiting) combines the
+// slots and, with Solve, takes the Gauss-Newton step.
+template <bool Solve, int Pix>
+__global__ void __launch_bounds__(kIcpBlock, 2)
+    icp_iteration_kernel(IcpLevelArgs a, IcpState* __restrict__ st, float* __restrict__ partials, IcpParams p,
+                         int want_values) {
+  __shared__ int s_flag;
+  __shared__ float s_warp[kIcpBlock / 32][kIcpSlot];
+  __shared__ CombineShared s_combine;
+  extern __shared__ float s_parts[];
+  if (threadIdx.x == 0) s_flag = (st->status != kIcpRunning);
+  __syncthreads();
+  if (s_flag) return;
+  sweep_cta<Pix>(a, rigid_load(st->camera), rigid_load(st->model), p, blockIdx.x, gridDim.x,
+                 partials + blockIdx.x * kIcpSlot, s_warp);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned ticket = atomicAdd(&st->arrived, 1u);
+    s_flag = (ticket == gridDim.x - 1) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s_flag) return;
+  __threadfence();
+  combine_slots(partials, gridDim.x, s_parts, s_combine);
   if (threadIdx.x == 0) {
     st->arrived = 0;
-    for (int i = 0; i < kIcpSums; ++i) st->sums[i] = s_total[i];
-    st->count = s_count;
-    if (Solve) gauss_newton_step(st, s_total, s_count, p, want_values != 0);
+    for (int i = 0; i < kIcpSums; ++i) st->sums[i] = s_combine.total[i];
+    st->count = s_combine.count;
+    if (Solve) gauss_newton_step(st, s_combine.total, s_combine.count, p, want_values != 0);
   }
 }
 
-__global__ void icp_level_begin_kernel(IcpState* st, float damping_lambda) {
-  if (threadIdx.x != 0) return;
+// ProjectiveIcpTracker's level start (icp_optimizer.cpp:208-230): counters
+// and damping reset, status running unless a previous level of the frame
+// failed, the float camera and the model world_to_camera from the pose.
+__device__ void level_begin(IcpState* st, float damping_lambda) {
   st->arrived = 0;
   st->iterations = 0;
   st->have_best = 0;
@@ -707,8 +731,10 @@ __global__ void icp_level_begin_kernel(IcpState* st, float damping_lambda) {
   write_float_inverse(st->pose, st->model);
 }
 
-__global__ void icp_level_end_kernel(IcpState* st, int level) {
-  if (threadIdx.x != 0) return;
+// The level's outcome: a loop that ran out of steps is MAX_ITERATIONS; a
+// status other than that or CONVERGED fails the frame (later levels skip).
+// level >= 0 records the per-level results of the frame.
+__device__ void level_end(IcpState* st, int level) {
   if (st->status == kIcpRunning) st->status = KF_ICP_MAX_ITERATIONS;
   if (level >= 0 && level < 4) {
     st->level_status[level] = st->status;
@@ -718,6 +744,127 @@ __global__ void icp_level_end_kernel(IcpState* st, int level) {
   if (st->status != KF_ICP_MAX_ITERATIONS && st->status != KF_ICP_CONVERGED) st->failed = 1;
   pose_to_rigid_floats(st->pose, st->camera);
   write_float_inverse(st->pose, st->world_to_camera);
+}
+
+__device__ __forceinline__ unsigned load_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// A grid-barrier wait gives up after 250 ms (the sweep it waits for takes
+// microseconds), or after kBarrierPolls polls should the timer not advance.
+constexpr unsigned long long kBarrierWaitNs = 250000000ull;
+constexpr uint32_t kBarrierPolls = 1u << 24;
+
+// Generation-counting grid barrier, called by thread 0 of every CTA of a
+// cooperative launch (all CTAs resident, so every arrival comes).  The last
+// CTA to arrive clears the count and advances the generation; the others
+// wait for the generation to move.  A wait that runs out of polls, or sees
+// another CTA's give-up, marks the barrier broken and returns false; the
+// kernel then returns and the host reports KF_ERR_DEVICE_TIMEOUT.  The count
+// is back at zero after every completed barrier, so the next launch starts
+// from a clean barrier without a reset.
+__device__ bool grid_barrier(IcpBarrier* b, unsigned ctas) {
+  const unsigned generation = load_acquire(&b->generation);
+  __threadfence();
+  if (atomicAdd(&b->count, 1u) == ctas - 1u) {
+    atomicExch(&b->count, 0u);
+    __threadfence();
+    atomicAdd(&b->generation, 1u);
+    return true;
+  }
+  const unsigned long long start = global_ns();
+  for (uint32_t poll = 0; poll < kBarrierPolls; ++poll) {
+    if (load_acquire(&b->generation) != generation) {
+      __threadfence();
+      return true;
+    }
+    if ((poll & 63u) == 63u) {
+      if (load_acquire(&b->broken) != 0u) return false;
+      if (global_ns() - start > kBarrierWaitNs) break;
+    }
+    __nanosleep(100);
+  }
+  atomicExch(&b->broken, 1u);
+  return false;
+}
+
+// One whole ICP level in one cooperative launch
+// (BasicDeviceCorrespondenceSweep::run_loop, icp_correspondence.cu:397-439,
+// with the sweep of :216-343): with `begin`, the level start; then up to
+// `iterations` Gauss-Newton steps, each a sweep by every CTA, a grid
+// barrier, and the combine plus FP64 step run redundantly by every CTA on
+// its own shared-memory copy of the tracker state (the same inputs in the
+// same order, so every copy takes the same step and no second barrier is
+// needed); then the level end, written back by CTA 0.  The partial slots
+// alternate between two buffers by step parity: a CTA may write step i+1's
+// slot while another still reads step i's.  Every CTA sees the same status
+// and leaves the loop at the same step.  The sweep, the slot layout and the
+// combine are icp_iteration_kernel's, so the steps are bit-identical to a
+// launch per step at the same grid.
+template <int Pix>
+__global__ void __launch_bounds__(kIcpBlock, 2)
+    icp_level_kernel(IcpLevelArgs a, IcpState* __restrict__ st, float* __restrict__ partials, IcpParams p,
+                     uint32_t iterations, int level, int begin, int want_values) {
+  __shared__ int s_flag;
+  __shared__ float s_warp[kIcpBlock / 32][kIcpSlot];
+  __shared__ CombineShared s_combine;
+  __shared__ IcpState s_st;
+  extern __shared__ float s_parts[];
+  constexpr unsigned kWords = offsetof(IcpState, barrier) / sizeof(unsigned);
+  static_assert(offsetof(IcpState, barrier) % sizeof(unsigned) == 0, "state words");
+  {
+    const unsigned* src = reinterpret_cast<const unsigned*>(st);
+    unsigned* dst = reinterpret_cast<unsigned*>(&s_st);
+    for (unsigned w = threadIdx.x; w < kWords; w += kIcpBlock) dst[w] = src[w];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && begin) level_begin(&s_st, p.damping_lambda);
+  __syncthreads();
+  const unsigned ctas = gridDim.x;
+  for (uint32_t it = 0; it < iterations; ++it) {
+    if (s_st.status != kIcpRunning) break;
+    float* slots = partials + (it & 1u) * (kIcpMaxGrid * kIcpSlot);
+    sweep_cta<Pix>(a, rigid_load(s_st.camera), rigid_load(s_st.model), p, blockIdx.x, ctas,
+                   slots + blockIdx.x * kIcpSlot, s_warp);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      s_flag = grid_barrier(&st->barrier, ctas) ? 1 : 0;
+      // a barrier that gave up fails the frame: later levels skip, the
+      // integration does not run, and the host reports the timeout
+      if (!s_flag) st->failed = 1;
+    }
+    __syncthreads();
+    if (!s_flag) return;
+    combine_slots(slots, ctas, s_parts, s_combine);
+    if (threadIdx.x == 0) {
+      for (int i = 0; i < kIcpSums; ++i) s_st.sums[i] = s_combine.total[i];
+      s_st.count = s_combine.count;
+      gauss_newton_step(&s_st, s_combine.total, s_combine.count, p, want_values != 0);
+    }
+    __syncthreads();
+  }
+  if (blockIdx.x != 0) return;
+  if (threadIdx.x == 0) level_end(&s_st, level);
+  __syncthreads();
+  const unsigned* src = reinterpret_cast<const unsigned*>(&s_st);
+  unsigned* dst = reinterpret_cast<unsigned*>(st);
+  for (unsigned w = threadIdx.x; w < kWords; w += kIcpBlock) dst[w] = src[w];
+}
+
+__global__ void icp_level_begin_kernel(IcpState* st, float damping_lambda) {
+  if (threadIdx.x == 0) level_begin(st, damping_lambda);
+}
+
+__global__ void icp_level_end_kernel(IcpState* st, int level) {
+  if (threadIdx.x == 0) level_end(st, level);
 }
 
 __global__ void icp_set_pose_kernel(IcpState* st, kf_rigid pose, int reset_frame) {
@@ -767,6 +914,22 @@ unsigned icp_grid_for(uint32_t pixels) {
   return g < static_cast<unsigned>(kIcpMaxGrid) ? (g == 0 ? 1 : g) : static_cast<unsigned>(kIcpMaxGrid);
 }
 
+namespace {
+
+// Largest cooperative grid of icp_level_kernel per device (all CTAs
+// resident at once), set by prepare_icp_kernels.
+constexpr int kMaxIcpDevices = 64;
+std::atomic<unsigned> g_level_grid_cap[kMaxIcpDevices];
+
+int current_device() {
+  int device = 0;
+  check(cudaGetDevice(&device), "cudaGetDevice");
+  require(device >= 0 && device < kMaxIcpDevices, "ICP: device ordinal out of range");
+  return device;
+}
+
+}  // namespace
+
 void prepare_icp_kernels() {
   const int bytes = kIcpMaxGrid * kIcpSlot * static_cast<int>(sizeof(float));
   check(cudaFuncSetAttribute(icp_iteration_kernel<true, kIcpPixels>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
@@ -774,6 +937,16 @@ void prepare_icp_kernels() {
   check(cudaFuncSetAttribute(icp_iteration_kernel<false, kIcpPixels>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              bytes),
         "icp kernel attribute");
+  check(cudaFuncSetAttribute(icp_level_kernel<kIcpPixels>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+        "icp kernel attribute");
+  const int device = current_device();
+  int per_sm = 0, sms = 0;
+  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icp_level_kernel<kIcpPixels>, kIcpBlock, bytes),
+        "icp level kernel occupancy");
+  check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+  const long cap = static_cast<long>(per_sm) * sms;
+  require(cap >= 1, "ICP: the level kernel cannot be resident on this device");
+  g_level_grid_cap[device].store(static_cast<unsigned>(cap < kIcpMaxGrid ? cap : kIcpMaxGrid));
 }
 
 void launch_icp_level_begin(IcpState* state, float damping_lambda, cudaStream_t s) {
@@ -798,6 +971,36 @@ void launch_icp_iteration(const IcpLevelArgs& args, IcpState* state, float* part
 void launch_icp_level_end(IcpState* state, int level, cudaStream_t s) {
   icp_level_end_kernel<<<1, 32, 0, s>>>(state, level);
   check(cudaGetLastError(), "icp_level_end launch");
+}
+
+void launch_icp_level(const IcpLevelArgs& args, IcpState* state, float* partials, const IcpParams& params,
+                      uint32_t iterations, int level, int begin, int want_values, cudaStream_t s) {
+  const unsigned cap = g_level_grid_cap[current_device()].load();
+  require(cap != 0, "ICP: level kernel not prepared on this device");
+  unsigned grid = icp_grid_for(args.live_width * args.live_height);
+  if (grid > cap) grid = cap;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kIcpBlock);
+  cfg.dynamicSmemBytes = static_cast<size_t>(grid) * kIcpSlot * sizeof(float);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  check(cudaLaunchKernelEx(&cfg, icp_level_kernel<kIcpPixels>, args, state, partials, params, iterations, level, begin,
+                           want_values),
+        "icp_level_kernel launch");
+}
+
+void check_icp_barrier(const IcpState& host, IcpState* device, cudaStream_t s) {
+  if (host.barrier.broken == 0u) return;
+  check(cudaMemsetAsync(reinterpret_cast<char*>(device) + offsetof(IcpState, barrier), 0, sizeof(IcpBarrier), s),
+        "ICP barrier reset");
+  check(cudaStreamSynchronize(s), "ICP barrier reset");
+  throw DeviceTimeout(
+      "ICP level kernel: a grid-barrier wait gave up before every CTA arrived; the frame is marked failed");
 }
 
 void launch_icp_set_pose(IcpState* state, kf_rigid pose, int reset_frame, cudaStream_t s) {

@@ -26,6 +26,10 @@ struct CudaError : std::runtime_error {
 struct Unsupported : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
+// A bounded device-side wait gave up.
+struct DeviceTimeout : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
 // File read, write or decode failure (std::runtime_error in the reference,
 // image_proc/read_png.cpp, src/app/frame_output.cpp).
 struct IoError : std::runtime_error {
@@ -51,6 +55,9 @@ kf_status guarded(Body&& body) {
   } catch (const CudaError& e) {
     set_last_error(e.what());
     return KF_ERR_CUDA;
+  } catch (const DeviceTimeout& e) {
+    set_last_error(e.what());
+    return KF_ERR_DEVICE_TIMEOUT;
   } catch (const IoError& e) {
     set_last_error(e.what());
     return KF_ERR_IO;
@@ -160,6 +167,16 @@ constexpr int kIcpPixels = 1;         // live pixels per thread and grid step of
 constexpr int kIcpMaxGrid = 2 * 148;  // two CTAs per SM on a 148-SM B200
 constexpr int kIcpRunning = -1;
 
+// Grid barrier of the whole-level ICP kernel: arrival count (zero between
+// barriers), generation, and a sticky give-up flag set by a wait that ran
+// out of polls.
+struct IcpBarrier {
+  unsigned count;
+  unsigned generation;
+  unsigned broken;
+  unsigned pad;
+};
+
 // Lives in device memory; one per tracker.  All poses are camera_to_world.
 struct IcpState {
   double pose[12];       // FP64 pose, row-major 3x4
@@ -192,6 +209,9 @@ struct IcpState {
   // last raw sweep (for kf_icp_normal_equations)
   float sums[kIcpSums];
   unsigned long long count;
+  // last member: the whole-level kernel copies and writes back the state
+  // before it, never the barrier other CTAs may be polling
+  IcpBarrier barrier;
 };
 
 struct IcpParams {
@@ -210,7 +230,7 @@ struct Tracker {
   kf_icp_options options{};
   IcpParams params{};
   DeviceArray<IcpState> state;
-  DeviceArray<float> partials;  // kIcpMaxGrid x kIcpSlot, scratch of the sweep
+  DeviceArray<float> partials;  // 2 x kIcpMaxGrid x kIcpSlot, scratch of the sweeps
   PinnedArray<IcpState> staging;
 };
 
@@ -238,6 +258,15 @@ void launch_icp_iteration(const IcpLevelArgs& args, IcpState* state, float* part
                           const IcpParams& params, int solve, int want_values,
                           cudaStream_t stream);
 void launch_icp_level_end(IcpState* state, int level, cudaStream_t stream);
+// A whole level in one cooperative launch: with `begin` the level start,
+// then up to `iterations` Gauss-Newton steps (the loop leaves at the first
+// non-running status), then the level end (level >= 0 records the frame's
+// per-level results).  `partials` holds two sweeps' slots.
+void launch_icp_level(const IcpLevelArgs& args, IcpState* state, float* partials, const IcpParams& params,
+                      uint32_t iterations, int level, int begin, int want_values, cudaStream_t stream);
+// Throws DeviceTimeout when the downloaded state `host` shows a grid barrier
+// that gave up; the device barrier is cleared first (ordered on `stream`).
+void check_icp_barrier(const IcpState& host, IcpState* device, cudaStream_t stream);
 // Set the device pose (FP64 + float) from a float rigid transform.
 void launch_icp_set_pose(IcpState* state, kf_rigid pose, int reset_frame, cudaStream_t stream);
 
