@@ -407,7 +407,8 @@ kf_status kf_tracker_destroy(kf_tracker* tracker);
  * ICP level runs as one cooperative kernel whose CTAs meet at a grid barrier
  * once per Gauss-Newton step; every wait there gives up after 250 ms.  This
  * arms the tracker so that the barrier of its next level never completes
- * (its arrival count is set beyond any grid): the waits run out, the frame
+ * (its start count is set beyond any count the arrivals reach): the waits
+ * run out, the frame
  * is marked failed (no integration), and the call that reads the result
  * returns KF_ERR_DEVICE_TIMEOUT and clears the barrier, after which the
  * tracker runs normally.  Call it with no work of the tracker in flight. */

@@ -664,10 +664,11 @@ kf_status kf_tracker_destroy(kf_tracker* tracker) {
 kf_status kf_tracker_stall_next_level(kf_tracker* tracker) {
   return guarded([&] {
     require(tracker != nullptr, "kf_tracker_stall_next_level: null tracker");
-    const unsigned beyond_any_grid = 0x80000000u;
+    // a start far above any count the arrivals reach: no wait completes
+    const unsigned long long unreachable = 1ull << 62;
     check(cudaMemcpy(reinterpret_cast<char*>(tracker->impl.state.ptr) + offsetof(IcpState, barrier) +
-                         offsetof(IcpBarrier, count),
-                     &beyond_any_grid, sizeof(beyond_any_grid), cudaMemcpyHostToDevice),
+                         offsetof(IcpBarrier, base),
+                     &unreachable, sizeof(unreachable), cudaMemcpyHostToDevice),
           "barrier stall");
   });
 }

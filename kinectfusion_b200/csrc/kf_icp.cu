@@ -611,53 +611,47 @@ struct CombineShared {
 };
 
 // Deterministic Kahan-compensated combine of `ctas` partial slots, by all
-// threads of the CTA: every slot is staged in shared memory (`staged`, ctas x
-// kIcpSlot floats; independent coalesced L2 loads, eight in flight per
-// thread), then thread (sum i, segment g) compensates over slots g, g+8,
-// g+16, ... and the eight segment results of each sum are combined in
+// threads of the CTA: warp g (segment g of 8) lane i (sum i) loads value i
+// of slots g, g+8, g+16, ... - every load in flight at once, each warp's
+// loads one coalesced row per slot - and compensates over them in slot
+// order; then the eight segment results of each sum are combined in
 // segment order.  Ends with c.total / c.count valid after a barrier.
-__device__ __forceinline__ void combine_slots(const float* __restrict__ slots, unsigned ctas, float* staged,
-                                              CombineShared& c) {
-  {
-    const unsigned n = ctas * kIcpSlot;
-    for (unsigned e0 = threadIdx.x; e0 < n; e0 += 8 * kIcpBlock) {
-      float v[8];
+__device__ __forceinline__ void combine_slots(const float* __restrict__ slots, unsigned ctas, CombineShared& c) {
+  static_assert(kIcpBlock == 8 * 32 && kIcpSlot == 32, "one warp per segment, one lane per slot value");
+  constexpr unsigned kPerSegment = (kIcpMaxGrid + 7) / 8;
+  const unsigned i = threadIdx.x & 31u, g = threadIdx.x >> 5;
+  float v[kPerSegment];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const unsigned e = e0 + u * kIcpBlock;
-        v[u] = e < n ? __ldcg(slots + e) : 0.0f;
-      }
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const unsigned e = e0 + u * kIcpBlock;
-        if (e < n) staged[e] = v[u];
-      }
-    }
+  for (unsigned u = 0; u < kPerSegment; ++u) {
+    const unsigned b = g + 8u * u;
+    v[u] = b < ctas ? __ldcg(slots + b * kIcpSlot + i) : 0.0f;
   }
-  __syncthreads();
-  {
-    const unsigned i = threadIdx.x % kIcpSlot, g = threadIdx.x / kIcpSlot;  // 8 x 32 threads
-    if (i < kIcpSums) {
-      float sum = 0.0f, comp = 0.0f;
-      for (unsigned b = g; b < ctas; b += 8) {
-        const float y = staged[b * kIcpSlot + i] - comp;
-        const float t = sum + y;
-        comp = (t - sum) - y;
-        sum = t;
-      }
-      c.seg_sum[g][i] = sum;
-      c.seg_comp[g][i] = comp;
-    } else if (i == kIcpSums) {
-      unsigned n = 0;
-      for (unsigned b = g; b < ctas; b += 8) n += __float_as_uint(staged[b * kIcpSlot + kIcpSums]);
-      c.seg_sum[g][i] = __uint_as_float(n);
+  if (i < kIcpSums) {
+    float sum = 0.0f, comp = 0.0f;
+#pragma unroll
+    for (unsigned u = 0; u < kPerSegment; ++u) {
+      if (g + 8u * u >= ctas) break;
+      const float y = v[u] - comp;
+      const float t = sum + y;
+      comp = (t - sum) - y;
+      sum = t;
     }
+    c.seg_sum[g][i] = sum;
+    c.seg_comp[g][i] = comp;
+  } else if (i == kIcpSums) {
+    unsigned n = 0;
+#pragma unroll
+    for (unsigned u = 0; u < kPerSegment; ++u) {
+      if (g + 8u * u >= ctas) break;
+      n += __float_as_uint(v[u]);
+    }
+    c.seg_sum[g][i] = __uint_as_float(n);
   }
   __syncthreads();
   if (threadIdx.x < kIcpSums) {
     float sum = 0.0f, comp = 0.0f;
-    for (int g = 0; g < 8; ++g) {
-      const float y = (c.seg_sum[g][threadIdx.x] - c.seg_comp[g][threadIdx.x]) - comp;
+    for (int g2 = 0; g2 < 8; ++g2) {
+      const float y = (c.seg_sum[g2][threadIdx.x] - c.seg_comp[g2][threadIdx.x]) - comp;
       const float t = sum + y;
       comp = (t - sum) - y;
       sum = t;
@@ -665,7 +659,7 @@ __device__ __forceinline__ void combine_slots(const float* __restrict__ slots, u
     c.total[threadIdx.x] = sum;
   } else if (threadIdx.x == kIcpSums) {
     unsigned long long n = 0;
-    for (int g = 0; g < 8; ++g) n += __float_as_uint(c.seg_sum[g][kIcpSums]);
+    for (int g2 = 0; g2 < 8; ++g2) n += __float_as_uint(c.seg_sum[g2][kIcpSums]);
     c.count = n;
   }
   __syncthreads();
@@ -682,7 +676,6 @@ __global__ void __launch_bounds__(kIcpBlock, 2)
   __shared__ int s_flag;
   __shared__ float s_warp[kIcpBlock / 32][kIcpSlot];
   __shared__ CombineShared s_combine;
-  extern __shared__ float s_parts[];
   if (threadIdx.x == 0) s_flag = (st->status != kIcpRunning);
   __syncthreads();
   if (s_flag) return;
@@ -696,7 +689,7 @@ __global__ void __launch_bounds__(kIcpBlock, 2)
   __syncthreads();
   if (!s_flag) return;
   __threadfence();
-  combine_slots(partials, gridDim.x, s_parts, s_combine);
+  combine_slots(partials, gridDim.x, s_combine);
   if (threadIdx.x == 0) {
     st->arrived = 0;
     for (int i = 0; i < kIcpSums; ++i) st->sums[i] = s_combine.total[i];
@@ -759,30 +752,34 @@ __device__ __forceinline__ unsigned long long global_ns() {
 }
 
 // A grid-barrier wait gives up after 250 ms (the sweep it waits for takes
-// microseconds), or after kBarrierPolls polls should the timer not advance.
+// microseconds), or after kBarrierPolls polls should the timer not advance
+// (the first kBarrierSpinPolls polls back to back, the rest about 100 ns
+// apart).
 constexpr unsigned long long kBarrierWaitNs = 250000000ull;
 constexpr uint32_t kBarrierPolls = 1u << 24;
+constexpr uint32_t kBarrierSpinPolls = 4096u;
 
-// Generation-counting grid barrier, called by thread 0 of every CTA of a
-// cooperative launch (all CTAs resident, so every arrival comes).  The last
-// CTA to arrive clears the count and advances the generation; the others
-// wait for the generation to move.  A wait that runs out of polls, or sees
-// another CTA's give-up, marks the barrier broken and returns false; the
-// kernel then returns and the host reports KF_ERR_DEVICE_TIMEOUT.  The count
-// is back at zero after every completed barrier, so the next launch starts
-// from a clean barrier without a reset.
-__device__ bool grid_barrier(IcpBarrier* b, unsigned ctas) {
-  const unsigned generation = load_acquire(&b->generation);
+__device__ __forceinline__ unsigned long long load_acquire64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Counting grid barrier, called by thread 0 of every CTA of a cooperative
+// launch (all CTAs resident, so every arrival comes): barrier `index` of a
+// launch whose arrivals started at `base` completes once the count reaches
+// base + (index + 1) * ctas.  An arrival is one fire-and-forget add after a
+// fence; the count only grows, so nothing is cleared between barriers.  A
+// wait that runs out of time, or sees another CTA's give-up, marks the
+// barrier broken and returns false; the kernel then returns and the host
+// reports KF_ERR_DEVICE_TIMEOUT (and clears the barrier).
+__device__ bool grid_barrier(IcpBarrier* b, unsigned long long base, uint32_t index, unsigned ctas) {
+  const unsigned long long target = base + (static_cast<unsigned long long>(index) + 1ull) * ctas;
   __threadfence();
-  if (atomicAdd(&b->count, 1u) == ctas - 1u) {
-    atomicExch(&b->count, 0u);
-    __threadfence();
-    atomicAdd(&b->generation, 1u);
-    return true;
-  }
+  atomicAdd(&b->count, 1ull);
   const unsigned long long start = global_ns();
   for (uint32_t poll = 0; poll < kBarrierPolls; ++poll) {
-    if (load_acquire(&b->generation) != generation) {
+    if (load_acquire64(&b->count) >= target) {
       __threadfence();
       return true;
     }
@@ -790,7 +787,8 @@ __device__ bool grid_barrier(IcpBarrier* b, unsigned ctas) {
       if (load_acquire(&b->broken) != 0u) return false;
       if (global_ns() - start > kBarrierWaitNs) break;
     }
-    __nanosleep(100);
+    // the waits are microseconds: poll back to back at first, then sleep
+    if (poll >= kBarrierSpinPolls) __nanosleep(100);
   }
   atomicExch(&b->broken, 1u);
   return false;
@@ -817,7 +815,6 @@ __global__ void __launch_bounds__(kIcpBlock, 2)
   __shared__ float s_warp[kIcpBlock / 32][kIcpSlot];
   __shared__ CombineShared s_combine;
   __shared__ IcpState s_st;
-  extern __shared__ float s_parts[];
   constexpr unsigned kWords = offsetof(IcpState, barrier) / sizeof(unsigned);
   static_assert(offsetof(IcpState, barrier) % sizeof(unsigned) == 0, "state words");
   {
@@ -827,8 +824,12 @@ __global__ void __launch_bounds__(kIcpBlock, 2)
   }
   __syncthreads();
   if (threadIdx.x == 0 && begin) level_begin(&s_st, p.damping_lambda);
+  // where this launch's barrier arrivals start (set by the previous launch's
+  // CTA 0 after its last barrier, when every CTA of that launch had arrived)
+  const unsigned long long base = st->barrier.base;
   __syncthreads();
   const unsigned ctas = gridDim.x;
+  uint32_t steps = 0;
   for (uint32_t it = 0; it < iterations; ++it) {
     if (s_st.status != kIcpRunning) break;
     float* slots = partials + (it & 1u) * (kIcpMaxGrid * kIcpSlot);
@@ -836,23 +837,29 @@ __global__ void __launch_bounds__(kIcpBlock, 2)
                    slots + blockIdx.x * kIcpSlot, s_warp);
     __syncthreads();
     if (threadIdx.x == 0) {
-      s_flag = grid_barrier(&st->barrier, ctas) ? 1 : 0;
+      s_flag = grid_barrier(&st->barrier, base, it, ctas) ? 1 : 0;
       // a barrier that gave up fails the frame: later levels skip, the
       // integration does not run, and the host reports the timeout
       if (!s_flag) st->failed = 1;
     }
     __syncthreads();
     if (!s_flag) return;
-    combine_slots(slots, ctas, s_parts, s_combine);
+    combine_slots(slots, ctas, s_combine);
     if (threadIdx.x == 0) {
       for (int i = 0; i < kIcpSums; ++i) s_st.sums[i] = s_combine.total[i];
       s_st.count = s_combine.count;
       gauss_newton_step(&s_st, s_combine.total, s_combine.count, p, want_values != 0);
     }
     __syncthreads();
+    ++steps;
   }
   if (blockIdx.x != 0) return;
-  if (threadIdx.x == 0) level_end(&s_st, level);
+  if (threadIdx.x == 0) {
+    level_end(&s_st, level);
+    // every CTA read `base` before its first arrival, so after CTA 0's last
+    // barrier nothing reads it any more
+    if (steps != 0u) st->barrier.base = base + static_cast<unsigned long long>(steps) * ctas;
+  }
   __syncthreads();
   const unsigned* src = reinterpret_cast<const unsigned*>(&s_st);
   unsigned* dst = reinterpret_cast<unsigned*>(st);
@@ -931,17 +938,9 @@ int current_device() {
 }  // namespace
 
 void prepare_icp_kernels() {
-  const int bytes = kIcpMaxGrid * kIcpSlot * static_cast<int>(sizeof(float));
-  check(cudaFuncSetAttribute(icp_iteration_kernel<true, kIcpPixels>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
-        "icp kernel attribute");
-  check(cudaFuncSetAttribute(icp_iteration_kernel<false, kIcpPixels>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             bytes),
-        "icp kernel attribute");
-  check(cudaFuncSetAttribute(icp_level_kernel<kIcpPixels>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
-        "icp kernel attribute");
   const int device = current_device();
   int per_sm = 0, sms = 0;
-  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icp_level_kernel<kIcpPixels>, kIcpBlock, bytes),
+  check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, icp_level_kernel<kIcpPixels>, kIcpBlock, 0),
         "icp level kernel occupancy");
   check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
   const long cap = static_cast<long>(per_sm) * sms;
@@ -958,12 +957,10 @@ void launch_icp_iteration(const IcpLevelArgs& args, IcpState* state, float* part
                           int solve, int want_values, cudaStream_t s) {
   const uint32_t pixels = args.live_width * args.live_height;
   const unsigned grid = icp_grid_for(pixels);
-  // dynamic shared memory: the last CTA's staging of every partial
-  const size_t smem = static_cast<size_t>(grid) * kIcpSlot * sizeof(float);
   if (solve) {
-    icp_iteration_kernel<true, kIcpPixels><<<grid, kIcpBlock, smem, s>>>(args, state, partials, params, want_values);
+    icp_iteration_kernel<true, kIcpPixels><<<grid, kIcpBlock, 0, s>>>(args, state, partials, params, want_values);
   } else {
-    icp_iteration_kernel<false, kIcpPixels><<<grid, kIcpBlock, smem, s>>>(args, state, partials, params, want_values);
+    icp_iteration_kernel<false, kIcpPixels><<<grid, kIcpBlock, 0, s>>>(args, state, partials, params, want_values);
   }
   check(cudaGetLastError(), "icp_iteration_kernel launch");
 }
@@ -982,7 +979,7 @@ void launch_icp_level(const IcpLevelArgs& args, IcpState* state, float* partials
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(kIcpBlock);
-  cfg.dynamicSmemBytes = static_cast<size_t>(grid) * kIcpSlot * sizeof(float);
+  cfg.dynamicSmemBytes = 0;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;

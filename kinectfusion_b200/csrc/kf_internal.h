@@ -167,14 +167,15 @@ constexpr int kIcpPixels = 1;         // live pixels per thread and grid step of
 constexpr int kIcpMaxGrid = 2 * 148;  // two CTAs per SM on a 148-SM B200
 constexpr int kIcpRunning = -1;
 
-// Grid barrier of the whole-level ICP kernel: arrival count (zero between
-// barriers), generation, and a sticky give-up flag set by a wait that ran
-// out of polls.
+// Grid barrier of the whole-level ICP kernel: the arrivals of every CTA at
+// every barrier since the tracker's creation (never reset while the barrier
+// completes), the count at which the next launch starts, and a sticky
+// give-up flag set by a wait that ran out of polls.
 struct IcpBarrier {
-  unsigned count;
-  unsigned generation;
+  unsigned long long count;
+  unsigned long long base;
   unsigned broken;
-  unsigned pad;
+  unsigned pad[3];
 };
 
 // Lives in device memory; one per tracker.  All poses are camera_to_world.
