@@ -358,26 +358,32 @@ std::unique_ptr<PyramidSource> PyramidSource::create_device(const DepthProcessin
 
 std::unique_ptr<DepthUploader> DepthUploader::create() { return std::make_unique<B200DepthUploader>(); }
 
+// Field by field (a struct's padding bytes are arbitrary).
+inline bool same_options(const kf_icp_options& a, const kf_icp_options& b) {
+  return a.min_correspondences == b.min_correspondences && a.max_point_distance == b.max_point_distance &&
+         a.min_normal_dot == b.min_normal_dot && a.min_update_translation == b.min_update_translation &&
+         a.min_update_rotation == b.min_update_rotation && a.max_update_translation == b.max_update_translation &&
+         a.max_update_rotation == b.max_update_rotation && a.min_system_eigenvalue == b.min_system_eigenvalue &&
+         a.max_condition_number == b.max_condition_number && a.damping_mode == b.damping_mode &&
+         a.damping_lambda == b.damping_lambda && a.adaptive_damping == b.adaptive_damping &&
+         a.lambda_increase == b.lambda_increase && a.lambda_decrease == b.lambda_decrease &&
+         a.min_lambda == b.min_lambda && a.max_lambda == b.max_lambda;
+}
+
 // The sweep's scratch: one tracker of this library per sweep (its device
-// state and partial sums), re-created when the search's gates change.
+// state and partial sums), re-created only when the options it would be
+// created with change.
 template <GraphBuildStrategy Build>
 struct BasicDeviceCorrespondenceSweep<Build>::Scratch {
   kf_tracker* tracker = nullptr;
-  CorrespondenceGates gates{};
-  DeviceIcpLoopParams params{};
+  kf_icp_options options{};
 
   ~Scratch() {
     if (tracker != nullptr) kf_tracker_destroy(tracker);
   }
 
   kf_tracker* for_search(const CorrespondenceGates& g, const DeviceIcpLoopParams* p) {
-    const bool same_gates = tracker != nullptr && g.max_point_distance == gates.max_point_distance &&
-                            g.min_normal_dot == gates.min_normal_dot;
-    const bool same_params = p == nullptr || std::memcmp(p, &params, sizeof(params)) == 0;
-    if (same_gates && same_params) return tracker;
-    if (tracker != nullptr) kf_tracker_destroy(tracker);
-    tracker = nullptr;
-    kf_icp_options o;
+    kf_icp_options o{};
     kf_default_icp_options(&o);
     o.max_point_distance = g.max_point_distance;
     o.min_normal_dot = g.min_normal_dot;
@@ -395,10 +401,18 @@ struct BasicDeviceCorrespondenceSweep<Build>::Scratch {
       o.lambda_decrease = p->schedule.decrease;
       o.min_lambda = p->schedule.min_lambda;
       o.max_lambda = p->schedule.max_lambda;
-      params = *p;
+    } else if (tracker != nullptr) {
+      // a plain sweep uses only the gates: keep the loop options in place
+      kf_icp_options kept = options;
+      kept.max_point_distance = o.max_point_distance;
+      kept.min_normal_dot = o.min_normal_dot;
+      o = kept;
     }
+    if (tracker != nullptr && same_options(o, options)) return tracker;
+    if (tracker != nullptr) kf_tracker_destroy(tracker);
+    tracker = nullptr;
     check(kf_tracker_create(&o, &tracker));
-    gates = g;
+    options = o;
     return tracker;
   }
 };
