@@ -803,7 +803,7 @@ kf_status kf_icp_normal_equations(kf_tracker* tracker, const kf_level_view* live
     a.model_width = model_width;
     a.model_height = model_height;
     a.model_intrinsics = intr_from(model_intrinsics);
-    launch_icp_iteration(a, st, t.partials.ptr, t.params, 0, 0, 0);
+    launch_icp_sweep(a, st, t.partials.ptr, t.params, 0);
     check(cudaMemcpy(t.staging.ptr, st, sizeof(IcpState), cudaMemcpyDeviceToHost), "sums download");
     std::memcpy(sums, t.staging.ptr->sums, kIcpSums * sizeof(float));
     *count = t.staging.ptr->count;

@@ -1,23 +1,25 @@
 // kf_icp.cu - projective point-to-plane ICP on the device.
 //
-// One kernel launch per Gauss-Newton step (all steps of a frame are nodes of
-// one CUDA graph).  The kernel:
-//  1. associates every live pixel with the model render
+// One cooperative launch per pyramid level (icp_level_kernel; the three
+// levels of a frame are nodes of its CUDA graph).  Each Gauss-Newton step:
+//  1. every CTA associates its live pixels with the model render
 //     (CorrespondenceSearch::match, icp_correspondence.hpp:244-294) and
 //     accumulates the 29 float sums of IcpNormalEquations::accumulate
 //     (icp_correspondence.hpp:111-129) per thread;
 //  2. reduces them per warp with register shuffles and per CTA through
 //     shared memory in a fixed order, writing one partial slot per CTA;
-//  3. the last CTA to arrive (an atomic ticket, no spinning) combines the
-//     slots in CTA order with Kahan-compensated FP32 sums, and one thread runs
-//     the Gauss-Newton/LM step of ProjectiveIcpTracker::estimate_with
-//     (icp_optimizer.cpp:208-302) in FP64: stability veto, damped LDL^T
-//     solve, Rodrigues increment, pose composition and the convergence test.
-//     The outcome latches in device memory; later steps of the level return at
-//     their first instruction (the reference's device loop does the same,
+//  3. meets the other CTAs at a bounded grid barrier, combines every slot in
+//     CTA order with Kahan-compensated FP32 sums, and runs the Gauss-Newton/
+//     LM step of ProjectiveIcpTracker::estimate_with (icp_optimizer.cpp:
+//     208-302) in FP64 on its own copy of the tracker state: stability veto,
+//     damped LDL^T solve, Rodrigues increment, pose composition and the
+//     convergence test.  The loop leaves at the first step whose status is
+//     not running (the reference's device loop stops the same way,
 //     icp_correspondence.cu:68-78).
-// The reference reduces with FP32 atomics (non-deterministic,
-// icp_correspondence.cu:131-145); this reduction is deterministic.
+// icp_iteration_kernel is one sweep of the same association, slots and
+// combine (kf_icp_normal_equations).  The reference reduces with FP32 atomics
+// (non-deterministic, icp_correspondence.cu:131-145); this reduction is
+// deterministic.
 #include <atomic>
 #include <cmath>
 #include <cstddef>
@@ -665,14 +667,12 @@ __device__ __forceinline__ void combine_slots(const float* __restrict__ slots, u
   __syncthreads();
 }
 
-// Two CTAs per SM (the FP64 solve is a separate function and spills there,
-// not here).  Pix live pixels per thread and grid step.  One sweep per
-// launch; the last CTA to arrive (an atomic ticket, no waiting) combines the
-// slots and, with Solve, takes the Gauss-Newton step.
-template <bool Solve, int Pix>
+// One sweep per launch, two CTAs per SM, Pix live pixels per thread and
+// grid step; the last CTA to arrive (an atomic ticket, no waiting) combines
+// the slots into the state's sums and count.
+template <int Pix>
 __global__ void __launch_bounds__(kIcpBlock, 2)
-    icp_iteration_kernel(IcpLevelArgs a, IcpState* __restrict__ st, float* __restrict__ partials, IcpParams p,
-                         int want_values) {
+    icp_iteration_kernel(IcpLevelArgs a, IcpState* __restrict__ st, float* __restrict__ partials, IcpParams p) {
   __shared__ int s_flag;
   __shared__ float s_warp[kIcpBlock / 32][kIcpSlot];
   __shared__ CombineShared s_combine;
@@ -694,7 +694,6 @@ __global__ void __launch_bounds__(kIcpBlock, 2)
     st->arrived = 0;
     for (int i = 0; i < kIcpSums; ++i) st->sums[i] = s_combine.total[i];
     st->count = s_combine.count;
-    if (Solve) gauss_newton_step(st, s_combine.total, s_combine.count, p, want_values != 0);
   }
 }
 
@@ -870,10 +869,6 @@ __global__ void icp_level_begin_kernel(IcpState* st, float damping_lambda) {
   if (threadIdx.x == 0) level_begin(st, damping_lambda);
 }
 
-__global__ void icp_level_end_kernel(IcpState* st, int level) {
-  if (threadIdx.x == 0) level_end(st, level);
-}
-
 __global__ void icp_set_pose_kernel(IcpState* st, kf_rigid pose, int reset_frame) {
   if (threadIdx.x != 0) return;
   for (int i = 0; i < 3; ++i) {
@@ -953,21 +948,11 @@ void launch_icp_level_begin(IcpState* state, float damping_lambda, cudaStream_t 
   check(cudaGetLastError(), "icp_level_begin launch");
 }
 
-void launch_icp_iteration(const IcpLevelArgs& args, IcpState* state, float* partials, const IcpParams& params,
-                          int solve, int want_values, cudaStream_t s) {
+void launch_icp_sweep(const IcpLevelArgs& args, IcpState* state, float* partials, const IcpParams& params,
+                      cudaStream_t s) {
   const uint32_t pixels = args.live_width * args.live_height;
-  const unsigned grid = icp_grid_for(pixels);
-  if (solve) {
-    icp_iteration_kernel<true, kIcpPixels><<<grid, kIcpBlock, 0, s>>>(args, state, partials, params, want_values);
-  } else {
-    icp_iteration_kernel<false, kIcpPixels><<<grid, kIcpBlock, 0, s>>>(args, state, partials, params, want_values);
-  }
+  icp_iteration_kernel<kIcpPixels><<<icp_grid_for(pixels), kIcpBlock, 0, s>>>(args, state, partials, params);
   check(cudaGetLastError(), "icp_iteration_kernel launch");
-}
-
-void launch_icp_level_end(IcpState* state, int level, cudaStream_t s) {
-  icp_level_end_kernel<<<1, 32, 0, s>>>(state, level);
-  check(cudaGetLastError(), "icp_level_end launch");
 }
 
 void launch_icp_level(const IcpLevelArgs& args, IcpState* state, float* partials, const IcpParams& params,

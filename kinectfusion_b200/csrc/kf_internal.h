@@ -253,12 +253,10 @@ void prepare_icp_kernels();
 // Begin a level: model world_to_camera from the current pose, status running,
 // unless a previous level failed (then the level stays skipped).
 void launch_icp_level_begin(IcpState* state, float damping_lambda, cudaStream_t stream);
-// One Gauss-Newton step: sweep + (last CTA) FP64 solve and pose update.
-// `want_values` computes the exact eigenvalue diagnostics every step.
-void launch_icp_iteration(const IcpLevelArgs& args, IcpState* state, float* partials,
-                          const IcpParams& params, int solve, int want_values,
-                          cudaStream_t stream);
-void launch_icp_level_end(IcpState* state, int level, cudaStream_t stream);
+// One correspondence sweep: the state's sums and count at its camera and
+// model transforms (no solve).
+void launch_icp_sweep(const IcpLevelArgs& args, IcpState* state, float* partials, const IcpParams& params,
+                      cudaStream_t stream);
 // A whole level in one cooperative launch: with `begin` the level start,
 // then up to `iterations` Gauss-Newton steps (the loop leaves at the first
 // non-running status), then the level end (level >= 0 records the frame's
