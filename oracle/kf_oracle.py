@@ -418,6 +418,25 @@ def mc_case_triangle_counts() -> np.ndarray:
 ICP_ITERATIONS = {0: 10, 1: 5, 2: 4}
 
 
+def track(vol: OracleVolume, levels, raw_shape, pose, ray_opts, icp_opts, threads=1):
+    """The tracking half of a frame of the reference loop (track_pose,
+    reconstruction.cpp:218-250): levels 2, 1, 0 against renders of `vol` at
+    the current estimate; returns (pose, tracked, per-level outcomes)."""
+    outcomes = {}
+    tracked_pose = pose
+    for level in range(len(levels) - 1, -1, -1):
+        lv = levels[level]
+        h, w = raw_shape[0] >> level, raw_shape[1] >> level
+        mp, mn, _ = raycast(vol, lv["intrinsics"], w, h, tracked_pose, ray_opts, threads=threads)
+        out = icp_estimate(lv["vertices"], lv["normals"], mp, mn, lv["intrinsics"], tracked_pose, tracked_pose,
+                           ICP_ITERATIONS.get(level, 4), icp_opts)
+        outcomes[level] = out
+        tracked_pose = abi.matrix_from_rigid(out.pose)
+        if out.status not in (abi.KF_ICP_MAX_ITERATIONS, abi.KF_ICP_CONVERGED):
+            return tracked_pose, False, outcomes
+    return tracked_pose, True, outcomes
+
+
 def track_frame(vol: OracleVolume, raw_depth, k, pose, depth_opts, integ_opts, ray_opts, icp_opts,
                 rule=abi.KF_RULE_ANGLE_WEIGHTED, color=None, threads=1, first=False, band_walk="host"):
     """One frame of the reference loop on the oracle; returns (pose, tracked, per-level outcomes)."""
@@ -426,17 +445,7 @@ def track_frame(vol: OracleVolume, raw_depth, k, pose, depth_opts, integ_opts, r
     tracked_pose = pose
     ok = True
     if not first:
-        for level in range(len(levels) - 1, -1, -1):
-            lv = levels[level]
-            h, w = raw_depth.shape[0] >> level, raw_depth.shape[1] >> level
-            mp, mn, _ = raycast(vol, lv["intrinsics"], w, h, tracked_pose, ray_opts, threads=threads)
-            out = icp_estimate(lv["vertices"], lv["normals"], mp, mn, lv["intrinsics"], tracked_pose, tracked_pose,
-                               ICP_ITERATIONS.get(level, 4), icp_opts)
-            outcomes[level] = out
-            tracked_pose = abi.matrix_from_rigid(out.pose)
-            if out.status not in (abi.KF_ICP_MAX_ITERATIONS, abi.KF_ICP_CONVERGED):
-                ok = False
-                break
+        tracked_pose, ok, outcomes = track(vol, levels, raw_depth.shape, pose, ray_opts, icp_opts, threads=threads)
     if ok:
         w2c = rigid_inverse(abi.rigid_from_matrix(tracked_pose))
         integrate(vol, raw_depth, k, w2c, integ_opts, rule, color=color, normals_map=levels[0]["normals"],
