@@ -536,30 +536,40 @@ __global__ void stencil_bits_kernel(const uint4* __restrict__ voxel_bits, uint4*
   }
 }
 
-// Per group of 4 x 4 x 4 bricks (32^3 voxels): 1 when every brick of the
-// group has class 1 (every stencil nullopt), 2 when every one has class 2
-// (every stencil exactly 1.0), 0 otherwise; bricks past the volume's brick
-// extent are not part of a group.  The raycast crosses such a group in one
-// go, as it crosses a single brick of that class.
-__global__ void group_class_kernel(const uint8_t* __restrict__ brick_class, uint32_t bx, uint32_t by, uint32_t bz,
-                                   uint8_t* __restrict__ group_class, const IcpState* __restrict__ state) {
+// Per brick of class 1 or 2: the largest r <= kBrickRadiusCap such that
+// every brick within Chebyshev distance r (in bricks) has the same class;
+// bricks past the brick grid count as different, so the cube stays inside
+// it.  Mixed bricks get 0.  The raycast crosses such a cube in one go, as it
+// crosses a single brick of that class.  Three separable passes, one per
+// axis: `lower` (the previous pass's radius: the run along x, then the
+// square in x and y) bounds the radius at every brick of the new axis'
+// segment; the x pass has none.
+constexpr uint32_t kBrickRadiusCap = 7;
+__global__ void brick_radius_kernel(const uint8_t* __restrict__ brick_class, const uint8_t* __restrict__ lower,
+                                    uint8_t* __restrict__ out, uint32_t bx, uint32_t by, uint32_t bz, int axis,
+                                    const IcpState* __restrict__ state) {
   if (state != nullptr && state->failed) return;  // no integration this frame: the classes stand
-  const uint32_t gx = (bx + 3u) >> 2, gy = (by + 3u) >> 2, gz = (bz + 3u) >> 2;
-  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= gx * gy * gz) return;
-  const uint32_t x0 = (g % gx) * 4u, y0 = ((g / gx) % gy) * 4u, z0 = (g / (gx * gy)) * 4u;
-  uint32_t first = 0xFFu;
-  bool same = true;
-  for (uint32_t z = z0; z < min(z0 + 4u, bz); ++z) {
-    for (uint32_t y = y0; y < min(y0 + 4u, by); ++y) {
-      for (uint32_t x = x0; x < min(x0 + 4u, bx); ++x) {
-        const uint32_t c = brick_class[(static_cast<size_t>(z) * by + y) * bx + x];
-        if (first == 0xFFu) first = c;
-        same = same && c == first;
-      }
-    }
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= bx * by * bz) return;
+  const uint32_t c = brick_class[b];
+  if (c != 1u && c != 2u) {
+    out[b] = 0;
+    return;
   }
-  group_class[g] = static_cast<uint8_t>(same && (first == 1u || first == 2u) ? first : 0u);
+  const uint32_t coord = axis == 0 ? b % bx : (axis == 1 ? (b / bx) % by : b / (bx * by));
+  const uint32_t extent = axis == 0 ? bx : (axis == 1 ? by : bz);
+  const size_t stride = axis == 0 ? 1u : (axis == 1 ? bx : static_cast<size_t>(bx) * by);
+  uint32_t m = lower != nullptr ? lower[b] : kBrickRadiusCap;
+  uint32_t r = 0;
+  for (uint32_t k = 1; k <= kBrickRadiusCap && k <= m; ++k) {
+    if (coord < k || coord + k >= extent) break;
+    const size_t lo = b - k * stride, hi = b + k * stride;
+    if (brick_class[lo] != c || brick_class[hi] != c) break;
+    if (lower != nullptr) m = min(m, static_cast<uint32_t>(min(lower[lo], lower[hi])));
+    if (m < k) break;
+    r = k;
+  }
+  out[b] = static_cast<uint8_t>(r);
 }
 
 // ---- band integration (BandIntegrationSweep<kDevice>, tsdf_integration.cu:
@@ -851,7 +861,8 @@ void prepare_blocks(Pipeline& p, uint32_t width, uint32_t height, cudaStream_t s
       p.voxel_bits.resize(static_cast<size_t>(blocks) * 32u);
       p.stencil_bits.resize(static_cast<size_t>(blocks) * 32u);
       p.brick_class.resize(blocks);
-      p.group_class.resize(static_cast<size_t>((p.view.bx + 3) / 4) * ((p.view.by + 3) / 4) * ((p.view.bz + 3) / 4));
+      p.brick_radius.resize(blocks);
+      p.radius_scratch.resize(2 * static_cast<size_t>(blocks));
     } else {
       p.new_bits.resize(words);
       p.word_prefix.resize(words);
@@ -885,7 +896,7 @@ void reset_blocks(Pipeline& p, cudaStream_t s) {
   check(cudaMemsetAsync(p.voxel_bits.ptr, 0, p.voxel_bits.bytes(), s), "skip bits reset");
   check(cudaMemsetAsync(p.stencil_bits.ptr, 0, p.stencil_bits.bytes(), s), "skip bits reset");
   check(cudaMemsetAsync(p.brick_class.ptr, 1, p.brick_class.bytes(), s), "skip bits reset");
-  check(cudaMemsetAsync(p.group_class.ptr, 1, p.group_class.bytes(), s), "skip bits reset");
+  check(cudaMemsetAsync(p.brick_radius.ptr, 0, p.brick_radius.bytes(), s), "skip bits reset");
 }
 
 void reset_sparse(Pipeline& p, cudaStream_t s) {
@@ -1000,10 +1011,16 @@ void launch_integrate(Pipeline& p, const float4* table, uint32_t width, uint32_t
       p.brick_class.ptr, p.brick_dirty.ptr, p.view.bx, p.view.by, p.view.bz, p.config.raycast.corner_policy == KF_CORNERS_REQUIRE_ALL,
       state);
   check(cudaGetLastError(), "stencil_bits_kernel launch");
-  const uint32_t groups = static_cast<uint32_t>(p.group_class.count);
-  group_class_kernel<<<ceil_div(groups, 256u), 256, 0, s>>>(p.brick_class.ptr, p.view.bx, p.view.by, p.view.bz,
-                                                             p.group_class.ptr, state);
-  check(cudaGetLastError(), "group_class_kernel launch");
+  const uint32_t bricks = static_cast<uint32_t>(p.brick_radius.count);
+  uint8_t* run_x = p.radius_scratch.ptr;
+  uint8_t* square_xy = p.radius_scratch.ptr + bricks;
+  brick_radius_kernel<<<ceil_div(bricks, 256u), 256, 0, s>>>(p.brick_class.ptr, nullptr, run_x, p.view.bx, p.view.by,
+                                                              p.view.bz, 0, state);
+  brick_radius_kernel<<<ceil_div(bricks, 256u), 256, 0, s>>>(p.brick_class.ptr, run_x, square_xy, p.view.bx,
+                                                              p.view.by, p.view.bz, 1, state);
+  brick_radius_kernel<<<ceil_div(bricks, 256u), 256, 0, s>>>(p.brick_class.ptr, square_xy, p.brick_radius.ptr,
+                                                              p.view.bx, p.view.by, p.view.bz, 2, state);
+  check(cudaGetLastError(), "brick_radius_kernel launch");
 }
 
 void launch_fill_volume(Pipeline& p, cudaStream_t s) {

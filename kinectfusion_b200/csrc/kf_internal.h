@@ -289,9 +289,12 @@ struct Pipeline {
   // Per brick: 1 = every stencil based in the brick is nullopt, 2 = every
   // one is exactly 1.0 (all eight corners observed with tsdf exactly 1).
   DeviceArray<uint8_t> brick_class;
-  // Per group of 4x4x4 bricks: the class shared by all of its bricks (1 or
-  // 2), or 0 (group_class_kernel); the raycast crosses such a group at once.
-  DeviceArray<uint8_t> group_class;
+  // Per brick of class 1 or 2: the radius (in bricks, up to 7) of the cube of
+  // bricks around it that all share its class, inside the brick grid, 0 for
+  // mixed bricks (brick_radius_kernel); the raycast crosses such a cube at
+  // once.  radius_scratch holds the passes' run and square radii.
+  DeviceArray<uint8_t> brick_radius;
+  DeviceArray<uint8_t> radius_scratch;
   DeviceArray<uint32_t> band_bits;       // band integration: blocks the bands cross
   // band-march raycast (BasicBandBitmap, occupancy.hpp:240-278): block bits
   // in z-major order (32 z-blocks per word), raw and 3^3-dilated; rebuilt

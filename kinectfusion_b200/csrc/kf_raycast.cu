@@ -159,25 +159,24 @@ __device__ __forceinline__ int record_class(uint4 r, uint32_t bit) {
   return (one & 1u) ? 1 : 2;
 }
 
-// Ray parameter up to which the samples' stencil bases stay in brick
-// (bxi, byi, bzi): the sample's grid position stays in the brick shifted by
-// half a voxel, [8b + 0.5, 8b + 8.5) per axis, clipped to the volume when
-// `clip` is set.  The ray is taken as g0 + gdir * t in grid units; `margin`
-// (voxels) shrinks the box by more than the rounding that separates this
-// line from the march's own sample positions, so every sample before the
-// returned parameter has its base in the brick.
-// `size` is the box's edge in voxels: 8 for a brick, 32 for a group of 4^3
-// bricks (the box of group (bxi, byi, bzi) is [32b + 0.5, 32b + 32.5)).
-__device__ __forceinline__ float brick_exit(const VolumeDev& v, f3 g0, f3 inv_gdir, uint32_t bxi, uint32_t byi,
-                                            uint32_t bzi, bool clip, float margin, uint32_t size = 8u) {
-  auto axis = [margin, clip, size](float g, float inv, uint32_t b, uint32_t extent) {
-    const float lo = static_cast<float>(b * size) + 0.5f + margin;
-    float hi = static_cast<float>(b * size + size) + 0.5f - margin;
+// Ray parameter up to which the samples' stencil bases stay in a box of
+// bricks: the box of `size` voxels per axis whose lowest voxel is (lox, loy,
+// loz); a sample's grid position keeps its base in the box while it stays in
+// the box shifted by half a voxel, [lo + 0.5, lo + size + 0.5) per axis,
+// clipped to the volume when `clip` is set.  The ray is taken as g0 + gdir *
+// t in grid units; `margin` (voxels) shrinks the box by more than the
+// rounding that separates this line from the march's own sample positions,
+// so every sample before the returned parameter has its base in the box.
+__device__ __forceinline__ float box_exit(const VolumeDev& v, f3 g0, f3 inv_gdir, uint32_t lox, uint32_t loy,
+                                          uint32_t loz, uint32_t size, bool clip, float margin) {
+  auto axis = [margin, clip, size](float g, float inv, uint32_t lo_voxel, uint32_t extent) {
+    const float lo = static_cast<float>(lo_voxel) + 0.5f + margin;
+    float hi = static_cast<float>(lo_voxel + size) + 0.5f - margin;
     if (clip) hi = fminf(hi, static_cast<float>(extent) - margin);
     return ((inv >= 0.0f ? hi : lo) - g) * inv;
   };
-  return fminf(axis(g0.x, inv_gdir.x, bxi, v.rx), fminf(axis(g0.y, inv_gdir.y, byi, v.ry),
-                                                          axis(g0.z, inv_gdir.z, bzi, v.rz)));
+  return fminf(axis(g0.x, inv_gdir.x, lox, v.rx), fminf(axis(g0.y, inv_gdir.y, loy, v.ry),
+                                                          axis(g0.z, inv_gdir.z, loz, v.rz)));
 }
 
 // A march sample: nullopt, a value, or past the march's end.
@@ -189,17 +188,18 @@ enum : int { kNone = 0, kFound = 1, kStop = 2 };
 // 176-205): kNull or kValue with its value in `tsdf`.  With the skip
 // structures, a sample the stencil bits decide needs no corner gather, and
 // `jump` gets its brick (bit 31 | x | y << 10 | z << 20) when every stencil
-// of that brick has the sample's class, or its group of 4^3 bricks (bits 31
-// and 30 | group x | y << 10 | z << 20) when every brick of the group does.
+// of that brick has the sample's class, with `radius` the radius in bricks
+// of the cube around it whose bricks all have that class.
 template <int Kind>
 __device__ __forceinline__ int march_sample(const Sampler<Kind>& s, const VolumeDev& v,
                                             const uint32_t* __restrict__ voxel_bits,
                                             const uint4* __restrict__ stencil_bits,
                                             const uint8_t* __restrict__ brick_class,
-                                            const uint8_t* __restrict__ group_class,
+                                            const uint8_t* __restrict__ brick_radius,
                                             const uint8_t* __restrict__ null_bricks, int policy, f3 point,
-                                            float& tsdf, uint32_t& jump) {
+                                            float& tsdf, uint32_t& jump, uint32_t& radius) {
   jump = 0u;
+  radius = 0u;
   if (null_bricks != nullptr) {
     // sparse storage: a stencil based in a block whose 2x2x2 block
     // neighbourhood is unallocated has no observed corner
@@ -222,9 +222,11 @@ __device__ __forceinline__ int march_sample(const Sampler<Kind>& s, const Volume
     if (!in_grid(v, g)) return kNull;
     Slot slot;
     int cls = 0, summary = 0;
+    uint32_t cube = 0u;
     if (stencil_slot(v, g, slot)) {
       const uint4 rec = __ldg(stencil_bits + slot.record);
       summary = __ldg(brick_class + (slot.record >> 3));
+      if (brick_radius != nullptr) cube = __ldg(brick_radius + (slot.record >> 3));
       cls = record_class(rec, slot.bit);
     }
     if (cls == 0) {
@@ -236,13 +238,7 @@ __device__ __forceinline__ int march_sample(const Sampler<Kind>& s, const Volume
     if (cls != 0) {
       if (summary == (cls == 1 ? 2 : 1) && slot.bx < 1024u && slot.by < 1024u && slot.bz < 1024u) {
         jump = 0x80000000u | slot.bx | (slot.by << 10) | (slot.bz << 20);
-        if (group_class != nullptr) {
-          const uint32_t gx = (v.bx + 3u) >> 2, gy = (v.by + 3u) >> 2;
-          const uint32_t gxi = slot.bx >> 2, gyi = slot.by >> 2, gzi = slot.bz >> 2;
-          if (__ldg(group_class + (static_cast<size_t>(gzi) * gy + gyi) * gx + gxi) == summary) {
-            jump = 0xC0000000u | gxi | (gyi << 10) | (gzi << 20);
-          }
-        }
+        radius = cube;
       }
       if (cls == 2) return kNull;
       tsdf = 1.0f;
@@ -303,7 +299,7 @@ __device__ __forceinline__ void box_range(const VolumeDev& v, f3 o, f3 d, float&
 template <int Kind>
 __global__ void __launch_bounds__(64)
     raycast_kernel(VolumeDev v, const uint32_t* __restrict__ voxel_bits, const uint4* __restrict__ stencil_bits,
-                   const uint8_t* __restrict__ brick_class, const uint8_t* __restrict__ group_class,
+                   const uint8_t* __restrict__ brick_class, const uint8_t* __restrict__ brick_radius,
                    const uint8_t* __restrict__ null_bricks,
                    RaycastParams rp, Intr k, uint32_t width,
                    uint32_t height, Rigid pose, const IcpState* __restrict__ state, float* __restrict__ points) {
@@ -379,8 +375,8 @@ __global__ void __launch_bounds__(64)
   };
   // Take a sample (known kind and event) into the march state; a decided
   // sample whose brick holds only its class also takes every following
-  // sample up to the brick exit.
-  auto apply = [&](int event, int kind, float tsdf, f3 point, float r, uint32_t jump, f3 surf) {
+  // sample up to the exit of the cube of bricks of that class around it.
+  auto apply = [&](int event, int kind, float tsdf, f3 point, float r, uint32_t jump, uint32_t radius, f3 surf) {
     if (event == kFound) {
       found = true;
       surface = surf;
@@ -394,8 +390,9 @@ __global__ void __launch_bounds__(64)
     const float step = step_after(kind, tsdf);
     float last = r, next = r + step;
     if (jump != 0u) {
-      const float t_exit = brick_exit(v, g0, inv_gdir, jump & 1023u, (jump >> 10) & 1023u, (jump >> 20) & 1023u,
-                                      kind == kValue, margin, (jump & 0x40000000u) ? 32u : 8u);
+      const uint32_t bxi = jump & 1023u, byi = (jump >> 10) & 1023u, bzi = (jump >> 20) & 1023u;
+      const float t_exit = box_exit(v, g0, inv_gdir, 8u * (bxi - radius), 8u * (byi - radius), 8u * (bzi - radius),
+                                    8u * (2u * radius + 1u), kind == kValue, margin);
       while (next < t_exit && next <= rp.max_depth && !(next > t_out)) {
         last = next;
         next += step;
@@ -418,15 +415,16 @@ __global__ void __launch_bounds__(64)
         const float r = ray_length;
         int kind = kEnd;
         float tsdf = 0.0f;
-        uint32_t jump = 0u;
+        uint32_t jump = 0u, radius = 0u;
         f3 point = make(0.0f, 0.0f, 0.0f);
         if (r <= rp.max_depth && !(r > t_out)) {
           point = pose.t + (dir * r);
-          kind = march_sample(s, v, voxel_bits, stencil_bits, brick_class, group_class, null_bricks, rp.policy, point, tsdf, jump);
+          kind = march_sample(s, v, voxel_bits, stencil_bits, brick_class, brick_radius, null_bricks, rp.policy,
+                              point, tsdf, jump, radius);
         }
         f3 surf = make(0.0f, 0.0f, 0.0f);
         const int event = sample_event(kind, tsdf, point, have_prev, prev_tsdf, prev_point, surf);
-        apply(event, kind, tsdf, point, r, jump, surf);
+        apply(event, kind, tsdf, point, r, jump, radius, surf);
       }
       continue;
     }
@@ -459,11 +457,12 @@ __global__ void __launch_bounds__(64)
     for (unsigned i = 0; i < off; ++i) r += o_s;
     int kind = kEnd;
     float tsdf = 0.0f;
-    uint32_t jump = 0u;
+    uint32_t jump = 0u, radius = 0u;
     f3 point = make(0.0f, 0.0f, 0.0f);
     if (active && r <= rp.max_depth && !(r > o_tout)) {
       point = pose.t + (o_dir * r);
-      kind = march_sample(s, v, voxel_bits, stencil_bits, brick_class, group_class, null_bricks, rp.policy, point, tsdf, jump);
+      kind = march_sample(s, v, voxel_bits, stencil_bits, brick_class, brick_radius, null_bricks, rp.policy, point,
+                          tsdf, jump, radius);
     }
     // the state before this sample: the previous lane's sample, or the ray's
     const int up_kind = __shfl_up_sync(0xFFFFFFFFu, kind, 1);
@@ -487,11 +486,12 @@ __global__ void __launch_bounds__(64)
     const float m_r = __shfl_sync(0xFFFFFFFFu, r, src);
     const float m_tsdf = __shfl_sync(0xFFFFFFFFu, tsdf, src);
     const uint32_t m_jump = __shfl_sync(0xFFFFFFFFu, jump, src);
+    const uint32_t m_radius = __shfl_sync(0xFFFFFFFFu, radius, src);
     const f3 m_point = make(__shfl_sync(0xFFFFFFFFu, point.x, src), __shfl_sync(0xFFFFFFFFu, point.y, src),
                             __shfl_sync(0xFFFFFFFFu, point.z, src));
     const f3 m_surf = make(__shfl_sync(0xFFFFFFFFu, surf.x, src), __shfl_sync(0xFFFFFFFFu, surf.y, src),
                            __shfl_sync(0xFFFFFFFFu, surf.z, src));
-    if (!done) apply(m_event, m_kind, m_tsdf, m_point, m_r, m_jump, m_surf);
+    if (!done) apply(m_event, m_kind, m_tsdf, m_point, m_r, m_jump, m_radius, m_surf);
   }
   if (in_image) store3(points + pix * 3, found ? surface : nan3());
 }
@@ -829,8 +829,8 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
     check(cudaGetLastError(), "band_march_kernel launch");
   } else {
     const uint8_t* null_bricks = p.view.table != nullptr ? p.null_bricks.ptr : nullptr;
-    const uint8_t* group_class = voxel_bits != nullptr && p.group_class.count ? p.group_class.ptr : nullptr;
-    raycast_kernel<Kind><<<grid, block, 0, s>>>(p.view, voxel_bits, stencil_bits, p.brick_class.ptr, group_class,
+    const uint8_t* brick_radius = voxel_bits != nullptr && p.brick_radius.count ? p.brick_radius.ptr : nullptr;
+    raycast_kernel<Kind><<<grid, block, 0, s>>>(p.view, voxel_bits, stencil_bits, p.brick_class.ptr, brick_radius,
                                                 null_bricks, rp,
                                                 intr_from(cam.intrinsics), cam.width, cam.height, pose, state,
                                                 points);
