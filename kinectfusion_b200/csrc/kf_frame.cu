@@ -89,8 +89,15 @@ void record_frame(Pipeline& p, Pyramid& pyr, Tracker& t, const Pipeline::GraphKe
       }
       // the level's start, steps and end in one cooperative launch; the
       // render above used the camera the previous level (or the frame
-      // start) left, which is the level start's camera
-      launch_icp_level(a, st, t.partials.ptr, t.params, iters[level], level, 1, 0, s);
+      // start) left, which is the level start's camera.  A frame graph that
+      // runs beside others (a batch member) takes the same level as
+      // launches that need no co-residency: cooperative launches of several
+      // members could not share the GPU.
+      if (key.cooperative) {
+        launch_icp_level(a, st, t.partials.ptr, t.params, iters[level], level, 1, 0, s);
+      } else {
+        launch_icp_level_steps(a, st, t.partials.ptr, t.params, iters[level], level, s);
+      }
     }
   }
   if (fork) check(cudaStreamWaitEvent(s, p.inputs_event, 0), "graph join");  // also joins the pyramid
@@ -103,7 +110,7 @@ void record_frame(Pipeline& p, Pyramid& pyr, Tracker& t, const Pipeline::GraphKe
 Pipeline::FrameGraph& frame_graph_for(kf_pipeline* pipeline, kf_pyramid* pyramid, kf_tracker* tracker,
                                       uint32_t width, uint32_t height, kf_intrinsics intrinsics,
                                       const uint32_t* iterations, int32_t first_frame, bool has_color,
-                                      bool fork = true) {
+                                      bool fork = true, bool cooperative = true) {
   require(pipeline && pyramid && tracker, "kf_frame_enqueue: null argument");
   require(intrinsics.fx > 0.0f && intrinsics.fy > 0.0f, "Depth frame intrinsics must have positive focal lengths");
   Pipeline& p = pipeline->impl;
@@ -123,7 +130,8 @@ Pipeline::FrameGraph& frame_graph_for(kf_pipeline* pipeline, kf_pyramid* pyramid
   if (p.pixel_table.count != n) p.pixel_table.resize(n);
   if (p.frame_color.count != n) p.frame_color.resize(n);
   p.result_staging.resize(1);
-  Pipeline::GraphKey key{width, height, 0, 0, 0, 0, first_frame ? 1u : 0u, has_color ? 1u : 0u, fork ? 1u : 0u};
+  Pipeline::GraphKey key{width, height, 0, 0, 0, 0, first_frame ? 1u : 0u, has_color ? 1u : 0u, fork ? 1u : 0u,
+                         cooperative ? 1u : 0u};
   uint32_t* its[4] = {&key.it0, &key.it1, &key.it2, &key.it3};
   for (uint32_t l = 0; l < 4; ++l) *its[l] = (iterations != nullptr && l < pyr.level_count) ? iterations[l] : 0u;
   if (iterations == nullptr) {
@@ -301,7 +309,7 @@ void batch_step(kf_batch* b, const uint16_t* const* depths, uint32_t width, uint
     if (depths[i] == nullptr) continue;  // this member sits out the step
     // one branch per member: the members already fill the GPU side by side
     graphs[i] = &frame_graph_for(b->pipelines[i], b->pyramids[i], b->trackers[i], width, height, intrinsics[i],
-                                 iterations, first != nullptr && first[i] != 0, false, false);
+                                 iterations, first != nullptr && first[i] != 0, false, false, false);
     key[2 * i] = reinterpret_cast<uint64_t>(graphs[i]->graph);
     key[2 * i + 1] = b->pipelines[i]->impl.graph_epoch;
   }

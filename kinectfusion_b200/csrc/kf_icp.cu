@@ -669,10 +669,13 @@ __device__ __forceinline__ void combine_slots(const float* __restrict__ slots, u
 
 // One sweep per launch, two CTAs per SM, Pix live pixels per thread and
 // grid step; the last CTA to arrive (an atomic ticket, no waiting) combines
-// the slots into the state's sums and count.
-template <int Pix>
+// the slots into the state's sums and count and, with Solve, takes the
+// Gauss-Newton step - icp_level_kernel's step, one launch per step (the
+// frame graphs of a batch, whose members' levels must share the GPU).
+template <bool Solve, int Pix>
 __global__ void __launch_bounds__(kIcpBlock, 2)
-    icp_iteration_kernel(IcpLevelArgs a, IcpState* __restrict__ st, float* __restrict__ partials, IcpParams p) {
+    icp_iteration_kernel(IcpLevelArgs a, IcpState* __restrict__ st, float* __restrict__ partials, IcpParams p,
+                         int want_values) {
   __shared__ int s_flag;
   __shared__ float s_warp[kIcpBlock / 32][kIcpSlot];
   __shared__ CombineShared s_combine;
@@ -694,6 +697,7 @@ __global__ void __launch_bounds__(kIcpBlock, 2)
     st->arrived = 0;
     for (int i = 0; i < kIcpSums; ++i) st->sums[i] = s_combine.total[i];
     st->count = s_combine.count;
+    if (Solve) gauss_newton_step(st, s_combine.total, s_combine.count, p, want_values != 0);
   }
 }
 
@@ -869,6 +873,10 @@ __global__ void icp_level_begin_kernel(IcpState* st, float damping_lambda) {
   if (threadIdx.x == 0) level_begin(st, damping_lambda);
 }
 
+__global__ void icp_level_end_kernel(IcpState* st, int level) {
+  if (threadIdx.x == 0) level_end(st, level);
+}
+
 __global__ void icp_set_pose_kernel(IcpState* st, kf_rigid pose, int reset_frame) {
   if (threadIdx.x != 0) return;
   for (int i = 0; i < 3; ++i) {
@@ -951,8 +959,22 @@ void launch_icp_level_begin(IcpState* state, float damping_lambda, cudaStream_t 
 void launch_icp_sweep(const IcpLevelArgs& args, IcpState* state, float* partials, const IcpParams& params,
                       cudaStream_t s) {
   const uint32_t pixels = args.live_width * args.live_height;
-  icp_iteration_kernel<kIcpPixels><<<icp_grid_for(pixels), kIcpBlock, 0, s>>>(args, state, partials, params);
+  icp_iteration_kernel<false, kIcpPixels><<<icp_grid_for(pixels), kIcpBlock, 0, s>>>(args, state, partials, params, 0);
   check(cudaGetLastError(), "icp_iteration_kernel launch");
+}
+
+void launch_icp_level_steps(const IcpLevelArgs& args, IcpState* state, float* partials, const IcpParams& params,
+                            uint32_t iterations, int level, cudaStream_t s) {
+  icp_level_begin_kernel<<<1, 32, 0, s>>>(state, params.damping_lambda);
+  check(cudaGetLastError(), "icp_level_begin launch");
+  const uint32_t pixels = args.live_width * args.live_height;
+  for (uint32_t i = 0; i < iterations; ++i) {
+    icp_iteration_kernel<true, kIcpPixels><<<icp_grid_for(pixels), kIcpBlock, 0, s>>>(args, state, partials, params,
+                                                                                       0);
+  }
+  check(cudaGetLastError(), "icp_iteration_kernel launch");
+  icp_level_end_kernel<<<1, 32, 0, s>>>(state, level);
+  check(cudaGetLastError(), "icp_level_end launch");
 }
 
 void launch_icp_level(const IcpLevelArgs& args, IcpState* state, float* partials, const IcpParams& params,

@@ -263,6 +263,13 @@ void launch_icp_sweep(const IcpLevelArgs& args, IcpState* state, float* partials
 // per-level results).  `partials` holds two sweeps' slots.
 void launch_icp_level(const IcpLevelArgs& args, IcpState* state, float* partials, const IcpParams& params,
                       uint32_t iterations, int level, int begin, int want_values, cudaStream_t stream);
+// The same level as launches that need no co-residency: a begin kernel,
+// one sweep-and-step launch per iteration (later ones return at once once
+// the level's status is settled), an end kernel.  Bit-identical to
+// launch_icp_level at begin = 1, want_values = 0 (the same sweep grid,
+// combine and step); for frame graphs that run beside others (batches).
+void launch_icp_level_steps(const IcpLevelArgs& args, IcpState* state, float* partials, const IcpParams& params,
+                            uint32_t iterations, int level, cudaStream_t stream);
 // Throws DeviceTimeout when the downloaded state `host` shows a grid barrier
 // that gave up; the device barrier is cleared first (ordered on `stream`).
 void check_icp_barrier(const IcpState& host, IcpState* device, cudaStream_t stream);
@@ -335,11 +342,11 @@ struct Pipeline {
   // fork: the frame's inputs on a side branch (standalone frames; batch
   // members run concurrently already and keep one branch)
   struct GraphKey {
-    uint32_t w, h, it0, it1, it2, it3, first, color, fork;
+    uint32_t w, h, it0, it1, it2, it3, first, color, fork, cooperative;
     bool operator<(const GraphKey& o) const {
-      const uint32_t a[9] = {w, h, it0, it1, it2, it3, first, color, fork};
-      const uint32_t b[9] = {o.w, o.h, o.it0, o.it1, o.it2, o.it3, o.first, o.color, o.fork};
-      for (int i = 0; i < 9; ++i) {
+      const uint32_t a[10] = {w, h, it0, it1, it2, it3, first, color, fork, cooperative};
+      const uint32_t b[10] = {o.w, o.h, o.it0, o.it1, o.it2, o.it3, o.first, o.color, o.fork, o.cooperative};
+      for (int i = 0; i < 10; ++i) {
         if (a[i] != b[i]) return a[i] < b[i];
       }
       return false;
