@@ -391,6 +391,13 @@ typedef struct {
 } kf_launch_shapes;
 kf_status kf_pipeline_get_launch_shapes(kf_pipeline* pipeline, kf_launch_shapes* shapes);
 kf_status kf_pipeline_set_launch_shapes(kf_pipeline* pipeline, const kf_launch_shapes* shapes);
+/* Declares whether the pipeline's frames run beside other GPU work (the
+ * members of a pipeline set, several sequences on their own streams; no
+ * reference counterpart).  A pipeline alone (the default, concurrent = 0)
+ * runs each ICP level as one cooperative launch, which needs all its CTAs
+ * resident at once; a concurrent one records each level as per-step launches
+ * that can share the GPU.  Results are bit-identical either way. */
+kf_status kf_pipeline_set_concurrent(kf_pipeline* pipeline, int32_t concurrent);
 /* Times the candidate shapes on a scratch pipeline of the same configuration
  * over `count` consecutive device-resident width x height depth frames (the
  * first fused, the rest tracked), applies the fastest to `pipeline` and

@@ -201,6 +201,7 @@ _PROTOTYPES = {
     "kf_gemm_bf16": (C.c_int, [P, P, P, C.c_int32, C.c_int32, C.c_int32, P, C.c_int32, P]),
     "kf_pipeline_get_launch_shapes": (C.c_int, [P, C.POINTER(LaunchShapes)]),
     "kf_pipeline_set_launch_shapes": (C.c_int, [P, C.POINTER(LaunchShapes)]),
+    "kf_pipeline_set_concurrent": (C.c_int, [P, C.c_int32]),
     "kf_pipeline_autotune": (C.c_int, [P, P, C.c_uint32, C.c_uint32, C.c_uint32, Intrinsics, C.POINTER(LaunchShapes),
                                        C.POINTER(C.c_float)]),
     "kf_batch_destroy": (C.c_int, [P]),

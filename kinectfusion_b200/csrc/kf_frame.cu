@@ -131,7 +131,7 @@ Pipeline::FrameGraph& frame_graph_for(kf_pipeline* pipeline, kf_pyramid* pyramid
   if (p.frame_color.count != n) p.frame_color.resize(n);
   p.result_staging.resize(1);
   Pipeline::GraphKey key{width, height, 0, 0, 0, 0, first_frame ? 1u : 0u, has_color ? 1u : 0u, fork ? 1u : 0u,
-                         cooperative ? 1u : 0u};
+                         cooperative && !p.concurrent ? 1u : 0u};
   uint32_t* its[4] = {&key.it0, &key.it1, &key.it2, &key.it3};
   for (uint32_t l = 0; l < 4; ++l) *its[l] = (iterations != nullptr && l < pyr.level_count) ? iterations[l] : 0u;
   if (iterations == nullptr) {

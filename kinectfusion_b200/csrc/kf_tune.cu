@@ -109,6 +109,18 @@ kf_status kf_pipeline_set_launch_shapes(kf_pipeline* pipeline, const kf_launch_s
   });
 }
 
+kf_status kf_pipeline_set_concurrent(kf_pipeline* pipeline, int32_t concurrent) {
+  return guarded([&] {
+    require(pipeline != nullptr, "kf_pipeline_set_concurrent: null pipeline");
+    Pipeline& p = pipeline->impl;
+    const bool want = concurrent != 0;
+    if (p.concurrent == want) return;
+    check(cudaStreamSynchronize(p.stream), "concurrency switch");
+    p.concurrent = want;
+    p.clear_graphs();  // the graphs hold the other form of the ICP levels
+  });
+}
+
 kf_status kf_pipeline_autotune(kf_pipeline* pipeline, const uint16_t* frames, uint32_t count, uint32_t width,
                                uint32_t height, kf_intrinsics intrinsics, kf_launch_shapes* chosen,
                                float* best_ms) {

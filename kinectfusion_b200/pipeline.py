@@ -257,6 +257,11 @@ class Pipeline:
         shapes = abi.LaunchShapes(raycast_block[0], raycast_block[1], integrate_ctas, (C.c_uint32 * 3)(*lanes))
         _check(lib().kf_pipeline_set_launch_shapes(self.handle, C.byref(shapes)))
 
+    def set_concurrent(self, concurrent: bool = True):
+        """Frames run beside other GPU work (kf_pipeline_set_concurrent): the
+        ICP levels become per-step launches that can share the GPU."""
+        _check(lib().kf_pipeline_set_concurrent(self.handle, 1 if concurrent else 0))
+
     def autotune(self, device_frames: int, count: int, intrinsics: abi.Intrinsics, width: int = 640,
                  height: int = 480) -> tuple[abi.LaunchShapes, float]:
         """kf_pipeline_autotune over `count` consecutive device-resident frames."""

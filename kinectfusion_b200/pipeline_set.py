@@ -186,6 +186,10 @@ class PipelineSet:
                 raise ValueError("Pipeline set reference must name a configured pipeline")
             self.reference_index = names.index(reference)
         self.members = list(pipelines)
+        # the members' frames run side by side on their own streams
+        if len(self.members) > 1:
+            for member in self.members:
+                member.set_concurrent(True)
         self.compare_every_n_frames = compare_every_n_frames
         self._maps: dict[tuple[int, int, int], DeviceSurfaceMaps] = {}
 

@@ -132,7 +132,8 @@ def _fake(name, res=32, voxel=0.05):
     cfg = abi.PipelineConfig()
     cfg.volume.res_x = cfg.volume.res_y = cfg.volume.res_z = res
     cfg.volume.voxel_size = voxel
-    return types.SimpleNamespace(name=name, config=cfg)
+    # a set switches its members to concurrent frames (no device here)
+    return types.SimpleNamespace(name=name, config=cfg, set_concurrent=lambda concurrent=True: None)
 
 
 def test_pipeline_set_validation():

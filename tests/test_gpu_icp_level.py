@@ -8,6 +8,8 @@ icp_correspondence.cu:397-439, over the sweep of :216-343).
   kf_icp_normal_equations at the same camera and model, at every level.
 * A level of N steps follows the oracle's ProjectiveIcpTracker loop
   (icp_optimizer.cpp:208-302): same status, poses within 1e-4 m / 1e-4 rad.
+* A pipeline declared concurrent runs the same levels as per-step launches
+  with bit-identical poses and voxels.
 * The barrier's waits are bounded: with the barrier stalled
   (kf_tracker_stall_next_level) the level's waits give up after their time
   limit, the call returns KF_ERR_DEVICE_TIMEOUT, the frame is not fused, and
@@ -151,3 +153,22 @@ def test_stalled_barrier_times_out_and_recovers(seq):
     assert status == abi.KF_ERR_DEVICE_TIMEOUT
     abi.check(lib.kf_pipeline_track(gpu.handle, tracker.handle, C.byref(cam), C.byref(pyr.level(2)), 4, C.byref(out)))
     assert out.status in (abi.KF_ICP_MAX_ITERATIONS, abi.KF_ICP_CONVERGED)
+
+
+def test_concurrent_pipeline_is_bit_identical(seq):
+    """A pipeline declared concurrent (kf_pipeline_set_concurrent) records the
+    ICP levels as per-step launches; the frames give the same poses and
+    voxels as the cooperative level kernel."""
+    runs = []
+    for concurrent in (False, True):
+        gpu = kf.Pipeline(kf.pipeline_config(RES, VOXEL, ORIGIN, TRUNC, color=abi.KF_COLOR_NONE))
+        gpu.set_concurrent(concurrent)
+        loop = kf.Reconstruction(gpu, K640)
+        for f in range(4):
+            loop.process(seq.depth[f])
+        assert all(r.tracked for r in loop.results)
+        runs.append((np.array(loop.trajectory), gpu.download_raw().view(np.uint32),
+                     [list(r.iterations) for r in loop.results]))
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])
+    assert runs[0][2] == runs[1][2]
