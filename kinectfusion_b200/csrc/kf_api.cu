@@ -302,6 +302,12 @@ kf_status kf_pipeline_destroy(kf_pipeline* pipeline) {
     if (p.stream) cudaStreamSynchronize(p.stream);
     p.clear_graphs();
     if (p.staging_done) cudaEventDestroy(p.staging_done);
+    if (p.copy_stream) cudaStreamSynchronize(p.copy_stream);
+    for (int i = 0; i < 2; ++i) {
+      if (p.uploaded[i]) cudaEventDestroy(p.uploaded[i]);
+      if (p.consumed[i]) cudaEventDestroy(p.consumed[i]);
+    }
+    if (p.copy_stream) cudaStreamDestroy(p.copy_stream);
     for (cudaEvent_t e : {p.fork_event, p.pyramid_event, p.inputs_event}) {
       if (e) cudaEventDestroy(e);
     }

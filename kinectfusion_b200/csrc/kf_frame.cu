@@ -207,19 +207,50 @@ void stage_inputs(Pipeline& p, Pyramid& pyr, const uint16_t* depth, const uint32
     if (color) check(cudaMemcpyAsync(p.frame_color.ptr, color, n * 4, cudaMemcpyDeviceToDevice, s), "color copy");
     return;
   }
-  const bool direct_depth = caller_waits && page_locked(depth);
+  if (!caller_waits) {
+    // Frames in flight: the depth goes up on the pipeline's copy stream into
+    // one of two device buffers, in turn, while the frames before it run;
+    // the frame stream then only moves it into the graph's buffer on the
+    // device.  A turn's buffers are reused once its previous frame's copy
+    // into the graph's buffer is done.
+    const int b = p.upload_turn;
+    p.upload_turn ^= 1;
+    if (p.copy_stream == nullptr) {
+      check(cudaStreamCreateWithFlags(&p.copy_stream, cudaStreamNonBlocking), "copy stream");
+      for (int i = 0; i < 2; ++i) {
+        check(cudaEventCreateWithFlags(&p.uploaded[i], cudaEventDisableTiming), "upload event");
+        check(cudaEventCreateWithFlags(&p.consumed[i], cudaEventDisableTiming), "upload event");
+      }
+    }
+    check(cudaEventSynchronize(p.consumed[b]), "upload buffer reuse");  // returns at once before first use
+    p.depth_pinned[b].resize(n);
+    p.depth_upload[b].resize(n);
+    std::memcpy(p.depth_pinned[b].ptr, depth, n * sizeof(uint16_t));
+    check(cudaMemcpyAsync(p.depth_upload[b].ptr, p.depth_pinned[b].ptr, n * sizeof(uint16_t), cudaMemcpyHostToDevice,
+                          p.copy_stream),
+          "depth upload");
+    check(cudaEventRecord(p.uploaded[b], p.copy_stream), "upload event");
+    check(cudaStreamWaitEvent(s, p.uploaded[b], 0), "upload wait");
+    check(cudaMemcpyAsync(pyr.raw.ptr, p.depth_upload[b].ptr, n * sizeof(uint16_t), cudaMemcpyDeviceToDevice, s),
+          "depth copy");
+    check(cudaEventRecord(p.consumed[b], s), "upload event");
+    depth = nullptr;  // done: only the colour (if any) takes the staged path below
+  }
+  const bool direct_depth = depth == nullptr || (caller_waits && page_locked(depth));
   const bool direct_color = color != nullptr && caller_waits && page_locked(color);
   const bool staged = !direct_depth || (color != nullptr && !direct_color);
   // wait for the last upload from the staging before overwriting it (not for
   // the frames after it: the host fills the staging while they run)
   if (staged && p.staging_done != nullptr) check(cudaEventSynchronize(p.staging_done), "staging reuse");
-  const void* depth_src = depth;
-  if (!direct_depth) {
-    p.depth_staging.resize(n);
-    std::memcpy(p.depth_staging.ptr, depth, n * sizeof(uint16_t));
-    depth_src = p.depth_staging.ptr;
+  if (depth != nullptr) {
+    const void* depth_src = depth;
+    if (!direct_depth) {
+      p.depth_staging.resize(n);
+      std::memcpy(p.depth_staging.ptr, depth, n * sizeof(uint16_t));
+      depth_src = p.depth_staging.ptr;
+    }
+    check(cudaMemcpyAsync(pyr.raw.ptr, depth_src, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s), "depth upload");
   }
-  check(cudaMemcpyAsync(pyr.raw.ptr, depth_src, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s), "depth upload");
   if (color) {
     const void* color_src = color;
     if (!direct_color) {

@@ -371,6 +371,13 @@ struct Pipeline {
   PinnedArray<uint16_t> depth_staging;
   PinnedArray<uint32_t> color_staging;
   cudaEvent_t staging_done = nullptr;  // after the last upload from the staging buffers
+  // kf_frame_submit's depth uploads: two pinned staging and device buffers
+  // used in turn, copied on their own stream while earlier frames run
+  PinnedArray<uint16_t> depth_pinned[2];
+  DeviceArray<uint16_t> depth_upload[2];
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t uploaded[2] = {}, consumed[2] = {};
+  int upload_turn = 0;
   // the frame graph's side branch (frame inputs beside the first model render)
   cudaStream_t side_stream = nullptr;
   cudaEvent_t fork_event = nullptr, pyramid_event = nullptr, inputs_event = nullptr;
