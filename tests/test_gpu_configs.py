@@ -22,7 +22,7 @@ the 128^3 test size:
 * cfg4 precision - a small batch of int16 and bf16 members of uneven
   resolution stepped in one graph launch; each member's TSDF against the
   FP64 oracle integration at the device's poses and one ICP sweep against the
-  FP64 reduction, with the bounds stated in DESIGN.md.
+  FP64 reduction, with the bounds stated in the test's own docstring.
 """
 
 import ctypes as C
