@@ -24,7 +24,13 @@ frame's SHA-256; the tests regenerate the frames and check it).  Outputs:
   the 29 sums and the count;
 * the reference's frame loop (Reconstruction::process_frame,
   reconstruction.cpp:184-277) over frames 0-3 on a fresh 64^3 volume: the
-  poses and level statuses.
+  poses and level statuses;
+* the marching-cubes mesh of the 64^3 volume at min weight 0
+  (MarchingCubes::extract, marching_cubes.cpp:367-507): the vertex positions
+  in lexicographic order and the triangle count;
+* a sparse bf16 store over a 128^3 domain at 2 cm (BlockRep<kHost>,
+  block_rep.hpp:193-329) after frames 0-2 with band integration: the blocks
+  it allocated and each allocated block's voxels, in block order.
 """
 
 import hashlib
@@ -44,6 +50,8 @@ from kinectfusion_b200 import abi, synthetic  # noqa: E402
 SEED, FRAMES = 7, 4
 RES, VOXEL, TRUNC = 64, 0.04, 0.12
 ORIGIN = (-0.5 * RES * VOXEL, -0.5 * RES * VOXEL, -0.5)
+SPARSE_RES, SPARSE_VOXEL, SPARSE_TRUNC = 128, 0.02, 0.05
+SPARSE_ORIGIN = (-0.5 * SPARSE_RES * SPARSE_VOXEL, -0.5 * SPARSE_RES * SPARSE_VOXEL, -0.5)
 
 
 def frame_hashes(seq) -> np.ndarray:
@@ -63,9 +71,9 @@ def main() -> None:
         normals = kr.pyramid(seq.depth[f], k, ko.depth_options())[0]["normals"]
         ref.integrate(seq.depth[f], k, ko.rigid_inverse(abi.rigid_from_matrix(seq.poses[f])), normals=normals)
     k2 = ko.scaled(k, 2)
-    points, normals, _ = ref.raycast(k2, 160, 120, seq.poses[3])
+    map_points, map_normals, _ = ref.raycast(k2, 160, 120, seq.poses[3])
     camera = abi.rigid_from_matrix(seq.poses[3])
-    sums, count = kr.icp_equations(pyr3[2]["vertices"], pyr3[2]["normals"], points, normals, k2, camera,
+    sums, count = kr.icp_equations(pyr3[2]["vertices"], pyr3[2]["normals"], map_points, map_normals, k2, camera,
                                    ko.rigid_inverse(camera))
     loop = kr.RefPipeline(cfg)
     pose = np.eye(4, dtype=np.float32)
@@ -76,13 +84,28 @@ def main() -> None:
         assert tracked
         poses.append(pose)
         statuses.append(status)
+    mesh = ref.mesh(0.0)
+    order = np.lexsort(mesh["positions"].T[::-1])
+    scfg = kf.pipeline_config(SPARSE_RES, SPARSE_VOXEL, SPARSE_ORIGIN, SPARSE_TRUNC, voxel=abi.KF_VOXEL_BF16,
+                              color=abi.KF_COLOR_NONE, rule=abi.KF_RULE_ANGLE_WEIGHTED,
+                              storage=abi.KF_STORAGE_SPARSE, integration_mode=abi.KF_INTEGRATION_BAND)
+    sparse = kr.RefPipeline(scfg)
+    for f in range(3):
+        normals = kr.pyramid(seq.depth[f], k, ko.depth_options())[0]["normals"]
+        sparse.integrate(seq.depth[f], k, ko.rigid_inverse(abi.rigid_from_matrix(seq.poses[f])), normals=normals)
+    assert not sparse.overflowed()
+    grid = sparse.grid()
+    blocks = np.nonzero(grid != 0xFFFFFFFF)[0].astype(np.uint32)
+    pool = sparse.voxels().reshape(-1, 512)
     out = pathlib.Path(__file__).with_name("reference_small.npz")
     np.savez_compressed(out, frame_sha256=frame_hashes(seq),
                         pyramid_l0_depth=pyr3[0]["depth"], pyramid_l2_vertices=pyr3[2]["vertices"],
                         pyramid_l2_normals=pyr3[2]["normals"],
-                        voxels=ref.voxels(), raycast_points=points, raycast_normals=normals,
+                        voxels=ref.voxels(), raycast_points=map_points, raycast_normals=map_normals,
                         icp_sums=np.asarray(sums, np.float32), icp_count=np.uint64(count),
-                        loop_poses=np.array(poses, np.float32), loop_status=np.array(statuses, np.int32))
+                        loop_poses=np.array(poses, np.float32), loop_status=np.array(statuses, np.int32),
+                        mesh_positions=mesh["positions"][order], mesh_triangles=np.uint64(len(mesh["triangles"])),
+                        sparse_blocks=blocks, sparse_voxels=pool[grid[blocks]])
     print(out, out.stat().st_size, "bytes")
 
 

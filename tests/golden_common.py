@@ -72,3 +72,31 @@ def check_loop(g, poses, statuses=None):
         assert dt < 1e-4 and da < 1e-4, (f, dt, da)
     if statuses is not None:
         assert np.array_equal(np.asarray(statuses)[:, :3], g["loop_status"][:, :3])
+
+
+SPARSE_RES, SPARSE_VOXEL, SPARSE_TRUNC = 128, 0.02, 0.05
+SPARSE_ORIGIN = (-0.5 * SPARSE_RES * SPARSE_VOXEL, -0.5 * SPARSE_RES * SPARSE_VOXEL, -0.5)
+
+
+def check_mesh(g, positions, triangle_count):
+    """The vertex set of the reference's mesh (it depends only on which
+    edges cross; the triangle table is this project's own with the same
+    triangle count per case), up to the vertices of voxels an expf pixel
+    moved."""
+    order = np.lexsort(np.asarray(positions).T[::-1])
+    mine = np.asarray(positions)[order]
+    ref = g["mesh_positions"]
+    assert len(ref) > 1000
+    assert abs(len(mine) - len(ref)) <= 2 and abs(int(triangle_count) - int(g["mesh_triangles"])) <= 4
+    if len(mine) == len(ref):
+        assert np.all(mine == ref, axis=1).mean() >= 0.998
+
+
+def check_sparse(g, grid, block_voxels):
+    """The reference's BlockRep<kHost> allocation set, and each allocated
+    block's raw voxels (`block_voxels(blocks)` returns them in block order)."""
+    blocks = np.nonzero(np.asarray(grid) != 0xFFFFFFFF)[0]
+    assert np.array_equal(blocks, g["sparse_blocks"])
+    mine = np.asarray(block_voxels(blocks)).view(np.uint32)
+    diff = np.any(mine != g["sparse_voxels"].view(np.uint32), axis=1)
+    assert diff.sum() <= 2, diff.sum()

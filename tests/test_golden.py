@@ -4,8 +4,9 @@ compiled from its own sources, on seeded synthetic frames; see
 tests/golden/make_golden.py).  Runs without the reference or its compiled
 library: pyramid, 64^3 angle-weighted integration, 160x120 raycast, the
 level-2 ICP normal equations (bit-exact: the oracle sums in the reference's
-order) and the reference's 4-frame loop (poses within 1e-4 m / rad, level
-statuses equal)."""
+order), the reference's 4-frame loop (poses within 1e-4 m / rad, level
+statuses equal), the mesh's vertex set and triangle count, and a sparse
+band-integrated store's allocation set and voxels."""
 
 import numpy as np
 
@@ -45,3 +46,14 @@ def test_oracle_matches_reference_golden():
         poses.append(pose)
         statuses.append([outcomes[lv].status if lv in outcomes else abi.KF_ICP_NOT_RUN for lv in range(4)])
     gc.check_loop(g, poses, statuses)
+    mesh = ko.marching_cubes(vol, 0.0)
+    gc.check_mesh(g, mesh["positions"], len(mesh["triangles"]))
+    sparse = ko.OracleVolume(gc.SPARSE_RES, gc.SPARSE_VOXEL, gc.SPARSE_ORIGIN, gc.SPARSE_TRUNC,
+                             voxel=abi.KF_VOXEL_BF16, sparse=True)
+    io = ko.integration_options(mode=abi.KF_INTEGRATION_BAND)
+    for f in range(3):
+        normals = ko.pyramid(seq.depth[f], gc.K640, ko.depth_options())[0]["normals"]
+        ko.integrate(sparse, seq.depth[f], gc.K640, ko.rigid_inverse(abi.rigid_from_matrix(seq.poses[f])), io,
+                     abi.KF_RULE_ANGLE_WEIGHTED, normals_map=normals)
+    pool = sparse.voxels.reshape(-1, 512)
+    gc.check_sparse(g, sparse.grid, lambda blocks: pool[sparse.grid[blocks]])

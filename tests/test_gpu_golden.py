@@ -4,8 +4,10 @@ the reference's host implementation compiled from its own sources).  Needs
 neither the reference nor its compiled library on the GPU box: pyramid,
 64^3 angle-weighted integration, 160x120 raycast, the level-2 ICP normal
 equations (count equal, sums within 1e-4 relative: the device reduces in a
-fixed tree order, the reference sequentially) and the reference's 4-frame
-loop (poses within 1e-4 m / rad, level statuses equal)."""
+fixed tree order, the reference sequentially), the reference's 4-frame loop
+(poses within 1e-4 m / rad, level statuses equal), the mesh's vertex set and
+triangle count, and a sparse band-integrated store's allocation set and
+voxels (the device's voxel-block hash against BlockRep<kHost>)."""
 
 import ctypes as C
 
@@ -65,3 +67,17 @@ def test_device_matches_reference_golden():
         assert loop.process(seq.depth[f]).tracked
     statuses = [list(r.status) for r in loop.results]
     gc.check_loop(g, loop.trajectory, statuses)
+    mesh = gpu.extract_mesh(0.0)
+    gc.check_mesh(g, mesh["positions"], len(mesh["triangles"]))
+    scfg = kf.pipeline_config(gc.SPARSE_RES, gc.SPARSE_VOXEL, gc.SPARSE_ORIGIN, gc.SPARSE_TRUNC,
+                              voxel=abi.KF_VOXEL_BF16, color=abi.KF_COLOR_NONE, rule=abi.KF_RULE_ANGLE_WEIGHTED,
+                              storage=abi.KF_STORAGE_SPARSE, integration_mode=abi.KF_INTEGRATION_BAND)
+    sparse = kf.Pipeline(scfg)
+    for f in range(3):
+        pf = kf.PyramidSource()
+        pf.build(seq.depth[f], gc.K640)
+        sparse.integrate(seq.depth[f], gc.K640, ko.rigid_inverse(abi.rigid_from_matrix(seq.poses[f])),
+                         normals=pf.download_level(0)["normals"])
+    grid = sparse.block_grid()
+    pool = sparse.download_pool().view(np.uint32).reshape(-1, 512)
+    gc.check_sparse(g, grid, lambda blocks: pool[grid[blocks]])
