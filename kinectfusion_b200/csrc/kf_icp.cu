@@ -606,33 +606,33 @@ __device__ __forceinline__ void sweep_cta(const IcpLevelArgs& a, const Rigid& ca
 
 // Shared memory of the combine: the eight segment sums and compensations.
 struct CombineShared {
-  float seg_sum[8][kIcpSlot];
-  float seg_comp[8][kIcpSlot];
+  float seg_sum[kIcpSegments][kIcpSlot];
+  float seg_comp[kIcpSegments][kIcpSlot];
   float total[kIcpSlot];
   unsigned long long count;
 };
 
 // Deterministic Kahan-compensated combine of `ctas` partial slots, by all
-// threads of the CTA: warp g (segment g of 8) lane i (sum i) loads value i
-// of slots g, g+8, g+16, ... - every load in flight at once, each warp's
-// loads one coalesced row per slot - and compensates over them in slot
-// order; then the eight segment results of each sum are combined in
+// threads of the CTA: warp g (segment g of kIcpSegments) lane i (sum i)
+// loads value i of slots g, g + kIcpSegments, ... - every load in flight at
+// once, each warp's loads one coalesced row per slot - and compensates over
+// them in slot order; then the segment results of each sum are combined in
 // segment order.  Ends with c.total / c.count valid after a barrier.
 __device__ __forceinline__ void combine_slots(const float* __restrict__ slots, unsigned ctas, CombineShared& c) {
-  static_assert(kIcpBlock == 8 * 32 && kIcpSlot == 32, "one warp per segment, one lane per slot value");
-  constexpr unsigned kPerSegment = (kIcpMaxGrid + 7) / 8;
+  static_assert(kIcpBlock == kIcpSegments * 32 && kIcpSlot == 32, "one warp per segment, one lane per slot value");
+  constexpr unsigned kPerSegment = (kIcpMaxGrid + kIcpSegments - 1) / kIcpSegments;
   const unsigned i = threadIdx.x & 31u, g = threadIdx.x >> 5;
   float v[kPerSegment];
 #pragma unroll
   for (unsigned u = 0; u < kPerSegment; ++u) {
-    const unsigned b = g + 8u * u;
+    const unsigned b = g + kIcpSegments * u;
     v[u] = b < ctas ? __ldcg(slots + b * kIcpSlot + i) : 0.0f;
   }
   if (i < kIcpSums) {
     float sum = 0.0f, comp = 0.0f;
 #pragma unroll
     for (unsigned u = 0; u < kPerSegment; ++u) {
-      if (g + 8u * u >= ctas) break;
+      if (g + kIcpSegments * u >= ctas) break;
       const float y = v[u] - comp;
       const float t = sum + y;
       comp = (t - sum) - y;
@@ -644,7 +644,7 @@ __device__ __forceinline__ void combine_slots(const float* __restrict__ slots, u
     unsigned n = 0;
 #pragma unroll
     for (unsigned u = 0; u < kPerSegment; ++u) {
-      if (g + 8u * u >= ctas) break;
+      if (g + kIcpSegments * u >= ctas) break;
       n += __float_as_uint(v[u]);
     }
     c.seg_sum[g][i] = __uint_as_float(n);
@@ -652,7 +652,7 @@ __device__ __forceinline__ void combine_slots(const float* __restrict__ slots, u
   __syncthreads();
   if (threadIdx.x < kIcpSums) {
     float sum = 0.0f, comp = 0.0f;
-    for (int g2 = 0; g2 < 8; ++g2) {
+    for (unsigned g2 = 0; g2 < kIcpSegments; ++g2) {
       const float y = (c.seg_sum[g2][threadIdx.x] - c.seg_comp[g2][threadIdx.x]) - comp;
       const float t = sum + y;
       comp = (t - sum) - y;
@@ -661,19 +661,19 @@ __device__ __forceinline__ void combine_slots(const float* __restrict__ slots, u
     c.total[threadIdx.x] = sum;
   } else if (threadIdx.x == kIcpSums) {
     unsigned long long n = 0;
-    for (int g2 = 0; g2 < 8; ++g2) n += __float_as_uint(c.seg_sum[g2][kIcpSums]);
+    for (unsigned g2 = 0; g2 < kIcpSegments; ++g2) n += __float_as_uint(c.seg_sum[g2][kIcpSums]);
     c.count = n;
   }
   __syncthreads();
 }
 
-// One sweep per launch, two CTAs per SM, Pix live pixels per thread and
+// One sweep per launch, one CTA per SM, Pix live pixels per thread and
 // grid step; the last CTA to arrive (an atomic ticket, no waiting) combines
 // the slots into the state's sums and count and, with Solve, takes the
 // Gauss-Newton step - icp_level_kernel's step, one launch per step (the
 // frame graphs of a batch, whose members' levels must share the GPU).
 template <bool Solve, int Pix>
-__global__ void __launch_bounds__(kIcpBlock, 2)
+__global__ void __launch_bounds__(kIcpBlock, 1)
     icp_iteration_kernel(IcpLevelArgs a, IcpState* __restrict__ st, float* __restrict__ partials, IcpParams p,
                          int want_values) {
   __shared__ int s_flag;
@@ -811,7 +811,7 @@ __device__ bool grid_barrier(IcpBarrier* b, unsigned long long base, uint32_t in
 // combine are icp_iteration_kernel's, so the steps are bit-identical to a
 // launch per step at the same grid.
 template <int Pix>
-__global__ void __launch_bounds__(kIcpBlock, 2)
+__global__ void __launch_bounds__(kIcpBlock, 1)
     icp_level_kernel(IcpLevelArgs a, IcpState* __restrict__ st, float* __restrict__ partials, IcpParams p,
                      uint32_t iterations, int level, int begin, int want_values) {
   __shared__ int s_flag;
@@ -1032,7 +1032,8 @@ void launch_icp_set_pose(IcpState* state, kf_rigid pose, int reset_frame, cudaSt
 namespace kf {
 namespace {
 
-constexpr int kStaticPixelsPerCta = 4 * kIcpBlock;  // each CTA sweeps 1024 live pixels
+constexpr int kStaticBlock = 256;                       // threads per CTA of the static sweep
+constexpr int kStaticPixelsPerCta = 4 * kStaticBlock;  // each CTA sweeps 1024 live pixels
 constexpr int kStaticSlots = 1200;                  // one partial slot per CTA
 constexpr uint64_t kStaticMaxPixels = static_cast<uint64_t>(kStaticSlots) * kStaticPixelsPerCta;  // 1,228,800
 constexpr int kMaxDevices = 64;
@@ -1043,12 +1044,12 @@ static __device__ __align__(256) IcpState g_static_state;
 // Same association and accumulation as icp_iteration_kernel; the image is cut
 // into 1024-pixel tiles, one per CTA, and the last CTA to finish combines the
 // partial slots (Kahan-compensated, in slot order) straight from memory.
-__global__ void __launch_bounds__(kIcpBlock)
+__global__ void __launch_bounds__(kStaticBlock)
     icp_static_sweep_kernel(IcpLevelArgs a, IcpState* __restrict__ st, float* __restrict__ partials, float max_d,
                             float min_dot) {
   __shared__ int s_last;
-  __shared__ float s_warp[kIcpBlock / 32][kIcpSlot];
-  __shared__ unsigned s_warp_count[kIcpBlock / 32];
+  __shared__ float s_warp[kStaticBlock / 32][kIcpSlot];
+  __shared__ unsigned s_warp_count[kStaticBlock / 32];
   __shared__ float s_seg_sum[8][kIcpSlot];
   __shared__ float s_seg_comp[8][kIcpSlot];
   const Rigid cam = rigid_load(st->camera);
@@ -1060,8 +1061,8 @@ __global__ void __launch_bounds__(kIcpBlock)
   const uint32_t pixels = a.live_width * a.live_height;
   const uint32_t first = blockIdx.x * kStaticPixelsPerCta;
 #pragma unroll 1
-  for (uint32_t k = 0; k < kStaticPixelsPerCta / kIcpBlock; ++k) {
-    const uint32_t pix = first + k * kIcpBlock + threadIdx.x;
+  for (uint32_t k = 0; k < kStaticPixelsPerCta / kStaticBlock; ++k) {
+    const uint32_t pix = first + k * kStaticBlock + threadIdx.x;
     if (pix >= pixels) break;
     float j[6], residual, distance;
     if (!match(a, cam, model, max_d, min_dot, pix % a.live_width, pix / a.live_width, j, residual, distance)) {
@@ -1098,11 +1099,11 @@ __global__ void __launch_bounds__(kIcpBlock)
   __syncthreads();
   if (threadIdx.x < kIcpSums) {
     float s = 0.0f;
-    for (int w = 0; w < kIcpBlock / 32; ++w) s += s_warp[w][threadIdx.x];
+    for (int w = 0; w < kStaticBlock / 32; ++w) s += s_warp[w][threadIdx.x];
     partials[blockIdx.x * kIcpSlot + threadIdx.x] = s;
   } else if (threadIdx.x == kIcpSums) {
     unsigned c = 0;
-    for (int w = 0; w < kIcpBlock / 32; ++w) c += s_warp_count[w];
+    for (int w = 0; w < kStaticBlock / 32; ++w) c += s_warp_count[w];
     partials[blockIdx.x * kIcpSlot + kIcpSums] = __uint_as_float(c);
   }
   __threadfence();
@@ -1225,7 +1226,7 @@ extern "C" kf_status kf_icp_normal_equations_static(const kf_level_view* live, c
     a.model_height = model_height;
     a.model_intrinsics = intr_from(model_intrinsics);
     const unsigned grid = static_cast<unsigned>((pixels + kStaticPixelsPerCta - 1) / kStaticPixelsPerCta);
-    icp_static_sweep_kernel<<<grid, kIcpBlock, 0, 0>>>(a, scratch.state, scratch.partials, max_point_distance,
+    icp_static_sweep_kernel<<<grid, kStaticBlock, 0, 0>>>(a, scratch.state, scratch.partials, max_point_distance,
                                                        min_normal_dot);
     check(cudaGetLastError(), "icp_static_sweep_kernel launch");
     check(cudaMemcpy(sums, state + offsetof(IcpState, sums), kIcpSums * sizeof(float), cudaMemcpyDeviceToHost),

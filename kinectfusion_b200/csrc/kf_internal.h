@@ -162,9 +162,10 @@ struct Pyramid {
 // ---- ICP device state --------------------------------------------------------
 constexpr int kIcpSums = 29;          // 21 JtJ + 6 Jtr + distance + residual^2
 constexpr int kIcpSlot = 32;          // floats per CTA partial (29 sums + count)
-constexpr int kIcpBlock = 256;
+constexpr int kIcpBlock = 512;          // one CTA per SM: 16 warps, as two CTAs of 256 threads
+constexpr unsigned kIcpSegments = kIcpBlock / 32;  // the combine: one warp per segment of slots
 constexpr int kIcpPixels = 1;         // live pixels per thread and grid step of a sweep
-constexpr int kIcpMaxGrid = 2 * 148;  // two CTAs per SM on a 148-SM B200
+constexpr int kIcpMaxGrid = 148;      // one CTA per SM on a 148-SM B200
 constexpr int kIcpRunning = -1;
 
 // Grid barrier of the whole-level ICP kernel: the arrivals of every CTA at

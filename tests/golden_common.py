@@ -67,11 +67,19 @@ def check_maps(g, points, normals):
 
 
 def check_loop(g, poses, statuses=None):
+    """Poses within 1e-4 m / rad; per level the same outcome: a failure code
+    equal, a success (converged, or at the iteration cap) a success - which
+    of the two can flip where the last update sits at the 1e-5 threshold,
+    with the sums' rounding order."""
     for f in range(FRAMES):
         dt, da = pose_error(poses[f], g["loop_poses"][f])
         assert dt < 1e-4 and da < 1e-4, (f, dt, da)
     if statuses is not None:
-        assert np.array_equal(np.asarray(statuses)[:, :3], g["loop_status"][:, :3])
+        success = (abi.KF_ICP_MAX_ITERATIONS, abi.KF_ICP_CONVERGED)
+        mine = np.asarray(statuses)[:, :3]
+        ref = g["loop_status"][:, :3]
+        same = (mine == ref) | (np.isin(mine, success) & np.isin(ref, success))
+        assert same.all(), (mine, ref)
 
 
 SPARSE_RES, SPARSE_VOXEL, SPARSE_TRUNC = 128, 0.02, 0.05

@@ -5,7 +5,7 @@ correspondences at the coarsest level, the later levels do not run, the
 frame is not fused and the pose stays; the next frame tracks from that pose.
 Each frame is compared with the oracle tracking the same frame against the
 same state (its volume replayed at the device's poses, from the device's
-previous pose): flags and level statuses equal, poses within 1e-4 m / rad,
+previous pose): flags and level outcomes equal, poses within 1e-4 m / rad,
 and the replayed volume equal to the device's bit for bit.  Frames in
 flight and a batch member (per-step ICP launches) reproduce the synchronous
 run bit for bit."""
@@ -62,8 +62,12 @@ def test_failed_frame_against_the_oracle(synchronous):
             tracked, ok, outcomes = ko.track(replay, levels, depth[f].shape, loop.trajectory[f - 1],
                                              ko.raycast_options(), ko.icp_options())
             assert bool(r.tracked) == ok, f
+            success = (abi.KF_ICP_MAX_ITERATIONS, abi.KF_ICP_CONVERGED)
             for lv, o in outcomes.items():
-                assert r.status[lv] == o.status, (f, lv, r.status[lv], o.status)
+                # a failure code equal; converged or at the cap can flip
+                # where the last update sits at the threshold
+                assert r.status[lv] == o.status or (r.status[lv] in success and o.status in success), \
+                    (f, lv, r.status[lv], o.status)
             dt, da = pose_error(loop.trajectory[f], tracked if ok else loop.trajectory[f - 1])
             assert dt < 1e-4 and da < 1e-4, (f, dt, da)
         if r.tracked:
