@@ -522,9 +522,13 @@ __global__ void stencil_bits_kernel(const uint4* __restrict__ voxel_bits, uint4*
     // without any observed corner does
     const uint64_t decided = require_all ? (~all_obs | no_bad) : (~any_obs | one);
     undecided = ~decided;
+    // An undecided stencil keeps its "one" bit when every observed corner is
+    // exactly 1 (the corner weights decide between 1.0 and nullopt); without
+    // it, an observed corner holds another value and only the gather decides.
+    const uint64_t weigh = undecided & no_bad;
     stencil_bits[static_cast<size_t>(brick) * 8u + z] =
         make_uint4(static_cast<uint32_t>(undecided), static_cast<uint32_t>(undecided >> 32),
-                   static_cast<uint32_t>(one), static_cast<uint32_t>(one >> 32));
+                   static_cast<uint32_t>(one | weigh), static_cast<uint32_t>((one | weigh) >> 32));
   }
   // brick summary from its eight layers (eight consecutive lanes)
   const uint32_t all_null = __ballot_sync(0xFFFFFFFFu, undecided == 0u && one == 0u);

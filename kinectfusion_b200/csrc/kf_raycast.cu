@@ -151,11 +151,13 @@ __device__ __forceinline__ bool stencil_slot(const VolumeDev& v, f3 g, Slot& s) 
 }
 
 // Class of a stencil from its record: 1 = exactly 1.0, 2 = nullopt, 0 = not
-// decided by the stencil bits.
+// decided by the stencil bits, the corner weights may decide (every observed
+// corner is exactly 1), 3 = not decided, only the gather decides (an observed
+// corner holds another value).
 __device__ __forceinline__ int record_class(uint4 r, uint32_t bit) {
   const uint32_t undecided = bit < 32u ? r.x >> bit : r.y >> (bit - 32u);
   const uint32_t one = bit < 32u ? r.z >> bit : r.w >> (bit - 32u);
-  if (undecided & 1u) return 0;
+  if (undecided & 1u) return (one & 1u) ? 0 : 3;
   return (one & 1u) ? 1 : 2;
 }
 
@@ -234,6 +236,8 @@ __device__ __forceinline__ int march_sample(const Sampler<Kind>& s, const Volume
       stencil_masks(voxel_bits, v, static_cast<int>(floorf(g.x - 0.5f)), static_cast<int>(floorf(g.y - 0.5f)),
                     static_cast<int>(floorf(g.z - 0.5f)), observed, one);
       cls = stencil_class(observed, one, policy, g);
+    } else if (cls == 3) {
+      cls = 0;  // the masks would only confirm it: straight to the gather
     }
     if (cls != 0) {
       if (summary == (cls == 1 ? 2 : 1) && slot.bx < 1024u && slot.by < 1024u && slot.bz < 1024u) {
