@@ -504,7 +504,7 @@ __global__ void __launch_bounds__(64)
 // found a zero crossing (its point is finite): the normal, then the colour
 // or the shading; without a normal the pixel has no surface.
 template <int Kind, bool Color>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 6)
     surface_kernel(VolumeDev v, RaycastParams rp, uint32_t width, uint32_t height, Rigid pose,
                    const IcpState* __restrict__ state, float* __restrict__ points, float* __restrict__ normals,
                    uint32_t* __restrict__ colors) {
