@@ -364,7 +364,7 @@ struct Pipeline {
   uint32_t raycast_block_x = 8, raycast_block_y = 8;  // march CTA, at most 64 threads
   uint32_t integrate_ctas = 148 * 32;                 // fusion grid (grid-strided over listed blocks)
   bool concurrent = false;  // frames run beside other GPU work: per-step ICP launches (kf_pipeline_set_concurrent)
-  uint32_t raycast_lanes[3] = {4, 4, 1};              // lanes per ray: <= 20,000 rays, <= 80,000, more
+  uint32_t raycast_lanes[3] = {8, 4, 1};              // lanes per ray: <= 20,000 rays, <= 80,000, more
   uint32_t last_frame_kernels = 0;
   kf_pyramid* graph_pyramid = nullptr;
   kf_tracker* graph_tracker = nullptr;
