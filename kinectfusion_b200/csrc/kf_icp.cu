@@ -154,6 +154,76 @@ __device__ __forceinline__ void inverse_solve6(const double (&inv)[6][6], const 
   }
 }
 
+// The same three steps on the packed lower triangle (element (r, c), c <= r,
+// at tri(r, c)), in place: the factor overwrites the matrix and the inverse
+// overwrites the factor.  Each element takes cholesky6's, lower_inverse6's
+// and inverse_solve6's operations in their order (the upper zeros only ever
+// add exact zeros there), so the results are theirs bit for bit; a third of
+// the registers keeps the one-thread step free of local-memory spills.
+__host__ __device__ constexpr int tri(int r, int c) { return r * (r + 1) / 2 + c; }
+
+__device__ __forceinline__ bool cholesky_packed(double (&m)[21], double (&rinv)[6]) {
+  bool ok = true;
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    double d = m[tri(c, c)];
+#pragma unroll
+    for (int k = 0; k < c; ++k) d -= m[tri(c, k)] * m[tri(c, k)];
+    ok = ok && (d > 0.0);
+    const double lc = sqrt(fmax(d, 1e-300));
+    m[tri(c, c)] = lc;
+    rinv[c] = 1.0 / lc;
+#pragma unroll
+    for (int r = c + 1; r < 6; ++r) {
+      double s = m[tri(r, c)];
+#pragma unroll
+      for (int k = 0; k < c; ++k) s -= m[tri(r, k)] * m[tri(c, k)];
+      m[tri(r, c)] = s * rinv[c];
+    }
+  }
+  return ok;
+}
+
+// Column by column, rows downward: inv[r][c] reads the factor's row r from
+// column c on (not yet overwritten) and the inverse's column c above row r.
+__device__ __forceinline__ void lower_inverse_packed(double (&m)[21], const double (&rinv)[6]) {
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+#pragma unroll
+    for (int r = c; r < 6; ++r) {
+      double s = (r == c) ? 1.0 : 0.0;
+#pragma unroll
+      for (int k = c; k < r; ++k) s -= m[tri(r, k)] * m[tri(k, c)];
+      m[tri(r, c)] = s * rinv[r];
+    }
+  }
+}
+
+__device__ __forceinline__ void inverse_solve_packed(const double (&inv)[21], const double (&b)[6], double (&x)[6]) {
+  double y[6];
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k <= r; ++k) s += inv[tri(r, k)] * b[k];
+    y[r] = s;
+  }
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = r; k < 6; ++k) s += inv[tri(k, r)] * y[k];
+    x[r] = s;
+  }
+}
+
+// Element (r, c) of the normal matrix from the 29 sums (its upper triangle,
+// row-major, then the right-hand side and the residual terms).
+__device__ __forceinline__ double normal_entry(const float* sums, int r, int c) {
+  const int i = r < c ? r : c, j = r < c ? c : r;
+  return static_cast<double>(sums[i * 6 - i * (i - 1) / 2 + (j - i)]);
+}
+
 // LDL^T solve with symmetric diagonal pivoting (largest remaining diagonal
 // first).  An exactly zero pivot (a rank-deficient system such as a single
 // plane) takes a zero solution component, the minimum-norm convention of the
@@ -267,23 +337,34 @@ struct Stability {
 // well-conditioned case is decided without eigenvalues: with A = L L^T,
 // s = ||L^-1||_F^2 >= ||A^-1||_2, so lambda_min >= 1/s and
 // lambda_max / lambda_min <= ||A||_F * s; when both bounds meet the limits
-// the system is stable.  Any other case computes the spectrum.  `inv`
-// receives L^-1 when A factorises.
-__device__ Stability stability(const double (&a)[6][6], const IcpParams& p, bool want_values, double (&inv)[6][6],
+// the system is stable.  Any other case computes the spectrum.  `m`
+// receives L^-1 (packed) when A factorises.
+__device__ Stability stability(const float* sums, const IcpParams& p, bool want_values, double (&m)[21],
                                bool& chol_ok) {
   Stability s{false, 0.0f, 0.0f};
-  double l[6][6], rinv[6];
-  chol_ok = cholesky6(a, l, rinv);
-  if (chol_ok) lower_inverse6(l, rinv, inv);
+  double fro = 0.0;  // ||A||_F^2 over the full matrix, row-major
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      const double v = normal_entry(sums, i, j);
+      fro += v * v;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+#pragma unroll
+    for (int c = 0; c <= r; ++c) m[tri(r, c)] = normal_entry(sums, r, c);
+  }
+  double rinv[6];
+  chol_ok = cholesky_packed(m, rinv);
+  if (chol_ok) lower_inverse_packed(m, rinv);
   if (!want_values && chol_ok) {
-    double fro = 0.0, inv2 = 0.0;
+    double inv2 = 0.0;
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
 #pragma unroll
-      for (int j = 0; j < 6; ++j) {
-        fro += a[i][j] * a[i][j];
-        inv2 += inv[i][j] * inv[i][j];
-      }
+      for (int j = 0; j <= i; ++j) inv2 += m[tri(i, j)] * m[tri(i, j)];
     }
     if (1.0 >= static_cast<double>(p.min_system_eigenvalue) * inv2 &&
         sqrt(fro) * inv2 <= static_cast<double>(p.max_condition_number)) {
@@ -291,6 +372,9 @@ __device__ Stability stability(const double (&a)[6][6], const IcpParams& p, bool
       return s;
     }
   }
+  double a[6][6];
+  for (int r = 0; r < 6; ++r)
+    for (int c = 0; c < 6; ++c) a[r][c] = normal_entry(sums, r, c);
   double eig[6];
   if (!jacobi6(a, eig)) return s;
   double lo = eig[0], hi = eig[0];
@@ -349,26 +433,39 @@ __device__ bool within_caps(const Increment& inc, const IcpParams& p) {
 }
 
 // solve_increment (icp_optimizer.cpp:370-402) in FP64: a Cholesky solve for
-// positive definite systems (the factor of the undamped system is reused),
-// the pivoted LDL^T for the rank-deficient ones.
-__device__ Increment solve_increment(const float* sums, float lambda, const IcpParams& p,
-                                     const double (&inv)[6][6], bool chol_ok) {
+// positive definite systems, the pivoted LDL^T for the rank-deficient ones.
+// Undamped: one attempt, with the inverse factor of the stability test
+// (`inv`, packed) when the system factorised.
+__device__ Increment solve_increment(const float* sums, float lambda, const IcpParams& p, const double (&inv)[21],
+                                     bool chol_ok) {
   Increment last;
   last.solved = false;
   last.update_translation = last.update_rotation = last.lambda = 0.0f;
-  double base[6][6], rhs[6];
-  int e = 0;
-  for (int r = 0; r < 6; ++r) {
-    for (int c = r; c < 6; ++c) {
-      base[r][c] = base[c][r] = static_cast<double>(sums[e]);
-      ++e;
-    }
-  }
+  double rhs[6];
   for (int r = 0; r < 6; ++r) rhs[r] = static_cast<double>(sums[21 + r]);
-  const bool active = p.damping_mode != KF_DAMPING_NONE;
-  const int attempts = active ? 8 : 1;
+  if (p.damping_mode == KF_DAMPING_NONE) {
+    double x[6];
+    if (chol_ok) {
+      inverse_solve_packed(inv, rhs, x);
+    } else {
+      double a[6][6];
+      for (int r = 0; r < 6; ++r)
+        for (int c = 0; c < 6; ++c) a[r][c] = normal_entry(sums, r, c);
+      ldlt_solve6(a, rhs, x);
+    }
+    bool finite = true;
+    for (int i = 0; i < 6; ++i) finite = finite && isfinite(x[i]);
+    if (finite) {
+      increment_from(x, last);
+      last.lambda = lambda;
+    }
+    return last;
+  }
+  double base[6][6];
+  for (int r = 0; r < 6; ++r)
+    for (int c = 0; c < 6; ++c) base[r][c] = normal_entry(sums, r, c);
   float scale = lambda;
-  for (int attempt = 0; attempt < attempts; ++attempt) {
+  for (int attempt = 0; attempt < 8; ++attempt) {
     double damped[6][6], x[6];
     for (int i = 0; i < 6; ++i)
       for (int j = 0; j < 6; ++j) damped[i][j] = base[i][j];
@@ -379,9 +476,7 @@ __device__ Increment solve_increment(const float* sums, float lambda, const IcpP
       damped[r][r] += off;
     }
     double l[6][6], rinv[6], dinv[6][6];
-    if (p.damping_mode == KF_DAMPING_NONE && chol_ok) {
-      inverse_solve6(inv, rhs, x);
-    } else if (cholesky6(damped, l, rinv)) {
+    if (cholesky6(damped, l, rinv)) {
       lower_inverse6(l, rinv, dinv);
       inverse_solve6(dinv, rhs, x);
     } else {
@@ -392,7 +487,7 @@ __device__ Increment solve_increment(const float* sums, float lambda, const IcpP
     if (finite) {
       increment_from(x, last);
       last.lambda = scale;
-      if (!active || within_caps(last, p)) return last;
+      if (within_caps(last, p)) return last;
     }
     scale = grow(p, scale);
   }
@@ -426,8 +521,7 @@ __device__ void pose_to_rigid_floats(const double* pose, float* out) {
 // One Gauss-Newton / LM step of estimate_with on the combined sums.
 __device__ __noinline__ void gauss_newton_step(IcpState* st, const float* sums_in, unsigned long long count_in,
                                   const IcpParams& p, bool want_values) {
-  float sums[kIcpSums];
-  for (int i = 0; i < kIcpSums; ++i) sums[i] = sums_in[i];
+  const float* sums = sums_in;
   unsigned long long count = count_in;
   st->iterations += 1;
   st->correspondences = count;
@@ -452,22 +546,14 @@ __device__ __noinline__ void gauss_newton_step(IcpState* st, const float* sums_i
     } else {
       st->rejected_steps += 1;
       for (int i = 0; i < 12; ++i) st->pose[i] = st->best_pose[i];
-      for (int i = 0; i < kIcpSums; ++i) sums[i] = st->best_sums[i];
+      sums = st->best_sums;
       count = st->best_count;
       st->lambda = grow(p, st->lambda);
     }
   }
-  double a[6][6];
-  int e = 0;
-  for (int r = 0; r < 6; ++r) {
-    for (int c = r; c < 6; ++c) {
-      a[r][c] = a[c][r] = static_cast<double>(sums[e]);
-      ++e;
-    }
-  }
-  double inv[6][6];
+  double inv[21];
   bool chol_ok = false;
-  const Stability stab = stability(a, p, want_values, inv, chol_ok);
+  const Stability stab = stability(sums, p, want_values, inv, chol_ok);
   st->min_system_eigenvalue = stab.min_eigenvalue;
   st->condition_number = stab.condition_number;
   if (!stab.stable && !active) {
