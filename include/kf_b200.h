@@ -304,6 +304,20 @@ kf_status kf_pipeline_listed_blocks(kf_pipeline* pipeline, uint64_t* blocks);
 /* Sparse storage: the block-slot grid (BlockRep::grid, block_rep.hpp:26-110),
  * one uint32 per 8^3 block in x-major block order, 0xFFFFFFFF = unallocated. */
 kf_status kf_pipeline_download_block_grid(kf_pipeline* pipeline, uint32_t* grid, size_t count);
+/* Dense storage: the march's skip structures as the last integration left
+ * them (no counterpart in the reference, whose march reads the voxels).  Per
+ * 8^3 brick, x-major brick order: its class (0 mixed, 1 every stencil based
+ * in it nullopt, 2 every such stencil exactly 1.0) and the radius in bricks
+ * (0-7) of the cube around it, inside the brick grid, whose bricks all share
+ * its class (0 for mixed bricks).  Per brick layer z (brick * 8 + z) the
+ * 16-byte stencil record of the 64 stencils based in it, bit y*8+x: words
+ * 0-1 "not decided by the corner bits", words 2-3 "exactly 1.0" for a
+ * decided stencil and "every observed corner exactly 1.0" for an undecided
+ * one.  `bricks` = the brick count; `records` holds bricks * 32 words.
+ * KF_ERR_INVALID_ARGUMENT for sparse storage or before the structures
+ * exist. */
+kf_status kf_pipeline_download_skip_structures(kf_pipeline* pipeline, uint8_t* brick_class, uint8_t* brick_radius,
+                                               uint32_t* records, size_t bricks);
 /* The sparse block pool: capacity blocks of 512 raw voxels (slot order, each
  * block's voxels z*64 + y*8 + x, the reference's SparseVolumeView pool layout,
  * block_rep.hpp:93-100); `bytes` = capacity * 512 * voxel bytes.  With the

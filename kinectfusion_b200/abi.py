@@ -210,6 +210,7 @@ _PROTOTYPES = {
     "kf_batch_kernel_count": (C.c_int, [P, C.POINTER(C.c_uint32)]),
     "kf_pipeline_block_stats": (C.c_int, [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "kf_pipeline_download_block_grid": (C.c_int, [P, P, C.c_size_t]),
+    "kf_pipeline_download_skip_structures": (C.c_int, [P, P, P, P, C.c_size_t]),
     "kf_pipeline_download_band_bitmap": (C.c_int, [P, P, C.c_size_t]),
     "kf_pipeline_listed_blocks": (C.c_int, [P, C.POINTER(C.c_uint64)]),
     "kf_mesh_free": (None, [C.POINTER(Mesh)]),

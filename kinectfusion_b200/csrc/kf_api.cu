@@ -509,6 +509,24 @@ kf_status kf_pipeline_download_block_grid(kf_pipeline* pipeline, uint32_t* grid,
   });
 }
 
+kf_status kf_pipeline_download_skip_structures(kf_pipeline* pipeline, uint8_t* brick_class, uint8_t* brick_radius,
+                                               uint32_t* records, size_t bricks) {
+  return guarded([&] {
+    require(pipeline != nullptr && brick_class != nullptr && brick_radius != nullptr && records != nullptr,
+            "kf_pipeline_download_skip_structures: null argument");
+    Pipeline& p = pipeline->impl;
+    require(p.view.table == nullptr && p.brick_class.count != 0 && p.brick_radius.count != 0,
+            "kf_pipeline_download_skip_structures: no skip structures (sparse storage, or no integration yet)");
+    require(bricks == static_cast<size_t>(p.view.bx) * p.view.by * p.view.bz && bricks == p.brick_class.count,
+            "kf_pipeline_download_skip_structures: brick count mismatch");
+    check(cudaStreamSynchronize(p.stream), "skip structures sync");
+    check(cudaMemcpy(brick_class, p.brick_class.ptr, bricks, cudaMemcpyDeviceToHost), "brick class download");
+    check(cudaMemcpy(brick_radius, p.brick_radius.ptr, bricks, cudaMemcpyDeviceToHost), "brick radius download");
+    check(cudaMemcpy(records, p.stencil_bits.ptr, bricks * 32u * sizeof(uint32_t), cudaMemcpyDeviceToHost),
+          "stencil records download");
+  });
+}
+
 kf_status kf_pipeline_download_pool(kf_pipeline* pipeline, void* voxels, size_t bytes) {
   return guarded([&] {
     require(pipeline != nullptr && voxels != nullptr, "kf_pipeline_download_pool: null argument");

@@ -481,18 +481,19 @@ __global__ void stencil_bits_kernel(const uint4* __restrict__ voxel_bits, uint4*
   if (state != nullptr && state->failed) return;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t brick = t >> 3, z = t & 7u;
-  bool work = false;
   const uint32_t x0 = brick % bx, y0 = (brick / bx) % by, z0 = brick / (bx * by);
+  // the brick's eight lanes (one per layer) each test one of the eight
+  // bricks its stencils reach (itself and its +x, +y, +z neighbours); the
+  // brick is rewritten when any of them changed
+  bool changed = false;
   if (brick < bx * by * bz) {
-#pragma unroll
-    for (uint32_t c = 0; c < 8; ++c) {
-      const uint32_t nx = x0 + (c & 1u), ny = y0 + ((c >> 1) & 1u), nz = z0 + (c >> 2);
-      if (nx < bx && ny < by && nz < bz) {
-        const uint32_t nb = (nz * by + ny) * bx + nx;
-        work |= ((__ldg(dirty + (nb >> 5)) >> (nb & 31u)) & 1u) != 0u;
-      }
+    const uint32_t nx = x0 + (z & 1u), ny = y0 + ((z >> 1) & 1u), nz = z0 + (z >> 2);
+    if (nx < bx && ny < by && nz < bz) {
+      const uint32_t nb = (nz * by + ny) * bx + nx;
+      changed = ((__ldg(dirty + (nb >> 5)) >> (nb & 31u)) & 1u) != 0u;
     }
   }
+  const bool work = ((__ballot_sync(0xFFFFFFFFu, changed) >> ((threadIdx.x & 31u) & ~7u)) & 0xFFu) != 0u;
   uint64_t undecided = 0u, one = 0u;
   if (work) {
     uint64_t any_obs = 0u, all_obs = ~0ull, no_bad = ~0ull;
@@ -563,15 +564,24 @@ __global__ void brick_radius_kernel(const uint8_t* __restrict__ brick_class, con
   const uint32_t coord = axis == 0 ? b % bx : (axis == 1 ? (b / bx) % by : b / (bx * by));
   const uint32_t extent = axis == 0 ? bx : (axis == 1 ? by : bz);
   const size_t stride = axis == 0 ? 1u : (axis == 1 ? bx : static_cast<size_t>(bx) * by);
+  // r = the first k that fails, less one: both neighbours at distance k
+  // inside the grid and of class c, and (later passes) k within the bound
+  // of every brick passed so far.  Every distance's loads are independent
+  // of the others' outcome, so all are issued before the scan.
   uint32_t m = lower != nullptr ? lower[b] : kBrickRadiusCap;
   uint32_t r = 0;
-  for (uint32_t k = 1; k <= kBrickRadiusCap && k <= m; ++k) {
-    if (coord < k || coord + k >= extent) break;
-    const size_t lo = b - k * stride, hi = b + k * stride;
-    if (brick_class[lo] != c || brick_class[hi] != c) break;
-    if (lower != nullptr) m = min(m, static_cast<uint32_t>(min(lower[lo], lower[hi])));
-    if (m < k) break;
-    r = k;
+  bool run = true;
+#pragma unroll
+  for (uint32_t k = 1; k <= kBrickRadiusCap; ++k) {
+    const bool in = coord >= k && coord + k < extent;
+    const size_t lo = in ? b - k * stride : b, hi = in ? b + k * stride : b;
+    const uint32_t cl = brick_class[lo], ch = brick_class[hi];
+    const uint32_t ml = lower != nullptr ? lower[lo] : kBrickRadiusCap;
+    const uint32_t mh = lower != nullptr ? lower[hi] : kBrickRadiusCap;
+    run = run && k <= m && in && cl == c && ch == c;
+    if (run) m = min(m, min(ml, mh));
+    run = run && !(m < k);
+    if (run) r = k;
   }
   out[b] = static_cast<uint8_t>(r);
 }

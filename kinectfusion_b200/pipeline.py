@@ -234,6 +234,18 @@ class Pipeline:
         _check(lib().kf_pipeline_download_raw(self.handle, _ptr(raw), raw.nbytes, None, 0))
         return raw
 
+    def skip_structures(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Dense storage: the march's skip structures (kf_pipeline_download_skip_structures):
+        per-brick class and cube radius shaped (bz, by, bx), and the stencil records
+        shaped (bz, by, bx, 8 layers, 4 words)."""
+        rx, ry, rz = self.resolution
+        shape = ((rz + 7) // 8, (ry + 7) // 8, (rx + 7) // 8)
+        n = shape[0] * shape[1] * shape[2]
+        cls, radius = np.empty(n, dtype=np.uint8), np.empty(n, dtype=np.uint8)
+        records = np.empty(n * 32, dtype=np.uint32)
+        _check(lib().kf_pipeline_download_skip_structures(self.handle, _ptr(cls), _ptr(radius), _ptr(records), n))
+        return cls.reshape(shape), radius.reshape(shape), records.reshape(shape + (8, 4))
+
     def download_pool(self) -> np.ndarray:
         """Sparse storage: the raw block pool, (capacity, 512) voxels in slot
         order (kf_pipeline_download_pool)."""
