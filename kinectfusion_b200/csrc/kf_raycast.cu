@@ -31,7 +31,11 @@
 namespace kf {
 namespace {
 
-// Rays left in a warp at or below which they march cooperatively.
+// Rays left in a warp at or below which they march cooperatively, in renders
+// that start with lanes to spare (fewer rays than lanes per warp).  Where
+// every lane starts with a ray the rays march alone to the end: there the
+// cooperative rounds' extra shuffles cost more than their speculation saves
+// (640x480 render 0.405 -> 0.388 ms without them, maps identical).
 constexpr int kCoopLanes = 8;
 
 struct RaycastParams {
@@ -40,6 +44,7 @@ struct RaycastParams {
   int cell_normals;
   int seed_previous;
   uint32_t rays_per_warp;  // 32: one lane per ray, 2D CTA tile; 16 or 8: warp tiles below
+  int coop_rays;           // kCoopLanes, or 0 when rays_per_warp is 32
 };
 
 // Pixel tile of one warp that holds `rays` rays (lanes 0..rays-1; the other
@@ -413,7 +418,7 @@ __global__ void __launch_bounds__(64)
   unsigned live;
   while ((live = __ballot_sync(0xFFFFFFFFu, !done)) != 0u) {
     const int n = __popc(live);
-    if (n > kCoopLanes) {
+    if (n > rp.coop_rays) {
       // every live lane takes the next sample of its own ray
       if (!done) {
         const float r = ray_length;
@@ -814,6 +819,7 @@ void launch_typed(const Pipeline& p, const kf_raycast_camera& cam, float* points
   const uint64_t rays = static_cast<uint64_t>(cam.width) * cam.height;
   const uint32_t lanes = p.raycast_lanes[rays <= 20000u ? 0 : (rays <= 80000u ? 1 : 2)];
   rp.rays_per_warp = p.config.raycast_backend == KF_RAYCAST_BAND_MARCH ? 32u : 32u / lanes;
+  rp.coop_rays = rp.rays_per_warp < 32u ? kCoopLanes : 0;
   dim3 block(p.raycast_block_x, p.raycast_block_y);
   dim3 grid(ceil_div(cam.width, block.x), ceil_div(cam.height, block.y));
   if (rp.rays_per_warp < 32u) {
