@@ -361,8 +361,8 @@ struct Pipeline {
   std::map<GraphKey, FrameGraph> graphs;
   uint64_t graph_epoch = 0;  // bumped whenever the frame graphs are dropped
   // Launch shapes the autotuner may change (none of them changes a result bit)
-  uint32_t raycast_block_x = 8, raycast_block_y = 8;  // march CTA, at most 64 threads
-  uint32_t integrate_ctas = 148 * 32;                 // fusion grid (grid-strided over listed blocks)
+  uint32_t raycast_block_x = 16, raycast_block_y = 4;  // march CTA, at most 64 threads
+  uint32_t integrate_ctas = 148 * 48;                 // fusion grid (grid-strided over listed blocks)
   bool concurrent = false;  // frames run beside other GPU work: per-step ICP launches (kf_pipeline_set_concurrent)
   uint32_t raycast_lanes[3] = {8, 4, 1};              // lanes per ray: <= 20,000 rays, <= 80,000, more
   uint32_t last_frame_kernels = 0;

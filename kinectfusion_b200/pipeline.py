@@ -262,7 +262,7 @@ class Pipeline:
         _check(lib().kf_pipeline_get_launch_shapes(self.handle, C.byref(shapes)))
         return shapes
 
-    def set_launch_shapes(self, raycast_block=(8, 8), integrate_ctas=148 * 32, raycast_lanes=None):
+    def set_launch_shapes(self, raycast_block=(16, 4), integrate_ctas=148 * 48, raycast_lanes=None):
         """raycast_lanes: lanes per ray for renders of <= 20,000 rays, <=
         80,000 rays and more (each 1, 2 or 4); None keeps the current ones."""
         lanes = tuple(self.launch_shapes().raycast_lanes) if raycast_lanes is None else tuple(raycast_lanes)
